@@ -1,0 +1,309 @@
+"""freeshearlayer_b200 -- B200 (sm_100a) explicit time step of freeShearLayer.
+
+Python view of the C ABI in ``include/fsl_gpu.h`` (libfsl_gpu.so, built
+in-tree by ``make -C freeshearlayer_b200``).  One :class:`Domain` is one
+device-resident domain; its methods carry the reference's phase names
+(src/layer2.c:141-185) so a driver reads like the reference's main loop::
+
+    d = Domain(params)                 # Initialize()  (src/initialize.c:14)
+    d.upload_state(state)
+    d.checkCoNum()                     # src/helpers.c:23
+    d.draw_disturbance()               # src/layer2.c:152-162
+    for stage in (1, 2, 3):
+        d.BounCondInGhostCells()       # src/boundCondInGhostCells.c:10
+        d.Reconstruction()             # src/reconstruction.c:26
+        d.BounCondOnInterfaces()       # src/bounCondOnInterfaces.c:11
+        d.Fluxes()                     # src/fluxes.c:12 (includes DynamicSmagorinsky)
+        d.Evolution(3, stage)          # src/evolution.c:15
+
+or, fused and asynchronous, ``d.step(n)``.  There is no CPU path: loading
+fails with :class:`FslError` when the library is missing, and creating a
+domain fails when no sm_100 device is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["Params", "Domain", "FslError", "lib", "LIB_PATH", "default_params",
+           "params_from_ini", "params_from_bin", "initial_state", "temporal_state",
+           "SETUP_SPATIAL", "SETUP_TEMPORAL", "CFL_STREAMWISE", "CFL_ACOUSTIC",
+           "PREC_FP64", "PREC_FP32", "SGS_DYNAMIC", "SGS_LEARNED", "RECON_CHARMINMOD",
+           "RECON_PPM"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfsl_gpu.so")
+
+FSL_OK = 0
+ERRORS = {-1: "FSL_ERR_ARG", -2: "FSL_ERR_NOMEM", -3: "FSL_ERR_CUDA", -4: "FSL_ERR_NONFINITE",
+          -5: "FSL_ERR_TIMEOUT", -6: "FSL_ERR_IO", -7: "FSL_ERR_UNSUPPORTED", -8: "FSL_ERR_NODEVICE"}
+SETUP_SPATIAL, SETUP_TEMPORAL = 0, 1
+CFL_STREAMWISE, CFL_ACOUSTIC = 0, 1
+PREC_FP64, PREC_FP32 = 0, 1
+SGS_DYNAMIC, SGS_LEARNED = 0, 1
+RECON_CHARMINMOD, RECON_PPM = 0, 1
+
+
+class FslError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        super().__init__("%s (%d)%s" % (ERRORS.get(code, "FSL_ERR"), code, (": " + what) if what else ""))
+
+
+class Params(C.Structure):
+    """fsl_params: the 22 layer2.ini values in file order, then the options."""
+
+    _fields_ = [("LEN", C.c_int), ("HIG", C.c_int), ("DEP", C.c_int),
+                ("deltaX", C.c_double), ("deltaY", C.c_double), ("deltaZ", C.c_double),
+                ("deltaT", C.c_double), ("Answer", C.c_int), ("numstep", C.c_int),
+                ("mu_L", C.c_double), ("Pr_L", C.c_double), ("Pr_T", C.c_double),
+                ("Cs", C.c_double), ("BL_HIG", C.c_int), ("Ua", C.c_double),
+                ("Va", C.c_double), ("Wa", C.c_double), ("Ns_min", C.c_int),
+                ("Nst", C.c_int), ("f_step", C.c_int), ("nStages", C.c_int),
+                ("maxCoNum", C.c_double), ("setup", C.c_int), ("cfl_mode", C.c_int),
+                ("seed_X", C.c_double), ("precision", C.c_int), ("sgs", C.c_int),
+                ("recon", C.c_int), ("reserved", C.c_int * 8)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class Info(C.Structure):
+    _fields_ = [("deltaT", C.c_double), ("deltaT_X", C.c_double), ("deltaT_Y", C.c_double),
+                ("deltaT_Z", C.c_double), ("maxCo", C.c_double), ("X", C.c_double),
+                ("Ud", C.c_double), ("Vd", C.c_double), ("Wd", C.c_double),
+                ("k_min", C.c_uint), ("k_max", C.c_uint), ("step", C.c_uint),
+                ("counter", C.c_int), ("cur", C.c_int), ("DD", C.c_double),
+                ("lambda_L", C.c_double), ("cp_Pr_T", C.c_double),
+                ("device_bytes", C.c_ulonglong)]
+
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_lib = None
+
+
+def lib():
+    """Load libfsl_gpu.so (raises FslError if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FslError(-8, "libfsl_gpu.so not built: run `make -C %s`" % HERE)
+        L = C.CDLL(LIB_PATH)
+        vp, i, d, u = C.c_void_p, C.c_int, C.c_double, C.c_uint
+        P = C.POINTER(Params)
+        sig = {
+            "fsl_params_default": [P], "fsl_params_from_ini": [C.c_char_p, P],
+            "fsl_params_from_bin": [C.c_char_p, P], "fsl_params_check": [P],
+            "fsl_initial_state": [P, _dp],
+            "fsl_temporal_state": [P, d, d, d, C.c_ulonglong, _dp, C.POINTER(C.c_double)],
+            "fsl_init": [P, C.POINTER(C.c_void_p)], "fsl_destroy": [vp],
+            "fsl_get_info": [vp, C.POINTER(Info)], "fsl_sync": [vp],
+            "fsl_upload_state": [vp, _dp], "fsl_download_state": [vp, _dp],
+            "fsl_set_time": [vp, u, d],
+            "fsl_check_courant": [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+            "fsl_draw_disturbance": [vp], "fsl_set_disturbance": [vp, u, u, d, d, d],
+            "fsl_ghost_bc": [vp], "fsl_reconstruct": [vp], "fsl_interface_bc": [vp],
+            "fsl_dynamic_smagorinsky": [vp], "fsl_fluxes": [vp], "fsl_evolution": [vp, i],
+            "fsl_step": [vp, i], "fsl_step_phased": [vp, i],
+            "fsl_get_cells": [vp, i, i, _dp], "fsl_set_cells": [vp, i, i, _dp],
+            "fsl_get_faces": [vp, i, i, i, _dp], "fsl_set_faces": [vp, i, i, i, _dp],
+            "fsl_set_cur": [vp, i], "fsl_sums": [vp, _dp], "fsl_plane_sums": [vp, _dp],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.fsl_last_error.argtypes = [vp]
+        L.fsl_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, h=None):
+    if rc != FSL_OK:
+        what = lib().fsl_last_error(h).decode() if h else ""
+        raise FslError(rc, what)
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    _check(lib().fsl_params_default(C.byref(p)))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def params_from_ini(path: str, **kw) -> Params:
+    p = default_params()
+    _check(lib().fsl_params_from_ini(path.encode(), C.byref(p)))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def params_from_bin(path: str, **kw) -> Params:
+    p = default_params()
+    _check(lib().fsl_params_from_bin(path.encode(), C.byref(p)))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _as_params(p) -> Params:
+    if isinstance(p, Params):
+        return p
+    q = default_params()
+    for k, v in dict(p).items():
+        if hasattr(q, k):
+            setattr(q, k, v)
+    return q
+
+
+def state_size(p) -> int:
+    return p.LEN * p.HIG * 5 * p.DEP
+
+
+def initial_state(p) -> np.ndarray:
+    p = _as_params(p)
+    out = np.empty(state_size(p), np.float64)
+    _check(lib().fsl_initial_state(C.byref(p), out))
+    return out
+
+
+def temporal_state(p, Mc: float, delta_w0: float = 1.0, amp: float = 1e-3,
+                   seed: int = 20251203):
+    p = _as_params(p)
+    out = np.empty(state_size(p), np.float64)
+    dU = C.c_double()
+    _check(lib().fsl_temporal_state(C.byref(p), Mc, delta_w0, amp, seed, out, C.byref(dU)))
+    return out, dU.value
+
+
+class Domain:
+    """One device-resident domain (an fsl_ctx) on the current CUDA device."""
+
+    def __init__(self, params):
+        self.p = _as_params(params)
+        h = C.c_void_p()
+        _check(lib().fsl_init(C.byref(self.p), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fsl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, rc):
+        _check(rc, self.h)
+
+    # --- shapes -------------------------------------------------------------
+    @property
+    def padded_shape(self):
+        return (self.p.LEN + 2, self.p.HIG + 2, self.p.DEP + 2)
+
+    def face_shape(self, d: int):
+        return (self.p.LEN + (d == 0), self.p.HIG + (d == 1), self.p.DEP + (d == 2))
+
+    # --- state ----------------------------------------------------------------
+    def upload_state(self, state: np.ndarray):
+        self._c(lib().fsl_upload_state(self.h, np.ascontiguousarray(state, np.float64).ravel()))
+
+    def download_state(self) -> np.ndarray:
+        out = np.empty(state_size(self.p), np.float64)
+        self._c(lib().fsl_download_state(self.h, out))
+        return out
+
+    def set_time(self, step: int, dt: float):
+        self._c(lib().fsl_set_time(self.h, step, dt))
+
+    def info(self) -> Info:
+        i = Info()
+        self._c(lib().fsl_get_info(self.h, C.byref(i)))
+        return i
+
+    def sync(self):
+        self._c(lib().fsl_sync(self.h))
+
+    # --- driver scalar work -----------------------------------------------------
+    def check_courant(self):
+        mc, dt = C.c_double(), C.c_double()
+        self._c(lib().fsl_check_courant(self.h, C.byref(mc), C.byref(dt)))
+        return mc.value, dt.value
+
+    def draw_disturbance(self):
+        self._c(lib().fsl_draw_disturbance(self.h))
+
+    def set_disturbance(self, k_min, k_max, Ud, Vd, Wd):
+        self._c(lib().fsl_set_disturbance(self.h, k_min, k_max, Ud, Vd, Wd))
+
+    # --- phases -------------------------------------------------------------------
+    def ghost_bc(self): self._c(lib().fsl_ghost_bc(self.h))
+    def reconstruct(self): self._c(lib().fsl_reconstruct(self.h))
+    def interface_bc(self): self._c(lib().fsl_interface_bc(self.h))
+    def dynamic_smagorinsky(self): self._c(lib().fsl_dynamic_smagorinsky(self.h))
+    def fluxes(self): self._c(lib().fsl_fluxes(self.h))
+    def evolution(self, stage: int): self._c(lib().fsl_evolution(self.h, stage))
+    def step(self, n: int = 1): self._c(lib().fsl_step(self.h, n))
+    def step_phased(self, n: int = 1): self._c(lib().fsl_step_phased(self.h, n))
+
+    # reference names (src/layer2.c:147-176)
+    def checkCoNum(self): return self.check_courant()
+    def BounCondInGhostCells(self): self.ghost_bc()
+    def Reconstruction(self): self.reconstruct()
+    def BounCondOnInterfaces(self): self.interface_bc()
+    def DynamicSmagorinsky(self): self.dynamic_smagorinsky()
+
+    def Fluxes(self):
+        """Fluxes() including its DynamicSmagorinsky(U1..U4) call (src/fluxes.c:52-54)."""
+        self.dynamic_smagorinsky()
+        self.fluxes()
+
+    def Evolution(self, nStages: int, Stage: int):
+        if nStages != self.p.nStages:
+            raise FslError(-1, "nStages is fixed at domain creation (%d)" % self.p.nStages)
+        self.evolution(Stage)
+
+    # --- debug access -------------------------------------------------------------
+    def cells(self, which: int, var: int = 0) -> np.ndarray:
+        out = np.empty(self.padded_shape, np.float64)
+        self._c(lib().fsl_get_cells(self.h, which, var, out))
+        return out
+
+    def set_cells(self, which: int, var: int, a: np.ndarray):
+        self._c(lib().fsl_set_cells(self.h, which, var, np.ascontiguousarray(a, np.float64)))
+
+    def faces(self, d: int, side: int, var: int) -> np.ndarray:
+        out = np.empty(self.face_shape(d), np.float64)
+        self._c(lib().fsl_get_faces(self.h, d, side, var, out))
+        return out
+
+    def set_faces(self, d: int, side: int, var: int, a: np.ndarray):
+        self._c(lib().fsl_set_faces(self.h, d, side, var, np.ascontiguousarray(a, np.float64)))
+
+    def set_cur(self, which: int):
+        self._c(lib().fsl_set_cur(self.h, which))
+
+    # --- diagnostics ----------------------------------------------------------------
+    def sums(self) -> np.ndarray:
+        out = np.empty(5, np.float64)
+        self._c(lib().fsl_sums(self.h, out))
+        return out
+
+    def plane_sums(self) -> np.ndarray:
+        out = np.empty(8 * self.p.HIG, np.float64)
+        self._c(lib().fsl_plane_sums(self.h, out))
+        return out.reshape(self.p.HIG, 8)

@@ -1,0 +1,684 @@
+// fsl_api.cu -- C ABI of libfsl_gpu.so (declared in include/fsl_gpu.h).
+//
+// Host side of the explicit step: parameter parsing (layer2.ini / .bin),
+// device allocation, state transfer, the driver's per-step scalar work
+// (Courant rescale, disturbance RNG) and the launch sequences.  All device
+// work of a context is issued on its own CUDA stream.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "fsl_internal.h"
+
+using namespace fsl;
+
+struct fsl_ctx {
+    Ctx c;
+};
+
+namespace fsl {
+
+Grid make_grid(int L, int H, int D, int elem_bytes)
+{
+    Grid g;
+    g.L = L; g.H = H; g.D = D;
+    const int q = 32 / elem_bytes; // elements per 32-byte sector
+    g.pk = ((D + 2 + q - 1) / q) * q;
+    g.pi = (long long)g.pk * (H + 2);
+    g.off = q - 1;
+    const long long n = g.off + (long long)(L + 2) * g.pi;
+    g.fstride = ((n + 63) / 64) * 64;
+    return g;
+}
+
+} // namespace fsl
+
+namespace {
+
+const char *kNoCtx = "no context";
+
+int fail(Ctx &c, int code, const char *what, cudaError_t e = cudaSuccess)
+{
+    char buf[512];
+    if (e != cudaSuccess) snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    else snprintf(buf, sizeof buf, "%s", what);
+    c.err = buf;
+    return code;
+}
+
+#define CK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) return fail(c, FSL_ERR_CUDA, #call, e_);            \
+    } while (0)
+
+#define CKL()                                                                      \
+    do {                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                       \
+        if (e_ != cudaSuccess) return fail(c, FSL_ERR_CUDA, "kernel launch", e_); \
+    } while (0)
+
+int dev_alloc(Ctx &c, double **p, size_t n)
+{
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(double));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(c, FSL_ERR_NOMEM, "cudaMalloc", e);
+    }
+    c.bytes += n * sizeof(double);
+    e = cudaMemsetAsync(*p, 0, n * sizeof(double), c.stream);
+    if (e != cudaSuccess) return fail(c, FSL_ERR_CUDA, "cudaMemsetAsync", e);
+    return FSL_OK;
+}
+
+size_t face_count(const Grid &g, int d)
+{
+    return (size_t)(g.L + (d == 0)) * (g.H + (d == 1)) * (g.D + (d == 2));
+}
+
+int ensure_faces(Ctx &c)
+{
+    if (c.faces_alloc) return FSL_OK;
+    for (int d = 0; d < 3; d++)
+        for (int s = 0; s < 2; s++)
+            for (int v = 0; v < 5; v++) {
+                double *p;
+                int rc = dev_alloc(c, &p, face_count(c.g, d));
+                if (rc) return rc;
+                if (d == 0) c.f.x[s][v] = p;
+                else if (d == 1) c.f.y[s][v] = p;
+                else c.f.z[s][v] = p;
+            }
+    c.faces_alloc = true;
+    return FSL_OK;
+}
+
+int ensure_dyn(Ctx &c)
+{
+    if (c.dyn_alloc) return FSL_OK;
+    const size_t fs = (size_t)c.g.fstride;
+    int rc;
+    if ((rc = dev_alloc(c, &c.dyn.vel, 3 * fs))) return rc;
+    if ((rc = dev_alloc(c, &c.dyn.t1, 9 * fs))) return rc;
+    if ((rc = dev_alloc(c, &c.dyn.t2, 9 * fs))) return rc;
+    if ((rc = dev_alloc(c, &c.dyn.A, 6 * fs))) return rc;
+    if ((rc = dev_alloc(c, &c.dyn.Lst, 6 * fs))) return rc;
+    if ((rc = dev_alloc(c, &c.dyn.B, 6 * fs))) return rc;
+    if ((rc = dev_alloc(c, &c.dyn.S, fs))) return rc;
+    c.dyn_alloc = true;
+    return FSL_OK;
+}
+
+double *cur_ptr(Ctx &c) { return c.cur ? c.Up : c.U; }
+
+// Disturbance draw of src/layer2.c:152-162 with Random() of src/helpers.c:13-17.
+double rnd(double x)
+{
+    x = 11. * x + 3.14159265358979323846;
+    return x - (double)((int)x);
+}
+
+void draw(Ctx &c)
+{
+    const unsigned DEP = (unsigned)c.p.DEP;
+    double X = c.X;
+    if (c.counter > 0) c.counter--;
+    else {
+        c.counter = (int)(c.p.Ns_min + c.p.Nst * (X = rnd(X)));
+        c.dist.k_min = (unsigned)(DEP * (X = rnd(X)));
+        c.dist.k_max = (unsigned)(c.dist.k_min + DEP * (X = rnd(X)));
+        if (c.dist.k_max > DEP) c.dist.k_max -= DEP;
+        X = rnd(X); c.dist.Ud = c.p.Ua * (1 - X - X);
+        X = rnd(X); c.dist.Vd = c.p.Va * (1 - X - X);
+        X = rnd(X); c.dist.Wd = c.p.Wa * (1 - X - X);
+    }
+    c.X = X;
+}
+
+int sync_scalars(Ctx &c)
+{
+    CK(cudaMemcpyAsync(c.hs, c.ds, sizeof(DevScalars), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.dt_host = c.hs->dt;
+    c.maxco_host = c.hs->maxCo;
+    return FSL_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int fsl_params_default(fsl_params *p)
+{
+    if (!p) return FSL_ERR_ARG;
+    memset(p, 0, sizeof *p);
+    p->LEN = 100; p->HIG = 80; p->DEP = 35;
+    p->deltaX = 1.6666667; p->deltaY = 1.0; p->deltaZ = 1.5; p->deltaT = 0.0007;
+    p->Answer = 0; p->numstep = 3000;
+    p->mu_L = 0.253358; p->Pr_L = 0.72; p->Pr_T = 0.8; p->Cs = 0.01;
+    p->BL_HIG = 5; p->Ua = 35.; p->Va = 35.; p->Wa = 35.;
+    p->Ns_min = 10; p->Nst = 50; p->f_step = 50; p->nStages = 3; p->maxCoNum = 0.1;
+    p->setup = FSL_SETUP_SPATIAL; p->cfl_mode = FSL_CFL_STREAMWISE; p->seed_X = 0.317391239817;
+    p->precision = FSL_PREC_FP64; p->sgs = FSL_SGS_DYNAMIC; p->recon = FSL_RECON_CHARMINMOD;
+    return FSL_OK;
+}
+
+static void set_field(fsl_params *p, int i, double v, int from_float)
+{
+    (void)from_float;
+    switch (i) {
+    case 0: p->LEN = (int)v; break;
+    case 1: p->HIG = (int)v; break;
+    case 2: p->DEP = (int)v; break;
+    case 3: p->deltaX = v; break;
+    case 4: p->deltaY = v; break;
+    case 5: p->deltaZ = v; break;
+    case 6: p->deltaT = v; break;
+    case 7: p->Answer = (int)v; break;
+    case 8: p->numstep = (int)v; break;
+    case 9: p->mu_L = v; break;
+    case 10: p->Pr_L = v; break;
+    case 11: p->Pr_T = v; break;
+    case 12: p->Cs = v; break;
+    case 13: p->BL_HIG = (int)v; break;
+    case 14: p->Ua = v; break;
+    case 15: p->Va = v; break;
+    case 16: p->Wa = v; break;
+    case 17: p->Ns_min = (int)v; break;
+    case 18: p->Nst = (int)v; break;
+    case 19: p->f_step = (int)v; break;
+    case 20: p->nStages = (int)v; break;
+    case 21: p->maxCoNum = v; break;
+    default: break;
+    }
+}
+
+// src/initialize.c:17-58: 22 lines read with fgets(str, 79, ...), integers
+// with atoi and reals with atof (trailing text ignored).
+int fsl_params_from_ini(const char *path, fsl_params *p)
+{
+    if (!path || !p) return FSL_ERR_ARG;
+    FILE *f = fopen(path, "r");
+    if (!f) return FSL_ERR_IO;
+    fsl_params q = *p; // option fields are kept as the caller set them
+    char str[80];
+    int i = 0;
+    static const int is_int[22] = {1, 1, 1, 0, 0, 0, 0, 1, 1, 0, 0, 0, 0, 1, 0, 0, 0, 1, 1, 1, 1, 0};
+    while (i < 22) {
+        if (!fgets(str, 79, f)) {
+            fclose(f);
+            return FSL_ERR_IO;
+        }
+        set_field(&q, i, is_int[i] ? (double)atoi(str) : atof(str), 0);
+        i++;
+    }
+    fclose(f);
+    *p = q;
+    return FSL_OK;
+}
+
+// src-par/initialize.c:35-81: 22 native float32 values in ini order,
+// assigned to the typed globals by C conversion.
+int fsl_params_from_bin(const char *path, fsl_params *p)
+{
+    if (!path || !p) return FSL_ERR_ARG;
+    FILE *f = fopen(path, "rb");
+    if (!f) return FSL_ERR_IO;
+    float buf[22];
+    size_t n = fread(buf, sizeof(float), 22, f);
+    fclose(f);
+    if (n != 22) return FSL_ERR_IO;
+    fsl_params q = *p; // option fields are kept as the caller set them
+    for (int i = 0; i < 22; i++) set_field(&q, i, (double)buf[i], 1);
+    *p = q;
+    return FSL_OK;
+}
+
+int fsl_params_check(const fsl_params *p)
+{
+    if (!p) return FSL_ERR_ARG;
+    if (p->LEN < 2 || p->HIG < 2 || p->DEP < 2) return FSL_ERR_ARG;
+    if ((long long)p->LEN * p->HIG * p->DEP > (1LL << 31)) return FSL_ERR_ARG;
+    if (!(p->deltaX > 0) || !(p->deltaY > 0) || !(p->deltaZ > 0) || !(p->deltaT > 0)) return FSL_ERR_ARG;
+    if (!(p->Pr_L > 0) || !(p->Pr_T > 0) || !(p->maxCoNum > 0)) return FSL_ERR_ARG;
+    if (p->nStages < 1 || p->nStages > 3) return FSL_ERR_ARG;
+    if (p->setup != FSL_SETUP_SPATIAL && p->setup != FSL_SETUP_TEMPORAL) return FSL_ERR_ARG;
+    if (p->cfl_mode != FSL_CFL_STREAMWISE && p->cfl_mode != FSL_CFL_ACOUSTIC) return FSL_ERR_ARG;
+    // the disturbance block rows j in [HIG/2, HIG/2+BL_HIG) must exist
+    // (src/bounCondOnInterfaces.c:31 writes past the array otherwise)
+    if (p->setup == FSL_SETUP_SPATIAL && (p->BL_HIG < 0 || p->HIG / 2 + p->BL_HIG > p->HIG)) return FSL_ERR_ARG;
+    if (p->precision != FSL_PREC_FP64 && p->precision != FSL_PREC_FP32) return FSL_ERR_ARG;
+    if (p->sgs != FSL_SGS_DYNAMIC && p->sgs != FSL_SGS_LEARNED) return FSL_ERR_ARG;
+    if (p->recon != FSL_RECON_CHARMINMOD && p->recon != FSL_RECON_PPM) return FSL_ERR_ARG;
+    return FSL_OK;
+}
+
+// src/initialize.c:159-187
+int fsl_initial_state(const fsl_params *p, double *state)
+{
+    if (!p || !state || fsl_params_check(p)) return FSL_ERR_ARG;
+    const double P = 100000., R = 1.0;
+    size_t n = 0;
+    for (int i = 1; i <= p->LEN; i++)
+        for (int j = 1; j <= p->HIG; j++) {
+            const double U = (j <= p->HIG / 2) ? 76.4 : 200;
+            const double vals[5] = {R, R * U, 0., 0., P / 0.4 + 0.5 * R * (U * U)};
+            for (int v = 0; v < 5; v++)
+                for (int k = 0; k < p->DEP; k++) state[n++] = vals[v];
+        }
+    return FSL_OK;
+}
+
+static uint64_t splitmix64(uint64_t *s)
+{
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+int fsl_temporal_state(const fsl_params *p, double Mc, double delta_w0, double amp, unsigned long long seed,
+                       double *state, double *dU_out)
+{
+    if (!p || !state || fsl_params_check(p) || !(delta_w0 > 0) || !(Mc > 0)) return FSL_ERR_ARG;
+    const double p0 = 100000., rho0 = 1.0, cp = 717.75 * 1.4, Rg = 287.10;
+    const double Tinf = p0 / (Rg * rho0);
+    const double cinf = sqrt(1.4 * p0 / rho0);
+    const double dU = 2.0 * Mc * cinf;
+    const double Ly = p->HIG * p->deltaY;
+    uint64_t s = seed;
+    size_t n = 0;
+    const int D = p->DEP;
+    for (int i = 1; i <= p->LEN; i++)
+        for (int j = 1; j <= p->HIG; j++) {
+            const double y = (j - 0.5) * p->deltaY - 0.5 * Ly;
+            const double um = 0.5 * dU * tanh(2.0 * y / delta_w0);
+            const double T = Tinf + (0.25 * dU * dU - um * um) / (2.0 * cp);
+            const double rho = p0 / (Rg * T);
+            double *row = state + n;
+            for (int k = 0; k < D; k++) {
+                double r3[3];
+                for (int q = 0; q < 3; q++)
+                    r3[q] = amp * dU * ((double)(splitmix64(&s) >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0);
+                const double uu = um + r3[0];
+                row[k] = rho;
+                row[D + k] = rho * uu;
+                row[2 * D + k] = rho * r3[1];
+                row[3 * D + k] = rho * r3[2];
+                row[4 * D + k] = p0 / 0.4 + 0.5 * rho * (uu * uu + r3[1] * r3[1] + r3[2] * r3[2]);
+            }
+            n += 5 * (size_t)D;
+        }
+    if (dU_out) *dU_out = dU;
+    return FSL_OK;
+}
+
+int fsl_init(const fsl_params *p, fsl_ctx **out)
+{
+    if (!p || !out) return FSL_ERR_ARG;
+    *out = nullptr;
+    if (fsl_params_check(p)) return FSL_ERR_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return FSL_ERR_NODEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return FSL_ERR_NODEVICE;
+    if (prop.major != 10) return FSL_ERR_NODEVICE;
+    fsl_ctx *h = new (std::nothrow) fsl_ctx();
+    if (!h) return FSL_ERR_NOMEM;
+    Ctx &c = h->c;
+    c.p = *p;
+    c.device = dev;
+    c.g = make_grid(p->LEN, p->HIG, p->DEP, 8);
+    // derived constants, src/initialize.c:67-94
+    c.k.rdx = 1. / p->deltaX; c.k.rdy = 1. / p->deltaY; c.k.rdz = 1. / p->deltaZ;
+    c.k.r4dx = 1. / (4 * p->deltaX); c.k.r4dy = 1. / (4 * p->deltaY); c.k.r4dz = 1. / (4 * p->deltaZ);
+    c.k.r2dx = c.k.r4dx + c.k.r4dx; c.k.r2dy = c.k.r4dy + c.k.r4dy; c.k.r2dz = c.k.r4dz + c.k.r4dz;
+    c.k.mu_L = p->mu_L;
+    c.k.lambda_L = p->mu_L * 717.75 * 1.4 / p->Pr_L;
+    c.k.cp_Pr_T = 717.75 * 1.4 / p->Pr_T;
+    c.k.DD = pow(p->deltaX * p->deltaY * p->deltaZ, 0.666666666666667);
+    c.k.maxCoNum = p->maxCoNum;
+    c.k.deltaX = p->deltaX; c.k.deltaY = p->deltaY; c.k.deltaZ = p->deltaZ;
+    c.k.setup = p->setup; c.k.BL_HIG = p->BL_HIG; c.k.cfl_mode = p->cfl_mode; c.k.nStages = p->nStages;
+    c.X = p->seed_X;
+    int rc = FSL_OK;
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return FSL_ERR_CUDA;
+    }
+    const size_t fs = (size_t)c.g.fstride;
+    if (!rc) rc = dev_alloc(c, &c.U, 5 * fs);
+    if (!rc) rc = dev_alloc(c, &c.Up, 5 * fs);
+    if (!rc) rc = dev_alloc(c, &c.Uq, 5 * fs);
+    if (!rc) rc = dev_alloc(c, &c.mu, fs);
+    c.npartials = 148 * 4;
+    if (!rc) rc = dev_alloc(c, &c.partials, 4096);
+    if (!rc) rc = dev_alloc(c, &c.stage_dev, (size_t)p->LEN * p->HIG * 5 * p->DEP);
+    if (!rc) {
+        if (cudaMalloc((void **)&c.ds, sizeof(DevScalars)) != cudaSuccess) rc = FSL_ERR_NOMEM;
+        else if (cudaMallocHost((void **)&c.hs, sizeof(DevScalars)) != cudaSuccess) rc = FSL_ERR_NOMEM;
+    }
+    if (!rc) {
+        memset(c.hs, 0, sizeof(DevScalars));
+        c.hs->dt = p->deltaT;
+        c.hs->dtx = p->deltaT / p->deltaX; c.hs->dty = p->deltaT / p->deltaY; c.hs->dtz = p->deltaT / p->deltaZ;
+        if (cudaMemcpyAsync(c.ds, c.hs, sizeof(DevScalars), cudaMemcpyHostToDevice, c.stream) != cudaSuccess ||
+            cudaStreamSynchronize(c.stream) != cudaSuccess)
+            rc = FSL_ERR_CUDA;
+        c.dt_host = p->deltaT;
+    }
+    if (rc) {
+        fsl_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return FSL_OK;
+}
+
+int fsl_destroy(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    cudaFree(c.U); cudaFree(c.Up); cudaFree(c.Uq); cudaFree(c.mu);
+    cudaFree(c.partials); cudaFree(c.stage_dev); cudaFree(c.ds);
+    if (c.hs) cudaFreeHost(c.hs);
+    if (c.faces_alloc)
+        for (int s = 0; s < 2; s++)
+            for (int v = 0; v < 5; v++) { cudaFree(c.f.x[s][v]); cudaFree(c.f.y[s][v]); cudaFree(c.f.z[s][v]); }
+    if (c.dyn_alloc) {
+        cudaFree(c.dyn.vel); cudaFree(c.dyn.t1); cudaFree(c.dyn.t2); cudaFree(c.dyn.A);
+        cudaFree(c.dyn.Lst); cudaFree(c.dyn.B); cudaFree(c.dyn.S);
+    }
+    if (c.stream) cudaStreamDestroy(c.stream);
+    delete h;
+    return FSL_OK;
+}
+
+const char *fsl_last_error(const fsl_ctx *h)
+{
+    if (!h) return kNoCtx;
+    return h->c.err.c_str();
+}
+
+int fsl_sync(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = sync_scalars(c);
+    if (rc) return rc;
+    if (c.hs->status) return fail(c, FSL_ERR_NONFINITE, "non-finite or non-positive Courant maximum or density");
+    return FSL_OK;
+}
+
+int fsl_get_info(fsl_ctx *h, fsl_info *info)
+{
+    if (!h || !info) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = sync_scalars(c);
+    if (rc) return rc;
+    memset(info, 0, sizeof *info);
+    info->deltaT = c.hs->dt; info->deltaT_X = c.hs->dtx; info->deltaT_Y = c.hs->dty; info->deltaT_Z = c.hs->dtz;
+    info->maxCo = c.hs->maxCo;
+    info->X = c.X; info->Ud = c.dist.Ud; info->Vd = c.dist.Vd; info->Wd = c.dist.Wd;
+    info->k_min = c.dist.k_min; info->k_max = c.dist.k_max;
+    info->step = c.step; info->counter = c.counter; info->cur = c.cur;
+    info->DD = c.k.DD; info->lambda_L = c.k.lambda_L; info->cp_Pr_T = c.k.cp_Pr_T;
+    info->device_bytes = c.bytes;
+    return FSL_OK;
+}
+
+int fsl_upload_state(fsl_ctx *h, const double *state)
+{
+    if (!h || !state) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
+    CK(cudaMemcpyAsync(c.stage_dev, state, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    launch_state_scatter(c, c.U, c.stage_dev);
+    CKL();
+    CK(cudaStreamSynchronize(c.stream));
+    c.cur = 0;
+    return FSL_OK;
+}
+
+int fsl_download_state(fsl_ctx *h, double *state)
+{
+    if (!h || !state) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
+    launch_state_gather(c, c.U, c.stage_dev);
+    CKL();
+    CK(cudaMemcpyAsync(state, c.stage_dev, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+int fsl_set_time(fsl_ctx *h, unsigned step, double deltaT)
+{
+    if (!h || !(deltaT > 0)) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = sync_scalars(c);
+    if (rc) return rc;
+    c.step = step;
+    c.hs->dt = deltaT;
+    c.hs->dtx = deltaT / c.p.deltaX; c.hs->dty = deltaT / c.p.deltaY; c.hs->dtz = deltaT / c.p.deltaZ;
+    CK(cudaMemcpyAsync(c.ds, c.hs, sizeof(DevScalars), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.dt_host = deltaT;
+    return FSL_OK;
+}
+
+int fsl_check_courant(fsl_ctx *h, double *maxCo, double *dt)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    launch_courant(c);
+    CKL();
+    int rc = sync_scalars(c);
+    if (rc) return rc;
+    if (maxCo) *maxCo = c.hs->maxCo;
+    if (dt) *dt = c.hs->dt;
+    if (c.hs->status) return fail(c, FSL_ERR_NONFINITE, "non-finite or non-positive Courant maximum or density");
+    return FSL_OK;
+}
+
+int fsl_draw_disturbance(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    draw(h->c);
+    return FSL_OK;
+}
+
+int fsl_set_disturbance(fsl_ctx *h, unsigned k_min, unsigned k_max, double Ud, double Vd, double Wd)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    c.dist.k_min = k_min; c.dist.k_max = k_max; c.dist.Ud = Ud; c.dist.Vd = Vd; c.dist.Wd = Wd;
+    return FSL_OK;
+}
+
+int fsl_ghost_bc(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    launch_ghost(c, cur_ptr(c));
+    CKL();
+    return FSL_OK;
+}
+
+int fsl_reconstruct(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = ensure_faces(c);
+    if (rc) return rc;
+    launch_recon(c, cur_ptr(c));
+    CKL();
+    return FSL_OK;
+}
+
+int fsl_interface_bc(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = ensure_faces(c);
+    if (rc) return rc;
+    launch_ifbc(c, c.dist);
+    CKL();
+    return FSL_OK;
+}
+
+int fsl_dynamic_smagorinsky(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = ensure_dyn(c);
+    if (rc) return rc;
+    launch_dynsmag(c, c.U);
+    CKL();
+    return FSL_OK;
+}
+
+int fsl_fluxes(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = ensure_faces(c);
+    if (rc) return rc;
+    launch_fluxes(c, cur_ptr(c));
+    CKL();
+    return FSL_OK;
+}
+
+int fsl_evolution(fsl_ctx *h, int stage)
+{
+    if (!h || stage < 1) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = ensure_faces(c);
+    if (rc) return rc;
+    launch_evolution(c, c.p.nStages, stage);
+    CKL();
+    // pointer swap of src/evolution.c:71,113,155 (and :188,228 for RK2)
+    c.cur = (stage == 1 || stage == 2) ? 1 : 0;
+    return FSL_OK;
+}
+
+int fsl_step_phased(fsl_ctx *h, int nsteps)
+{
+    if (!h || nsteps < 0) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc;
+    for (int n = 0; n < nsteps; n++) {
+        launch_courant(c);
+        CKL();
+        c.step++;
+        draw(c);
+        for (int s = 1; s <= c.p.nStages; s++) {
+            if ((rc = ensure_faces(c))) return rc;
+            if ((rc = ensure_dyn(c))) return rc;
+            double *cur = cur_ptr(c);
+            launch_ghost(c, cur);
+            launch_recon(c, cur);
+            launch_ifbc(c, c.dist);
+            if (s == 1) launch_dynsmag(c, c.U);
+            launch_fluxes(c, cur);
+            launch_evolution(c, c.p.nStages, s);
+            c.cur = (s == 1 || s == 2) ? 1 : 0;
+            CKL();
+        }
+    }
+    return FSL_OK;
+}
+
+int fsl_step(fsl_ctx *h, int nsteps)
+{
+    return fsl_step_phased(h, nsteps);
+}
+
+int fsl_get_cells(fsl_ctx *h, int which, int var, double *out)
+{
+    if (!h || !out || var < 0 || var > 4 || which < 0 || which > 3) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    const Grid &g = c.g;
+    const double *base = which == 0 ? c.U : which == 1 ? c.Up : which == 2 ? cur_ptr(c) : c.mu;
+    if (which == 3) var = 0;
+    base += var * g.fstride + g.off;
+    CK(cudaMemcpy2DAsync(out, (g.D + 2) * sizeof(double), base, g.pk * sizeof(double), (g.D + 2) * sizeof(double),
+                         (size_t)(g.L + 2) * (g.H + 2), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+int fsl_set_cells(fsl_ctx *h, int which, int var, const double *in)
+{
+    if (!h || !in || var < 0 || var > 4 || which < 0 || which > 3) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    const Grid &g = c.g;
+    double *base = which == 0 ? c.U : which == 1 ? c.Up : which == 2 ? cur_ptr(c) : c.mu;
+    if (which == 3) var = 0;
+    base += var * g.fstride + g.off;
+    CK(cudaMemcpy2DAsync(base, g.pk * sizeof(double), in, (g.D + 2) * sizeof(double), (g.D + 2) * sizeof(double),
+                         (size_t)(g.L + 2) * (g.H + 2), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+int fsl_get_faces(fsl_ctx *h, int dir, int side, int var, double *out)
+{
+    if (!h || !out || dir < 0 || dir > 2 || side < 0 || side > 1 || var < 0 || var > 4) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = ensure_faces(c);
+    if (rc) return rc;
+    const double *p = dir == 0 ? c.f.x[side][var] : dir == 1 ? c.f.y[side][var] : c.f.z[side][var];
+    CK(cudaMemcpyAsync(out, p, face_count(c.g, dir) * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+int fsl_set_faces(fsl_ctx *h, int dir, int side, int var, const double *in)
+{
+    if (!h || !in || dir < 0 || dir > 2 || side < 0 || side > 1 || var < 0 || var > 4) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = ensure_faces(c);
+    if (rc) return rc;
+    double *p = dir == 0 ? c.f.x[side][var] : dir == 1 ? c.f.y[side][var] : c.f.z[side][var];
+    CK(cudaMemcpyAsync(p, in, face_count(c.g, dir) * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+int fsl_set_cur(fsl_ctx *h, int which)
+{
+    if (!h || which < 0 || which > 1) return FSL_ERR_ARG;
+    h->c.cur = which;
+    return FSL_OK;
+}
+
+int fsl_sums(fsl_ctx *h, double sums[5])
+{
+    if (!h || !sums) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    double *d = c.partials + 4000;
+    launch_sums(c, c.U, d);
+    CKL();
+    CK(cudaMemcpyAsync(sums, d, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+int fsl_plane_sums(fsl_ctx *h, double *rows)
+{
+    if (!h || !rows) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    double *d = c.stage_dev; // scratch: 8*HIG <= LEN*HIG*5*DEP
+    launch_plane_sums(c, c.U, d);
+    CKL();
+    CK(cudaMemcpyAsync(rows, d, 8 * (size_t)c.p.HIG * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+} // extern "C"

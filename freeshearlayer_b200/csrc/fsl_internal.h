@@ -1,0 +1,113 @@
+// fsl_internal.h -- device layout, context and launcher declarations shared
+// by the translation units of libfsl_gpu.so.  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/fsl_gpu.h"
+
+namespace fsl {
+
+// Padded cell field layout in HBM: (LEN+2)(HIG+2) rows of pk elements, k
+// fastest, element (0,0,0) at `off`.  pk is a multiple of 32 bytes' worth of
+// elements and off = that multiple - 1, so interior rows (k = 1..DEP) start on
+// a 32-byte sector boundary and full rows are read with aligned, coalesced
+// sectors.  Fields of one kind sit `fstride` elements apart in one allocation.
+struct Grid {
+    int L, H, D;
+    int pk;
+    long long pi;      // elements between i planes = pk * (H+2)
+    long long off;     // offset of (0,0,0)
+    long long fstride; // elements between fields (multiple of 64)
+    __host__ __device__ __forceinline__ long long idx(int i, int j, int k) const
+    {
+        return off + (long long)i * pi + (long long)j * pk + k;
+    }
+};
+
+Grid make_grid(int L, int H, int D, int elem_bytes);
+
+// Physical and derived constants of one domain (src/initialize.c:67-94).
+struct Consts {
+    double rdx, rdy, rdz, r2dx, r2dy, r2dz, r4dx, r4dy, r4dz;
+    double mu_L, lambda_L, cp_Pr_T, DD, maxCoNum;
+    double deltaX, deltaY, deltaZ;
+    int setup, BL_HIG, cfl_mode, nStages;
+};
+
+// Device-resident scalars updated by the time-step reduction.
+struct DevScalars {
+    double dt, dtx, dty, dtz;
+    double maxCo;
+    unsigned int status; // bit 0: non-finite or non-positive Courant max; bit 1: non-positive density
+    unsigned int pad;
+};
+
+// Disturbance block of one step (host RNG state, src/layer2.c:152-162).
+struct Disturb {
+    unsigned k_min, k_max;
+    double Ud, Vd, Wd;
+};
+
+// Dense face arrays (reference face index ranges).
+struct Faces {
+    double *x[2][5], *y[2][5], *z[2][5];
+};
+
+// Scratch of the dynamic Smagorinsky procedure (padded layout, FP64).
+struct DynScratch {
+    double *vel;   // 3 fields u, v, w
+    double *t1;    // 9 fields (pass-1 / filtered output)
+    double *t2;    // 9 fields (pass-2)
+    double *A;     // 6 fields |S| S_ij, ghost layer kept zero
+    double *Lst;   // 6 fields Leonard stress
+    double *B;     // 6 fields |S^| S^_ij
+    double *S;     // 1 field |S|
+};
+
+struct Ctx {
+    fsl_params p;
+    Consts k;
+    Grid g;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    // cell fields (FP64): U^n, stage buffer, second stage buffer, mu_SGS
+    double *U = nullptr, *Up = nullptr, *Uq = nullptr, *mu = nullptr;
+    int cur = 0; // 0: U*_ = U, 1: U*_ = Up
+    Faces f{};
+    bool faces_alloc = false;
+    DynScratch dyn{};
+    bool dyn_alloc = false;
+    DevScalars *ds = nullptr; // device scalars
+    DevScalars *hs = nullptr; // pinned host mirror
+    double *partials = nullptr;
+    int npartials = 0;
+    double *stage_host = nullptr; // pinned staging for state transfer
+    double *stage_dev = nullptr;
+    // host driver state
+    double X = 0;
+    int counter = 0;
+    unsigned step = 0;
+    Disturb dist{};
+    double dt_host = 0; // host copy of dt, valid after sync
+    double maxco_host = 0;
+    unsigned long long bytes = 0;
+    std::string err;
+};
+
+// ---- launchers (fsl_phase.cu) ------------------------------------------------
+void launch_ghost(Ctx &c, double *cur);
+void launch_recon(Ctx &c, const double *cur);
+void launch_ifbc(Ctx &c, const Disturb &d);
+void launch_fluxes(Ctx &c, const double *cur);
+void launch_evolution(Ctx &c, int nstages, int stage);
+void launch_dynsmag(Ctx &c, const double *U);
+void launch_courant(Ctx &c);
+void launch_state_scatter(Ctx &c, double *dst, const double *packed);
+void launch_state_gather(Ctx &c, const double *src, double *packed);
+void launch_sums(Ctx &c, const double *U, double *out5);
+void launch_plane_sums(Ctx &c, const double *U, double *rows);
+
+} // namespace fsl

@@ -1,0 +1,798 @@
+// fsl_phase.cu -- one kernel per reference phase of the explicit step (FP64).
+//
+// These are the unfused path behind the per-phase C-ABI entry points
+// (fsl_ghost_bc, fsl_reconstruct, ...).  They keep the reference's data flow
+// (face-state arrays between reconstruction and fluxes) so each phase can be
+// checked on its own against the CPU oracle.  Compiled with --fmad=false:
+// results equal the reference's serial FP64 code bit for bit.
+#include "fsl_internal.h"
+#include "fsl_phys.cuh"
+
+namespace fsl {
+
+namespace {
+
+constexpr double H3 = 1. / 3.; // box test-filter weight, src/turbulence.c:113
+
+__device__ __forceinline__ long long ixf(int L, int H, int D, int i, int j, int k)
+{
+    return ((long long)i * H + j) * D + k;
+}
+__device__ __forceinline__ long long iyf(int L, int H, int D, int i, int j, int k)
+{
+    return ((long long)i * (H + 1) + j) * D + k;
+}
+__device__ __forceinline__ long long izf(int L, int H, int D, int i, int j, int k)
+{
+    return ((long long)i * H + j) * (D + 1) + k;
+}
+
+// ---------------------------------------------------------------------------
+// A1 ghost cells (src/boundCondInGhostCells.c:10-96).  The reference fills x,
+// then z over all i, then y over all i and k; every ghost value is therefore a
+// composition of copies of one interior cell (or of the inflow profile).  Each
+// thread evaluates that composition for one ghost cell, so all ghost cells are
+// written in one pass with the reference's values, edges and corners included.
+// ---------------------------------------------------------------------------
+__global__ void k_ghost(Grid g, int setup, double *__restrict__ u)
+{
+    const int L = g.L, H = g.H, D = g.D;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nx = 2LL * (H + 2) * (D + 2), ny = 2LL * L * (D + 2), nz = 2LL * L * H;
+    int i, j, k;
+    if (t < nx) {
+        long long a = (long long)(H + 2) * (D + 2);
+        i = (t / a) ? L + 1 : 0;
+        long long r = t % a;
+        j = (int)(r / (D + 2));
+        k = (int)(r % (D + 2));
+    } else if ((t -= nx) < ny) {
+        long long a = (long long)L * (D + 2);
+        j = (t / a) ? H + 1 : 0;
+        long long r = t % a;
+        i = 1 + (int)(r / (D + 2));
+        k = (int)(r % (D + 2));
+    } else if ((t -= ny) < nz) {
+        long long a = (long long)L * H;
+        k = (t / a) ? D + 1 : 0;
+        long long r = t % a;
+        i = 1 + (int)(r / H);
+        j = 1 + (int)(r % H);
+    } else {
+        return;
+    }
+    const bool spatial = (setup == FSL_SETUP_SPATIAL);
+    bool flip = false;
+    int jj = j, kk = k;
+    if (j == 0) { jj = 1; flip = spatial; }
+    else if (j == H + 1) { jj = H; flip = spatial; }
+    if (k == 0) kk = D;
+    else if (k == D + 1) kk = 1;
+    double v[5];
+    const long long fs = g.fstride;
+    typedef Kc<double> kc;
+    if (i == 0 && spatial) {
+        // inflow step profile, :17-40
+        const double P = 100000., R = 1.0;
+        const double U = (jj <= H / 2) ? 76.4 : 200;
+        v[0] = R; v[1] = R * U; v[2] = 0.; v[3] = 0.;
+        v[4] = P / kc::K_1 + 0.5 * R * (U * U);
+    } else {
+        int si = i;
+        if (i == 0) si = L;               // temporal: periodic x
+        else if (i == L + 1) si = spatial ? L : 1;
+        long long s = g.idx(si, jj, kk);
+#pragma unroll
+        for (int q = 0; q < 5; q++) v[q] = u[q * fs + s];
+        if (i == L + 1 && spatial) {
+            // outflow, :44-52: momenta copied, E rebuilt at P = 1e5
+            const double P = 100000.;
+            v[4] = P / kc::K_1 + 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]) / v[0];
+        }
+    }
+    if (flip) v[2] = -v[2];
+    long long d = g.idx(i, j, k);
+#pragma unroll
+    for (int q = 0; q < 5; q++) u[q * fs + d] = v[q];
+}
+
+// ---------------------------------------------------------------------------
+// A2 reconstruction (src/reconstruction.c:26-345): one thread per interior
+// cell, all three sweeps, six face states written to the face arrays.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_recon(Grid g, const double *__restrict__ u, Faces f)
+{
+    const int L = g.L, H = g.H, D = g.D;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int i = blockIdx.z + 1;
+    if (k > D || j > H) return;
+    const long long fs = g.fstride;
+    const long long c0 = g.idx(i, j, k);
+    CellC<double> c;
+#pragma unroll
+    for (int q = 0; q < 5; q++) c.u[q] = u[q * fs + c0];
+    cell_consts(c);
+    double fw[5], bw[5], hi[5], lo[5];
+    // x
+    {
+        const long long a = c0 + g.pi, b = c0 - g.pi;
+#pragma unroll
+        for (int q = 0; q < 5; q++) { fw[q] = u[q * fs + a]; bw[q] = u[q * fs + b]; }
+        recon_x(c, fw, bw, hi, lo);
+        const long long fh = ixf(L, H, D, i, j - 1, k - 1), fl = ixf(L, H, D, i - 1, j - 1, k - 1);
+#pragma unroll
+        for (int q = 0; q < 5; q++) { f.x[0][q][fh] = hi[q]; f.x[1][q][fl] = lo[q]; }
+    }
+    // y: (rho, rho v, rho w, rho u, E)
+    {
+        const long long a = c0 + g.pk, b = c0 - g.pk;
+        const int perm[5] = {0, 2, 3, 1, 4};
+#pragma unroll
+        for (int q = 0; q < 5; q++) { fw[q] = u[perm[q] * fs + a]; bw[q] = u[perm[q] * fs + b]; }
+        recon_y(c, fw, bw, hi, lo);
+        const long long fh = iyf(L, H, D, i - 1, j, k - 1), fl = iyf(L, H, D, i - 1, j - 1, k - 1);
+#pragma unroll
+        for (int q = 0; q < 5; q++) { f.y[0][q][fh] = hi[q]; f.y[1][q][fl] = lo[q]; }
+    }
+    // z: (rho, rho w, rho u, rho v, E)
+    {
+        const long long a = c0 + 1, b = c0 - 1;
+        const int perm[5] = {0, 3, 1, 2, 4};
+#pragma unroll
+        for (int q = 0; q < 5; q++) { fw[q] = u[perm[q] * fs + a]; bw[q] = u[perm[q] * fs + b]; }
+        recon_z(c, fw, bw, hi, lo);
+        const long long fh = izf(L, H, D, i - 1, j - 1, k), fl = izf(L, H, D, i - 1, j - 1, k - 1);
+#pragma unroll
+        for (int q = 0; q < 5; q++) { f.z[0][q][fh] = hi[q]; f.z[1][q][fl] = lo[q]; }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// A3 boundary face states (src/bounCondOnInterfaces.c:11-110).
+// ---------------------------------------------------------------------------
+__global__ void k_ifbc(Grid g, int setup, int BL_HIG, Disturb d, Faces f)
+{
+    const int L = g.L, H = g.H, D = g.D;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nx = (long long)H * D, ny = (long long)L * D, nz = (long long)L * H;
+    const bool spatial = (setup == FSL_SETUP_SPATIAL);
+    typedef Kc<double> kc;
+    if (t < nx) {
+        const int j = (int)(t / D), k = (int)(t % D);
+        const long long f0 = ixf(L, H, D, 0, j, k), fL = ixf(L, H, D, L, j, k);
+        if (spatial) {
+            const double P = 100000., R = 1.0;
+            double U, V = 0., W = 0.;
+            double v[5];
+            if (j < H / 2) { // :17-29
+                U = 76.4;
+                v[0] = R; v[1] = R * U; v[2] = 0.; v[3] = 0.; v[4] = P / kc::K_1 + 0.5 * R * (U * U);
+            } else if (j < H / 2 + BL_HIG) { // :31-49
+                const unsigned ku = (unsigned)k;
+                bool dist;
+                if (d.k_max > d.k_min) dist = (ku >= d.k_min && ku < d.k_max);
+                else dist = !(ku >= d.k_max && ku < d.k_min);
+                if (dist) { U = 200. + d.Ud; V = d.Vd; W = d.Wd; }
+                else { U = 200.; V = W = 0.; }
+                v[0] = R; v[1] = R * U; v[2] = R * V; v[3] = R * W;
+                v[4] = P / kc::K_1 + 0.5 * R * (U * U + V * V + W * W);
+            } else { // :51-60
+                U = 200.;
+                v[0] = R; v[1] = R * U; v[2] = 0.; v[3] = 0.; v[4] = P / kc::K_1 + 0.5 * R * (U * U);
+            }
+#pragma unroll
+            for (int q = 0; q < 5; q++) f.x[0][q][f0] = v[q];
+            // :62-71 outflow
+            const double r = f.x[0][0][fL], mu_ = f.x[0][1][fL], mv = f.x[0][2][fL], mw = f.x[0][3][fL];
+            f.x[1][0][fL] = r; f.x[1][1][fL] = mu_; f.x[1][2][fL] = mv; f.x[1][3][fL] = mw;
+            f.x[1][4][fL] = P / kc::K_1 + 0.5 * (mu_ * mu_ + mv * mv + mw * mw) / r;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                f.x[0][q][f0] = f.x[0][q][fL];
+                f.x[1][q][fL] = f.x[1][q][f0];
+            }
+        }
+    } else if ((t -= nx) < ny) { // :75-90
+        const int i = (int)(t / D), k = (int)(t % D);
+        const long long f0 = iyf(L, H, D, i, 0, k), fH = iyf(L, H, D, i, H, k);
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            if (q == 2 && spatial) {
+                f.y[0][q][f0] = -f.y[1][q][f0];
+                f.y[1][q][fH] = -f.y[0][q][fH];
+            } else {
+                f.y[0][q][f0] = f.y[1][q][f0];
+                f.y[1][q][fH] = f.y[0][q][fH];
+            }
+        }
+    } else if ((t -= ny) < nz) { // :94-109
+        const int i = (int)(t / H), j = (int)(t % H);
+        const long long f0 = izf(L, H, D, i, j, 0), fD = izf(L, H, D, i, j, D);
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            f.z[0][q][f0] = f.z[0][q][fD];
+            f.z[1][q][fD] = f.z[1][q][f0];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// A4 fluxes (src/fluxes.c:57-571): one thread per face of direction N.
+// The flux overwrites the minus-side state array, as in the reference.
+// ---------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(128) k_flux(Grid g, Consts kc, const double *__restrict__ u,
+                                              const double *__restrict__ mu, Faces f)
+{
+    const int L = g.L, H = g.H, D = g.D;
+    const int na = L + (N == 1), nb = H + (N == 2), nc = D + (N == 3);
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y * blockDim.y + threadIdx.y;
+    const int a = blockIdx.z;
+    if (c >= nc || b >= nb || a >= na) return;
+    const long long fs = g.fstride;
+    long long fi;
+    double *const *mS;
+    double *const *pS;
+    long long plus, dn, dt1, dt2;
+    double rdn, rt1, rt2;
+    if (N == 1) {
+        fi = ((long long)a * nb + b) * nc + c;
+        mS = f.x[0]; pS = f.x[1];
+        plus = g.idx(a + 1, b + 1, c + 1); dn = g.pi; dt1 = g.pk; dt2 = 1;
+        rdn = kc.rdx; rt1 = kc.r4dy; rt2 = kc.r4dz;
+    } else if (N == 2) {
+        fi = ((long long)a * nb + b) * nc + c;
+        mS = f.y[0]; pS = f.y[1];
+        plus = g.idx(a + 1, b + 1, c + 1); dn = g.pk; dt1 = g.pi; dt2 = 1;
+        rdn = kc.rdy; rt1 = kc.r4dx; rt2 = kc.r4dz;
+    } else {
+        fi = ((long long)a * nb + b) * nc + c;
+        mS = f.z[0]; pS = f.z[1];
+        plus = g.idx(a + 1, b + 1, c + 1); dn = 1; dt1 = g.pi; dt2 = g.pk;
+        rdn = kc.rdz; rt1 = kc.r4dx; rt2 = kc.r4dy;
+    }
+    const long long minus = plus - dn;
+    double Lm[5], Rp[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) { Lm[q] = mS[q][fi]; Rp[q] = pS[q][fi]; }
+    double Rho, P, vel[3];
+    riemann<double, N>(Lm, Rp, Rho, P, vel);
+    double vp[3], vm[3], Tp, Tm;
+    vel_div(u[plus], u[fs + plus], u[2 * fs + plus], u[3 * fs + plus], u[4 * fs + plus], vp, Tp);
+    vel_div(u[minus], u[fs + minus], u[2 * fs + minus], u[3 * fs + minus], u[4 * fs + minus], vm, Tm);
+    // tangential neighbours: P/M = plus/minus cell, h/l = +/- tangential offset
+    double Ph1[3], Mh1[3], Pl1[3], Ml1[3], Ph2[3], Mh2[3], Pl2[3], Ml2[3];
+#define LOADV(dst, at) vel_rcp(u[at], u[fs + (at)], u[2 * fs + (at)], u[3 * fs + (at)], dst)
+    LOADV(Ph1, plus + dt1); LOADV(Mh1, minus + dt1); LOADV(Pl1, plus - dt1); LOADV(Ml1, minus - dt1);
+    LOADV(Ph2, plus + dt2); LOADV(Mh2, minus + dt2); LOADV(Pl2, plus - dt2); LOADV(Ml2, minus - dt2);
+#undef LOADV
+    // g[a][b] = d u_a / d x_b
+    double gr[3][3];
+    const int n0 = N - 1;
+    const int t1 = (N == 1) ? 1 : 0;   // first tangential axis
+    const int t2 = (N == 3) ? 1 : 2;   // second tangential axis
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        gr[q][n0] = (vp[q] - vm[q]) * rdn;
+        gr[q][t1] = (Ph1[q] + Mh1[q] - Pl1[q] - Ml1[q]) * rt1;
+        gr[q][t2] = (Ph2[q] + Mh2[q] - Pl2[q] - Ml2[q]) * rt2;
+    }
+    // SGS viscosity at the face: x uses the two adjacent cells (:191); the y
+    // and z sweeps average the plus cell with its x-neighbour (:360, :531).
+    const double mu_T = 0.5 * (mu[plus] + mu[plus - g.pi]);
+    double F[5];
+    face_flux<double, N>(Rho, P, vel, gr, vp, vm, Tp, Tm, kc.mu_L, mu_T, kc.lambda_L, kc.cp_Pr_T, rdn, F);
+#pragma unroll
+    for (int q = 0; q < 5; q++) mS[q][fi] = F[q];
+}
+
+// ---------------------------------------------------------------------------
+// A7 TVD Runge-Kutta (src/evolution.c:15-245).  mode: 1..3 = RK3 stage,
+// 4 = the nStages == 2 chain of stage 1, 5 = the chain of stage 2 (RK2 stage
+// 2 followed by RK3 stage 2 on the updated U, src/evolution.c:19-23).
+// ---------------------------------------------------------------------------
+__global__ void k_evolution(Grid g, int mode, const DevScalars *__restrict__ ds, double *__restrict__ U,
+                            double *__restrict__ Up, Faces f)
+{
+    const int L = g.L, H = g.H, D = g.D;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int i = blockIdx.z + 1;
+    if (k > D || j > H) return;
+    const double dtx = ds->dtx, dty = ds->dty, dtz = ds->dtz;
+    const double one_third = 1. / 3., two_thirds = 2. / 3.;
+    const long long c = g.idx(i, j, k), fs = g.fstride;
+    const long long xm = ixf(L, H, D, i - 1, j - 1, k - 1), xp = ixf(L, H, D, i, j - 1, k - 1);
+    const long long ym = iyf(L, H, D, i - 1, j - 1, k - 1), yp = iyf(L, H, D, i - 1, j, k - 1);
+    const long long zm = izf(L, H, D, i - 1, j - 1, k - 1), zp = izf(L, H, D, i - 1, j - 1, k);
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        const double X = dtx * (f.x[0][q][xm] - f.x[0][q][xp]);
+        const double Y = dty * (f.y[0][q][ym] - f.y[0][q][yp]);
+        const double Z = dtz * (f.z[0][q][zm] - f.z[0][q][zp]);
+        double *u = U + q * fs, *up = Up + q * fs;
+        if (mode == 1 || mode == 4) {
+            up[c] = u[c] + X + Y + Z;
+        } else if (mode == 2) {
+            up[c] = 0.75 * u[c] + 0.25 * (up[c] + X + Y + Z);
+        } else if (mode == 3) {
+            u[c] = one_third * u[c] + two_thirds * (up[c] + X + Y + Z);
+        } else { // mode 5
+            const double un = 0.5 * (u[c] + up[c] + X + Y + Z);
+            u[c] = un;
+            up[c] = 0.75 * un + 0.25 * (up[c] + X + Y + Z);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// A8 Courant maximum (src/helpers.c:23-52).  NaN never wins a comparison, as
+// in the reference's `(CoNum = U*deltaT_X) > maxCo`, so the maximum is
+// independent of reduction order.
+// ---------------------------------------------------------------------------
+__global__ void k_courant_partial(Grid g, Consts kc, const double *__restrict__ U,
+                                  const DevScalars *__restrict__ ds, double *__restrict__ partials,
+                                  DevScalars *__restrict__ dsw)
+{
+    const int L = g.L, H = g.H, D = g.D;
+    const long long n = (long long)L * H * D;
+    const long long fs = g.fstride;
+    const double dtx = ds->dtx, dty = ds->dty, dtz = ds->dtz;
+    double m = 0.0;
+    unsigned bad = 0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % D) + 1;
+        const long long r = t / D;
+        const int j = (int)(r % H) + 1;
+        const int i = (int)(r / H) + 1;
+        const long long c = g.idx(i, j, k);
+        const double R = U[c];
+        const double Uv = U[fs + c] / R;
+        double Co;
+        if (kc.cfl_mode == FSL_CFL_ACOUSTIC) {
+            const double V = U[2 * fs + c] / R, W = U[3 * fs + c] / R;
+            const double P = (U[4 * fs + c] - 0.5 * R * (Uv * Uv + V * V + W * W)) * 0.4;
+            const double Cs = sqrt(1.4 * P / R);
+            Co = (fabs(Uv) + Cs) * dtx + (fabs(V) + Cs) * dty + (fabs(W) + Cs) * dtz;
+        } else {
+            Co = Uv * dtx;
+        }
+        m = (Co > m) ? Co : m;
+        if (!(R > 0.0)) bad = 1;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double x = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (x > m) ? x : m;
+    }
+    __shared__ double sm[32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sm[w] = m;
+    if (bad) atomicOr(&dsw->status, 2u);
+    __syncthreads();
+    if (w == 0) {
+        m = (l < (int)(blockDim.x >> 5)) ? sm[l] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double x = __shfl_xor_sync(0xffffffffu, m, o);
+            m = (x > m) ? x : m;
+        }
+        if (l == 0) partials[blockIdx.x] = m;
+    }
+}
+
+// Final reduction and the dt rescale of src/helpers.c:47-50.
+__global__ void k_courant_final(Consts kc, const double *__restrict__ partials, int np, DevScalars *ds)
+{
+    double m = 0.0;
+    for (int t = threadIdx.x; t < np; t += blockDim.x) {
+        const double x = partials[t];
+        m = (x > m) ? x : m;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double x = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (x > m) ? x : m;
+    }
+    __shared__ double sm[32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sm[w] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        m = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) m = (sm[q] > m) ? sm[q] : m;
+        const double maxCo = m;
+        double dt = ds->dt;
+        dt *= (kc.maxCoNum / maxCo);
+        ds->dt = dt;
+        ds->dtx = dt / kc.deltaX;
+        ds->dty = dt / kc.deltaY;
+        ds->dtz = dt / kc.deltaZ;
+        ds->maxCo = maxCo;
+        if (!(maxCo > 0.0) || !isfinite(maxCo) || !isfinite(dt)) ds->status |= 1u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// A5/A6 dynamic Smagorinsky (src/turbulence.c:17-507) as seven passes.
+// The filter keeps the reference's three sweeps (y, z, x), each
+// t = 0; t += a h; t += b h; t += c h, on zero-initialised scratch whose never
+// written bands stay zero (the oracle convention for src/turbulence.c:44-45).
+// ---------------------------------------------------------------------------
+__global__ void k_dyn_vel(Grid g, const double *__restrict__ U, double *__restrict__ vel)
+{
+    const long long n = (long long)(g.L + 2) * g.pi;
+    const long long fs = g.fstride;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long c = g.off + t;
+        const double rr = 1. / U[c]; // :201-205
+        vel[c] = U[fs + c] * rr;
+        vel[fs + c] = U[2 * fs + c] * rr;
+        vel[2 * fs + c] = U[3 * fs + c] * rr;
+    }
+}
+
+// y sweep (:47-61) of u, v, w and their six products (:213-230), computed
+// on the fly; i in [0,LEN], j in [1,HIG], k in [0,DEP].
+__global__ void k_filt_y_vel(Grid g, const double *__restrict__ vel, double *__restrict__ t1)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int i = blockIdx.z;
+    if (k > g.D || j > g.H) return;
+    const long long fs = g.fstride, c = g.idx(i, j, k);
+    double a[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const long long s = c + (r - 1) * (long long)g.pk;
+        a[r][0] = vel[s]; a[r][1] = vel[fs + s]; a[r][2] = vel[2 * fs + s];
+    }
+    double q[3][9];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const double uu = a[r][0], vv = a[r][1], ww = a[r][2];
+        q[r][0] = uu; q[r][1] = vv; q[r][2] = ww;
+        q[r][3] = uu * uu; q[r][4] = uu * vv; q[r][5] = uu * ww;
+        q[r][6] = vv * vv; q[r][7] = vv * ww; q[r][8] = ww * ww;
+    }
+#pragma unroll
+    for (int m = 0; m < 9; m++) {
+        double t = 0.;
+        t += q[0][m] * H3; t += q[1][m] * H3; t += q[2][m] * H3;
+        t1[m * fs + c] = t;
+    }
+}
+
+// generic y sweep of nf fields
+__global__ void k_filt_y(Grid g, int nf, const double *__restrict__ src, double *__restrict__ t1)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int i = blockIdx.z;
+    if (k > g.D || j > g.H) return;
+    const long long fs = g.fstride, c = g.idx(i, j, k);
+    for (int m = 0; m < nf; m++) {
+        const double *s = src + m * fs;
+        double t = 0.;
+        t += s[c - g.pk] * H3; t += s[c] * H3; t += s[c + g.pk] * H3;
+        t1[m * fs + c] = t;
+    }
+}
+
+// z sweep (:63-77): i in [0,LEN], j in [0,HIG], k in [1,DEP]
+__global__ void k_filt_z(Grid g, int nf, const double *__restrict__ t1, double *__restrict__ t2)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k > g.D || j > g.H) return;
+    const long long fs = g.fstride, c = g.idx(i, j, k);
+    for (int m = 0; m < nf; m++) {
+        const double *s = t1 + m * fs;
+        double t = 0.;
+        t += s[c - 1] * H3; t += s[c] * H3; t += s[c + 1] * H3;
+        t2[m * fs + c] = t;
+    }
+}
+
+// x sweep (:80-95) back into the pass-1 buffer: i in [1,LEN], j in [0,HIG],
+// k in [0,DEP]
+__global__ void k_filt_x(Grid g, int nf, const double *__restrict__ t2, double *__restrict__ t1)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z + 1;
+    if (k > g.D || j > g.H) return;
+    const long long fs = g.fstride, c = g.idx(i, j, k);
+    for (int m = 0; m < nf; m++) {
+        const double *s = t2 + m * fs;
+        double t = 0.;
+        t += s[c - g.pi] * H3; t += s[c] * H3; t += s[c + g.pi] * H3;
+        t1[m * fs + c] = t;
+    }
+}
+
+// Interior: Leonard stress, |S|, A_ij = |S| S_ij, B_ij = |S^| S^_ij
+// (:250-382).  Field order of the symmetric tensors: 11 12 13 22 23 33.
+__global__ void k_dyn_mid(Grid g, Consts kc, const double *__restrict__ vel, const double *__restrict__ F,
+                          double *__restrict__ Lst, double *__restrict__ A, double *__restrict__ B,
+                          double *__restrict__ Smag)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int i = blockIdx.z + 1;
+    if (k > g.D || j > g.H) return;
+    const long long fs = g.fstride, c = g.idx(i, j, k);
+    const double f0 = F[c], f1 = F[fs + c], f2 = F[2 * fs + c];
+    Lst[c] = F[3 * fs + c] - f0 * f0;
+    Lst[fs + c] = F[4 * fs + c] - f0 * f1;
+    Lst[2 * fs + c] = F[5 * fs + c] - f0 * f2;
+    Lst[3 * fs + c] = F[6 * fs + c] - f1 * f1;
+    Lst[4 * fs + c] = F[7 * fs + c] - f1 * f2;
+    Lst[5 * fs + c] = F[8 * fs + c] - f2 * f2;
+    const long long dI = g.pi, dJ = g.pk;
+#pragma unroll
+    for (int pass = 0; pass < 2; pass++) {
+        const double *uu = pass ? F : vel;
+        const double *vv = uu + fs, *ww = uu + 2 * fs;
+        const double du_dx = (uu[c + dI] - uu[c - dI]) * kc.r2dx;
+        const double du_dy = (uu[c + dJ] - uu[c - dJ]) * kc.r2dy;
+        const double du_dz = (uu[c + 1] - uu[c - 1]) * kc.r2dz;
+        const double dv_dx = (vv[c + dI] - vv[c - dI]) * kc.r2dx;
+        const double dv_dy = (vv[c + dJ] - vv[c - dJ]) * kc.r2dy;
+        const double dv_dz = (vv[c + 1] - vv[c - 1]) * kc.r2dz;
+        const double dw_dx = (ww[c + dI] - ww[c - dI]) * kc.r2dx;
+        const double dw_dy = (ww[c + dJ] - ww[c - dJ]) * kc.r2dy;
+        const double dw_dz = (ww[c + 1] - ww[c - 1]) * kc.r2dz;
+        const double S11 = du_dx, S12 = 0.5 * (du_dy + dv_dx), S13 = 0.5 * (du_dz + dw_dx);
+        const double S21 = S12, S22 = dv_dy, S23 = 0.5 * (dv_dz + dw_dy);
+        const double S31 = S13, S32 = S23, S33 = dw_dz;
+        const double S = sqrt(2 * (S11 * S11 + S12 * S12 + S13 * S13 + S21 * S21 + S22 * S22 + S23 * S23 +
+                                   S31 * S31 + S32 * S32 + S33 * S33));
+        double *o = pass ? B : A;
+        o[c] = S * S11; o[fs + c] = S * S12; o[2 * fs + c] = S * S13;
+        o[3 * fs + c] = S * S22; o[4 * fs + c] = S * S23; o[5 * fs + c] = S * S33;
+        if (!pass) Smag[c] = S;
+    }
+}
+
+// M_ij, Germano-Lilly coefficient with clipping to [0, 0.15], mu_SGS
+// (:398-445).
+__global__ void k_dyn_final(Grid g, Consts kc, const double *__restrict__ rho, const double *__restrict__ Lst,
+                            const double *__restrict__ B, const double *__restrict__ Ahat,
+                            const double *__restrict__ Smag, double *__restrict__ mu)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int i = blockIdx.z + 1;
+    if (k > g.D || j > g.H) return;
+    const long long fs = g.fstride, c = g.idx(i, j, k);
+    const double DD = kc.DD;
+    const double M11 = DD * (4 * B[c] - Ahat[c]);
+    const double M12 = DD * (4 * B[fs + c] - Ahat[fs + c]);
+    const double M13 = DD * (4 * B[2 * fs + c] - Ahat[2 * fs + c]);
+    const double M22 = DD * (4 * B[3 * fs + c] - Ahat[3 * fs + c]);
+    const double M23 = DD * (4 * B[4 * fs + c] - Ahat[4 * fs + c]);
+    const double M33 = DD * (4 * B[5 * fs + c] - Ahat[5 * fs + c]);
+    double L11 = Lst[c], L12 = Lst[fs + c], L13 = Lst[2 * fs + c];
+    double L22 = Lst[3 * fs + c], L23 = Lst[4 * fs + c], L33 = Lst[5 * fs + c];
+    const double tr = -(1.0 / 3.0) * (L11 + L22 + L33);
+    L11 += tr; L22 += tr; L33 += tr;
+    const double LLMM = (L11 * M11 + L12 * M12 + L13 * M13 + L12 * M12 + L22 * M22 + L23 * M23 +
+                         L13 * M13 + L23 * M23 + L33 * M33);
+    const double MMMM = (M11 * M11 + M12 * M12 + M13 * M13 + M12 * M12 + M22 * M22 + M23 * M23 +
+                         M13 * M13 + M23 * M23 + M33 * M33);
+    double Cd = -0.5 * (LLMM / (MMMM + 1e-30));
+    if (Cd > 0.15) Cd = 0.15;
+    else if (Cd < 0.0) Cd = 0.0;
+    mu[c] = rho[c] * Cd * DD * Smag[c];
+}
+
+// ---------------------------------------------------------------------------
+// state transfer and diagnostics
+// ---------------------------------------------------------------------------
+__global__ void k_state_scatter(Grid g, double *__restrict__ dst, const double *__restrict__ packed)
+{
+    const long long n = (long long)g.L * g.H * 5 * g.D;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % g.D);
+        long long r = t / g.D;
+        const int v = (int)(r % 5); r /= 5;
+        const int j = (int)(r % g.H);
+        const int i = (int)(r / g.H);
+        dst[v * g.fstride + g.idx(i + 1, j + 1, k + 1)] = packed[t];
+    }
+}
+
+__global__ void k_state_gather(Grid g, const double *__restrict__ src, double *__restrict__ packed)
+{
+    const long long n = (long long)g.L * g.H * 5 * g.D;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % g.D);
+        long long r = t / g.D;
+        const int v = (int)(r % 5); r /= 5;
+        const int j = (int)(r % g.H);
+        const int i = (int)(r / g.H);
+        packed[t] = src[v * g.fstride + g.idx(i + 1, j + 1, k + 1)];
+    }
+}
+
+// Deterministic block partial sums of the five conserved variables.
+__global__ void k_sums_partial(Grid g, const double *__restrict__ U, double *__restrict__ partials)
+{
+    const long long n = (long long)g.L * g.H * g.D;
+    double s[5] = {0, 0, 0, 0, 0};
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % g.D) + 1;
+        const long long r = t / g.D;
+        const int j = (int)(r % g.H) + 1;
+        const int i = (int)(r / g.H) + 1;
+        const long long c = g.idx(i, j, k);
+#pragma unroll
+        for (int q = 0; q < 5; q++) s[q] += U[q * g.fstride + c];
+    }
+    __shared__ double sm[5][32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        double x = s[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (l == 0) sm[q][w] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double x = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) x += sm[threadIdx.x][q];
+        partials[blockIdx.x * 5 + threadIdx.x] = x;
+    }
+}
+
+__global__ void k_sums_final(const double *__restrict__ partials, int np, double vol, double *__restrict__ out)
+{
+    if (threadIdx.x < 5) {
+        double x = 0;
+        for (int b = 0; b < np; b++) x += partials[b * 5 + threadIdx.x];
+        out[threadIdx.x] = x * vol;
+    }
+}
+
+// One block per y row: sums over the x-z plane of rho, rho u, rho v, rho w,
+// rho uu, rho vv, rho ww, rho uv.
+__global__ void k_plane_sums(Grid g, const double *__restrict__ U, double *__restrict__ rows)
+{
+    const int j = blockIdx.x + 1;
+    const long long n = (long long)g.L * g.D;
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+        const int k = (int)(t % g.D) + 1;
+        const int i = (int)(t / g.D) + 1;
+        const long long c = g.idx(i, j, k);
+        const double r = U[c], u = U[g.fstride + c] / r, v = U[2 * g.fstride + c] / r,
+                     w = U[3 * g.fstride + c] / r;
+        s[0] += r; s[1] += r * u; s[2] += r * v; s[3] += r * w;
+        s[4] += r * u * u; s[5] += r * v * v; s[6] += r * w * w; s[7] += r * u * v;
+    }
+    __shared__ double sm[8][32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        double x = s[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (l == 0) sm[q][w] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double x = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) x += sm[threadIdx.x][q];
+        rows[(long long)blockIdx.x * 8 + threadIdx.x] = x;
+    }
+}
+
+inline dim3 cells_grid(const Grid &g, dim3 b, int ni, int nj, int nk)
+{
+    return dim3((nk + b.x - 1) / b.x, (nj + b.y - 1) / b.y, ni);
+}
+
+} // namespace
+
+// ---- launchers -------------------------------------------------------------
+
+void launch_ghost(Ctx &c, double *cur)
+{
+    const Grid &g = c.g;
+    const long long n = 2LL * (g.H + 2) * (g.D + 2) + 2LL * g.L * (g.D + 2) + 2LL * g.L * g.H;
+    k_ghost<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(g, c.k.setup, cur);
+}
+
+void launch_recon(Ctx &c, const double *cur)
+{
+    const Grid &g = c.g;
+    dim3 b(32, 4, 1);
+    k_recon<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, cur, c.f);
+}
+
+void launch_ifbc(Ctx &c, const Disturb &d)
+{
+    const Grid &g = c.g;
+    const long long n = (long long)g.H * g.D + (long long)g.L * g.D + (long long)g.L * g.H;
+    k_ifbc<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(g, c.k.setup, c.k.BL_HIG, d, c.f);
+}
+
+void launch_fluxes(Ctx &c, const double *cur)
+{
+    const Grid &g = c.g;
+    dim3 b(32, 4, 1);
+    k_flux<1><<<cells_grid(g, b, g.L + 1, g.H, g.D), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f);
+    k_flux<2><<<cells_grid(g, b, g.L, g.H + 1, g.D), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f);
+    k_flux<3><<<cells_grid(g, b, g.L, g.H, g.D + 1), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f);
+}
+
+void launch_evolution(Ctx &c, int nstages, int stage)
+{
+    const Grid &g = c.g;
+    int mode = stage >= 3 ? 3 : stage;
+    if (nstages == 2) mode = (stage == 1) ? 4 : 5;
+    dim3 b(32, 4, 1);
+    k_evolution<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, mode, c.ds, c.U, c.Up, c.f);
+}
+
+void launch_dynsmag(Ctx &c, const double *U)
+{
+    const Grid &g = c.g;
+    DynScratch &s = c.dyn;
+    const long long ncell = (long long)(g.L + 2) * g.pi;
+    k_dyn_vel<<<(unsigned)std::min<long long>((ncell + 255) / 256, 148LL * 16), 256, 0, c.stream>>>(g, U, s.vel);
+    dim3 b(32, 4, 1);
+    // velocity and product filters: y over i in [0,L] j in [1,H] k in [0,D]
+    k_filt_y_vel<<<cells_grid(g, b, g.L + 1, g.H, g.D + 1), b, 0, c.stream>>>(g, s.vel, s.t1);
+    k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, c.stream>>>(g, 9, s.t1, s.t2);
+    k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, c.stream>>>(g, 9, s.t2, s.t1);
+    k_dyn_mid<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, c.k, s.vel, s.t1, s.Lst, s.A, s.B, s.S);
+    // filter of A (pass-1 buffer reused; its zero bands are preserved)
+    k_filt_y<<<cells_grid(g, b, g.L + 1, g.H, g.D + 1), b, 0, c.stream>>>(g, 6, s.A, s.t1);
+    k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, c.stream>>>(g, 6, s.t1, s.t2);
+    k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, c.stream>>>(g, 6, s.t2, s.t1);
+    k_dyn_final<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, c.k, U, s.Lst, s.B, s.t1, s.S, c.mu);
+}
+
+void launch_courant(Ctx &c)
+{
+    const Grid &g = c.g;
+    k_courant_partial<<<c.npartials, 256, 0, c.stream>>>(g, c.k, c.U, c.ds, c.partials, c.ds);
+    k_courant_final<<<1, 1024, 0, c.stream>>>(c.k, c.partials, c.npartials, c.ds);
+}
+
+void launch_state_scatter(Ctx &c, double *dst, const double *packed)
+{
+    k_state_scatter<<<148 * 8, 256, 0, c.stream>>>(c.g, dst, packed);
+}
+
+void launch_state_gather(Ctx &c, const double *src, double *packed)
+{
+    k_state_gather<<<148 * 8, 256, 0, c.stream>>>(c.g, src, packed);
+}
+
+void launch_sums(Ctx &c, const double *U, double *out5)
+{
+    const int nb = 148 * 4;
+    k_sums_partial<<<nb, 256, 0, c.stream>>>(c.g, U, c.partials);
+    const double vol = c.p.deltaX * c.p.deltaY * c.p.deltaZ;
+    k_sums_final<<<1, 32, 0, c.stream>>>(c.partials, nb, vol, out5);
+}
+
+void launch_plane_sums(Ctx &c, const double *U, double *rows)
+{
+    k_plane_sums<<<c.g.H, 256, 0, c.stream>>>(c.g, U, rows);
+}
+
+} // namespace fsl

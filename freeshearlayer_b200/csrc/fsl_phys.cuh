@@ -1,0 +1,259 @@
+// fsl_phys.cuh -- device arithmetic of the explicit step, templated on the
+// compute type T (double for the plain method, float for the FP32 bulk).
+//
+// Every expression keeps the reference's evaluation order; translation units
+// that instantiate T = double are compiled with --fmad=false so that the plain
+// method rounds exactly like the reference's serial CPU code (IEEE division
+// and square root are the CUDA defaults for double).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace fsl {
+
+// gas and scheme constants, src/def.h:25-45
+template <typename T> struct Kc {
+    static constexpr T K = T(1.4);
+    static constexpr T K_1 = T(0.4);
+    static constexpr T NK_1 = T(-0.4);
+    static constexpr T K05 = T(0.7);
+    static constexpr T K_K_1 = T(3.5);
+    static constexpr T K_1_2 = T(0.2);
+    static constexpr T H_K_1 = T(1.25);
+    static constexpr T R_VOZD = T(287.10);
+    static constexpr T C1 = T(0.333333333333333);
+    static constexpr T C2 = T(0.166666666666667);
+    static constexpr T TWO_THIRDS = T(0.666666666666667);
+};
+
+// Chakravarthy-Osher minmod, compression 4 (src/reconstruction.c:17-24)
+template <typename T> __device__ __forceinline__ T minmod(T x, T y)
+{
+    T ay;
+    if (x * y <= T(0)) return T(0);
+    ay = ((y *= T(4.0)) > T(0)) ? y : -y;
+    if (x > T(0)) return (x < ay) ? x : ay;
+    return ((-x < ay) ? x : -ay);
+}
+
+// Per-cell quantities shared by the three sweeps (src/reconstruction.c:63-88,
+// :104, :142-145).
+template <typename T> struct CellC {
+    T u[5];
+    T U, V, W, C;
+    T aa, ll, ee, gg, hh, nn, S11;
+    T bb, cc, dd;
+    T u_hh, v_hh, w_hh, u_ee, v_ee, w_ee;
+};
+
+template <typename T> __device__ __forceinline__ void cell_consts(CellC<T> &c)
+{
+    typedef Kc<T> k;
+    T R = T(1.) / c.u[0];
+    c.U = c.u[1] * R;
+    c.V = c.u[2] * R;
+    c.W = c.u[3] * R;
+    T P = (c.u[4] - T(0.5) * (c.u[1] * c.u[1] + c.u[2] * c.u[2] + c.u[3] * c.u[3]) * R) * k::K_1;
+    c.C = sqrt(k::K * P * R);
+    T ff = c.U * c.U + c.V * c.V + c.W * c.W;
+    c.aa = k::K_1_2 * ff;
+    c.bb = k::NK_1 * c.U;
+    c.cc = k::NK_1 * c.V;
+    c.dd = k::NK_1 * c.W;
+    c.ll = T(1.) / (c.C + c.C);
+    c.ee = c.ll / c.C;
+    c.gg = -ff * c.ee;
+    c.hh = -(c.ee + c.ee);
+    c.S11 = c.aa - c.C * c.C;
+    c.u_hh = c.U * c.hh;
+    c.v_hh = c.V * c.hh;
+    c.w_hh = c.W * c.hh;
+    c.u_ee = c.U * c.ee;
+    c.v_ee = c.V * c.ee;
+    c.w_ee = c.W * c.ee;
+    c.nn = T(-0.5) * c.gg;
+}
+
+// One sweep of the characteristic reconstruction.  N = index of the normal
+// momentum in u[] (1..3); T1, T2 = tangential momenta in the reference's
+// permuted order (x: 2 3 4 -> 1 2 3; y: 3 4 2 -> 2 3 1; z: 4 2 3 -> 3 1 2).
+// fw/bw: forward/backward neighbour values in the order (rho, N, T1, T2, E).
+// hi: state on the face towards the forward neighbour, lo: towards the
+// backward neighbour, natural variable order.  t2_ee is the coefficient the
+// reference applies to the T2 momentum (the z sweep uses w_ee for rho v,
+// src/reconstruction.c:328,340).
+template <typename T, int N, int T1, int T2>
+__device__ __forceinline__ void recon_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2,
+                                            T n_hh, T t1_hh, T t2_hh, T n_ee, T t1_ee, T t2_ee,
+                                            const T *fw, const T *bw, T *hi, T *lo)
+{
+    typedef Kc<T> k;
+    const T *u = c.u;
+    const T C = c.C;
+    T m1, m2, m3, m4, m5, w1, w2, w3, w4, w5;
+    T M1, M2, M3, M4, M5, W1, W2, W3, W4, W5;
+    T _M1, _M2, _M3, _M4, _M5, _W1, _W2, _W3, _W4, _W5;
+    T S12, S41, S42, S51, S52, _S24, _S25, _S54, _S55;
+    T k1, k2, k3, k4, k5, kk, mm;
+    mm = vn * c.ll;
+    m1 = fw[0] - u[0]; m2 = fw[1] - u[N]; m3 = fw[2] - u[T1]; m4 = fw[3] - u[T2]; m5 = fw[4] - u[4];
+    w1 = u[0] - bw[0]; w2 = u[N] - bw[1]; w3 = u[T1] - bw[2]; w4 = u[T2] - bw[3]; w5 = u[4] - bw[4];
+    S41 = c.aa - (kk = C * vn);
+    S51 = c.aa + kk;
+    S12 = S42 = S52 = bn;
+    S42 += C;
+    S52 -= C;
+    kk = k::K_1 * m5; k2 = bt1 * m3; k3 = bt2 * m4;
+    M1 = c.S11 * m1 + S12 * m2 + k2 + k3 + kk;
+    M2 = -vt1 * m1 + m3;
+    M3 = -vt2 * m1 + m4;
+    M4 = S41 * m1 + S42 * m2 + k2 + k3 + kk;
+    M5 = S51 * m1 + S52 * m2 + k2 + k3 + kk;
+    kk = k::K_1 * w5; k2 = bt1 * w3; k3 = bt2 * w4;
+    W1 = c.S11 * w1 + S12 * w2 + k2 + k3 + kk;
+    W2 = -vt1 * w1 + w3;
+    W3 = -vt2 * w1 + w4;
+    W4 = S41 * w1 + S42 * w2 + k2 + k3 + kk;
+    W5 = S51 * w1 + S52 * w2 + k2 + k3 + kk;
+    _M1 = minmod(M1, W1); _M2 = minmod(M2, W2); _M3 = minmod(M3, W3);
+    _M4 = minmod(M4, W4); _M5 = minmod(M5, W5);
+    _W1 = minmod(W1, M1); _W2 = minmod(W2, M2); _W3 = minmod(W3, M3);
+    _W4 = minmod(W4, M4); _W5 = minmod(W5, M5);
+    _S24 = n_ee + c.ll; _S25 = n_ee - c.ll;
+    _S54 = _S55 = c.nn + k::H_K_1;
+    _S54 += mm; _S55 -= mm;
+    k1 = _M1 * k::C1 + _W1 * k::C2; k2 = _M2 * k::C1 + _W2 * k::C2; k3 = _M3 * k::C1 + _W3 * k::C2;
+    k4 = _M4 * k::C1 + _W4 * k::C2; k5 = _M5 * k::C1 + _W5 * k::C2;
+    kk = k4 + k5;
+    hi[0] = u[0] + c.hh * k1 + c.ee * kk;
+    hi[N] = u[N] + n_hh * k1 + _S24 * k4 + _S25 * k5;
+    hi[T1] = u[T1] + t1_hh * k1 + k2 + t1_ee * kk;
+    hi[T2] = u[T2] + t2_hh * k1 + k3 + t2_ee * kk;
+    hi[4] = u[4] + c.gg * k1 + vt1 * k2 + vt2 * k3 + _S54 * k4 + _S55 * k5;
+    k1 = _M1 * k::C2 + _W1 * k::C1; k2 = _M2 * k::C2 + _W2 * k::C1; k3 = _M3 * k::C2 + _W3 * k::C1;
+    k4 = _M4 * k::C2 + _W4 * k::C1; k5 = _M5 * k::C2 + _W5 * k::C1;
+    kk = k4 + k5;
+    lo[0] = u[0] - c.hh * k1 - c.ee * kk;
+    lo[N] = u[N] - n_hh * k1 - _S24 * k4 - _S25 * k5;
+    lo[T1] = u[T1] - t1_hh * k1 - k2 - t1_ee * kk;
+    lo[T2] = u[T2] - t2_hh * k1 - k3 - t2_ee * kk;
+    lo[4] = u[4] - c.gg * k1 - vt1 * k2 - vt2 * k3 - _S54 * k4 - _S55 * k5;
+}
+
+// x, y and z sweeps with the reference's permutations.
+template <typename T> __device__ __forceinline__ void recon_x(const CellC<T> &c, const T *fw, const T *bw, T *hi, T *lo)
+{
+    recon_sweep<T, 1, 2, 3>(c, c.U, c.V, c.W, c.bb, c.cc, c.dd, c.u_hh, c.v_hh, c.w_hh, c.u_ee, c.v_ee,
+                            c.w_ee, fw, bw, hi, lo);
+}
+template <typename T> __device__ __forceinline__ void recon_y(const CellC<T> &c, const T *fw, const T *bw, T *hi, T *lo)
+{
+    recon_sweep<T, 2, 3, 1>(c, c.V, c.W, c.U, c.cc, c.dd, c.bb, c.v_hh, c.w_hh, c.u_hh, c.v_ee, c.w_ee,
+                            c.u_ee, fw, bw, hi, lo);
+}
+template <typename T> __device__ __forceinline__ void recon_z(const CellC<T> &c, const T *fw, const T *bw, T *hi, T *lo)
+{
+    recon_sweep<T, 3, 1, 2>(c, c.W, c.U, c.V, c.dd, c.bb, c.cc, c.w_hh, c.u_hh, c.v_hh, c.w_ee, c.u_ee,
+                            c.w_ee, fw, bw, hi, lo);
+}
+
+// Linearised characteristic Riemann solve on one face (src/fluxes.c:61-113,
+// :230-282, :401-453).  N = normal direction 1..3.  Lm/Rp: minus/plus
+// conserved states.  Returns interface density, pressure and velocity (the
+// normal component from the solve, the tangential ones upwinded by its sign).
+template <typename T, int N>
+__device__ __forceinline__ void riemann(const T *Lm, const T *Rp, T &Rho, T &Pr, T *vel)
+{
+    typedef Kc<T> k;
+    T _R, _P, _C, _jo, _jp, _jm, RU, R_, P_, C_, jo_, jp_, jm_;
+    T lv[3], rv[3];
+    T Un, C, C_p, C_m, C_o, al_p, al_m, al_o, J_p, J_m, J_o, P;
+    _R = Lm[0];
+    lv[0] = Lm[1] / _R; lv[1] = Lm[2] / _R; lv[2] = Lm[3] / _R;
+    _P = (Lm[4] - T(0.5) * _R * (lv[0] * lv[0] + lv[1] * lv[1] + lv[2] * lv[2])) * k::K_1;
+    _C = sqrt(k::K * _P / _R);
+    _jo = k::NK_1 * _P;
+    _jp = lv[N - 1] + (RU = _P / (_R * _C));
+    _jm = lv[N - 1] - RU;
+    R_ = Rp[0];
+    rv[0] = Rp[1] / R_; rv[1] = Rp[2] / R_; rv[2] = Rp[3] / R_;
+    P_ = (Rp[4] - T(0.5) * R_ * (rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2])) * k::K_1;
+    C_ = sqrt(k::K * P_ / R_);
+    jo_ = k::NK_1 * P_;
+    jp_ = rv[N - 1] + (RU = P_ / (R_ * C_));
+    jm_ = rv[N - 1] - RU;
+    Un = T(0.5) * (lv[N - 1] + rv[N - 1]);
+    C = T(0.5) * (_C + C_);
+    C_p = Un + C; C_m = Un - C; C_o = Un;
+    if (C_p > T(0.)) { al_p = k::K_1_2 * (_jm - _jp) / _jo; J_p = _jp; }
+    else { al_p = k::K_1_2 * (jm_ - jp_) / jo_; J_p = jp_; }
+    if (C_m > T(0.)) { al_m = k::K_1_2 * (_jp - _jm) / _jo; J_m = _jm; }
+    else { al_m = k::K_1_2 * (jp_ - jm_) / jo_; J_m = jm_; }
+    if (C_o > T(0.)) { al_o = k::K05 * (_jp - _jm); al_o = -al_o * al_o; J_o = _jo; }
+    else { al_o = k::K05 * (jp_ - jm_); al_o = -al_o * al_o; J_o = jo_; }
+    P = (J_p - J_m) / (al_p - al_m);
+    Un = J_p - al_p * P;
+    Rho = (J_o - P) / al_o;
+    Pr = P;
+    if (Un > T(0)) { vel[0] = lv[0]; vel[1] = lv[1]; vel[2] = lv[2]; }
+    else { vel[0] = rv[0]; vel[1] = rv[1]; vel[2] = rv[2]; }
+    vel[N - 1] = Un;
+}
+
+// Velocities by reciprocal, RU = 1./rho (src/fluxes.c:124-142).
+template <typename T> __device__ __forceinline__ void vel_rcp(T r, T mu_, T mv, T mw, T *o)
+{
+    T RU = T(1.) / r;
+    o[0] = mu_ * RU; o[1] = mv * RU; o[2] = mw * RU;
+}
+
+// Velocities and temperature by division (src/fluxes.c:117-122).
+template <typename T> __device__ __forceinline__ void vel_div(T R_, T mu_, T mv, T mw, T E, T *o, T &Tt)
+{
+    typedef Kc<T> k;
+    T U_ = mu_ / R_, V_ = mv / R_, W_ = mw / R_;
+    T P_ = (E - T(0.5) * R_ * (U_ * U_ + V_ * V_ + W_ * W_)) * k::K_1;
+    Tt = P_ / (k::R_VOZD * R_);
+    o[0] = U_; o[1] = V_; o[2] = W_;
+}
+
+// Flux assembly of one face from the Riemann state, the face velocity
+// gradient and the cell-centre velocities of the two adjacent cells
+// (src/fluxes.c:185-220, :353-391, :524-568).  N = normal direction.
+// g[a][b] = d u_a / d x_b.  fw/bw: velocities of the plus/minus cell.
+template <typename T, int N>
+__device__ __forceinline__ void face_flux(T Rho, T P, const T *vel, const T (*g)[3], const T *fw, const T *bw,
+                                          T Tp, T Tm, T mu_L, T mu_T, T lambda_L, T cp_Pr_T, T rdn, T *F)
+{
+    typedef Kc<T> k;
+    T uu = T(0.5) * (fw[0] + bw[0]), vv = T(0.5) * (fw[1] + bw[1]), ww = T(0.5) * (fw[2] + bw[2]);
+    T mu_E = mu_L + mu_T;
+    T s0, s1, s2; // sigma_N{x,y,z}
+    if (N == 1) {
+        s0 = k::TWO_THIRDS * mu_E * (g[0][0] + g[0][0] - g[1][1] - g[2][2]);
+        s1 = mu_E * (g[0][1] + g[1][0]);
+        s2 = mu_E * (g[0][2] + g[2][0]);
+    } else if (N == 2) {
+        s0 = mu_E * (g[1][0] + g[0][1]);
+        s1 = k::TWO_THIRDS * mu_E * (g[1][1] + g[1][1] - g[0][0] - g[2][2]);
+        s2 = mu_E * (g[1][2] + g[2][1]);
+    } else {
+        s0 = mu_E * (g[2][0] + g[0][2]);
+        s1 = mu_E * (g[2][1] + g[1][2]);
+        s2 = k::TWO_THIRDS * mu_E * (g[2][2] + g[2][2] - g[0][0] - g[1][1]);
+    }
+    T lambda_E = lambda_L + mu_T * cp_Pr_T;
+    T q = -lambda_E * (Tp - Tm) * rdn;
+    T RU = Rho * vel[N - 1];
+    F[0] = RU;
+    F[1] = RU * vel[0] - s0;
+    F[2] = RU * vel[1] - s1;
+    F[3] = RU * vel[2] - s2;
+    if (N == 1) F[1] = RU * vel[0] + P - s0;
+    if (N == 2) F[2] = RU * vel[1] + P - s1;
+    if (N == 3) F[3] = RU * vel[2] + P - s2;
+    F[4] = vel[N - 1] * (k::K_K_1 * P + T(0.5) * Rho * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2])) -
+           uu * s0 - vv * s1 - ww * s2 + q;
+}
+
+} // namespace fsl

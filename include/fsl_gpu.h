@@ -1,0 +1,213 @@
+/*
+ * fsl_gpu.h -- C ABI of the B200 (sm_100a) explicit time step of the
+ * freeShearLayer compressible LES solver.
+ *
+ * The reference's "operator API" for this path is the set of global void
+ * functions its ANSI-C driver calls once per stage (src/layer2.c:141-185),
+ * all communicating through globals (src/global.h:6-72).  This header gives
+ * the same entry points with explicit state: one fsl_ctx owns one
+ * device-resident domain (the five conserved variables, the stage buffer, the
+ * SGS viscosity and the boundary data) on the current CUDA device, and every
+ * call works on that context's single CUDA stream.
+ *
+ * Conventions (all entry points):
+ *   - return FSL_OK (0) on success or a negative FSL_ERR_* code; no call
+ *     exits the process (the reference calls exit(-1), src/helpers.c:63-76);
+ *   - calls on one context are not thread-safe; contexts are independent;
+ *   - the product has no CPU fallback: without a usable sm_100 device
+ *     fsl_init returns FSL_ERR_NODEVICE;
+ *   - host arrays are plain C arrays of double; no pointer is retained.
+ *
+ * Layouts:
+ *   state   : the interior in the reference's backup.dat row layout
+ *             (src/finalize.c:22-29): for i in 1..LEN, for j in 1..HIG:
+ *             DEP values of rho, then rho u, rho v, rho w, E.
+ *   padded  : (LEN+2)(HIG+2)(DEP+2) doubles, k fastest -- the reference's
+ *             Array3D(LEN+2,HIG+2,DEP+2) (src/helpers.c:58-80) flattened.
+ *   faces   : dense over the reference's face index ranges,
+ *             x (LEN+1)*HIG*DEP, y LEN*(HIG+1)*DEP, z LEN*HIG*(DEP+1).
+ */
+#ifndef FSL_GPU_H
+#define FSL_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FSL_ABI_VERSION 1
+
+/* return codes */
+#define FSL_OK 0
+#define FSL_ERR_ARG (-1)         /* invalid argument or parameter set */
+#define FSL_ERR_NOMEM (-2)       /* device or host allocation failed */
+#define FSL_ERR_CUDA (-3)        /* a CUDA runtime call failed */
+#define FSL_ERR_NONFINITE (-4)   /* non-finite state, non-positive density or Courant max */
+#define FSL_ERR_TIMEOUT (-5)     /* a bounded device wait gave up */
+#define FSL_ERR_IO (-6)          /* file could not be opened or parsed */
+#define FSL_ERR_UNSUPPORTED (-7) /* option combination not available */
+#define FSL_ERR_NODEVICE (-8)    /* no usable sm_100 CUDA device */
+
+/* boundary setups */
+#define FSL_SETUP_SPATIAL 0  /* the reference's BCs: step inflow / outflow in x, slip y, periodic z */
+#define FSL_SETUP_TEMPORAL 1 /* temporal shear layer: periodic x and z, zero-gradient y */
+
+/* Courant-number definitions */
+#define FSL_CFL_STREAMWISE 0 /* max of u dt/dx (src/helpers.c:31-43) */
+#define FSL_CFL_ACOUSTIC 1   /* max of dt((|u|+c)/dx + (|v|+c)/dy + (|w|+c)/dz) */
+
+/* arithmetic of the stage update */
+#define FSL_PREC_FP64 0 /* plain method: FP64 throughout, reference evaluation order */
+#define FSL_PREC_FP32 1 /* FP32 bulk, FP64 U^n, RK combination, dt reduction and sums */
+
+/* subgrid closure */
+#define FSL_SGS_DYNAMIC 0 /* dynamic Smagorinsky (Germano-Lilly), src/turbulence.c:103-507 */
+#define FSL_SGS_LEARNED 1 /* per-cell MLP Cs^2 with the dynamic procedure as judge */
+
+/* reconstruction */
+#define FSL_RECON_CHARMINMOD 0 /* characteristic kappa=1/3 minmod(beta=4), src/reconstruction.c:26-345 */
+#define FSL_RECON_PPM 1        /* Colella-Woodward PPM on characteristic variables */
+
+/* Parameters: the 22 positional values of layer2.ini in file order
+ * (src/initialize.c:25-58; src-par's mpi_layer2.bin holds the same 22 values
+ * as float32), followed by the options that have no counterpart in the ini. */
+typedef struct fsl_params {
+    int LEN, HIG, DEP;
+    double deltaX, deltaY, deltaZ, deltaT;
+    int Answer, numstep;
+    double mu_L, Pr_L, Pr_T, Cs;
+    int BL_HIG;
+    double Ua, Va, Wa;
+    int Ns_min, Nst, f_step, nStages;
+    double maxCoNum;
+    /* options */
+    int setup;       /* FSL_SETUP_* */
+    int cfl_mode;    /* FSL_CFL_* */
+    double seed_X;   /* disturbance RNG seed; the reference reads it from stdin (src/layer2.c:130) */
+    int precision;   /* FSL_PREC_* */
+    int sgs;         /* FSL_SGS_* */
+    int recon;       /* FSL_RECON_* */
+    int reserved[8];
+} fsl_params;
+
+typedef struct fsl_ctx fsl_ctx;
+
+/* Scalars of the driver state, read with fsl_get_info. */
+typedef struct fsl_info {
+    double deltaT, deltaT_X, deltaT_Y, deltaT_Z; /* current time step and ratios */
+    double maxCo;                                /* last Courant maximum */
+    double X;                                    /* disturbance RNG state */
+    double Ud, Vd, Wd;                           /* current disturbance velocities */
+    unsigned k_min, k_max;                       /* current disturbance span */
+    unsigned step;                               /* completed steps */
+    int counter;                                 /* disturbance block countdown */
+    int cur;                                     /* 0: U*_ = U, 1: U*_ = stage buffer */
+    double DD, lambda_L, cp_Pr_T;                /* derived constants */
+    unsigned long long device_bytes;             /* device memory held by the context */
+} fsl_info;
+
+/* ---- parameters ------------------------------------------------------- */
+
+/* The reference's shipped layer2.ini physics with nStages = 3, FP64,
+ * dynamic Smagorinsky, spatial setup, streamwise CFL. */
+int fsl_params_default(fsl_params *p);
+/* Parse layer2.ini: 22 positional lines read with atoi/atof, trailing text
+ * ignored (replaces Initialize(), src/initialize.c:17-58).  Only the 22 ini
+ * values of *p are written; its option fields are left as the caller set
+ * them (initialise *p with fsl_params_default first). */
+int fsl_params_from_ini(const char *path, fsl_params *p);
+/* Parse mpi_layer2.bin: 22 float32 values in ini order
+ * (src-par/initialize.c:35-81, written by src-par/ini2bin/ini2bin.c:63-64).
+ * Option fields are left as for fsl_params_from_ini. */
+int fsl_params_from_bin(const char *path, fsl_params *p);
+/* Check a parameter set; FSL_OK or FSL_ERR_ARG. */
+int fsl_params_check(const fsl_params *p);
+
+/* ---- initial states (host arrays in the state layout) ----------------- */
+
+/* The reference's fresh-start state, src/initialize.c:159-187. */
+int fsl_initial_state(const fsl_params *p, double *state);
+/* Temporal shear layer: u = dU/2 tanh(2y/delta_w0) about the domain centre,
+ * p = 1e5 Pa, free-stream density 1 kg/m^3, Crocco-Busemann temperature,
+ * dU = 2 Mc c_inf, uniform velocity perturbations of amplitude amp*dU from
+ * splitmix64(seed).  *dU receives the velocity difference. */
+int fsl_temporal_state(const fsl_params *p, double Mc, double delta_w0, double amp,
+                       unsigned long long seed, double *state, double *dU);
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Allocate a domain on the current CUDA device.  Replaces the allocation
+ * part of Initialize() (src/initialize.c:97-125). */
+int fsl_init(const fsl_params *p, fsl_ctx **ctx);
+int fsl_destroy(fsl_ctx *ctx);
+/* Message of the last error on this context (static storage, never NULL). */
+const char *fsl_last_error(const fsl_ctx *ctx);
+int fsl_get_info(fsl_ctx *ctx, fsl_info *info);
+/* Block until the context's stream is idle. */
+int fsl_sync(fsl_ctx *ctx);
+
+/* Upload/download U^n (backup.dat layout; src/initialize.c:134-148 reads,
+ * src/finalize.c:22-29 writes). */
+int fsl_upload_state(fsl_ctx *ctx, const double *state);
+int fsl_download_state(fsl_ctx *ctx, double *state);
+/* Set step counter and time step as a restart would (src/initialize.c:149-152). */
+int fsl_set_time(fsl_ctx *ctx, unsigned step, double deltaT);
+
+/* ---- the driver's per-step scalar work ---------------------------------- */
+
+/* checkCoNum(), src/helpers.c:23-52: reduce the Courant maximum over U^n on
+ * the device, rescale deltaT to maxCoNum.  maxCo and dt may be NULL.
+ * Returns FSL_ERR_NONFINITE when the maximum is not positive and finite. */
+int fsl_check_courant(fsl_ctx *ctx, double *maxCo, double *dt);
+/* The driver's disturbance-block draw, src/layer2.c:152-162 (host RNG,
+ * src/helpers.c:13-17). */
+int fsl_draw_disturbance(fsl_ctx *ctx);
+/* Set the disturbance block directly (k span and velocities). */
+int fsl_set_disturbance(fsl_ctx *ctx, unsigned k_min, unsigned k_max, double Ud, double Vd,
+                        double Wd);
+
+/* ---- per-phase entry points (reference names) ---------------------------
+ * Each works on the current-stage buffer U*_ exactly like the reference
+ * phase; they are the unfused path used for per-phase parity.  fsl_fluxes
+ * does not recompute the SGS viscosity (the reference's Fluxes() calls
+ * DynamicSmagorinsky first, src/fluxes.c:52-54); call
+ * fsl_dynamic_smagorinsky first to reproduce Fluxes() exactly. */
+int fsl_ghost_bc(fsl_ctx *ctx);            /* BounCondInGhostCells, src/boundCondInGhostCells.c:10 */
+int fsl_reconstruct(fsl_ctx *ctx);         /* Reconstruction, src/reconstruction.c:26 */
+int fsl_interface_bc(fsl_ctx *ctx);        /* BounCondOnInterfaces, src/bounCondOnInterfaces.c:11 */
+int fsl_dynamic_smagorinsky(fsl_ctx *ctx); /* DynamicSmagorinsky(U1..U4,mu_SGS), src/turbulence.c:103 */
+int fsl_fluxes(fsl_ctx *ctx);              /* Fluxes face loops, src/fluxes.c:57-571 */
+int fsl_evolution(fsl_ctx *ctx, int stage); /* Evolution(nStages, Stage), src/evolution.c:15 */
+
+/* ---- whole steps ---------------------------------------------------------
+ * nsteps iterations of the driver loop body without I/O (src/layer2.c:147-178):
+ * Courant check and dt rescale, disturbance draw, nStages stages.  Uses the
+ * fused stage kernels; the SGS viscosity is evaluated once per step (it
+ * depends only on U^n, src/fluxes.c:53, so this equals the reference's
+ * per-stage evaluation).  Asynchronous: returns after queuing the work. */
+int fsl_step(fsl_ctx *ctx, int nsteps);
+/* Same work through the per-phase entry points (reference phase order). */
+int fsl_step_phased(fsl_ctx *ctx, int nsteps);
+
+/* ---- debug / parity access ----------------------------------------------- */
+
+/* which: 0 = U^n, 1 = stage buffer, 2 = current-stage buffer, 3 = mu_SGS. */
+int fsl_get_cells(fsl_ctx *ctx, int which, int var, double *padded);
+int fsl_set_cells(fsl_ctx *ctx, int which, int var, const double *padded);
+/* dir 0/1/2; side 0 = minus-side state (flux after fsl_fluxes), 1 = plus-side. */
+int fsl_get_faces(fsl_ctx *ctx, int dir, int side, int var, double *faces);
+int fsl_set_faces(fsl_ctx *ctx, int dir, int side, int var, const double *faces);
+/* Point U*_ at U^n (0) or at the stage buffer (1). */
+int fsl_set_cur(fsl_ctx *ctx, int which);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+
+/* Volume integrals of rho, rho u, rho v, rho w, E over the interior (FP64). */
+int fsl_sums(fsl_ctx *ctx, double sums[5]);
+/* Per y-row sums over the interior x-z plane of rho, rho u, rho v, rho w,
+ * rho uu, rho vv, rho ww, rho uv (rows[8*HIG], FP64). */
+int fsl_plane_sums(fsl_ctx *ctx, double *rows);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FSL_GPU_H */

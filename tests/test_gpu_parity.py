@@ -1,0 +1,176 @@
+"""GPU parity: every phase of the CUDA path against the CPU oracle, through
+the C ABI.  The plain method (FP64) must be bit-identical to the oracle, which
+itself is bit-identical to the reference's serial code (test_oracle_vs_ref)."""
+import numpy as np
+import pytest
+
+from tests.helpers import max_ulp, per_var_rel_l2, random_state, spatial_params, temporal_params
+
+pytestmark = pytest.mark.gpu
+
+PARITY_RTOL = 1e-10  # relative L2 per conserved variable after N steps (plain FP64)
+
+
+@pytest.fixture(scope="module")
+def fsl():
+    import freeshearlayer_b200 as fsl
+    return fsl
+
+
+def _pair(fsl, oracle_lib, p, state):
+    o = oracle_lib.Oracle(p)
+    o.set_state(state)
+    d = fsl.Domain(p)
+    d.upload_state(state)
+    return o, d
+
+
+def _assert_same(a, b, what):
+    assert a.shape == b.shape, what
+    if not np.array_equal(a, b, equal_nan=True):
+        raise AssertionError("%s differs: max |d| = %g, max ulp = %d" %
+                             (what, np.nanmax(np.abs(a - b)), max_ulp(a, b)))
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_upload_download_roundtrip(fsl, oracle_lib, setup):
+    p = spatial_params() if setup == 0 else temporal_params()
+    s = random_state(p, 3)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    _assert_same(d.download_state(), s, "state")
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_phase_ghost(fsl, oracle_lib, setup):
+    p = spatial_params() if setup == 0 else temporal_params()
+    s = random_state(p, 4)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.ghost(); d.ghost_bc()
+    for v in range(5):
+        _assert_same(d.cells(0, v), o.cells(0, v), "U%d after ghost fill" % (v + 1))
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_phase_reconstruct_and_interface(fsl, oracle_lib, setup):
+    p = spatial_params() if setup == 0 else temporal_params()
+    s = random_state(p, 5)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.set_disturbance(1, 4, 12.5, -3.25, 7.0)
+    d.set_disturbance(1, 4, 12.5, -3.25, 7.0)
+    o.ghost(); d.ghost_bc()
+    o.recon(); d.reconstruct()
+    o.ifbc(); d.interface_bc()
+    for dd in range(3):
+        for side in range(2):
+            for v in range(5):
+                _assert_same(d.faces(dd, side, v), o.faces(dd, side, v),
+                             "face dir %d side %d var %d" % (dd, side, v))
+
+
+def test_phase_interface_wrapped_block(fsl, oracle_lib):
+    """Disturbance span with k_max <= k_min wraps around (src/bounCondOnInterfaces.c:134-138)."""
+    p = spatial_params(D=8)
+    s = random_state(p, 6)
+    for kmin, kmax in [(5, 2), (3, 3), (0, 8)]:
+        o, d = _pair(fsl, oracle_lib, p, s)
+        o.set_disturbance(kmin, kmax, 20.0, 5.0, -5.0)
+        d.set_disturbance(kmin, kmax, 20.0, 5.0, -5.0)
+        o.ghost(); d.ghost_bc(); o.recon(); d.reconstruct(); o.ifbc(); d.interface_bc()
+        for v in range(5):
+            _assert_same(d.faces(0, 0, v), o.faces(0, 0, v), "inflow face var %d" % v)
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_phase_dynamic_smagorinsky(fsl, oracle_lib, setup):
+    p = spatial_params() if setup == 0 else temporal_params()
+    s = random_state(p, 7)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.ghost(); d.ghost_bc()
+    o.dynsmag(); d.dynamic_smagorinsky()
+    mu_o, mu_d = o.cells(3), d.cells(3)
+    assert np.count_nonzero(mu_o) > 0
+    _assert_same(mu_d, mu_o, "mu_SGS")
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_phase_fluxes_and_evolution(fsl, oracle_lib, setup):
+    p = spatial_params() if setup == 0 else temporal_params()
+    s = random_state(p, 8)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.set_disturbance(0, 3, 10.0, 2.0, -1.0)
+    d.set_disturbance(0, 3, 10.0, 2.0, -1.0)
+    for stage in (1, 2, 3):
+        o.ghost(); d.ghost_bc()
+        o.recon(); d.reconstruct()
+        o.ifbc(); d.interface_bc()
+        if stage == 1:
+            o.dynsmag(); d.dynamic_smagorinsky()
+        o.fluxes_only(); d.fluxes()
+        for dd in range(3):
+            for v in range(5):
+                _assert_same(d.faces(dd, 0, v), o.faces(dd, 0, v), "flux dir %d var %d stage %d" % (dd, v, stage))
+        o.evolution(3, stage); d.evolution(stage)
+        for v in range(5):
+            _assert_same(d.cells(0, v), o.cells(0, v), "U%d after stage %d" % (v + 1, stage))
+            _assert_same(d.cells(1, v), o.cells(1, v), "Up%d after stage %d" % (v + 1, stage))
+
+
+@pytest.mark.parametrize("setup,cfl", [(0, 0), (1, 1)])
+def test_check_courant(fsl, oracle_lib, setup, cfl):
+    p = spatial_params(cfl_mode=cfl) if setup == 0 else temporal_params()
+    s = random_state(p, 9)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    mo = o.check_courant()
+    md, dt = d.check_courant()
+    assert md == mo
+    assert dt == o.scalars()[0]
+
+
+@pytest.mark.parametrize("nst", [3, 2])
+def test_steps_phased_spatial(fsl, oracle_lib, nst):
+    """Whole steps of the reference spatial case (disturbance RNG included);
+    nStages = 2 runs the reference's RK2-then-RK3 chain (src/evolution.c:19-23)."""
+    p = spatial_params(L=16, H=8, D=8, nStages=nst)
+    from oracle.oracle import spatial_initial_state
+    s = spatial_initial_state(p)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.step(6); d.step_phased(6)
+    _assert_same(d.download_state(), o.state(), "state after 6 steps")
+    info = d.info()
+    sc = o.scalars()
+    assert info.deltaT == sc[0] and info.X == sc[4] and info.step == 6
+
+
+def test_steps_phased_temporal(fsl, oracle_lib):
+    p = temporal_params(L=16, H=8, D=8)
+    s, _ = oracle_lib.Oracle.temporal_state(p, 0.4)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.step(5); d.step_phased(5)
+    _assert_same(d.download_state(), o.state(), "state after 5 steps")
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_steps_fused(fsl, oracle_lib, setup):
+    """fsl_step (the fused path) against the oracle, several steps."""
+    if setup == 0:
+        p = spatial_params(L=20, H=10, D=12)
+        from oracle.oracle import spatial_initial_state
+        s = spatial_initial_state(p)
+    else:
+        p = temporal_params(L=24, H=12, D=16)
+        s, _ = oracle_lib.Oracle.temporal_state(p, 0.4)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.step(8); d.step(8)
+    a, b = d.download_state(), o.state()
+    errs = per_var_rel_l2(a, b, p)
+    assert max(errs) <= PARITY_RTOL, errs
+    _assert_same(a, b, "state after 8 fused steps")
+
+
+def test_sums_and_plane_sums(fsl, oracle_lib):
+    p = temporal_params(L=16, H=8, D=8)
+    s, _ = oracle_lib.Oracle.temporal_state(p, 0.4)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    np.testing.assert_allclose(d.sums(), o.sums(), rtol=1e-13)
+    np.testing.assert_allclose(d.plane_sums(), o.plane_sums(), rtol=1e-12)
