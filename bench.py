@@ -1,0 +1,422 @@
+#!/usr/bin/env python3
+"""Benchmark: cell-stage-updates/s of the explicit RK3 step on B200.
+
+Workload (default): temporal compressible shear layer, 512 x 256 x 256 cells
+(33.5 M cells, 5 conserved variables), box 2pi x pi x pi, convective Mach
+0.7, Re_dw0 = 1000, acoustic CFL 0.5, RK3, dynamic Smagorinsky.  Synthetic
+data: the seeded tanh profile + Crocco-Busemann temperature + uniform
+velocity noise of amplitude 1e-3 dU (splitmix64 seed 20251203).
+
+One step = one full RK3 step (Courant rescale, disturbance draw, three stages,
+SGS viscosity once per step).  value = cells * 3 * steps / device seconds,
+max over ranks, summed over replicas (one independent domain per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W]
+    python bench.py --impl reference ...   # the reference's serial CPU solver
+
+Prints exactly one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "cell-stage-updates/s on 1 B200: FP32+learned closure vs plain FP64, matched error"
+UNIT = "cell-stage-updates/s"
+GRID = (512, 256, 256)
+MC, RE, DW0, AMP, SEED = 0.7, 1000.0, 1.0, 1e-3, 20251203
+STAGES = 3
+
+
+def workload_params(grid=GRID, precision=0, sgs=0, recon=0):
+    L, H, D = grid
+    dx = 2 * math.pi / L
+    dU = 2.0 * MC * math.sqrt(1.4 * 1e5 / 1.0)
+    return dict(LEN=L, HIG=H, DEP=D, deltaX=dx, deltaY=math.pi / H, deltaZ=math.pi / D,
+                deltaT=1e-5, Answer=0, numstep=0, mu_L=1.0 * dU * DW0 / RE, Pr_L=0.72,
+                Pr_T=0.8, Cs=0.01, BL_HIG=0, Ua=0.0, Va=0.0, Wa=0.0, Ns_min=10, Nst=50,
+                f_step=50, nStages=3, maxCoNum=0.5, setup=1, cfl_mode=1,
+                seed_X=0.317391239817, precision=precision, sgs=sgs, recon=recon)
+
+
+def workload_name(grid):
+    return ("temporal shear layer %dx%dx%d, Mc %.1f, Re_dw0 %.0f, RK3, acoustic CFL 0.5"
+            % (grid[0], grid[1], grid[2], MC, RE))
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference's own serial solver (oracle/_ref), one process per core
+# ---------------------------------------------------------------------------
+REF_SLAB = (4, 256, 256)  # per-process slab of the workload's cross-section
+
+
+def _ref_worker_main(nsteps: int, nwarm: int, slab, out_path: str):
+    """Runs in its own process: the reference's serial solver (FP64,
+    zero-fill patch) on one slab, timing each step; writes JSON to out_path."""
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)  # the reference prints every step
+    from oracle.oracle import RefOracle, spatial_initial_state
+    L, H, D = slab
+    p = dict(LEN=L, HIG=H, DEP=D, deltaX=1.6666667, deltaY=1.0, deltaZ=1.5, deltaT=0.0007,
+             Answer=0, numstep=nsteps + nwarm, mu_L=0.253358, Pr_L=0.72, Pr_T=0.8, Cs=0.01,
+             BL_HIG=5, Ua=35.0, Va=35.0, Wa=35.0, Ns_min=10, Nst=50, f_step=50, nStages=3,
+             maxCoNum=0.1, setup=0, cfl_mode=0, seed_X=0.317391239817)
+    r = RefOracle(p)
+    r.set_state(spatial_initial_state(p))
+    for _ in range(nwarm):
+        r.step(1)
+    times = []
+    for _ in range(nsteps):
+        t0 = time.perf_counter()
+        r.step(1)
+        times.append(time.perf_counter() - t0)
+    with open(out_path, "w") as f:
+        json.dump({"times": times, "cells": L * H * D}, f)
+
+
+def run_reference_cpu(nproc: int, nsteps: int, nwarm: int, slab=REF_SLAB):
+    """nproc concurrent reference processes; returns (value, seconds, detail)."""
+    import tempfile
+    from oracle import oracle as orc
+    if not orc.ref_available():
+        orc.build(ref=True)
+    if not orc.ref_available():
+        return None
+    tmp = tempfile.mkdtemp(prefix="fslref_")
+    procs = []
+    for q in range(nproc):
+        out = os.path.join(tmp, "w%d.json" % q)
+        cmd = [sys.executable, os.path.abspath(__file__), "--ref-worker", str(nsteps), str(nwarm),
+               "%d,%d,%d" % slab, out]
+        procs.append((subprocess.Popen(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE), out))
+    res = []
+    for pr, out in procs:
+        _, err = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError("reference worker failed: %s" % err.decode()[-500:])
+        with open(out) as f:
+            res.append(json.load(f))
+    wall = max(sum(r["times"]) for r in res)
+    units = sum(r["cells"] * STAGES * len(r["times"]) for r in res)
+    per_step = [max(r["times"][s] for r in res) for s in range(nsteps)]
+    return units / wall, wall, per_step
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_id: str):
+        self.dev = dev_id
+        self.lines = []
+        self.p = None
+
+    def start(self):
+        try:
+            cmd = ["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.dev:
+                cmd += ["-i", self.dev]
+            self.p = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# ---------------------------------------------------------------------------
+# the GPU arm
+# ---------------------------------------------------------------------------
+def main_gpu(args):
+    import numpy as np
+    import torch
+    import freeshearlayer_b200 as fsl
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    grid = tuple(int(x) for x in args.grid.split("x"))
+    p = workload_params(grid, precision=args.precision, sgs=0)
+    ncell = grid[0] * grid[1] * grid[2]
+    d = fsl.Domain(p)
+    if args.rows:
+        d.tune(d.TUNE_STAGE_ROWS, args.rows)
+    if args.seg:
+        d.tune(d.TUNE_STAGE_SEG, args.seg)
+    state, dU = fsl.temporal_state(d.p, MC, DW0, AMP, SEED + rank)
+    d.upload_state(state)
+    ext = torch.cuda.ExternalStream(d.stream)
+    run = d.step_phased if args.phased else d.step
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        run(1)
+    d.sync()
+
+    dev_uuid = ""
+    try:
+        dev_uuid = str(torch.cuda.get_device_properties(local).uuid)
+        if dev_uuid and not dev_uuid.startswith("GPU-"):
+            dev_uuid = "GPU-" + dev_uuid
+    except Exception:
+        dev_uuid = str(local)
+    clocks = Clocks(dev_uuid)
+
+    # ---- timed region: K steps, state resident in HBM ----
+    d.profile(True)
+    barrier()
+    torch.cuda.synchronize()
+    d.sync()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    run(args.steps)
+    e1.record(ext)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    kt = d.profile_read()
+    d.profile(False)
+    d.sync()  # raises on a non-finite state
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    units = ncell * STAGES * args.steps * world
+    value = units / (ms / 1e3)
+    ms_per_step = ms / args.steps
+
+    # ---- dominant kernel and its roofline ----
+    names = fsl.K_CLASSES
+    kms = {names[i]: kt.ms[i] for i in range(8)}
+    kl = {names[i]: int(kt.launches[i]) for i in range(8)}
+    top = max(kms, key=lambda k: kms[k])
+    peaks = measured_peaks()
+    # algorithmic bytes per cell-stage of the plain FP64 step (each array read
+    # or written once): stage 1 88 B, stages 2-3 128 B, SGS 40 B -> 384 B / 3
+    alg_per_cell_stage = {0: 128.0, 1: 96.0}[args.precision]
+    if top == "stage":
+        launches = max(kl["stage"], 1)
+        alg_bytes = alg_per_cell_stage * ncell
+        avg_ms = kms["stage"] / launches
+    else:
+        # per-phase path: the whole step's algorithmic bytes over its device time
+        launches = args.steps
+        alg_bytes = alg_per_cell_stage * ncell * STAGES
+        avg_ms = sum(kms.values()) / args.steps
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": top if top == "stage" else "whole step (per-phase kernels)",
+            "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": round(achieved / peaks["hbm_gbs"], 4),
+            "traffic": args.traffic, "peak_source": peaks["source"] + " HBM copy bandwidth",
+            "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": round(avg_ms, 4)}
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    host_in = torch.empty(state.size, dtype=torch.float64, pin_memory=True)
+    host_out = torch.empty(state.size, dtype=torch.float64, pin_memory=True)
+    hin = host_in.numpy()
+    hout = host_out.numpy()
+    hin[:] = d.download_state()
+    ne = max(1, min(args.steps, args.e2e_steps))
+    barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(ext)
+    for _ in range(ne):
+        d.upload_state(hin)
+        run(1)
+        hout[:] = 0.0
+        d.download_state(hout)
+    f1.record(ext)
+    f1.synchronize()
+    barrier()
+    e2e_ms = f0.elapsed_time(f1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": ncell * STAGES * ne * world / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(state.nbytes), "d2h_bytes_per_step": int(state.nbytes),
+           "steps": ne, "note": "per step: fsl_upload_state (pinned host -> HBM), fsl_step(1), "
+                                "fsl_download_state (HBM -> pinned host)"}
+
+    # ---- CPU baseline: the reference's serial solver, rank 0 at N = 1 only ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            r = run_reference_cpu(1, args.cpu_steps, 1)
+            if r:
+                cpu = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                       "sample": "reference serial src (FP64, zero-fill patch) on a %dx%dx%d slab of "
+                                 "the workload's cross-section, %d RK3 steps after 1 warm-up"
+                                 % (REF_SLAB + (args.cpu_steps,))}
+        except Exception as ex:  # report, never fall back
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "error": str(ex)[:200]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == 0 else "f32 bulk / f64 accumulation",
+                "data": "synthetic (seeded tanh shear layer, Crocco-Busemann T, uniform noise 1e-3 dU)",
+                "config": {"workload": workload_name(grid), "grid": list(grid), "cells": ncell,
+                           "stages_per_step": STAGES,
+                           "path": ("per-phase kernels" if args.phased else "fused stage kernels") +
+                                   (", plain FP64, dynamic Smagorinsky" if args.precision == 0 else
+                                    ", FP32 bulk, dynamic Smagorinsky"),
+                           "l2": "inputs larger than L2 (state %.2f GB per domain)" % (state.nbytes / 1e9),
+                           "parallelism": "replicas (one independent domain per GPU)"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": int(sum(kl.values())),
+                "kernels_ms": {k: round(v, 3) for k, v in kms.items()},
+                "clocks": clk}
+        print(json.dumps(line), flush=True)
+    d.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    grid = tuple(int(x) for x in args.grid.split("x"))
+    nproc = min(host_cores(), 128)
+    why = "reference oracle library (oracle/_ref) is not built and the reference sources are absent"
+    try:
+        r = run_reference_cpu(nproc, args.steps, args.warmup)
+    except Exception as ex:
+        r = None
+        why = "reference run failed: " + str(ex)[:200]
+    if not r:
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return
+    value, wall, per_step = r
+    sample = ("reference serial src (FP64, zero-fill patch), %d concurrent processes each on a "
+              "%dx%dx%d slab of the workload's cross-section (no halo exchange: src-par needs MPI, "
+              "absent), %d RK3 steps after %d warm-up" % ((nproc,) + REF_SLAB + (args.steps, args.warmup)))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * max(per_step) if per_step else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the reference's own step-profile initial state)",
+            "config": {"workload": workload_name(grid), "grid": list(grid),
+                       "parallelism": "%d host processes" % nproc},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fsl", choices=["fsl", "reference"])
+    ap.add_argument("--grid", default="x".join(str(x) for x in GRID))
+    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--phased", action="store_true", help="per-phase kernels instead of the fused step")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--rows", type=int, default=0, help="fused stage tile rows (8, 12, 16)")
+    ap.add_argument("--seg", type=int, default=0, help="x planes per fused stage block")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="DRAM bytes per launch of the dominant kernel from an ncu capture")
+    ap.add_argument("--ref-worker", nargs=4, default=None, help=argparse.SUPPRESS)
+    args = ap.parse_args()
+    if args.ref_worker:
+        n, w, slab, out = args.ref_worker
+        _ref_worker_main(int(n), int(w), tuple(int(x) for x in slab.split(",")), out)
+        return
+    if args.warmup < 3 and args.impl == "fsl":
+        args.warmup = 3
+    if args.impl == "reference":
+        main_reference(args)
+    else:
+        main_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -80,6 +80,16 @@ class Info(C.Structure):
                 ("device_bytes", C.c_ulonglong)]
 
 
+K_CLASSES = ["stage", "recon", "flux", "sgs", "evol", "bc", "cfl", "other"]
+
+
+class KTimes(C.Structure):
+    _fields_ = [("ms", C.c_double * 8), ("launches", C.c_ulonglong * 8)]
+
+    def as_dict(self) -> dict:
+        return {n: (self.ms[i], self.launches[i]) for i, n in enumerate(K_CLASSES)}
+
+
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _lib = None
 
@@ -111,12 +121,17 @@ def lib():
             "fsl_get_faces": [vp, i, i, i, _dp], "fsl_set_faces": [vp, i, i, i, _dp],
             "fsl_set_cur": [vp, i], "fsl_sums": [vp, _dp], "fsl_plane_sums": [vp, _dp],
         }
+        sig["fsl_tune"] = [vp, i, i]
+        sig["fsl_profile"] = [vp, i]
+        sig["fsl_profile_read"] = [vp, C.POINTER(KTimes)]
         for name, args in sig.items():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = C.c_int
         L.fsl_last_error.argtypes = [vp]
         L.fsl_last_error.restype = C.c_char_p
+        L.fsl_stream.argtypes = [vp]
+        L.fsl_stream.restype = C.c_void_p
         _lib = L
     return _lib
 
@@ -222,8 +237,13 @@ class Domain:
     def upload_state(self, state: np.ndarray):
         self._c(lib().fsl_upload_state(self.h, np.ascontiguousarray(state, np.float64).ravel()))
 
-    def download_state(self) -> np.ndarray:
-        out = np.empty(state_size(self.p), np.float64)
+    def download_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """U^n into `out` (a contiguous float64 array, e.g. over pinned memory)
+        or into a new array."""
+        if out is None:
+            out = np.empty(state_size(self.p), np.float64)
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size != state_size(self.p):
+            raise FslError(-1, "download_state: out must be contiguous float64 of the state size")
         self._c(lib().fsl_download_state(self.h, out))
         return out
 
@@ -296,6 +316,26 @@ class Domain:
 
     def set_cur(self, which: int):
         self._c(lib().fsl_set_cur(self.h, which))
+
+    TUNE_STAGE_ROWS, TUNE_STAGE_SEG = 1, 2
+
+    def tune(self, key: int, value: int):
+        """Launch-shape knob of the fused kernels (results do not depend on it)."""
+        self._c(lib().fsl_tune(self.h, key, value))
+
+    # --- profiling ------------------------------------------------------------------
+    def profile(self, on: bool = True):
+        self._c(lib().fsl_profile(self.h, 1 if on else 0))
+
+    def profile_read(self) -> KTimes:
+        t = KTimes()
+        self._c(lib().fsl_profile_read(self.h, C.byref(t)))
+        return t
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the domain (for torch.cuda.ExternalStream)."""
+        return lib().fsl_stream(self.h)
 
     # --- diagnostics ----------------------------------------------------------------
     def sums(self) -> np.ndarray:

@@ -34,6 +34,37 @@ Grid make_grid(int L, int H, int D, int elem_bytes)
     return g;
 }
 
+static cudaEvent_t take_event(Ctx &c)
+{
+    if (!c.evpool.empty()) {
+        cudaEvent_t e = c.evpool.back();
+        c.evpool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void prof_begin(Ctx &c, int cls)
+{
+    if (!c.prof) return;
+    c.open_cls = cls;
+    c.open_ev = take_event(c);
+    cudaEventRecord(c.open_ev, c.stream);
+}
+
+void prof_end(Ctx &c, int cls, int nkernels)
+{
+    c.klaunch[cls] += (unsigned long long)nkernels;
+    if (!c.prof || c.open_cls != cls || !c.open_ev) return;
+    cudaEvent_t b = take_event(c);
+    cudaEventRecord(b, c.stream);
+    c.recs.push_back({cls, c.open_ev, b});
+    c.open_ev = nullptr;
+    c.open_cls = -1;
+}
+
 } // namespace fsl
 
 namespace {
@@ -109,6 +140,22 @@ int ensure_dyn(Ctx &c)
     if ((rc = dev_alloc(c, &c.dyn.B, 6 * fs))) return rc;
     if ((rc = dev_alloc(c, &c.dyn.S, fs))) return rc;
     c.dyn_alloc = true;
+    return FSL_OK;
+}
+
+int ensure_bf(Ctx &c)
+{
+    if (c.bf_alloc) return FSL_OK;
+    const Grid &g = c.g;
+    const size_t nx = 5 * (size_t)g.H * g.D, ny = 5 * (size_t)g.L * g.D, nz = 5 * (size_t)g.L * g.H;
+    int rc;
+    if ((rc = dev_alloc(c, &c.bf.x0, nx))) return rc;
+    if ((rc = dev_alloc(c, &c.bf.xL, nx))) return rc;
+    if ((rc = dev_alloc(c, &c.bf.y0, ny))) return rc;
+    if ((rc = dev_alloc(c, &c.bf.yH, ny))) return rc;
+    if ((rc = dev_alloc(c, &c.bf.z0, nz))) return rc;
+    if ((rc = dev_alloc(c, &c.bf.zD, nz))) return rc;
+    c.bf_alloc = true;
     return FSL_OK;
 }
 
@@ -393,6 +440,13 @@ int fsl_destroy(fsl_ctx *h)
         cudaFree(c.dyn.vel); cudaFree(c.dyn.t1); cudaFree(c.dyn.t2); cudaFree(c.dyn.A);
         cudaFree(c.dyn.Lst); cudaFree(c.dyn.B); cudaFree(c.dyn.S);
     }
+    if (c.bf_alloc) {
+        cudaFree(c.bf.x0); cudaFree(c.bf.xL); cudaFree(c.bf.y0);
+        cudaFree(c.bf.yH); cudaFree(c.bf.z0); cudaFree(c.bf.zD);
+    }
+    for (auto &r : c.recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : c.evpool) cudaEventDestroy(e);
+    if (c.open_ev) cudaEventDestroy(c.open_ev);
     if (c.stream) cudaStreamDestroy(c.stream);
     delete h;
     return FSL_OK;
@@ -593,9 +647,52 @@ int fsl_step_phased(fsl_ctx *h, int nsteps)
     return FSL_OK;
 }
 
+// Fused path: per stage a ghost fill, the boundary outer states and one
+// fused stage kernel; stages ping-pong U^n -> Up -> Uq -> U^n.
 int fsl_step(fsl_ctx *h, int nsteps)
 {
-    return fsl_step_phased(h, nsteps);
+    if (!h || nsteps < 0) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    if (c.p.nStages != 3) return fsl_step_phased(h, nsteps);
+    int rc;
+    if ((rc = ensure_dyn(c))) return rc;
+    if ((rc = ensure_bf(c))) return rc;
+    if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_step: the current-stage buffer is not U^n");
+    for (int n = 0; n < nsteps; n++) {
+        launch_courant(c);
+        c.step++;
+        draw(c);
+        launch_ghost(c, c.U);
+        launch_bface(c, c.U, c.dist);
+        launch_dynsmag(c, c.U);
+        if (launch_stage(c, 1, c.U, c.U, c.Up)) return fail(c, FSL_ERR_CUDA, "stage kernel attribute");
+        launch_ghost(c, c.Up);
+        launch_bface(c, c.Up, c.dist);
+        launch_stage(c, 2, c.Up, c.U, c.Uq);
+        launch_ghost(c, c.Uq);
+        launch_bface(c, c.Uq, c.dist);
+        launch_stage(c, 3, c.Uq, c.U, c.U);
+        CKL();
+    }
+    return FSL_OK;
+}
+
+int fsl_tune(fsl_ctx *h, int key, int value)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    switch (key) {
+    case FSL_TUNE_STAGE_ROWS:
+        if (value != 8 && value != 12 && value != 16) return FSL_ERR_ARG;
+        c.stage_tje = value;
+        return FSL_OK;
+    case FSL_TUNE_STAGE_SEG:
+        if (value < 1 || value > 1 << 20) return FSL_ERR_ARG;
+        c.stage_seg = value;
+        return FSL_OK;
+    default:
+        return FSL_ERR_ARG;
+    }
 }
 
 int fsl_get_cells(fsl_ctx *h, int which, int var, double *out)
@@ -656,6 +753,37 @@ int fsl_set_cur(fsl_ctx *h, int which)
     h->c.cur = which;
     return FSL_OK;
 }
+
+int fsl_profile(fsl_ctx *h, int on)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    CK(cudaStreamSynchronize(c.stream));
+    for (auto &r : c.recs) { c.evpool.push_back(r.a); c.evpool.push_back(r.b); }
+    c.recs.clear();
+    for (int k = 0; k < FSL_K_COUNT; k++) { c.kms[k] = 0; c.klaunch[k] = 0; }
+    c.prof = on != 0;
+    return FSL_OK;
+}
+
+int fsl_profile_read(fsl_ctx *h, fsl_ktimes *out)
+{
+    if (!h || !out) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    CK(cudaStreamSynchronize(c.stream));
+    for (auto &r : c.recs) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, r.a, r.b));
+        c.kms[r.cls] += ms;
+        c.evpool.push_back(r.a);
+        c.evpool.push_back(r.b);
+    }
+    c.recs.clear();
+    for (int k = 0; k < FSL_K_COUNT; k++) { out->ms[k] = c.kms[k]; out->launches[k] = c.klaunch[k]; }
+    return FSL_OK;
+}
+
+void *fsl_stream(fsl_ctx *h) { return h ? (void *)h->c.stream : nullptr; }
 
 int fsl_sums(fsl_ctx *h, double sums[5])
 {

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <vector>
 
 #include "../../include/fsl_gpu.h"
 
@@ -56,6 +57,13 @@ struct Faces {
     double *x[2][5], *y[2][5], *z[2][5];
 };
 
+// Outer states of the domain-boundary faces for the fused stage kernel (the
+// reference's BounCondOnInterfaces values): x0/xL [5][HIG][DEP] (minus side of
+// x face 0, plus side of x face LEN), y0/yH [5][LEN][DEP], z0/zD [5][LEN][HIG].
+struct BFaces {
+    double *x0, *xL, *y0, *yH, *z0, *zD;
+};
+
 // Scratch of the dynamic Smagorinsky procedure (padded layout, FP64).
 struct DynScratch {
     double *vel;   // 3 fields u, v, w
@@ -80,6 +88,10 @@ struct Ctx {
     bool faces_alloc = false;
     DynScratch dyn{};
     bool dyn_alloc = false;
+    BFaces bf{};
+    bool bf_alloc = false;
+    int stage_tje = 12; // rows per fused-stage tile (incl. the two halo rows)
+    int stage_seg = 64; // x planes per fused-stage block
     DevScalars *ds = nullptr; // device scalars
     DevScalars *hs = nullptr; // pinned host mirror
     double *partials = nullptr;
@@ -95,7 +107,23 @@ struct Ctx {
     double maxco_host = 0;
     unsigned long long bytes = 0;
     std::string err;
+    // profiler: event pairs per kernel class, launch counters
+    bool prof = false;
+    struct Rec {
+        int cls;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> evpool;
+    double kms[FSL_K_COUNT] = {0};
+    unsigned long long klaunch[FSL_K_COUNT] = {0};
+    int open_cls = -1;
+    cudaEvent_t open_ev = nullptr;
 };
+
+// Bracket a group of launches of one kernel class (no-ops unless profiling).
+void prof_begin(Ctx &c, int cls);
+void prof_end(Ctx &c, int cls, int nkernels);
 
 // ---- launchers (fsl_phase.cu) ------------------------------------------------
 void launch_ghost(Ctx &c, double *cur);
@@ -109,5 +137,10 @@ void launch_state_scatter(Ctx &c, double *dst, const double *packed);
 void launch_state_gather(Ctx &c, const double *src, double *packed);
 void launch_sums(Ctx &c, const double *U, double *out5);
 void launch_plane_sums(Ctx &c, const double *U, double *rows);
+
+// ---- fused path (fsl_fused.cu) ----------------------------------------------
+void launch_bface(Ctx &c, const double *cur, const Disturb &d);
+// One RK3 stage: cur (ghosts filled) -> out; un = U^n.
+int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double *out);
 
 } // namespace fsl

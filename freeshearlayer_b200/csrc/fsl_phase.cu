@@ -711,30 +711,38 @@ void launch_ghost(Ctx &c, double *cur)
 {
     const Grid &g = c.g;
     const long long n = 2LL * (g.H + 2) * (g.D + 2) + 2LL * g.L * (g.D + 2) + 2LL * g.L * g.H;
+    prof_begin(c, FSL_K_BC);
     k_ghost<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(g, c.k.setup, cur);
+    prof_end(c, FSL_K_BC, 1);
 }
 
 void launch_recon(Ctx &c, const double *cur)
 {
     const Grid &g = c.g;
     dim3 b(32, 4, 1);
+    prof_begin(c, FSL_K_RECON);
     k_recon<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, cur, c.f);
+    prof_end(c, FSL_K_RECON, 1);
 }
 
 void launch_ifbc(Ctx &c, const Disturb &d)
 {
     const Grid &g = c.g;
     const long long n = (long long)g.H * g.D + (long long)g.L * g.D + (long long)g.L * g.H;
+    prof_begin(c, FSL_K_BC);
     k_ifbc<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(g, c.k.setup, c.k.BL_HIG, d, c.f);
+    prof_end(c, FSL_K_BC, 1);
 }
 
 void launch_fluxes(Ctx &c, const double *cur)
 {
     const Grid &g = c.g;
     dim3 b(32, 4, 1);
+    prof_begin(c, FSL_K_FLUX);
     k_flux<1><<<cells_grid(g, b, g.L + 1, g.H, g.D), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f);
     k_flux<2><<<cells_grid(g, b, g.L, g.H + 1, g.D), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f);
     k_flux<3><<<cells_grid(g, b, g.L, g.H, g.D + 1), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f);
+    prof_end(c, FSL_K_FLUX, 3);
 }
 
 void launch_evolution(Ctx &c, int nstages, int stage)
@@ -743,7 +751,9 @@ void launch_evolution(Ctx &c, int nstages, int stage)
     int mode = stage >= 3 ? 3 : stage;
     if (nstages == 2) mode = (stage == 1) ? 4 : 5;
     dim3 b(32, 4, 1);
+    prof_begin(c, FSL_K_EVOL);
     k_evolution<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, mode, c.ds, c.U, c.Up, c.f);
+    prof_end(c, FSL_K_EVOL, 1);
 }
 
 void launch_dynsmag(Ctx &c, const double *U)
@@ -751,6 +761,7 @@ void launch_dynsmag(Ctx &c, const double *U)
     const Grid &g = c.g;
     DynScratch &s = c.dyn;
     const long long ncell = (long long)(g.L + 2) * g.pi;
+    prof_begin(c, FSL_K_SGS);
     k_dyn_vel<<<(unsigned)std::min<long long>((ncell + 255) / 256, 148LL * 16), 256, 0, c.stream>>>(g, U, s.vel);
     dim3 b(32, 4, 1);
     // velocity and product filters: y over i in [0,L] j in [1,H] k in [0,D]
@@ -763,36 +774,47 @@ void launch_dynsmag(Ctx &c, const double *U)
     k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, c.stream>>>(g, 6, s.t1, s.t2);
     k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, c.stream>>>(g, 6, s.t2, s.t1);
     k_dyn_final<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, c.k, U, s.Lst, s.B, s.t1, s.S, c.mu);
+    prof_end(c, FSL_K_SGS, 9);
 }
 
 void launch_courant(Ctx &c)
 {
     const Grid &g = c.g;
+    prof_begin(c, FSL_K_CFL);
     k_courant_partial<<<c.npartials, 256, 0, c.stream>>>(g, c.k, c.U, c.ds, c.partials, c.ds);
     k_courant_final<<<1, 1024, 0, c.stream>>>(c.k, c.partials, c.npartials, c.ds);
+    prof_end(c, FSL_K_CFL, 2);
 }
 
 void launch_state_scatter(Ctx &c, double *dst, const double *packed)
 {
+    prof_begin(c, FSL_K_OTHER);
     k_state_scatter<<<148 * 8, 256, 0, c.stream>>>(c.g, dst, packed);
+    prof_end(c, FSL_K_OTHER, 1);
 }
 
 void launch_state_gather(Ctx &c, const double *src, double *packed)
 {
+    prof_begin(c, FSL_K_OTHER);
     k_state_gather<<<148 * 8, 256, 0, c.stream>>>(c.g, src, packed);
+    prof_end(c, FSL_K_OTHER, 1);
 }
 
 void launch_sums(Ctx &c, const double *U, double *out5)
 {
     const int nb = 148 * 4;
+    prof_begin(c, FSL_K_OTHER);
     k_sums_partial<<<nb, 256, 0, c.stream>>>(c.g, U, c.partials);
     const double vol = c.p.deltaX * c.p.deltaY * c.p.deltaZ;
     k_sums_final<<<1, 32, 0, c.stream>>>(c.partials, nb, vol, out5);
+    prof_end(c, FSL_K_OTHER, 2);
 }
 
 void launch_plane_sums(Ctx &c, const double *U, double *rows)
 {
+    prof_begin(c, FSL_K_OTHER);
     k_plane_sums<<<c.g.H, 256, 0, c.stream>>>(c.g, U, rows);
+    prof_end(c, FSL_K_OTHER, 1);
 }
 
 } // namespace fsl

@@ -188,6 +188,11 @@ int fsl_step(fsl_ctx *ctx, int nsteps);
 /* Same work through the per-phase entry points (reference phase order). */
 int fsl_step_phased(fsl_ctx *ctx, int nsteps);
 
+/* Launch-shape knobs of the fused kernels (the results do not depend on them). */
+#define FSL_TUNE_STAGE_ROWS 1 /* rows per stage tile incl. 2 halo rows: 8, 12 or 16 */
+#define FSL_TUNE_STAGE_SEG 2  /* x planes marched per stage block */
+int fsl_tune(fsl_ctx *ctx, int key, int value);
+
 /* ---- debug / parity access ----------------------------------------------- */
 
 /* which: 0 = U^n, 1 = stage buffer, 2 = current-stage buffer, 3 = mu_SGS. */
@@ -198,6 +203,32 @@ int fsl_get_faces(fsl_ctx *ctx, int dir, int side, int var, double *faces);
 int fsl_set_faces(fsl_ctx *ctx, int dir, int side, int var, const double *faces);
 /* Point U*_ at U^n (0) or at the stage buffer (1). */
 int fsl_set_cur(fsl_ctx *ctx, int which);
+
+/* ---- profiling ------------------------------------------------------------- */
+
+/* Kernel classes timed by the context's profiler. */
+#define FSL_K_STAGE 0 /* fused stage kernel */
+#define FSL_K_RECON 1 /* per-phase reconstruction */
+#define FSL_K_FLUX 2  /* per-phase fluxes */
+#define FSL_K_SGS 3   /* SGS viscosity (dynamic procedure or learned closure) */
+#define FSL_K_EVOL 4  /* per-phase RK update */
+#define FSL_K_BC 5    /* ghost cells and boundary faces */
+#define FSL_K_CFL 6   /* Courant reduction and dt rescale */
+#define FSL_K_OTHER 7 /* state transfer, diagnostics */
+#define FSL_K_COUNT 8
+
+typedef struct fsl_ktimes {
+    double ms[FSL_K_COUNT];                  /* device time per class (CUDA events on the context stream) */
+    unsigned long long launches[FSL_K_COUNT]; /* kernels launched per class */
+} fsl_ktimes;
+
+/* Reset the counters; with on != 0, bracket every kernel class with CUDA
+ * events from now on (launch counts are always kept). */
+int fsl_profile(fsl_ctx *ctx, int on);
+/* Synchronise and read the accumulated times and launch counts. */
+int fsl_profile_read(fsl_ctx *ctx, fsl_ktimes *out);
+/* The CUDA stream (cudaStream_t) all work of the context runs on. */
+void *fsl_stream(fsl_ctx *ctx);
 
 /* ---- diagnostics ----------------------------------------------------------- */
 
