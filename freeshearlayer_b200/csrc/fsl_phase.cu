@@ -818,3 +818,95 @@ void launch_plane_sums(Ctx &c, const double *U, double *rows)
 }
 
 } // namespace fsl
+
+// ---------------------------------------------------------------------------
+// Allocation-free SGS viscosity (fsl_dynamic_smagorinsky_noalloc).
+//
+// Callers that cannot allocate device memory hand in their own input and
+// output buffers; the procedure's 40 scratch fields live in this fixed static
+// device array instead of cudaMalloc'd memory.  Every GPU that loads the
+// library holds the array until the process exits.  On the host the symbol
+// name only stands in for the array; the device address is looked up once per
+// device with cudaGetSymbolAddress (that device current) and cached.
+// ---------------------------------------------------------------------------
+#include <cmath>
+#include <mutex>
+
+static __device__ __align__(256) double fsl_noalloc_scratch[FSL_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double *g_noalloc_ptr[kNoallocMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device.
+int noalloc_scratch(double **out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return FSL_ERR_NODEVICE;
+    if (dev < 0 || dev >= kNoallocMaxDevices) return FSL_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, fsl_noalloc_scratch);
+        if (e != cudaSuccess || !p) return FSL_ERR_CUDA;
+        g_noalloc_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return FSL_OK;
+}
+
+// The launch sequence of launch_dynsmag on explicit buffers and stream.
+void noalloc_dyn_sequence(const fsl::Grid &g, const fsl::Consts &k, const fsl::DynScratch &s, const double *U,
+                          double *mu, cudaStream_t st)
+{
+    using namespace fsl;
+    const long long ncell = (long long)(g.L + 2) * g.pi;
+    k_dyn_vel<<<(unsigned)std::min<long long>((ncell + 255) / 256, 148LL * 16), 256, 0, st>>>(g, U, s.vel);
+    dim3 b(32, 4, 1);
+    k_filt_y_vel<<<cells_grid(g, b, g.L + 1, g.H, g.D + 1), b, 0, st>>>(g, s.vel, s.t1);
+    k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, st>>>(g, 9, s.t1, s.t2);
+    k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, st>>>(g, 9, s.t2, s.t1);
+    k_dyn_mid<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, st>>>(g, k, s.vel, s.t1, s.Lst, s.A, s.B, s.S);
+    k_filt_y<<<cells_grid(g, b, g.L + 1, g.H, g.D + 1), b, 0, st>>>(g, 6, s.A, s.t1);
+    k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, st>>>(g, 6, s.t1, s.t2);
+    k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, st>>>(g, 6, s.t2, s.t1);
+    k_dyn_final<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, st>>>(g, k, U, s.Lst, s.B, s.t1, s.S, mu);
+}
+
+} // namespace
+
+extern "C" int fsl_dynamic_smagorinsky_noalloc(const double *U, double *mu, int LEN, int HIG, int DEP,
+                                                double deltaX, double deltaY, double deltaZ, void *stream)
+{
+    if (!U || !mu || LEN < 2 || HIG < 2 || DEP < 2 || !(deltaX > 0) || !(deltaY > 0) || !(deltaZ > 0))
+        return FSL_ERR_ARG;
+    const long long n = (long long)(LEN + 2) * (HIG + 2) * (DEP + 2);
+    if (n > (long long)FSL_NOALLOC_MAX_CELLS) return FSL_ERR_TOO_LARGE;
+    double *s = nullptr;
+    int rc = noalloc_scratch(&s);
+    if (rc) return rc;
+    fsl::Grid g;
+    g.L = LEN; g.H = HIG; g.D = DEP;
+    g.pk = DEP + 2;
+    g.pi = (long long)(DEP + 2) * (HIG + 2);
+    g.off = 0;
+    g.fstride = n;
+    // derived constants exactly as fsl_init computes them (src/initialize.c:67-94)
+    fsl::Consts k{};
+    k.r4dx = 1. / (4 * deltaX); k.r4dy = 1. / (4 * deltaY); k.r4dz = 1. / (4 * deltaZ);
+    k.r2dx = k.r4dx + k.r4dx; k.r2dy = k.r4dy + k.r4dy; k.r2dz = k.r4dz + k.r4dz;
+    k.DD = pow(deltaX * deltaY * deltaZ, 0.666666666666667);
+    fsl::DynScratch d;
+    d.vel = s; d.t1 = s + 3 * n; d.t2 = s + 12 * n; d.A = s + 21 * n;
+    d.Lst = s + 27 * n; d.B = s + 33 * n; d.S = s + 39 * n;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // zero bands of the filter passes and the A ghost layer must start at 0;
+    // the previous call left its values in the shared scratch
+    if (cudaMemsetAsync(s, 0, (size_t)(40 * n) * sizeof(double), st) != cudaSuccess) return FSL_ERR_CUDA;
+    if (cudaMemsetAsync(mu, 0, (size_t)n * sizeof(double), st) != cudaSuccess) return FSL_ERR_CUDA;
+    noalloc_dyn_sequence(g, k, d, U, mu, st);
+    if (cudaGetLastError() != cudaSuccess) return FSL_ERR_CUDA;
+    return FSL_OK;
+}

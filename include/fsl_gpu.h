@@ -178,6 +178,36 @@ int fsl_dynamic_smagorinsky(fsl_ctx *ctx); /* DynamicSmagorinsky(U1..U4,mu_SGS),
 int fsl_fluxes(fsl_ctx *ctx);              /* Fluxes face loops, src/fluxes.c:57-571 */
 int fsl_evolution(fsl_ctx *ctx, int stage); /* Evolution(nStages, Stage), src/evolution.c:15 */
 
+/* SGS viscosity without any device allocation.  No counterpart in the
+ * reference (which allocates 42 fresh arrays per call); it exists for callers
+ * that cannot allocate device memory themselves or through this library: a
+ * host application whose own allocator has reserved the device memory
+ * up front, or a time-critical loop that must not stall on cudaFree's
+ * device-wide synchronisation.
+ *
+ * Same arithmetic as fsl_dynamic_smagorinsky (bit-identical mu).  U: device
+ * pointer to four consecutive (LEN+2)(HIG+2)(DEP+2) double arrays rho, rho u,
+ * rho v, rho w (k fastest, ghost layer filled, e.g. by fsl_ghost_bc); mu:
+ * device pointer to one such array, fully written (interior values, ghost
+ * layer 0).  stream: a cudaStream_t, or NULL for the legacy default stream.
+ *
+ * Scratch is a fixed static device array of FSL_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until process exit; it needs
+ * 40 (LEN+2)(HIG+2)(DEP+2) doubles, so (LEN+2)(HIG+2)(DEP+2) may be at most
+ * FSL_NOALLOC_MAX_CELLS (e.g. 64x32x32 fits); larger sizes return
+ * FSL_ERR_TOO_LARGE before any device work.  The call allocates nothing: no
+ * cudaMalloc, no cudaFree, no library allocator.  The first call on a device
+ * looks up the scratch address for that device (cudaGetSymbolAddress, with
+ * that device current); make that first call before any stream capture.
+ * All calls share the one scratch array, which keeps the previous call's
+ * contents (the call clears what must start at zero): calls that overlap on
+ * the GPU (different streams, or different host threads) race on it. */
+#define FSL_ERR_TOO_LARGE (-9)
+#define FSL_NOALLOC_SCRATCH_BYTES (32u << 20)
+#define FSL_NOALLOC_MAX_CELLS (FSL_NOALLOC_SCRATCH_BYTES / (40u * 8u))
+int fsl_dynamic_smagorinsky_noalloc(const double *U, double *mu, int LEN, int HIG, int DEP, double deltaX,
+                                    double deltaY, double deltaZ, void *stream);
+
 /* ---- whole steps ---------------------------------------------------------
  * nsteps iterations of the driver loop body without I/O (src/layer2.c:147-178):
  * Courant check and dt rescale, disturbance draw, nStages stages.  Uses the
