@@ -1,0 +1,116 @@
+"""C ABI and host logic without a GPU: the library loads, exports every entry
+point include/fsl_gpu.h declares, parses layer2.ini / mpi_layer2.bin the way
+the reference does, validates parameters, builds initial states identical to
+the oracle's, and refuses to run without an sm_100 device (no CPU path)."""
+import ctypes as C
+import os
+import re
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests.helpers import spatial_params, temporal_params
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "fsl_gpu.h")
+
+# the reference's shipped layer2.ini (22 positional lines with trailing text)
+SHIPPED_INI = """100 120        LEN      Number of cells in length     [-]
+80  90         HIG      Number of cells in height     [-]
+35  41         DEP      Number of cells in depth      [-]
+1.6666667  deltaX   X-step                        [m]
+1.         deltaY   Y-step                        [m]
+1.5        deltaZ   Z-step                        [m]
+0.0007     deltaT   Time step                     [sec]
+0         Answer   1-continue, 0-start new	      [boolean]
+3000      numstep  Number of overall time steps  [-]
+0.253358   mu_L     Dynamic mol. viscosity 	      [Pa*sec]
+0.72       Pr_L     Mol. Prandtl number
+0.8        Pr_T     Turb. Prandtl number
+0.01       Cs       Square of the Smagorinsky constant
+5          BL_HIG   Height of the random disturbing block
+35.        Ua       Amplitude of disturbed U      [m/sec]
+35.        Va       Amplitude of disturbed V	  [m/sec]
+35.        Wa       Amplitude of disturbed W	  [m/sec]
+10         Nst_min  Minimal period of disturbing block
+50         Nst      Its max-min
+50         f_step   Frame taking step (!output for winfield.exe!)
+2          nStages  number of stages (2,3) of TVD Runge-Kutta Algorithm
+0.1        maxCoNum    Maximum Courant number for timestepping stability
+"""
+
+
+@pytest.fixture(scope="module")
+def fsl():
+    import freeshearlayer_b200 as fsl
+    fsl.lib()
+    return fsl
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(fsl_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declarations_exported(fsl):
+    names = declared_functions()
+    assert len(names) > 30
+    lib = C.CDLL(fsl.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_params_from_ini_matches_reference_parser(fsl, tmp_path):
+    path = tmp_path / "layer2.ini"
+    path.write_text(SHIPPED_INI)
+    p = fsl.params_from_ini(str(path))
+    assert (p.LEN, p.HIG, p.DEP) == (100, 80, 35)
+    assert p.deltaX == 1.6666667 and p.deltaY == 1.0 and p.deltaZ == 1.5 and p.deltaT == 0.0007
+    assert p.numstep == 3000 and p.BL_HIG == 5 and p.Ns_min == 10 and p.Nst == 50
+    assert p.nStages == 2 and p.maxCoNum == 0.1 and p.mu_L == 0.253358 and p.Cs == 0.01
+    short = tmp_path / "short.ini"
+    short.write_text("\n".join(SHIPPED_INI.splitlines()[:10]) + "\n")
+    with pytest.raises(fsl.FslError) as e:
+        fsl.params_from_ini(str(short))
+    assert e.value.code == -6
+
+
+def test_params_from_bin(fsl, tmp_path):
+    vals = [64, 32, 32, 0.1, 0.1, 0.1, 1e-4, 0, 200, 0.6, 0.72, 0.8, 0.01, 4, 35, 35, 35,
+            10, 50, 50, 3, 0.5]
+    path = tmp_path / "mpi_layer2.bin"
+    path.write_bytes(struct.pack("<22f", *vals))
+    p = fsl.params_from_bin(str(path))
+    assert (p.LEN, p.HIG, p.DEP, p.numstep, p.nStages, p.BL_HIG) == (64, 32, 32, 200, 3, 4)
+    assert p.deltaX == float(np.float32(0.1)) and p.maxCoNum == float(np.float32(0.5))
+
+
+def test_params_check(fsl):
+    lib = fsl.lib()
+    ok = fsl.default_params()
+    assert lib.fsl_params_check(C.byref(ok)) == 0
+    for bad in [dict(BL_HIG=100), dict(LEN=1), dict(deltaX=0.0), dict(nStages=4), dict(setup=7),
+                dict(cfl_mode=3), dict(maxCoNum=-1.0)]:
+        p = fsl.default_params(**bad)
+        assert lib.fsl_params_check(C.byref(p)) == -1, bad
+
+
+def test_initial_states_match_oracle(fsl, oracle_lib):
+    p = spatial_params(L=9, H=7, D=5)
+    assert np.array_equal(fsl.initial_state(p), oracle_lib.spatial_initial_state(p))
+    q = temporal_params(L=12, H=8, D=6)
+    a, dUa = fsl.temporal_state(q, 0.4)
+    b, dUb = oracle_lib.Oracle.temporal_state(q, 0.4)
+    assert dUa == dUb and np.array_equal(a, b)
+
+
+def test_no_cpu_fallback(fsl):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(fsl.FslError) as e:
+        fsl.Domain(spatial_params())
+    assert e.value.code == -8
