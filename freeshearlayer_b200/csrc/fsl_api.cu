@@ -159,6 +159,36 @@ int ensure_bf(Ctx &c)
     return FSL_OK;
 }
 
+int dev_alloc_f(Ctx &c, float **p, size_t n)
+{
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(float));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(c, FSL_ERR_NOMEM, "cudaMalloc", e);
+    }
+    c.bytes += n * sizeof(float);
+    e = cudaMemsetAsync(*p, 0, n * sizeof(float), c.stream);
+    if (e != cudaSuccess) return fail(c, FSL_ERR_CUDA, "cudaMemsetAsync", e);
+    return FSL_OK;
+}
+
+int ensure_fp32(Ctx &c)
+{
+    if (c.fp32_alloc) return FSL_OK;
+    const Grid &g = c.g;
+    const size_t nx = 5 * (size_t)g.H * g.D, ny = 5 * (size_t)g.L * g.D, nz = 5 * (size_t)g.L * g.H;
+    int rc;
+    if ((rc = dev_alloc_f(c, &c.bf32.x0, nx))) return rc;
+    if ((rc = dev_alloc_f(c, &c.bf32.xL, nx))) return rc;
+    if ((rc = dev_alloc_f(c, &c.bf32.y0, ny))) return rc;
+    if ((rc = dev_alloc_f(c, &c.bf32.yH, ny))) return rc;
+    if ((rc = dev_alloc_f(c, &c.bf32.z0, nz))) return rc;
+    if ((rc = dev_alloc_f(c, &c.bf32.zD, nz))) return rc;
+    if ((rc = dev_alloc_f(c, &c.mu32, (size_t)g.fstride))) return rc;
+    c.fp32_alloc = true;
+    return FSL_OK;
+}
+
 double *cur_ptr(Ctx &c) { return c.cur ? c.Up : c.U; }
 
 // Disturbance draw of src/layer2.c:152-162 with Random() of src/helpers.c:13-17.
@@ -444,6 +474,10 @@ int fsl_destroy(fsl_ctx *h)
         cudaFree(c.bf.x0); cudaFree(c.bf.xL); cudaFree(c.bf.y0);
         cudaFree(c.bf.yH); cudaFree(c.bf.z0); cudaFree(c.bf.zD);
     }
+    if (c.fp32_alloc) {
+        cudaFree(c.bf32.x0); cudaFree(c.bf32.xL); cudaFree(c.bf32.y0);
+        cudaFree(c.bf32.yH); cudaFree(c.bf32.z0); cudaFree(c.bf32.zD); cudaFree(c.mu32);
+    }
     for (auto &r : c.recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto e : c.evpool) cudaEventDestroy(e);
     if (c.open_ev) cudaEventDestroy(c.open_ev);
@@ -653,11 +687,35 @@ int fsl_step(fsl_ctx *h, int nsteps)
 {
     if (!h || nsteps < 0) return FSL_ERR_ARG;
     Ctx &c = h->c;
-    if (c.p.nStages != 3) return fsl_step_phased(h, nsteps);
+    if (c.p.nStages != 3) {
+        if (c.p.precision != FSL_PREC_FP64) return fail(c, FSL_ERR_UNSUPPORTED, "FP32 bulk needs nStages = 3");
+        return fsl_step_phased(h, nsteps);
+    }
     int rc;
     if ((rc = ensure_dyn(c))) return rc;
     if ((rc = ensure_bf(c))) return rc;
     if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_step: the current-stage buffer is not U^n");
+    if (c.p.precision == FSL_PREC_FP32) {
+        if ((rc = ensure_fp32(c))) return rc;
+        for (int n = 0; n < nsteps; n++) {
+            launch_courant(c);
+            c.step++;
+            draw(c);
+            launch_ghost(c, c.U);
+            launch_bface32(c, c.U, c.dist);
+            launch_dynsmag(c, c.U);
+            launch_mu_to_f32(c);
+            if (launch_stage32(c, 1, c.U, c.U, c.Up)) return fail(c, FSL_ERR_CUDA, "FP32 stage kernel");
+            launch_ghost(c, c.Up);
+            launch_bface32(c, c.Up, c.dist);
+            launch_stage32(c, 2, c.Up, c.U, c.Uq);
+            launch_ghost(c, c.Uq);
+            launch_bface32(c, c.Uq, c.dist);
+            launch_stage32(c, 3, c.Uq, c.U, c.U);
+            CKL();
+        }
+        return FSL_OK;
+    }
     for (int n = 0; n < nsteps; n++) {
         launch_courant(c);
         c.step++;

@@ -1,0 +1,47 @@
+// fsl_fused32.cu -- FP32-bulk instantiation of the fused stage kernel.
+//
+// Reconstruction, Riemann and viscous fluxes run in FP32 (compiled with
+// --use_fast_math: FMA contraction, approximate FP32 division and square
+// root); the conserved variables, the RK stage accumulation, the time-step
+// reduction and the conservation sums stay FP64.  Each stage reads the FP64
+// state, converts it once to FP32 in shared memory, and adds the FP32 flux
+// divergence to the FP64 state in FP64.
+#include "fsl_stage.cuh"
+
+namespace fsl {
+
+static stage::BF<float> bf32(Ctx &c)
+{
+    stage::BF<float> b;
+    b.x0 = c.bf32.x0; b.xL = c.bf32.xL; b.y0 = c.bf32.y0; b.yH = c.bf32.yH; b.z0 = c.bf32.z0; b.zD = c.bf32.zD;
+    return b;
+}
+
+void launch_bface32(Ctx &c, const double *cur, const Disturb &d)
+{
+    stage::launch_bface_t<float>(c, cur, d, bf32(c));
+}
+
+static __global__ void k_mu_to_f32(long long n, const double *__restrict__ mu, float *__restrict__ mu32)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        mu32[t] = (float)mu[t];
+}
+
+void launch_mu_to_f32(Ctx &c)
+{
+    prof_begin(c, FSL_K_SGS);
+    k_mu_to_f32<<<148 * 8, 256, 0, c.stream>>>(c.g.fstride, c.mu, c.mu32);
+    prof_end(c, FSL_K_SGS, 1);
+}
+
+int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out)
+{
+    switch (c.stage_tje) {
+    case 8: return stage::launch_stage_t<float, 8, 2>(c, stage, cur, un, out, c.mu32, bf32(c));
+    case 12: return stage::launch_stage_t<float, 12, 1>(c, stage, cur, un, out, c.mu32, bf32(c));
+    default: return stage::launch_stage_t<float, 16, 1>(c, stage, cur, un, out, c.mu32, bf32(c));
+    }
+}
+
+} // namespace fsl

@@ -63,6 +63,9 @@ struct Faces {
 struct BFaces {
     double *x0, *xL, *y0, *yH, *z0, *zD;
 };
+struct BFaces32 {
+    float *x0, *xL, *y0, *yH, *z0, *zD;
+};
 
 // Scratch of the dynamic Smagorinsky procedure (padded layout, FP64).
 struct DynScratch {
@@ -90,8 +93,12 @@ struct Ctx {
     bool dyn_alloc = false;
     BFaces bf{};
     bool bf_alloc = false;
-    int stage_tje = 12; // rows per fused-stage tile (incl. the two halo rows)
-    int stage_seg = 64; // x planes per fused-stage block
+    // FP32-bulk path
+    BFaces32 bf32{};
+    float *mu32 = nullptr;
+    bool fp32_alloc = false;
+    int stage_tje = 16; // rows per fused-stage tile (incl. the two halo rows)
+    int stage_seg = 32; // x planes per fused-stage block
     DevScalars *ds = nullptr; // device scalars
     DevScalars *hs = nullptr; // pinned host mirror
     double *partials = nullptr;
@@ -142,5 +149,9 @@ void launch_plane_sums(Ctx &c, const double *U, double *rows);
 void launch_bface(Ctx &c, const double *cur, const Disturb &d);
 // One RK3 stage: cur (ghosts filled) -> out; un = U^n.
 int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double *out);
+// FP32-bulk variants (fsl_fused32.cu): boundary states in bf32, SGS viscosity in mu32.
+void launch_bface32(Ctx &c, const double *cur, const Disturb &d);
+int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out);
+void launch_mu_to_f32(Ctx &c); // mu (FP64) -> mu32
 
 } // namespace fsl

@@ -1,0 +1,512 @@
+// fsl_stage.cuh -- fused RK3 stage kernel and boundary-face pass, templated on
+// the compute type T.  Instantiated for T = double (fsl_fused.cu, compiled
+// with --fmad=false: the plain method, bit-identical to the reference) and
+// T = float (fsl_fused32.cu: FP32 bulk, FP64 stage accumulation).
+//
+// Decomposition ("2.5-D" streaming): a block owns a tile of (TJE-2) x 30
+// cell columns in (y, z) plus a one-cell halo ring (TJE rows = warps, 32
+// lanes along the contiguous k axis) and marches along x over `seg` planes.
+// Per plane it stages in shared memory the current-stage state (two planes,
+// halo 2), the two velocity forms the viscous stencil reads (src/fluxes.c
+// divides for the two cells adjacent to a face, :117-122, and multiplies by a
+// reciprocal for the eight tangential neighbours, :124-142), temperature and
+// the face-averaged SGS viscosity.  Every face flux of the tile is computed
+// once (x faces in registers carried along the march, y faces through shared
+// memory, z faces through warp shuffles); the state is read once and the
+// stage result written once.  Plane i+2 is fetched into registers at the top
+// of iteration i and stored to shared memory at its end, hiding the load
+// latency behind the flux work.  Domain-boundary faces take their outer state
+// from the boundary pass (k_bface), which applies the reference's interface
+// rules (src/bounCondOnInterfaces.c:11-110) to the reconstructed boundary cells.
+#pragma once
+
+#include "fsl_internal.h"
+#include "fsl_phys.cuh"
+
+namespace fsl {
+namespace stage {
+
+template <typename T> struct BF {
+    T *x0, *xL, *y0, *yH, *z0, *zD;
+};
+
+template <typename T>
+__device__ __forceinline__ void load5(const double *__restrict__ u, long long fs, long long c, T *v)
+{
+#pragma unroll
+    for (int q = 0; q < 5; q++) v[q] = T(u[q * fs + c]);
+}
+
+// reconstruction sweep DIR (0 x, 1 y, 2 z) of the padded cell c
+template <typename T, int DIR>
+__device__ __forceinline__ void recon_at(const Grid &g, const double *__restrict__ u, long long c, T *hi, T *lo)
+{
+    const long long fs = g.fstride;
+    CellC<T> cc;
+    load5(u, fs, c, cc.u);
+    cell_consts(cc);
+    const long long d = DIR == 0 ? g.pi : DIR == 1 ? (long long)g.pk : 1LL;
+    const int p1 = DIR == 0 ? 1 : DIR == 1 ? 2 : 3;
+    const int p2 = DIR == 0 ? 2 : DIR == 1 ? 3 : 1;
+    const int p3 = DIR == 0 ? 3 : DIR == 1 ? 1 : 2;
+    T fw[5], bw[5];
+    fw[0] = T(u[c + d]); fw[1] = T(u[p1 * fs + c + d]); fw[2] = T(u[p2 * fs + c + d]);
+    fw[3] = T(u[p3 * fs + c + d]); fw[4] = T(u[4 * fs + c + d]);
+    bw[0] = T(u[c - d]); bw[1] = T(u[p1 * fs + c - d]); bw[2] = T(u[p2 * fs + c - d]);
+    bw[3] = T(u[p3 * fs + c - d]); bw[4] = T(u[4 * fs + c - d]);
+    if (DIR == 0) recon_x(cc, fw, bw, hi, lo);
+    else if (DIR == 1) recon_y(cc, fw, bw, hi, lo);
+    else recon_z(cc, fw, bw, hi, lo);
+}
+
+// Outer states of all domain-boundary faces (src/bounCondOnInterfaces.c:11-110).
+template <typename T>
+__global__ void k_bface(Grid g, int setup, int BL_HIG, Disturb d, const double *__restrict__ u, BF<T> bf)
+{
+    const int L = g.L, H = g.H, D = g.D;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nx = (long long)H * D, ny = (long long)L * D, nz = (long long)L * H;
+    const bool spatial = (setup == FSL_SETUP_SPATIAL);
+    typedef Kc<T> kc;
+    T hi[5], lo[5];
+    if (t < nx) {
+        const int jf = (int)(t / D), kf = (int)(t % D);
+        const int j = jf + 1, k = kf + 1;
+        const long long fo = t;
+        if (spatial) {
+            // inflow profile in the reference's FP64 arithmetic (:17-60)
+            const double P = 100000., R = 1.0;
+            double U, V = 0., W = 0., v[5];
+            if (jf < H / 2) {
+                U = 76.4;
+                v[0] = R; v[1] = R * U; v[2] = 0.; v[3] = 0.; v[4] = P / 0.4 + 0.5 * R * (U * U);
+            } else if (jf < H / 2 + BL_HIG) {
+                const unsigned ku = (unsigned)kf;
+                bool dist;
+                if (d.k_max > d.k_min) dist = (ku >= d.k_min && ku < d.k_max);
+                else dist = !(ku >= d.k_max && ku < d.k_min);
+                if (dist) { U = 200. + d.Ud; V = d.Vd; W = d.Wd; }
+                else { U = 200.; V = W = 0.; }
+                v[0] = R; v[1] = R * U; v[2] = R * V; v[3] = R * W;
+                v[4] = P / 0.4 + 0.5 * R * (U * U + V * V + W * W);
+            } else {
+                U = 200.;
+                v[0] = R; v[1] = R * U; v[2] = 0.; v[3] = 0.; v[4] = P / 0.4 + 0.5 * R * (U * U);
+            }
+#pragma unroll
+            for (int q = 0; q < 5; q++) bf.x0[q * nx + fo] = T(v[q]);
+            // :62-71 outflow from the minus state of face LEN
+            recon_at<T, 0>(g, u, g.idx(L, j, k), hi, lo);
+            const T r = hi[0], mu_ = hi[1], mv = hi[2], mw = hi[3];
+            const T P_ = T(100000.);
+            bf.xL[fo] = r; bf.xL[nx + fo] = mu_; bf.xL[2 * nx + fo] = mv; bf.xL[3 * nx + fo] = mw;
+            bf.xL[4 * nx + fo] = P_ / kc::K_1 + T(0.5) * (mu_ * mu_ + mv * mv + mw * mw) / r;
+        } else { // periodic x, the reference's z rule (:94-109)
+            recon_at<T, 0>(g, u, g.idx(L, j, k), hi, lo);
+#pragma unroll
+            for (int q = 0; q < 5; q++) bf.x0[q * nx + fo] = hi[q];
+            recon_at<T, 0>(g, u, g.idx(1, j, k), hi, lo);
+#pragma unroll
+            for (int q = 0; q < 5; q++) bf.xL[q * nx + fo] = lo[q];
+        }
+    } else if ((t -= nx) < ny) { // :75-90
+        const int i = (int)(t / D) + 1, k = (int)(t % D) + 1;
+        recon_at<T, 1>(g, u, g.idx(i, 1, k), hi, lo);
+#pragma unroll
+        for (int q = 0; q < 5; q++) bf.y0[q * ny + t] = (q == 2 && spatial) ? -lo[q] : lo[q];
+        recon_at<T, 1>(g, u, g.idx(i, H, k), hi, lo);
+#pragma unroll
+        for (int q = 0; q < 5; q++) bf.yH[q * ny + t] = (q == 2 && spatial) ? -hi[q] : hi[q];
+    } else if ((t -= ny) < nz) { // :94-109
+        const int i = (int)(t / H) + 1, j = (int)(t % H) + 1;
+        recon_at<T, 2>(g, u, g.idx(i, j, D), hi, lo);
+#pragma unroll
+        for (int q = 0; q < 5; q++) bf.z0[q * nz + t] = hi[q];
+        recon_at<T, 2>(g, u, g.idx(i, j, 1), hi, lo);
+#pragma unroll
+        for (int q = 0; q < 5; q++) bf.zD[q * nz + t] = lo[q];
+    }
+}
+
+template <typename T, int TJE> struct Smem {
+    T U[2][TJE + 2][34][5]; // current-stage state, planes i and i+1 (ring), halo 2
+    T R[3][TJE][32][3];     // velocities by reciprocal, planes i-1, i, i+1 (ring)
+    T Dv[2][TJE][32][5];    // velocities by division, temperature, mu face average, planes i, i+1
+    T Lo[TJE][32][5];       // y sweep: state on the face below each cell
+    T Fy[TJE][32][5];       // y flux on the face above each row
+};
+
+template <typename T> struct Args {
+    const double *cur; // current-stage state, ghost layer filled
+    const double *un;  // U^n
+    double *out;
+    const T *mu;
+    BF<T> bf;
+    const DevScalars *ds;
+    int stage;
+    int seg;
+};
+
+// Flux of one face (src/fluxes.c): Riemann state from the two face states,
+// viscous and heat flux from the two adjacent cells (vm/Tm minus side, vp/Tp
+// plus side, by division) and the eight tangential neighbours (by
+// reciprocal; P/M = plus/minus cell, h/l = +/- along the first (1) and
+// second (2) tangential axis).
+template <typename T, int N>
+__device__ __forceinline__ void fused_face(const T *Lm, const T *Rp, const T *vm, T Tm, const T *vp, T Tp,
+                                           const T *Ph1, const T *Mh1, const T *Pl1, const T *Ml1, const T *Ph2,
+                                           const T *Mh2, const T *Pl2, const T *Ml2, T muT, const Consts &kc, T *F)
+{
+    T Rho, P, vel[3];
+    riemann<T, N>(Lm, Rp, Rho, P, vel);
+    const int n0 = N - 1;
+    const int t1 = (N == 1) ? 1 : 0;
+    const int t2 = (N == 3) ? 1 : 2;
+    const T rdn = T(N == 1 ? kc.rdx : N == 2 ? kc.rdy : kc.rdz);
+    const T rt1 = T(N == 1 ? kc.r4dy : kc.r4dx);
+    const T rt2 = T(N == 3 ? kc.r4dy : kc.r4dz);
+    T gr[3][3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        gr[q][n0] = (vp[q] - vm[q]) * rdn;
+        gr[q][t1] = (Ph1[q] + Mh1[q] - Pl1[q] - Ml1[q]) * rt1;
+        gr[q][t2] = (Ph2[q] + Mh2[q] - Pl2[q] - Ml2[q]) * rt2;
+    }
+    face_flux<T, N>(Rho, P, vel, gr, vp, vm, Tp, Tm, T(kc.mu_L), muT, T(kc.lambda_L), T(kc.cp_Pr_T), rdn, F);
+}
+
+template <typename T> __device__ __forceinline__ void vdiv(const T *U, T *o)
+{
+    T Tt;
+    vel_div(U[0], U[1], U[2], U[3], U[4], o, Tt);
+    o[3] = Tt;
+}
+
+// Own column of plane `pl` (and, on the tile edge, the halo neighbour the y
+// and z sweeps need) from global memory into registers.
+// Kept in the storage type (FP64) while in flight: a conversion at load
+// time would wait on the load immediately.
+struct PlaneLoad {
+    double own[5], halo[5];
+};
+
+template <typename T, int TJE>
+__device__ __forceinline__ void plane_issue(const Grid &g, const double *__restrict__ cu, int pl, int r, int l, int j,
+                                            int k, bool live, PlaneLoad &p)
+{
+    const long long fs = g.fstride;
+    if (!live || pl > g.L + 1) return;
+    const long long c = g.idx(pl, j, k);
+    load5(cu, fs, c, p.own);
+    if (r == 0 && j >= 1) load5(cu, fs, c - g.pk, p.halo);
+    else if (r == TJE - 1 && j <= g.H) load5(cu, fs, c + g.pk, p.halo);
+    else if (l == 0 && k >= 1) load5(cu, fs, c - 1, p.halo);
+    else if (l == 31 && k <= g.D) load5(cu, fs, c + 1, p.halo);
+}
+
+template <typename T, int TJE>
+__device__ __forceinline__ void plane_store(Smem<T, TJE> &s, int slot, int r, int l, int j, int k, int H, int D,
+                                            bool live, const PlaneLoad &p)
+{
+    if (!live) return;
+#pragma unroll
+    for (int q = 0; q < 5; q++) s.U[slot][r + 1][l + 1][q] = T(p.own[q]);
+    T *h = nullptr;
+    if (r == 0 && j >= 1) h = s.U[slot][0][l + 1];
+    else if (r == TJE - 1 && j <= H) h = s.U[slot][TJE + 1][l + 1];
+    else if (l == 0 && k >= 1) h = s.U[slot][r + 1][0];
+    else if (l == 31 && k <= D) h = s.U[slot][r + 1][33];
+    if (h) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) h[q] = T(p.halo[q]);
+    }
+}
+
+// Velocities of plane `pl` (own column, from the shared ring) into the
+// reciprocal ring and the division plane with the face-averaged viscosity.
+template <typename T, int TJE>
+__device__ __forceinline__ void plane_prims(Smem<T, TJE> &s, int pl, int r, int l, T mu_pl, T mu_prev)
+{
+    const T *u = s.U[pl & 1][r + 1][l + 1];
+    vel_rcp(u[0], u[1], u[2], u[3], s.R[pl % 3][r][l]);
+    T dv[4];
+    vdiv(u, dv);
+    T *o = s.Dv[pl & 1][r][l];
+    o[0] = dv[0]; o[1] = dv[1]; o[2] = dv[2]; o[3] = dv[3];
+    o[4] = T(0.5) * (mu_pl + mu_prev);
+}
+
+template <typename T, int TJE, int MINB>
+__global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Args<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Smem<T, TJE> &s = *reinterpret_cast<Smem<T, TJE> *>(smraw);
+    const int L = g.L, H = g.H, D = g.D;
+    constexpr int TJ = TJE - 2;
+    const int r = threadIdx.y, l = threadIdx.x;
+    const int j = blockIdx.y * TJ + r;
+    const int k = blockIdx.x * 30 + l;
+    const int i0 = 1 + blockIdx.z * a.seg;
+    const int i1 = min(L, i0 + a.seg - 1);
+    const bool live = (j <= H + 1) && (k <= D + 1);
+    const bool inter = live && r >= 1 && r <= TJE - 2 && l >= 1 && l <= 30 && j <= H && k <= D;
+    const bool ycol = live && l >= 1 && l <= 30 && k <= D;     // column takes part in y faces
+    const bool zrow = live && r >= 1 && r <= TJE - 2 && j <= H; // row takes part in z faces
+    const long long fs = g.fstride;
+    const double *__restrict__ cu = a.cur;
+    const T *__restrict__ mu = a.mu;
+    const long long nxf = (long long)H * D, nyf = (long long)L * D, nzf = (long long)L * H;
+    const long long cj = g.idx(0, j, k); // column base (plane 0)
+
+    T hix[5], Fxp[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) hix[q] = Fxp[q] = T(0.);
+    T mu0 = 0, mu1 = 0, mu2 = 0; // mu of planes i, i+1, i+2 (own column)
+    PlaneLoad pl;
+#pragma unroll
+    for (int q = 0; q < 5; q++) pl.own[q] = pl.halo[q] = 0.;
+    double base[5], unv[5]; // FP64 operands of the stage combination, fetched early
+#pragma unroll
+    for (int q = 0; q < 5; q++) base[q] = unv[q] = 0.;
+
+    // ---- prologue: planes i0-1 .. i0+1, flux of face i0 - 1/2 ----
+    {
+        T Um[5] = {0, 0, 0, 0, 0}, mum = 0;
+        plane_issue<T, TJE>(g, cu, i0, r, l, j, k, live, pl);
+        plane_store<T, TJE>(s, i0 & 1, r, l, j, k, H, D, live, pl);
+        plane_issue<T, TJE>(g, cu, i0 + 1, r, l, j, k, live, pl);
+        plane_store<T, TJE>(s, (i0 + 1) & 1, r, l, j, k, H, D, live, pl);
+        if (live) {
+            load5(cu, fs, cj + (long long)(i0 - 1) * g.pi, Um);
+            vel_rcp(Um[0], Um[1], Um[2], Um[3], s.R[(i0 - 1) % 3][r][l]);
+            mum = mu[cj + (long long)(i0 - 1) * g.pi];
+            mu0 = mu[cj + (long long)i0 * g.pi];
+            mu1 = mu[cj + (long long)(i0 + 1) * g.pi];
+            plane_prims<T, TJE>(s, i0, r, l, mu0, mum);
+        }
+        __syncthreads();
+        if (inter) {
+            T hm[5], lo[5], hin[5], dm[4], tmp[5];
+            const T *Uc = s.U[i0 & 1][r + 1][l + 1], *Un = s.U[(i0 + 1) & 1][r + 1][l + 1];
+            {
+                CellC<T> cc;
+#pragma unroll
+                for (int q = 0; q < 5; q++) cc.u[q] = Uc[q];
+                cell_consts(cc);
+                recon_x(cc, Un, Um, hin, lo);
+            }
+            if (i0 == 1) {
+                const long long fo = (long long)(j - 1) * D + (k - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) hm[q] = a.bf.x0[q * nxf + fo];
+            } else {
+                recon_at<T, 0>(g, cu, cj + (long long)(i0 - 1) * g.pi, hm, tmp);
+            }
+            vdiv(Um, dm);
+            const T *dc = s.Dv[i0 & 1][r][l];
+            const int sb = (i0 - 1) % 3, sf = i0 % 3;
+            fused_face<T, 1>(hm, lo, dm, dm[3], dc, dc[3], s.R[sf][r + 1][l], s.R[sb][r + 1][l],
+                             s.R[sf][r - 1][l], s.R[sb][r - 1][l], s.R[sf][r][l + 1], s.R[sb][r][l + 1],
+                             s.R[sf][r][l - 1], s.R[sb][r][l - 1], dc[4], kc, Fxp);
+#pragma unroll
+            for (int q = 0; q < 5; q++) hix[q] = hin[q];
+        }
+    }
+    const double dtx = a.ds->dtx, dty = a.ds->dty, dtz = a.ds->dtz;
+    const double one_third = 1. / 3., two_thirds = 2. / 3.;
+    __syncthreads();
+
+    for (int i = i0; i <= i1; i++) {
+        const int sm1 = (i + 2) % 3, s0 = i % 3, sp1 = (i + 1) % 3;
+        const int u0 = i & 1, u1 = (i + 1) & 1;
+        // (a) issue plane i+2 loads; velocities of plane i+1
+        plane_issue<T, TJE>(g, cu, i + 2, r, l, j, k, live, pl);
+        if (inter) {
+            const long long c = cj + (long long)i * g.pi;
+            // FP32 bulk keeps only a converted copy of the state in shared
+            // memory; the FP64 operands of the combination are fetched here
+            if (sizeof(T) != 8) {
+#pragma unroll
+                for (int q = 0; q < 5; q++) base[q] = cu[q * fs + c];
+                if (a.stage != 1) {
+#pragma unroll
+                    for (int q = 0; q < 5; q++) unv[q] = a.un[q * fs + c];
+                }
+            }
+        }
+        if (live) {
+            if (i + 2 <= L + 1) mu2 = mu[cj + (long long)(i + 2) * g.pi];
+            plane_prims<T, TJE>(s, i + 1, r, l, mu1, mu0);
+        }
+        __syncthreads();
+        // (b) y and z reconstruction of cell (i, j, k)
+        T hy[5], hz[5], lz[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) hy[q] = hz[q] = lz[q] = T(0.);
+        {
+            const bool ry = ycol && j >= 1 && j <= H;
+            const bool rz = zrow && k >= 1 && k <= D;
+            if (ry || rz) {
+                CellC<T> cc;
+                const T *Uc = s.U[u0][r + 1][l + 1];
+#pragma unroll
+                for (int q = 0; q < 5; q++) cc.u[q] = Uc[q];
+                cell_consts(cc);
+                T fw[5], bw[5], lo[5];
+                if (ry) {
+                    const T *a1 = s.U[u0][r + 2][l + 1], *b1 = s.U[u0][r][l + 1];
+                    fw[0] = a1[0]; fw[1] = a1[2]; fw[2] = a1[3]; fw[3] = a1[1]; fw[4] = a1[4];
+                    bw[0] = b1[0]; bw[1] = b1[2]; bw[2] = b1[3]; bw[3] = b1[1]; bw[4] = b1[4];
+                    recon_y(cc, fw, bw, hy, lo);
+#pragma unroll
+                    for (int q = 0; q < 5; q++) s.Lo[r][l][q] = lo[q];
+                }
+                if (rz) {
+                    const T *a1 = s.U[u0][r + 1][l + 2], *b1 = s.U[u0][r + 1][l];
+                    fw[0] = a1[0]; fw[1] = a1[3]; fw[2] = a1[1]; fw[3] = a1[2]; fw[4] = a1[4];
+                    bw[0] = b1[0]; bw[1] = b1[3]; bw[2] = b1[1]; bw[3] = b1[2]; bw[4] = b1[4];
+                    recon_z(cc, fw, bw, hz, lz);
+                }
+            }
+            if (ycol && j == 0) {
+                const long long fo = (long long)(i - 1) * D + (k - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) hy[q] = a.bf.y0[q * nyf + fo];
+            }
+            if (ycol && j == H + 1) {
+                const long long fo = (long long)(i - 1) * D + (k - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) s.Lo[r][l][q] = a.bf.yH[q * nyf + fo];
+            }
+            if (zrow && k == 0) {
+                const long long fo = (long long)(i - 1) * H + (j - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) hz[q] = a.bf.z0[q * nzf + fo];
+            }
+            if (zrow && k == D + 1) {
+                const long long fo = (long long)(i - 1) * H + (j - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) lz[q] = a.bf.zD[q * nzf + fo];
+            }
+        }
+        __syncthreads();
+        // (c) y face above the cell: (i, j + 1/2), j in [0, HIG]
+        if (ycol && r <= TJE - 2 && j <= H) {
+            T F[5];
+            const T *vm = s.Dv[u0][r][l], *vp = s.Dv[u0][r + 1][l];
+            fused_face<T, 2>(hy, s.Lo[r + 1][l], vm, vm[3], vp, vp[3], s.R[sp1][r + 1][l], s.R[sp1][r][l],
+                             s.R[sm1][r + 1][l], s.R[sm1][r][l], s.R[s0][r + 1][l + 1], s.R[s0][r][l + 1],
+                             s.R[s0][r + 1][l - 1], s.R[s0][r][l - 1], vp[4], kc, F);
+#pragma unroll
+            for (int q = 0; q < 5; q++) s.Fy[r][l][q] = F[q];
+        }
+        // (d) z face nearer than the cell: (i, j, k + 1/2), k in [0, DEP]
+        T Fz[5], Fzm[5];
+        {
+            T lzn[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) lzn[q] = __shfl_down_sync(0xffffffffu, lz[q], 1);
+#pragma unroll
+            for (int q = 0; q < 5; q++) Fz[q] = T(0.);
+            if (zrow && l <= 30 && k <= D) {
+                const T *vm = s.Dv[u0][r][l], *vp = s.Dv[u0][r][l + 1];
+                fused_face<T, 3>(hz, lzn, vm, vm[3], vp, vp[3], s.R[sp1][r][l + 1], s.R[sp1][r][l],
+                                 s.R[sm1][r][l + 1], s.R[sm1][r][l], s.R[s0][r + 1][l + 1], s.R[s0][r + 1][l],
+                                 s.R[s0][r - 1][l + 1], s.R[s0][r - 1][l], vp[4], kc, Fz);
+            }
+#pragma unroll
+            for (int q = 0; q < 5; q++) Fzm[q] = __shfl_up_sync(0xffffffffu, Fz[q], 1);
+        }
+        // (e) x face (i + 1/2, j, k): reconstruct cell i+1, flux
+        T Fx[5], hin[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) Fx[q] = hin[q] = T(0.);
+        if (inter) {
+            T lo[5];
+            if (i + 1 <= L) {
+                CellC<T> cc;
+                const T *Un = s.U[u1][r + 1][l + 1];
+#pragma unroll
+                for (int q = 0; q < 5; q++) cc.u[q] = Un[q];
+                cell_consts(cc);
+                T fw2[5];
+#pragma unroll
+                for (int q = 0; q < 5; q++) fw2[q] = T(pl.own[q]);
+                recon_x(cc, fw2, s.U[u0][r + 1][l + 1], hin, lo);
+            } else {
+                const long long fo = (long long)(j - 1) * D + (k - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) lo[q] = a.bf.xL[q * nxf + fo];
+            }
+            const T *dc = s.Dv[u0][r][l], *dn = s.Dv[u1][r][l];
+            fused_face<T, 1>(hix, lo, dc, dc[3], dn, dn[3], s.R[sp1][r + 1][l], s.R[s0][r + 1][l],
+                             s.R[sp1][r - 1][l], s.R[s0][r - 1][l], s.R[sp1][r][l + 1], s.R[s0][r][l + 1],
+                             s.R[sp1][r][l - 1], s.R[s0][r][l - 1], dn[4], kc, Fx);
+        }
+        __syncthreads();
+        // (f) divergence and stage combination (src/evolution.c:29-161), FP64
+        if (inter) {
+            const long long c = cj + (long long)i * g.pi;
+            const T *Uc = s.U[u0][r + 1][l + 1];
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                const double X = dtx * ((double)Fxp[q] - (double)Fx[q]);
+                const double Y = dty * ((double)s.Fy[r - 1][l][q] - (double)s.Fy[r][l][q]);
+                const double Z = dtz * ((double)Fzm[q] - (double)Fz[q]);
+                // the stage state itself in FP64 (shared copy is exact for T = double)
+                const double b0 = sizeof(T) == 8 ? (double)Uc[q] : base[q];
+                if (sizeof(T) == 8 && a.stage != 1) unv[q] = a.un[q * fs + c];
+                double o;
+                if (a.stage == 1) o = b0 + X + Y + Z;
+                else if (a.stage == 2) o = 0.75 * unv[q] + 0.25 * (b0 + X + Y + Z);
+                else o = one_third * unv[q] + two_thirds * (b0 + X + Y + Z);
+                a.out[q * fs + c] = o;
+            }
+        }
+        // (g) plane i+2 into the ring slot of plane i (all readers of plane i
+        // passed the barrier above); advance the march
+        plane_store<T, TJE>(s, u0, r, l, j, k, H, D, live && i + 2 <= L + 1, pl);
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            Fxp[q] = Fx[q];
+            hix[q] = hin[q];
+        }
+        mu0 = mu1;
+        mu1 = mu2;
+    }
+}
+
+template <typename T, int TJE, int MINB>
+int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, double *out, const T *mu, BF<T> bf)
+{
+    const Grid &g = c.g;
+    Args<T> a;
+    a.cur = cur; a.un = un; a.out = out; a.mu = mu; a.bf = bf; a.ds = c.ds; a.stage = stage;
+    a.seg = c.stage_seg;
+    const size_t smem = sizeof(Smem<T, TJE>);
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_stage<T, TJE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return -1;
+        attr = true;
+    }
+    dim3 b(32, TJE, 1);
+    dim3 gr((g.D + 29) / 30, (g.H + TJE - 3) / (TJE - 2), (g.L + a.seg - 1) / a.seg);
+    prof_begin(c, FSL_K_STAGE);
+    k_stage<T, TJE, MINB><<<gr, b, smem, c.stream>>>(g, c.k, a);
+    prof_end(c, FSL_K_STAGE, 1);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+template <typename T> void launch_bface_t(Ctx &c, const double *cur, const Disturb &d, BF<T> bf)
+{
+    const Grid &g = c.g;
+    const long long n = (long long)g.H * g.D + (long long)g.L * g.D + (long long)g.L * g.H;
+    prof_begin(c, FSL_K_BC);
+    k_bface<T><<<(unsigned)((n + 127) / 128), 128, 0, c.stream>>>(g, c.k.setup, c.k.BL_HIG, d, cur, bf);
+    prof_end(c, FSL_K_BC, 1);
+}
+
+} // namespace stage
+} // namespace fsl

@@ -168,6 +168,37 @@ def test_steps_fused(fsl, oracle_lib, setup):
     _assert_same(a, b, "state after 8 fused steps")
 
 
+FP32_RTOL = 1e-5  # FP32 bulk: relative L2 of rho and E against the FP64 oracle after 8 steps
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_steps_fp32_bulk(fsl, oracle_lib, setup):
+    """FP32 reconstruction/fluxes with FP64 stage accumulation against the
+    FP64 oracle.  rho and E within FP32_RTOL; the momenta, normalised by the
+    largest momentum magnitude, within 1e-4."""
+    if setup == 0:
+        p = spatial_params(L=20, H=10, D=12)
+        from oracle.oracle import spatial_initial_state
+        s = spatial_initial_state(p)
+    else:
+        p = temporal_params(L=24, H=12, D=16)
+        s, _ = oracle_lib.Oracle.temporal_state(p, 0.4)
+    o = oracle_lib.Oracle(p)
+    o.set_state(s)
+    d = fsl.Domain(dict(p, precision=1))
+    d.upload_state(s)
+    o.step(8)
+    d.step(8)
+    a = d.download_state().reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    b = o.state().reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    assert np.all(np.isfinite(a))
+    errs = per_var_rel_l2(a, b, p)
+    assert errs[0] < FP32_RTOL and errs[4] < FP32_RTOL, errs
+    mscale = max(np.linalg.norm(b[:, :, v]) for v in (1, 2, 3))
+    for v in (1, 2, 3):
+        assert np.linalg.norm(a[:, :, v] - b[:, :, v]) / mscale < 1e-4, (v, errs)
+
+
 def test_sums_and_plane_sums(fsl, oracle_lib):
     p = temporal_params(L=16, H=8, D=8)
     s, _ = oracle_lib.Oracle.temporal_state(p, 0.4)
