@@ -81,6 +81,13 @@ class Info(C.Structure):
 
 
 K_CLASSES = ["stage", "recon", "flux", "sgs", "evol", "bc", "cfl", "other"]
+CLOSURE_NPARAMS = 9473
+
+
+class ClosureStats(C.Structure):
+    _fields_ = [("profile_err", C.c_double), ("cell_err", C.c_double), ("mu_profile_err", C.c_double),
+                ("judgements", C.c_int),
+                ("fallbacks", C.c_int), ("using_dynamic", C.c_int), ("last_step", C.c_uint)]
 
 
 class KTimes(C.Structure):
@@ -121,6 +128,21 @@ def lib():
             "fsl_get_faces": [vp, i, i, i, _dp], "fsl_set_faces": [vp, i, i, i, _dp],
             "fsl_set_cur": [vp, i], "fsl_sums": [vp, _dp], "fsl_plane_sums": [vp, _dp],
         }
+        fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+        ll = C.c_longlong
+        sig.update({
+            "fsl_closure_set_scales": [vp, d, d], "fsl_closure_set_weights": [vp, fp],
+            "fsl_closure_get_weights": [vp, fp], "fsl_closure_judge": [vp, i, d],
+            "fsl_closure_get_stats": [vp, C.POINTER(ClosureStats)],
+            "fsl_closure_compare": [vp, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double)],
+            "fsl_trainer_create": [ll, C.c_ulonglong, C.POINTER(C.c_void_p)],
+            "fsl_trainer_destroy": [vp], "fsl_trainer_harvest": [vp, vp, i],
+            "fsl_trainer_get_samples": [vp, fp, fp, ll], "fsl_trainer_set_samples": [vp, fp, fp, ll],
+            "fsl_trainer_get_weights": [vp, fp], "fsl_trainer_set_weights": [vp, fp],
+            "fsl_trainer_gradient": [vp, ll, fp, C.POINTER(C.c_double)], "fsl_trainer_set_loss": [vp, i],
+            "fsl_trainer_train": [vp, i, ll, d, C.POINTER(C.c_double)],
+        })
         sig["fsl_tune"] = [vp, i, i]
         sig["fsl_profile"] = [vp, i]
         sig["fsl_profile_read"] = [vp, C.POINTER(KTimes)]
@@ -132,6 +154,8 @@ def lib():
         L.fsl_last_error.restype = C.c_char_p
         L.fsl_stream.argtypes = [vp]
         L.fsl_stream.restype = C.c_void_p
+        L.fsl_trainer_size.argtypes = [vp]
+        L.fsl_trainer_size.restype = C.c_longlong
         _lib = L
     return _lib
 
@@ -317,6 +341,36 @@ class Domain:
     def set_cur(self, which: int):
         self._c(lib().fsl_set_cur(self.h, which))
 
+    # --- learned closure ----------------------------------------------------------
+    def closure_set_scales(self, t_ref: float, len_ref: float):
+        self._c(lib().fsl_closure_set_scales(self.h, t_ref, len_ref))
+
+    def closure_set_weights(self, params: np.ndarray):
+        self._c(lib().fsl_closure_set_weights(self.h, np.ascontiguousarray(params, np.float32)))
+
+    def closure_get_weights(self) -> np.ndarray:
+        out = np.empty(CLOSURE_NPARAMS, np.float32)
+        self._c(lib().fsl_closure_get_weights(self.h, out))
+        return out
+
+    def closure_judge(self, every: int, threshold: float):
+        self._c(lib().fsl_closure_judge(self.h, every, threshold))
+
+    def closure_stats(self) -> ClosureStats:
+        s = ClosureStats()
+        self._c(lib().fsl_closure_get_stats(self.h, C.byref(s)))
+        return s
+
+    def closure_compare(self, fields: bool = False):
+        """(Cs2 profile err, Cs2 cell err, mu profile err[, cs2_mlp, cs2_dyn]) on U^n."""
+        pe, ce, me = C.c_double(), C.c_double(), C.c_double()
+        a = np.empty(self.padded_shape, np.float32) if fields else None
+        b = np.empty(self.padded_shape, np.float32) if fields else None
+        self._c(lib().fsl_closure_compare(self.h, a.ctypes.data if fields else None,
+                                          b.ctypes.data if fields else None, C.byref(pe), C.byref(ce),
+                                          C.byref(me)))
+        return (pe.value, ce.value, me.value, a, b) if fields else (pe.value, ce.value, me.value)
+
     TUNE_STAGE_ROWS, TUNE_STAGE_SEG = 1, 2
 
     def tune(self, key: int, value: int):
@@ -347,3 +401,67 @@ class Domain:
         out = np.empty(8 * self.p.HIG, np.float64)
         self._c(lib().fsl_plane_sums(self.h, out))
         return out.reshape(self.p.HIG, 8)
+
+
+class Trainer:
+    """Training of the learned closure on (features, dynamic Cs^2) samples
+    harvested on the GPU; forward and backward run on the tensor cores."""
+
+    def __init__(self, capacity: int, seed: int = 1):
+        h = C.c_void_p()
+        _check(lib().fsl_trainer_create(capacity, seed, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fsl_trainer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def size(self) -> int:
+        return lib().fsl_trainer_size(self.h)
+
+    def harvest(self, domain: "Domain", stride: int = 1):
+        _check(lib().fsl_trainer_harvest(self.h, domain.h, stride), domain.h)
+
+    def samples(self, n: int | None = None):
+        n = self.size if n is None else n
+        X = np.empty((n, 8), np.float32)
+        Y = np.empty(n, np.float32)
+        _check(lib().fsl_trainer_get_samples(self.h, X, Y, n))
+        return X, Y
+
+    def set_samples(self, X: np.ndarray, Y: np.ndarray):
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(Y, np.float32)
+        _check(lib().fsl_trainer_set_samples(self.h, X, Y, len(Y)))
+
+    def weights(self) -> np.ndarray:
+        out = np.empty(CLOSURE_NPARAMS, np.float32)
+        _check(lib().fsl_trainer_get_weights(self.h, out))
+        return out
+
+    def set_weights(self, p: np.ndarray):
+        _check(lib().fsl_trainer_set_weights(self.h, np.ascontiguousarray(p, np.float32)))
+
+    def set_loss(self, mode: int):
+        """0: MSE of Cs^2; 1: squared error of mu_SGS (samples weighted by (rho |S| t_ref)^2)."""
+        _check(lib().fsl_trainer_set_loss(self.h, mode))
+
+    def gradient(self, n: int | None = None):
+        n = self.size if n is None else n
+        g = np.empty(CLOSURE_NPARAMS, np.float32)
+        loss = C.c_double()
+        _check(lib().fsl_trainer_gradient(self.h, n, g, C.byref(loss)))
+        return g, loss.value
+
+    def train(self, epochs: int, batch: int = 65536, lr: float = 1e-3) -> float:
+        loss = C.c_double()
+        _check(lib().fsl_trainer_train(self.h, epochs, batch, lr, C.byref(loss)))
+        return loss.value

@@ -15,9 +15,6 @@
 
 using namespace fsl;
 
-struct fsl_ctx {
-    Ctx c;
-};
 
 namespace fsl {
 
@@ -190,6 +187,14 @@ int ensure_fp32(Ctx &c)
 }
 
 double *cur_ptr(Ctx &c) { return c.cur ? c.Up : c.U; }
+
+} // namespace
+
+namespace fsl {
+int ensure_dyn_scratch(Ctx &c) { return ensure_dyn(c); }
+} // namespace fsl
+
+namespace {
 
 // Disturbance draw of src/layer2.c:152-162 with Random() of src/helpers.c:13-17.
 double rnd(double x)
@@ -474,6 +479,7 @@ int fsl_destroy(fsl_ctx *h)
         cudaFree(c.bf.x0); cudaFree(c.bf.xL); cudaFree(c.bf.y0);
         cudaFree(c.bf.yH); cudaFree(c.bf.z0); cudaFree(c.bf.zD);
     }
+    closure_free(c);
     if (c.fp32_alloc) {
         cudaFree(c.bf32.x0); cudaFree(c.bf32.xL); cudaFree(c.bf32.y0);
         cudaFree(c.bf32.yH); cudaFree(c.bf32.z0); cudaFree(c.bf32.zD); cudaFree(c.mu32);
@@ -703,8 +709,12 @@ int fsl_step(fsl_ctx *h, int nsteps)
             draw(c);
             launch_ghost(c, c.U);
             launch_bface32(c, c.U, c.dist);
-            launch_dynsmag(c, c.U);
-            launch_mu_to_f32(c);
+            if (c.p.sgs == FSL_SGS_LEARNED) {
+                if ((rc = closure_step_sgs(c))) return rc;
+            } else {
+                launch_dynsmag(c, c.U);
+                launch_mu_to_f32(c);
+            }
             if (launch_stage32(c, 1, c.U, c.U, c.Up)) return fail(c, FSL_ERR_CUDA, "FP32 stage kernel");
             launch_ghost(c, c.Up);
             launch_bface32(c, c.Up, c.dist);
@@ -722,7 +732,11 @@ int fsl_step(fsl_ctx *h, int nsteps)
         draw(c);
         launch_ghost(c, c.U);
         launch_bface(c, c.U, c.dist);
-        launch_dynsmag(c, c.U);
+        if (c.p.sgs == FSL_SGS_LEARNED) {
+            if ((rc = closure_step_sgs(c))) return rc;
+        } else {
+            launch_dynsmag(c, c.U);
+        }
         if (launch_stage(c, 1, c.U, c.U, c.Up)) return fail(c, FSL_ERR_CUDA, "stage kernel attribute");
         launch_ghost(c, c.Up);
         launch_bface(c, c.Up, c.dist);

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/fsl_gpu.h"
+#include "fsl_mlp.h"
 
 namespace fsl {
 
@@ -99,6 +100,22 @@ struct Ctx {
     bool fp32_alloc = false;
     int stage_tje = 16; // rows per fused-stage tile (incl. the two halo rows)
     int stage_seg = 32; // x planes per fused-stage block
+    // learned closure
+    ClosureScales cls{};
+    float *cl_params = nullptr; // FP32 parameter vector (kNParams)
+    float *cd32 = nullptr;      // dynamic-procedure Cs^2, padded FP32
+    float *cs2_32 = nullptr;    // closure Cs^2, padded FP32
+    double *mu_alt = nullptr;   // closure mu on judgement steps (FP64 path)
+    float *mu32_alt = nullptr;  // closure mu on judgement steps (FP32 path)
+    int *cl_err = nullptr;      // device error flag of the tensor-core kernels
+    double *judge_rows = nullptr; // [2][HIG][4] plane sums of the judgement (Cs^2, mu_SGS)
+    bool cl_alloc = false, cl_weights = false;
+    int judge_every = 100;
+    double judge_thr = 0.35;
+    bool using_dynamic = false;
+    int judgements = 0, fallbacks = 0;
+    double last_perr = -1, last_cerr = -1, last_merr = -1;
+    unsigned last_judge_step = 0;
     DevScalars *ds = nullptr; // device scalars
     DevScalars *hs = nullptr; // pinned host mirror
     double *partials = nullptr;
@@ -132,13 +149,21 @@ struct Ctx {
 void prof_begin(Ctx &c, int cls);
 void prof_end(Ctx &c, int cls, int nkernels);
 
+int ensure_dyn_scratch(Ctx &c);  // SGS scratch of the dynamic procedure (fsl_api.cu)
+int closure_step_sgs(Ctx &c);    // SGS of one step under FSL_SGS_LEARNED (fsl_closure.cu)
+int closure_ensure(Ctx &c);
+void closure_free(Ctx &c);
+
 // ---- launchers (fsl_phase.cu) ------------------------------------------------
 void launch_ghost(Ctx &c, double *cur);
 void launch_recon(Ctx &c, const double *cur);
 void launch_ifbc(Ctx &c, const Disturb &d);
 void launch_fluxes(Ctx &c, const double *cur);
 void launch_evolution(Ctx &c, int nstages, int stage);
-void launch_dynsmag(Ctx &c, const double *U);
+void launch_dynsmag(Ctx &c, const double *U, float *cd = nullptr); // cd: optional Cs^2 output
+void launch_judge_rows(Ctx &c, const float *a, const float *b, double *rows);
+void launch_judge_rows(Ctx &c, const float *a, const double *b, double *rows);
+void launch_judge_rows(Ctx &c, const double *a, const double *b, double *rows);
 void launch_courant(Ctx &c);
 void launch_state_scatter(Ctx &c, double *dst, const double *packed);
 void launch_state_gather(Ctx &c, const double *src, double *packed);
@@ -154,4 +179,19 @@ void launch_bface32(Ctx &c, const double *cur, const Disturb &d);
 int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out);
 void launch_mu_to_f32(Ctx &c); // mu (FP64) -> mu32
 
+// ---- learned closure (fsl_mlp.cu) ---------------------------------------------
+int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, float *cs2_out, const float *P,
+                         int *err);
+void launch_harvest(Ctx &c, const float *cd, long long stride, long long offset, float *X, float *Y, long long cap,
+                    long long base);
+int launch_train_grad(cudaStream_t st, const float *X, const float *Y, long long n, int tpb, const float *P,
+                      float *Gpart, float *loss_part, int *err, int *nblk_out, float inv_wmean);
+void launch_reduce_adam(cudaStream_t st, const float *Gpart, int nblk, float *P, float *M, float *V, float *Gout,
+                        float lr, float b1t, float b2t);
+
 } // namespace fsl
+
+// The opaque handle of the C ABI.
+struct fsl_ctx {
+    fsl::Ctx c;
+};

@@ -565,7 +565,7 @@ __global__ void k_dyn_mid(Grid g, Consts kc, const double *__restrict__ vel, con
 // (:398-445).
 __global__ void k_dyn_final(Grid g, Consts kc, const double *__restrict__ rho, const double *__restrict__ Lst,
                             const double *__restrict__ B, const double *__restrict__ Ahat,
-                            const double *__restrict__ Smag, double *__restrict__ mu)
+                            const double *__restrict__ Smag, double *__restrict__ mu, float *__restrict__ cd = nullptr)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -591,6 +591,43 @@ __global__ void k_dyn_final(Grid g, Consts kc, const double *__restrict__ rho, c
     if (Cd > 0.15) Cd = 0.15;
     else if (Cd < 0.0) Cd = 0.0;
     mu[c] = rho[c] * Cd * DD * Smag[c];
+    if (cd) cd[c] = (float)Cd; // Cs^2 for the learned closure's harvest and judgement
+}
+
+// Per y row: sums over the x-z plane of a, b, (a-b)^2 and b^2 (two padded
+// fields) -- the judgement of the learned closure, over the band two cells
+// away from every boundary (nearer, the dynamic procedure's values carry the
+// zero padding of the reference's test filter); rows outside it are zero.
+template <typename TA, typename TB>
+__global__ void k_judge_rows(Grid g, const TA *__restrict__ a, const TB *__restrict__ b,
+                             double *__restrict__ rows)
+{
+    const int j = blockIdx.x + 1;
+    const int bL = g.L - 4, bD = g.D - 4;
+    const long long n = (j >= 3 && j <= g.H - 2) ? (long long)bL * bD : 0;
+    double s[4] = {0, 0, 0, 0};
+    for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+        const int k = (int)(t % bD) + 3;
+        const int i = (int)(t / bD) + 3;
+        const long long c = g.idx(i, j, k);
+        const double x = a[c], y = b[c];
+        s[0] += x; s[1] += y; s[2] += (x - y) * (x - y); s[3] += y * y;
+    }
+    __shared__ double sm[4][32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        double x = s[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (l == 0) sm[q][w] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double x = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) x += sm[threadIdx.x][q];
+        rows[(long long)blockIdx.x * 4 + threadIdx.x] = x;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -756,7 +793,7 @@ void launch_evolution(Ctx &c, int nstages, int stage)
     prof_end(c, FSL_K_EVOL, 1);
 }
 
-void launch_dynsmag(Ctx &c, const double *U)
+void launch_dynsmag(Ctx &c, const double *U, float *cd)
 {
     const Grid &g = c.g;
     DynScratch &s = c.dyn;
@@ -773,7 +810,7 @@ void launch_dynsmag(Ctx &c, const double *U)
     k_filt_y<<<cells_grid(g, b, g.L + 1, g.H, g.D + 1), b, 0, c.stream>>>(g, 6, s.A, s.t1);
     k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, c.stream>>>(g, 6, s.t1, s.t2);
     k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, c.stream>>>(g, 6, s.t2, s.t1);
-    k_dyn_final<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, c.k, U, s.Lst, s.B, s.t1, s.S, c.mu);
+    k_dyn_final<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, c.k, U, s.Lst, s.B, s.t1, s.S, c.mu, cd);
     prof_end(c, FSL_K_SGS, 9);
 }
 
@@ -809,6 +846,16 @@ void launch_sums(Ctx &c, const double *U, double *out5)
     k_sums_final<<<1, 32, 0, c.stream>>>(c.partials, nb, vol, out5);
     prof_end(c, FSL_K_OTHER, 2);
 }
+
+template <typename TA, typename TB> static void judge_rows_t(Ctx &c, const TA *a, const TB *b, double *rows)
+{
+    prof_begin(c, FSL_K_OTHER);
+    k_judge_rows<TA, TB><<<c.g.H, 256, 0, c.stream>>>(c.g, a, b, rows);
+    prof_end(c, FSL_K_OTHER, 1);
+}
+void launch_judge_rows(Ctx &c, const float *a, const float *b, double *rows) { judge_rows_t(c, a, b, rows); }
+void launch_judge_rows(Ctx &c, const float *a, const double *b, double *rows) { judge_rows_t(c, a, b, rows); }
+void launch_judge_rows(Ctx &c, const double *a, const double *b, double *rows) { judge_rows_t(c, a, b, rows); }
 
 void launch_plane_sums(Ctx &c, const double *U, double *rows)
 {

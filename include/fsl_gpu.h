@@ -234,6 +234,64 @@ int fsl_set_faces(fsl_ctx *ctx, int dir, int side, int var, const double *faces)
 /* Point U*_ at U^n (0) or at the stage buffer (1). */
 int fsl_set_cur(fsl_ctx *ctx, int which);
 
+/* ---- learned subgrid closure ---------------------------------------------------
+ * No counterpart in the reference (project extension).  A per-cell MLP
+ * 8 -> 64 -> 64 -> 64 -> 1 (SiLU; BF16 weights and activations, FP32
+ * accumulation on the tensor cores) maps the local strain rate |S| (as
+ * log(1 + |S| t_ref)), the five independent strain-rate components over |S|,
+ * the density and the filter width over len_ref to the Smagorinsky
+ * coefficient Cs^2; mu_SGS = rho Cs^2 (dx dy dz)^(2/3) |S| as in the dynamic
+ * procedure (src/turbulence.c:442).  With params.sgs = FSL_SGS_LEARNED the
+ * steps use it; every `every` steps the dynamic procedure runs beside it as the
+ * judge, and while the error of the plane-averaged SGS viscosity profile
+ * <mu_SGS>(y) exceeds the threshold the steps fall back to the dynamic
+ * procedure (the Cs^2 errors are reported too; per cell the dynamic Cs^2 is
+ * dominated by cell-to-cell noise, and where |S| vanishes it does not act). */
+#define FSL_CLOSURE_NPARAMS 9473 /* W1[64][16] b1 W2[64][64] b2 W3[64][64] b3 w4[64] b4 */
+
+typedef struct fsl_closure_stats {
+    double profile_err;    /* last judgement: |<Cs2_mlp>(y) - <Cs2_dyn>(y)|_2 / |<Cs2_dyn>(y)|_2 */
+    double cell_err;       /* last judgement: |Cs2_mlp - Cs2_dyn|_2 / |Cs2_dyn|_2 over cells */
+    double mu_profile_err; /* last judgement: the same profile error of mu_SGS (the fallback criterion) */
+    int judgements, fallbacks, using_dynamic;
+    unsigned last_step;
+} fsl_closure_stats;
+
+/* Feature scales: t_ref = delta_w0 / dU (time scale of |S|), len_ref = delta_w0. */
+int fsl_closure_set_scales(fsl_ctx *ctx, double t_ref, double len_ref);
+int fsl_closure_set_weights(fsl_ctx *ctx, const float *params);
+int fsl_closure_get_weights(fsl_ctx *ctx, float *params);
+int fsl_closure_judge(fsl_ctx *ctx, int every, double threshold);
+int fsl_closure_get_stats(fsl_ctx *ctx, fsl_closure_stats *stats);
+/* Both closures on the current U^n: Cs^2 of the MLP and of the dynamic
+ * procedure (padded FP32 host arrays, either may be NULL) and the three errors
+ * of fsl_closure_stats. */
+int fsl_closure_compare(fsl_ctx *ctx, float *cs2_mlp, float *cs2_dyn, double *profile_err, double *cell_err,
+                        double *mu_profile_err);
+
+/* Training on (features, dynamic Cs^2) samples harvested on the GPU. */
+typedef struct fsl_trainer fsl_trainer;
+int fsl_trainer_create(long long capacity, unsigned long long seed, fsl_trainer **tr);
+int fsl_trainer_destroy(fsl_trainer *tr);
+/* Append every stride-th cell of ctx's U^n at least two cells from every
+ * boundary, with the dynamic procedure's Cs^2 (nearer the boundary that value
+ * carries the zero padding of the reference's test filter).  Judgements use
+ * the same band. */
+int fsl_trainer_harvest(fsl_trainer *tr, fsl_ctx *ctx, int stride);
+long long fsl_trainer_size(fsl_trainer *tr);
+int fsl_trainer_get_samples(fsl_trainer *tr, float *X, float *Y, long long n); /* first n: X[n][8], Y[n] */
+int fsl_trainer_set_samples(fsl_trainer *tr, const float *X, const float *Y, long long n);
+int fsl_trainer_get_weights(fsl_trainer *tr, float *params);
+int fsl_trainer_set_weights(fsl_trainer *tr, const float *params);
+/* Loss: 0 = mean squared error of Cs^2; 1 (default) = each sample weighted by
+ * (rho |S| t_ref)^2 over the mean weight of all samples, i.e. the squared
+ * error of mu_SGS = rho Cs^2 DD |S| the closure feeds into the fluxes. */
+int fsl_trainer_set_loss(fsl_trainer *tr, int mode);
+/* Loss gradient over the first n samples at the current weights. */
+int fsl_trainer_gradient(fsl_trainer *tr, long long n, float *grad, double *loss);
+/* Adam on shuffled mini-batches; *loss receives the final full-set MSE. */
+int fsl_trainer_train(fsl_trainer *tr, int epochs, long long batch, double lr, double *loss);
+
 /* ---- profiling ------------------------------------------------------------- */
 
 /* Kernel classes timed by the context's profiler. */
