@@ -1,0 +1,116 @@
+"""Train the learned subgrid closure on the dynamic procedure's Cs^2.
+
+    python -m freeshearlayer_b200.train_closure --out freeshearlayer_b200/closure_weights.f32
+
+Runs temporal shear layers on the GPU (FP32 bulk, dynamic Smagorinsky) at
+convective Mach 0.3, 0.5 and 0.7 on a 256x128x128 and a 512x256x256 grid
+(box 2pi x pi x pi, Re_dw0 1000), harvests (features, dynamic Cs^2) samples
+every 50 steps, trains the MLP with Adam on the tensor-core kernels and writes
+the FP32 parameter vector (FSL_CLOSURE_NPARAMS little-endian floats).  The
+initial velocity noise is 5% of dU so that the layers develop small scales
+within a few hundred steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_WEIGHTS = os.path.join(HERE, "closure_weights.f32")
+
+
+def shear_params(grid, Mc, Re=1000.0, precision=1):
+    L, H, D = grid
+    dU = 2.0 * Mc * math.sqrt(1.4 * 1e5 / 1.0)
+    return dict(LEN=L, HIG=H, DEP=D, deltaX=2 * math.pi / L, deltaY=math.pi / H, deltaZ=math.pi / D,
+                deltaT=1e-5, Answer=0, numstep=0, mu_L=dU * 1.0 / Re, Pr_L=0.72, Pr_T=0.8, Cs=0.01,
+                BL_HIG=0, Ua=0.0, Va=0.0, Wa=0.0, Ns_min=10, Nst=50, f_step=50, nStages=3,
+                maxCoNum=0.5, setup=1, cfl_mode=1, seed_X=0.317391239817, precision=precision,
+                sgs=0, recon=0), dU
+
+
+def load_weights(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
+    w = np.fromfile(path, dtype="<f4")
+    if w.size != 9473:
+        raise ValueError("%s: expected 9473 float32 parameters, found %d" % (path, w.size))
+    return w
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--grids", default="256x128x128,512x256x256")
+    ap.add_argument("--mach", default="0.3,0.5,0.7")
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--every", type=int, default=50)
+    ap.add_argument("--samples", type=float, default=2e8, help="target number of harvested samples")
+    ap.add_argument("--amp", type=float, default=0.05)
+    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=20251203)
+    args = ap.parse_args(argv)
+    sys.path.insert(0, os.path.dirname(HERE))
+    import freeshearlayer_b200 as fsl
+
+    grids = [tuple(int(x) for x in g.split("x")) for g in args.grids.split(",")]
+    machs = [float(m) for m in args.mach.split(",")]
+    nsnap = args.steps // args.every
+    per_snap = args.samples / (len(grids) * len(machs) * nsnap)
+    tr = fsl.Trainer(int(args.samples * 1.05) + 1, seed=args.seed)
+    log = {"runs": []}
+    t0 = time.time()
+    for grid in grids:
+        band = (grid[0] - 4) * (grid[1] - 4) * (grid[2] - 4)
+        stride = max(1, int(math.ceil(band / per_snap)))
+        for Mc in machs:
+            p, dU = shear_params(grid, Mc)
+            state, _ = fsl.temporal_state(p, Mc, 1.0, args.amp, args.seed + int(Mc * 10))
+            d = fsl.Domain(p)
+            d.upload_state(state)
+            d.closure_set_scales(1.0 / dU, 1.0)
+            for _ in range(nsnap):
+                d.step(args.every)
+                d.sync()
+                tr.harvest(d, stride)
+            log["runs"].append({"grid": list(grid), "Mc": Mc, "stride": stride, "samples": tr.size})
+            print("harvest %s Mc %.1f stride %d -> %d samples (%.0f s)" % (grid, Mc, stride, tr.size,
+                                                                       time.time() - t0), flush=True)
+            d.close()
+    X, Y = tr.samples(min(tr.size, 1 << 20))
+    p0 = tr.weights()
+    p0[9472] = float(np.mean(Y))
+    tr.set_weights(p0)
+    _, loss0 = tr.gradient()
+    t1 = time.time()
+    loss = tr.train(epochs=args.epochs, batch=args.batch, lr=args.lr)
+    t2 = time.time()
+    w = tr.weights()
+    w.astype("<f4").tofile(args.out)
+    log.update({"samples": tr.size, "loss0": loss0, "loss": loss, "epochs": args.epochs,
+                "batch": args.batch, "lr": args.lr, "train_s": t2 - t1,
+                "samples_per_s": tr.size * args.epochs / max(t2 - t1, 1e-9)})
+    # judge the trained closure on a fresh run of each Mach number (smaller grid)
+    for Mc in machs:
+        p, dU = shear_params(grids[0], Mc)
+        state, _ = fsl.temporal_state(p, Mc, 1.0, args.amp, args.seed + 99 + int(Mc * 10))
+        d = fsl.Domain(p)
+        d.upload_state(state)
+        d.closure_set_scales(1.0 / dU, 1.0)
+        d.closure_set_weights(w)
+        d.step(args.steps)
+        pe, ce, me = d.closure_compare()
+        log.setdefault("judge", []).append({"Mc": Mc, "cs2_profile_err": pe, "cs2_cell_err": ce,
+                                            "mu_profile_err": me})
+        d.close()
+    print(json.dumps(log), flush=True)
+
+
+if __name__ == "__main__":
+    main()
