@@ -11,7 +11,16 @@ One step = one full RK3 step (Courant rescale, disturbance draw, three stages,
 SGS viscosity once per step).  value = cells * 3 * steps / device seconds,
 max over ranks, summed over replicas (one independent domain per GPU).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W]
+The headline arm (--arm fp32-learned) is the FP32-bulk step with the learned
+closure (weights shipped in freeshearlayer_b200/closure_weights.f32) and the
+dynamic procedure as judge every 100 steps.  Beside it the same box times the
+plain FP64 dynamic-Smagorinsky path (plain_fp64, speedup_vs_plain_fp64) and,
+from the same initial state, advances FP64, FP32 + dynamic and FP32 + learned
+for --match-steps steps and reports per-variable relative L2 against FP64,
+momentum-thickness growth and Reynolds-stress profile differences
+(matched_error).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--arm ARM]
     python bench.py --impl reference ...   # the reference's serial CPU solver
 
 Prints exactly one JSON line on rank 0.
@@ -190,6 +199,126 @@ def measured_peaks() -> dict:
 # ---------------------------------------------------------------------------
 # the GPU arm
 # ---------------------------------------------------------------------------
+ARMS = {"fp32-learned": (1, 1), "fp32-dynamic": (1, 0), "fp64-dynamic": (0, 0), "fp64-learned": (0, 1)}
+ARM_NAMES = {"fp32-learned": "FP32 bulk (FP64 RK accumulation), learned closure judged by the dynamic "
+                             "procedure every 100 steps",
+             "fp32-dynamic": "FP32 bulk (FP64 RK accumulation), dynamic Smagorinsky",
+             "fp64-dynamic": "plain FP64, dynamic Smagorinsky",
+             "fp64-learned": "FP64, learned closure judged by the dynamic procedure every 100 steps"}
+# Algorithmic HBM bytes per cell of one fused stage launch (each array read or
+# written once, halo re-reads not counted), averaged over the three RK3 stages:
+#   FP64:  stage 1 reads U^n 40 + mu 8, writes 40 (88 B); stages 2, 3 read
+#          U^(s) 40 + U^n 40 + mu 8, write 40 (128 B each)   -> 114.67 B
+#   FP32 bulk with FP64 stage buffers: mu is FP32 (4 B)    -> 110.67 B
+STAGE_BYTES = {0: (88.0 + 128.0 + 128.0) / 3.0, 1: (84.0 + 124.0 + 124.0) / 3.0}
+
+
+def make_domain(fsl, grid, arm, state, dU, rows=0, seg=0):
+    prec, sgs = ARMS[arm]
+    d = fsl.Domain(workload_params(grid, precision=prec, sgs=sgs))
+    if rows:
+        d.tune(d.TUNE_STAGE_ROWS, rows)
+    if seg:
+        d.tune(d.TUNE_STAGE_SEG, seg)
+    d.upload_state(state)
+    if sgs == 1:
+        d.closure_set_scales(DW0 / dU, DW0)
+        d.closure_set_weights(fsl.closure_weights())
+    return d
+
+
+def time_steps(torch, d, run, steps, barrier, clocks=None):
+    """K steps bracketed by barrier + synchronize; CUDA events on the domain's stream."""
+    ext = torch.cuda.ExternalStream(d.stream)
+    d.profile(True)
+    barrier()
+    torch.cuda.synchronize()
+    d.sync()
+    if clocks:
+        clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    run(steps)
+    e1.record(ext)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop() if clocks else None
+    kt = d.profile_read()
+    d.profile(False)
+    d.sync()  # raises on a non-finite state
+    return ms, kt, clk
+
+
+def stage_roofline(kt, names, ncell, prec, peaks, traffic):
+    kms = {names[i]: kt.ms[i] for i in range(8)}
+    kl = {names[i]: int(kt.launches[i]) for i in range(8)}
+    launches = max(kl["stage"], 1)
+    alg = STAGE_BYTES[prec] * ncell
+    avg_ms = kms["stage"] / launches
+    achieved = alg / (avg_ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": "k_stage<%s> (fused reconstruction + Riemann + viscous flux + "
+                                       "divergence + RK stage)" % ("double" if prec == 0 else "float"),
+            "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
+            "peak_source": peaks["source"] + " HBM copy bandwidth (burst)",
+            "alg_bytes_per_cell": round(STAGE_BYTES[prec], 2), "alg_bytes_per_launch": alg,
+            "avg_launch_ms": round(avg_ms, 4), "launches": launches}, kms, kl
+
+
+def rel_l2(a, b):
+    import numpy as np
+    return [float(np.linalg.norm(a[v] - b[v]) / max(np.linalg.norm(b[v]), 1e-300)) for v in range(5)]
+
+
+def matched_error(fsl, grid, state, dU, nsteps, rows, seg):
+    """Advance the same initial state nsteps with the plain FP64 path, FP32
+    bulk + dynamic and FP32 bulk + learned closure; compare the conserved
+    variables, momentum thickness growth and Reynolds-stress profiles."""
+    import numpy as np
+    L, H, D = grid
+    dy = math.pi / H
+    out = {"steps": nsteps}
+    res = {}
+    for arm in ("fp64-dynamic", "fp32-dynamic", "fp32-learned"):
+        d = make_domain(fsl, grid, arm, state, dU, rows, seg)
+        s0 = fsl.shear_statistics(d.plane_sums(), L * D, dU, dy)
+        d.step(nsteps)
+        d.sync()
+        s1 = fsl.shear_statistics(d.plane_sums(), L * D, dU, dy)
+        u = d.download_state().reshape(L, H, 5, D).transpose(2, 0, 1, 3).copy()
+        cst = d.closure_stats() if ARMS[arm][1] else None
+        res[arm] = (u, s0, s1, cst)
+        d.close()
+    ref_u, ref_s0, ref_s1, _ = res["fp64-dynamic"]
+    g_ref = ref_s1["theta"] - ref_s0["theta"]
+    out["theta0"] = ref_s0["theta"]
+    out["theta_growth_fp64"] = g_ref
+    for arm in ("fp32-dynamic", "fp32-learned"):
+        u, s0, s1, cst = res[arm]
+        g = s1["theta"] - s0["theta"]
+        rs = {}
+        for comp in ("R11", "R22", "R33", "R12"):
+            den = float(np.max(np.abs(ref_s1[comp])))
+            rs[comp] = float(np.max(np.abs(s1[comp] - ref_s1[comp])) / den) if den > 0 else None
+        mom = float(np.sqrt(sum(np.linalg.norm(ref_u[v]) ** 2 for v in (1, 2, 3))))
+        e = {"rel_l2_vs_fp64": dict(zip(["rho", "rho_u", "rho_v", "rho_w", "E"], rel_l2(u, ref_u))),
+             "l2_vs_fp64_over_momentum_norm": {n: float(np.linalg.norm(u[v] - ref_u[v]) / mom)
+                                               for n, v in (("rho_u", 1), ("rho_v", 2), ("rho_w", 3))},
+             "theta_growth": g,
+             "theta_growth_rel_diff": (g - g_ref) / g_ref if g_ref != 0 else None,
+             "reynolds_stress_max_rel_diff": rs}
+        if cst is not None:
+            e["closure"] = {"judgements": int(cst.judgements), "fallbacks": int(cst.fallbacks),
+                            "using_dynamic": int(cst.using_dynamic),
+                            "cs2_profile_err": cst.profile_err, "mu_sgs_profile_err": cst.mu_profile_err,
+                            "visc_err": cst.visc_err}
+        out[arm] = e
+    return out
+
+
 def main_gpu(args):
     import numpy as np
     import torch
@@ -206,26 +335,24 @@ def main_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    grid = tuple(int(x) for x in args.grid.split("x"))
-    p = workload_params(grid, precision=args.precision, sgs=0)
-    ncell = grid[0] * grid[1] * grid[2]
-    d = fsl.Domain(p)
-    if args.rows:
-        d.tune(d.TUNE_STAGE_ROWS, args.rows)
-    if args.seg:
-        d.tune(d.TUNE_STAGE_SEG, args.seg)
-    state, dU = fsl.temporal_state(d.p, MC, DW0, AMP, SEED + rank)
-    d.upload_state(state)
-    ext = torch.cuda.ExternalStream(d.stream)
-    run = d.step_phased if args.phased else d.step
-
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    for _ in range(args.warmup):
-        run(1)
-    d.sync()
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    grid = tuple(int(x) for x in args.grid.split("x"))
+    ncell = grid[0] * grid[1] * grid[2]
+    arm = args.arm
+    prec = ARMS[arm][0]
+    state, dU = fsl.temporal_state(workload_params(grid), MC, DW0, AMP, SEED + rank)
+    peaks = measured_peaks()
+    names = fsl.K_CLASSES
 
     dev_uuid = ""
     try:
@@ -234,59 +361,18 @@ def main_gpu(args):
             dev_uuid = "GPU-" + dev_uuid
     except Exception:
         dev_uuid = str(local)
-    clocks = Clocks(dev_uuid)
 
-    # ---- timed region: K steps, state resident in HBM ----
-    d.profile(True)
-    barrier()
-    torch.cuda.synchronize()
+    # ---- the headline arm: K steps, state resident in HBM ----
+    d = make_domain(fsl, grid, arm, state, dU, args.rows, args.seg)
+    run = d.step_phased if args.phased else d.step
+    for _ in range(args.warmup):
+        run(1)
     d.sync()
-    clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(ext)
-    run(args.steps)
-    e1.record(ext)
-    e1.synchronize()
-    torch.cuda.synchronize()
-    barrier()
-    ms = e0.elapsed_time(e1)
-    clk = clocks.stop()
-    kt = d.profile_read()
-    d.profile(False)
-    d.sync()  # raises on a non-finite state
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    units = ncell * STAGES * args.steps * world
-    value = units / (ms / 1e3)
-    ms_per_step = ms / args.steps
-
-    # ---- dominant kernel and its roofline ----
-    names = fsl.K_CLASSES
-    kms = {names[i]: kt.ms[i] for i in range(8)}
-    kl = {names[i]: int(kt.launches[i]) for i in range(8)}
-    top = max(kms, key=lambda k: kms[k])
-    peaks = measured_peaks()
-    # algorithmic bytes per cell-stage of the plain FP64 step (each array read
-    # or written once): stage 1 88 B, stages 2-3 128 B, SGS 40 B -> 384 B / 3
-    alg_per_cell_stage = {0: 128.0, 1: 96.0}[args.precision]
-    if top == "stage":
-        launches = max(kl["stage"], 1)
-        alg_bytes = alg_per_cell_stage * ncell
-        avg_ms = kms["stage"] / launches
-    else:
-        # per-phase path: the whole step's algorithmic bytes over its device time
-        launches = args.steps
-        alg_bytes = alg_per_cell_stage * ncell * STAGES
-        avg_ms = sum(kms.values()) / args.steps
-    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
-    roof = {"bound": "hbm", "kernel": top if top == "stage" else "whole step (per-phase kernels)",
-            "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": round(achieved / peaks["hbm_gbs"], 4),
-            "traffic": args.traffic, "peak_source": peaks["source"] + " HBM copy bandwidth",
-            "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": round(avg_ms, 4)}
+    ms, kt, clk = time_steps(torch, d, run, args.steps, barrier, Clocks(dev_uuid))
+    ms = max_over_ranks(ms)
+    value = ncell * STAGES * args.steps * world / (ms / 1e3)
+    roof, kms, kl = stage_roofline(kt, names, ncell, prec, peaks, args.traffic)
+    cst = d.closure_stats() if ARMS[arm][1] else None
 
     # ---- end to end through the C ABI with pinned host buffers ----
     host_in = torch.empty(state.size, dtype=torch.float64, pin_memory=True)
@@ -294,7 +380,8 @@ def main_gpu(args):
     hin = host_in.numpy()
     hout = host_out.numpy()
     hin[:] = d.download_state()
-    ne = max(1, min(args.steps, args.e2e_steps))
+    ne = max(1, args.e2e_steps)
+    ext = torch.cuda.ExternalStream(d.stream)
     barrier()
     torch.cuda.synchronize()
     f0 = torch.cuda.Event(enable_timing=True)
@@ -308,15 +395,32 @@ def main_gpu(args):
     f1.record(ext)
     f1.synchronize()
     barrier()
-    e2e_ms = f0.elapsed_time(f1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
     e2e = {"value": ncell * STAGES * ne * world / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(state.nbytes), "d2h_bytes_per_step": int(state.nbytes),
            "steps": ne, "note": "per step: fsl_upload_state (pinned host -> HBM), fsl_step(1), "
                                 "fsl_download_state (HBM -> pinned host)"}
+    d.close()
+
+    # ---- the plain FP64 dynamic-Smagorinsky GPU path on the same box ----
+    plain = None
+    if arm != "fp64-dynamic" and not args.no_plain:
+        dp = make_domain(fsl, grid, "fp64-dynamic", state, dU, args.rows, args.seg)
+        for _ in range(args.warmup):
+            dp.step(1)
+        dp.sync()
+        pms, pkt, _ = time_steps(torch, dp, dp.step, args.steps, barrier)
+        pms = max_over_ranks(pms)
+        proof, pkms, pkl = stage_roofline(pkt, names, ncell, 0, peaks, None)
+        plain = {"path": ARM_NAMES["fp64-dynamic"], "value": ncell * STAGES * args.steps * world / (pms / 1e3),
+                 "ms_per_step": pms / args.steps, "kernels_ms": {k: round(v, 3) for k, v in pkms.items()},
+                 "roofline": proof}
+        dp.close()
+
+    # ---- matched error: same initial state, M steps, against the plain FP64 path ----
+    match = None
+    if rank == 0 and args.match_steps > 0:
+        match = matched_error(fsl, grid, state, dU, args.match_steps, args.rows, args.seg)
 
     # ---- CPU baseline: the reference's serial solver, rank 0 at N = 1 only ----
     cpu = None
@@ -333,23 +437,30 @@ def main_gpu(args):
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision == 0 else "f32 bulk / f64 accumulation",
+                "dtype": "f64" if prec == 0 else "f32 bulk / f64 accumulation",
                 "data": "synthetic (seeded tanh shear layer, Crocco-Busemann T, uniform noise 1e-3 dU)",
                 "config": {"workload": workload_name(grid), "grid": list(grid), "cells": ncell,
                            "stages_per_step": STAGES,
-                           "path": ("per-phase kernels" if args.phased else "fused stage kernels") +
-                                   (", plain FP64, dynamic Smagorinsky" if args.precision == 0 else
-                                    ", FP32 bulk, dynamic Smagorinsky"),
+                           "path": ("per-phase kernels, " if args.phased else "fused stage kernels, ") +
+                                   ARM_NAMES[arm],
                            "l2": "inputs larger than L2 (state %.2f GB per domain)" % (state.nbytes / 1e9),
                            "parallelism": "replicas (one independent domain per GPU)"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(sum(kl.values())),
                 "kernels_ms": {k: round(v, 3) for k, v in kms.items()},
                 "clocks": clk}
+        if cst is not None:
+            line["closure"] = {"judgements": int(cst.judgements), "fallbacks": int(cst.fallbacks),
+                               "using_dynamic": int(cst.using_dynamic), "mu_sgs_profile_err": cst.mu_profile_err,
+                               "visc_err": cst.visc_err}
+        if plain is not None:
+            line["plain_fp64"] = plain
+            line["speedup_vs_plain_fp64"] = value / plain["value"]
+        if match is not None:
+            line["matched_error"] = match
         print(json.dumps(line), flush=True)
-    d.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -391,17 +502,20 @@ def main_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fsl", choices=["fsl", "reference"])
     ap.add_argument("--grid", default="x".join(str(x) for x in GRID))
-    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--arm", default="fp32-learned", choices=sorted(ARMS))
     ap.add_argument("--phased", action="store_true", help="per-phase kernels instead of the fused step")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--rows", type=int, default=0, help="fused stage tile rows (8, 12, 16)")
     ap.add_argument("--seg", type=int, default=0, help="x planes per fused stage block")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 path beside the arm")
+    ap.add_argument("--match-steps", type=int, default=200,
+                    help="steps of the matched-error comparison against the plain FP64 path (0: skip)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the dominant kernel from an ncu capture")
     ap.add_argument("--ref-worker", nargs=4, default=None, help=argparse.SUPPRESS)

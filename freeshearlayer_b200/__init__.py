@@ -31,7 +31,7 @@ __all__ = ["Params", "Domain", "FslError", "lib", "LIB_PATH", "default_params",
            "params_from_ini", "params_from_bin", "initial_state", "temporal_state",
            "SETUP_SPATIAL", "SETUP_TEMPORAL", "CFL_STREAMWISE", "CFL_ACOUSTIC",
            "PREC_FP64", "PREC_FP32", "SGS_DYNAMIC", "SGS_LEARNED", "RECON_CHARMINMOD",
-           "RECON_PPM"]
+           "RECON_PPM", "Trainer", "closure_weights", "shear_statistics"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfsl_gpu.so")
@@ -86,7 +86,7 @@ CLOSURE_NPARAMS = 9473
 
 class ClosureStats(C.Structure):
     _fields_ = [("profile_err", C.c_double), ("cell_err", C.c_double), ("mu_profile_err", C.c_double),
-                ("judgements", C.c_int),
+                ("visc_err", C.c_double), ("judgements", C.c_int),
                 ("fallbacks", C.c_int), ("using_dynamic", C.c_int), ("last_step", C.c_uint)]
 
 
@@ -134,8 +134,7 @@ def lib():
             "fsl_closure_set_scales": [vp, d, d], "fsl_closure_set_weights": [vp, fp],
             "fsl_closure_get_weights": [vp, fp], "fsl_closure_judge": [vp, i, d],
             "fsl_closure_get_stats": [vp, C.POINTER(ClosureStats)],
-            "fsl_closure_compare": [vp, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
-                                    C.POINTER(C.c_double), C.POINTER(C.c_double)],
+            "fsl_closure_compare": [vp, C.c_void_p, C.c_void_p, C.POINTER(ClosureStats)],
             "fsl_trainer_create": [ll, C.c_ulonglong, C.POINTER(C.c_void_p)],
             "fsl_trainer_destroy": [vp], "fsl_trainer_harvest": [vp, vp, i],
             "fsl_trainer_get_samples": [vp, fp, fp, ll], "fsl_trainer_set_samples": [vp, fp, fp, ll],
@@ -362,14 +361,15 @@ class Domain:
         return s
 
     def closure_compare(self, fields: bool = False):
-        """(Cs2 profile err, Cs2 cell err, mu profile err[, cs2_mlp, cs2_dyn]) on U^n."""
-        pe, ce, me = C.c_double(), C.c_double(), C.c_double()
+        """One judgement on U^n: a ClosureStats whose profile_err, cell_err,
+        mu_profile_err and visc_err compare the MLP with the dynamic procedure
+        (with fields=True also the padded Cs^2 arrays: (stats, cs2_mlp, cs2_dyn))."""
+        st = ClosureStats()
         a = np.empty(self.padded_shape, np.float32) if fields else None
         b = np.empty(self.padded_shape, np.float32) if fields else None
         self._c(lib().fsl_closure_compare(self.h, a.ctypes.data if fields else None,
-                                          b.ctypes.data if fields else None, C.byref(pe), C.byref(ce),
-                                          C.byref(me)))
-        return (pe.value, ce.value, me.value, a, b) if fields else (pe.value, ce.value, me.value)
+                                          b.ctypes.data if fields else None, C.byref(st)))
+        return (st, a, b) if fields else st
 
     TUNE_STAGE_ROWS, TUNE_STAGE_SEG = 1, 2
 
@@ -465,3 +465,36 @@ class Trainer:
         loss = C.c_double()
         _check(lib().fsl_trainer_train(self.h, epochs, batch, lr, C.byref(loss)))
         return loss.value
+
+
+# --- shear-layer statistics ----------------------------------------------------------
+CLOSURE_WEIGHTS = os.path.join(HERE, "closure_weights.f32")
+
+
+def closure_weights(path: str | None = None) -> np.ndarray:
+    """The trained closure parameters shipped with the package (FSL_CLOSURE_NPARAMS
+    little-endian float32, written by ``python -m freeshearlayer_b200.train_closure``)."""
+    w = np.fromfile(path or CLOSURE_WEIGHTS, dtype="<f4")
+    if w.size != CLOSURE_NPARAMS:
+        raise ValueError("closure weights: expected %d float32 values, found %d" % (CLOSURE_NPARAMS, w.size))
+    return w
+
+
+def shear_statistics(rows: np.ndarray, cells_per_row: int, dU: float, dy: float, rho0: float = 1.0) -> dict:
+    """Favre statistics of a temporal shear layer from :meth:`Domain.plane_sums`
+    rows (per y row: sums of rho, rho u, rho v, rho w, rho uu, rho vv, rho ww,
+    rho uv over the cells_per_row = LEN * DEP cells of the x-z plane).
+
+    Returns the momentum thickness theta = (1 / (rho0 dU^2)) int rho_bar
+    (dU/2 - u~)(u~ + dU/2) dy, the Favre mean velocity u~ and the Favre
+    Reynolds stresses R_ij = {rho u_i u_j}/{rho} - u~_i u~_j per row."""
+    r = np.asarray(rows, np.float64)
+    rho = r[:, 0]
+    u, v, w = r[:, 1] / rho, r[:, 2] / rho, r[:, 3] / rho
+    R11 = r[:, 4] / rho - u * u
+    R22 = r[:, 5] / rho - v * v
+    R33 = r[:, 6] / rho - w * w
+    R12 = r[:, 7] / rho - u * v
+    rho_bar = rho / cells_per_row
+    return {"theta": float(np.sum(rho_bar * (0.5 * dU - u) * (u + 0.5 * dU)) * dy / (rho0 * dU * dU)),
+            "rho": rho_bar, "u": u, "R11": R11, "R22": R22, "R33": R33, "R12": R12}

@@ -335,6 +335,10 @@ int fsl_params_check(const fsl_params *p)
     if (p->precision != FSL_PREC_FP64 && p->precision != FSL_PREC_FP32) return FSL_ERR_ARG;
     if (p->sgs != FSL_SGS_DYNAMIC && p->sgs != FSL_SGS_LEARNED) return FSL_ERR_ARG;
     if (p->recon != FSL_RECON_CHARMINMOD && p->recon != FSL_RECON_PPM) return FSL_ERR_ARG;
+    // the only scheme the solver has is src/reconstruction.c's characteristic
+    // kappa=1/3 reconstruction (README.md:9 calls it PPM); a Colella-Woodward
+    // parabolic reconstruction is not built, so asking for it is an error
+    if (p->recon == FSL_RECON_PPM) return FSL_ERR_UNSUPPORTED;
     return FSL_OK;
 }
 

@@ -121,7 +121,8 @@ int check_tc_error(Ctx &c)
 // One judgement on U^n (ghost layer filled): the dynamic procedure into c.mu
 // and c.cd32, the MLP into the alternate viscosity buffer and c.cs2_32, and
 // the plane-averaged comparisons.  Sets c.last_perr / last_cerr (Cs^2) and
-// c.last_merr (SGS viscosity profile).
+// c.last_merr (SGS viscosity profile) and c.last_verr (SGS viscosity profile
+// against the effective viscosity mu_L + <mu_dyn>).
 int judge_now(Ctx &c)
 {
     const bool fp32 = c.p.precision == FSL_PREC_FP32;
@@ -143,6 +144,15 @@ int judge_now(Ctx &c)
     std::vector<double> mrows(rows.begin() + 4 * H, rows.end());
     double mcell;
     judge_errors(mrows, H, &c.last_merr, &mcell);
+    // rows j in [3, H-2] hold sums over the (L-4)(D-4) band cells of the plane
+    const double nb = (double)(c.g.L - 4) * (c.g.D - 4);
+    double num = 0, den = 0;
+    for (int j = 2; j <= H - 3; j++) {
+        const double a = mrows[4 * j] / nb, b = mrows[4 * j + 1] / nb;
+        num += (a - b) * (a - b);
+        den += (c.p.mu_L + b) * (c.p.mu_L + b);
+    }
+    c.last_verr = den > 0 ? std::sqrt(num / den) : (num > 0 ? INFINITY : 0.0);
     return FSL_OK;
 }
 
@@ -165,7 +175,7 @@ int closure_step_sgs(Ctx &c)
         if (rc) return rc;
         c.judgements++;
         c.last_judge_step = c.step;
-        const bool fail_ = !(c.last_merr <= c.judge_thr);
+        const bool fail_ = !(c.last_verr <= c.judge_thr);
         if (fail_ && !c.using_dynamic) c.fallbacks++;
         c.using_dynamic = fail_;
         const size_t fs = (size_t)c.g.fstride;
@@ -249,6 +259,7 @@ int fsl_closure_get_stats(fsl_ctx *h, fsl_closure_stats *s)
     s->profile_err = c.last_perr;
     s->mu_profile_err = c.last_merr;
     s->cell_err = c.last_cerr;
+    s->visc_err = c.last_verr;
     s->judgements = c.judgements;
     s->fallbacks = c.fallbacks;
     s->using_dynamic = c.using_dynamic ? 1 : 0;
@@ -256,7 +267,7 @@ int fsl_closure_get_stats(fsl_ctx *h, fsl_closure_stats *s)
     return FSL_OK;
 }
 
-int fsl_closure_compare(fsl_ctx *h, float *cs2_mlp, float *cs2_dyn, double *perr, double *cerr, double *merr)
+int fsl_closure_compare(fsl_ctx *h, float *cs2_mlp, float *cs2_dyn, fsl_closure_stats *errs)
 {
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
@@ -265,9 +276,7 @@ int fsl_closure_compare(fsl_ctx *h, float *cs2_mlp, float *cs2_dyn, double *perr
     launch_ghost(c, c.U);
     if ((rc = ensure_dyn_scratch(c))) return rc;
     if ((rc = judge_now(c))) return rc;
-    if (perr) *perr = c.last_perr;
-    if (cerr) *cerr = c.last_cerr;
-    if (merr) *merr = c.last_merr;
+    if (errs) fsl_closure_get_stats(h, errs);
     const Grid &g = c.g;
     for (int which = 0; which < 2; which++) {
         float *dst = which ? cs2_dyn : cs2_mlp;

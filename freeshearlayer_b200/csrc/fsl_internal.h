@@ -111,10 +111,10 @@ struct Ctx {
     double *judge_rows = nullptr; // [2][HIG][4] plane sums of the judgement (Cs^2, mu_SGS)
     bool cl_alloc = false, cl_weights = false;
     int judge_every = 100;
-    double judge_thr = 0.35;
+    double judge_thr = 0.02;
     bool using_dynamic = false;
     int judgements = 0, fallbacks = 0;
-    double last_perr = -1, last_cerr = -1, last_merr = -1;
+    double last_perr = -1, last_cerr = -1, last_merr = -1, last_verr = -1;
     unsigned last_judge_step = 0;
     DevScalars *ds = nullptr; // device scalars
     DevScalars *hs = nullptr; // pinned host mirror

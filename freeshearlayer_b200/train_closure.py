@@ -3,12 +3,15 @@
     python -m freeshearlayer_b200.train_closure --out freeshearlayer_b200/closure_weights.f32
 
 Runs temporal shear layers on the GPU (FP32 bulk, dynamic Smagorinsky) at
-convective Mach 0.3, 0.5 and 0.7 on a 256x128x128 and a 512x256x256 grid
-(box 2pi x pi x pi, Re_dw0 1000), harvests (features, dynamic Cs^2) samples
-every 50 steps, trains the MLP with Adam on the tensor-core kernels and writes
-the FP32 parameter vector (FSL_CLOSURE_NPARAMS little-endian floats).  The
-initial velocity noise is 5% of dU so that the layers develop small scales
-within a few hundred steps.
+convective Mach 0.3, 0.5 and 0.7 (box 2pi x pi x pi, Re_dw0 1000), each
+GRID:AMP:STEPS entry of --runs once per Mach number: velocity noise of 1e-3 dU
+(the laminar-to-transitional phase the production runs start in) and 5e-2 dU
+(small scales within a few hundred steps), on a 256x128x128 and a 512x256x256
+grid.  Every 50 steps it harvests (features, dynamic Cs^2) samples, with a
+cell stride per grid that spreads the --samples budget over all snapshots,
+trains the MLP with Adam on the tensor-core kernels and writes the FP32
+parameter vector (FSL_CLOSURE_NPARAMS little-endian floats).  Finally it
+judges the trained closure on fresh runs and prints one JSON log line.
 """
 from __future__ import annotations
 
@@ -42,15 +45,29 @@ def load_weights(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
     return w
 
 
+def judge(fsl, w, grid, Mc, amp, steps, seed):
+    p, dU = shear_params(grid, Mc)
+    state, _ = fsl.temporal_state(p, Mc, 1.0, amp, seed)
+    d = fsl.Domain(p)
+    d.upload_state(state)
+    d.closure_set_scales(1.0 / dU, 1.0)
+    d.closure_set_weights(w)
+    if steps:
+        d.step(steps)
+    st = d.closure_compare()
+    d.close()
+    return {"grid": list(grid), "Mc": Mc, "amp": amp, "steps": steps, "cs2_profile_err": st.profile_err,
+            "cs2_cell_err": st.cell_err, "mu_profile_err": st.mu_profile_err, "visc_err": st.visc_err}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
-    ap.add_argument("--grids", default="256x128x128,512x256x256")
+    ap.add_argument("--runs", default="256x128x128:0.001:2000,256x128x128:0.05:300,"
+                                      "512x256x256:0.001:1000,512x256x256:0.05:300")
     ap.add_argument("--mach", default="0.3,0.5,0.7")
-    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--every", type=int, default=50)
     ap.add_argument("--samples", type=float, default=2e8, help="target number of harvested samples")
-    ap.add_argument("--amp", type=float, default=0.05)
     ap.add_argument("--epochs", type=int, default=3)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
@@ -59,29 +76,33 @@ def main(argv=None):
     sys.path.insert(0, os.path.dirname(HERE))
     import freeshearlayer_b200 as fsl
 
-    grids = [tuple(int(x) for x in g.split("x")) for g in args.grids.split(",")]
+    runs = []
+    for r in args.runs.split(","):
+        g, amp, steps = r.split(":")
+        runs.append((tuple(int(x) for x in g.split("x")), float(amp), int(steps)))
     machs = [float(m) for m in args.mach.split(",")]
-    nsnap = args.steps // args.every
-    per_snap = args.samples / (len(grids) * len(machs) * nsnap)
-    tr = fsl.Trainer(int(args.samples * 1.05) + 1, seed=args.seed)
+    nsnap = sum(len(machs) * (steps // args.every + 1) for _, _, steps in runs)
+    per_snap = args.samples / nsnap
+    tr = fsl.Trainer(int(args.samples * 1.1) + 1, seed=args.seed)
     log = {"runs": []}
     t0 = time.time()
-    for grid in grids:
+    for grid, amp, steps in runs:
         band = (grid[0] - 4) * (grid[1] - 4) * (grid[2] - 4)
         stride = max(1, int(math.ceil(band / per_snap)))
         for Mc in machs:
             p, dU = shear_params(grid, Mc)
-            state, _ = fsl.temporal_state(p, Mc, 1.0, args.amp, args.seed + int(Mc * 10))
+            state, _ = fsl.temporal_state(p, Mc, 1.0, amp, args.seed + int(Mc * 10) + int(amp * 1e4))
             d = fsl.Domain(p)
             d.upload_state(state)
             d.closure_set_scales(1.0 / dU, 1.0)
-            for _ in range(nsnap):
+            tr.harvest(d, stride)
+            for _ in range(steps // args.every):
                 d.step(args.every)
-                d.sync()
                 tr.harvest(d, stride)
-            log["runs"].append({"grid": list(grid), "Mc": Mc, "stride": stride, "samples": tr.size})
-            print("harvest %s Mc %.1f stride %d -> %d samples (%.0f s)" % (grid, Mc, stride, tr.size,
-                                                                       time.time() - t0), flush=True)
+            log["runs"].append({"grid": list(grid), "Mc": Mc, "amp": amp, "steps": steps, "stride": stride,
+                                "samples": tr.size})
+            print("harvest %s Mc %.1f amp %g stride %d -> %d samples (%.0f s)" % (
+                grid, Mc, amp, stride, tr.size, time.time() - t0), flush=True)
             d.close()
     X, Y = tr.samples(min(tr.size, 1 << 20))
     p0 = tr.weights()
@@ -96,19 +117,11 @@ def main(argv=None):
     log.update({"samples": tr.size, "loss0": loss0, "loss": loss, "epochs": args.epochs,
                 "batch": args.batch, "lr": args.lr, "train_s": t2 - t1,
                 "samples_per_s": tr.size * args.epochs / max(t2 - t1, 1e-9)})
-    # judge the trained closure on a fresh run of each Mach number (smaller grid)
+    # the trained closure against the dynamic procedure on fresh runs
+    s = args.seed + 99
+    log["judge"] = [judge(fsl, w, (512, 256, 256), 0.7, 1e-3, 0, s), judge(fsl, w, (512, 256, 256), 0.7, 1e-3, 300, s)]
     for Mc in machs:
-        p, dU = shear_params(grids[0], Mc)
-        state, _ = fsl.temporal_state(p, Mc, 1.0, args.amp, args.seed + 99 + int(Mc * 10))
-        d = fsl.Domain(p)
-        d.upload_state(state)
-        d.closure_set_scales(1.0 / dU, 1.0)
-        d.closure_set_weights(w)
-        d.step(args.steps)
-        pe, ce, me = d.closure_compare()
-        log.setdefault("judge", []).append({"Mc": Mc, "cs2_profile_err": pe, "cs2_cell_err": ce,
-                                            "mu_profile_err": me})
-        d.close()
+        log["judge"] += [judge(fsl, w, (256, 128, 128), Mc, 1e-3, 1000, s), judge(fsl, w, (256, 128, 128), Mc, 0.05, 300, s)]
     print(json.dumps(log), flush=True)
 
 

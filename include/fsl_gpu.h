@@ -65,7 +65,7 @@ extern "C" {
 
 /* reconstruction */
 #define FSL_RECON_CHARMINMOD 0 /* characteristic kappa=1/3 minmod(beta=4), src/reconstruction.c:26-345 */
-#define FSL_RECON_PPM 1        /* Colella-Woodward PPM on characteristic variables */
+#define FSL_RECON_PPM 1        /* Colella-Woodward PPM: not built, fsl_init returns FSL_ERR_UNSUPPORTED */
 
 /* Parameters: the 22 positional values of layer2.ini in file order
  * (src/initialize.c:25-58; src-par's mpi_layer2.bin holds the same 22 values
@@ -119,7 +119,8 @@ int fsl_params_from_ini(const char *path, fsl_params *p);
  * (src-par/initialize.c:35-81, written by src-par/ini2bin/ini2bin.c:63-64).
  * Option fields are left as for fsl_params_from_ini. */
 int fsl_params_from_bin(const char *path, fsl_params *p);
-/* Check a parameter set; FSL_OK or FSL_ERR_ARG. */
+/* Check a parameter set; FSL_OK, FSL_ERR_ARG, or FSL_ERR_UNSUPPORTED for an
+ * option that is not built (FSL_RECON_PPM). */
 int fsl_params_check(const fsl_params *p);
 
 /* ---- initial states (host arrays in the state layout) ----------------- */
@@ -243,16 +244,21 @@ int fsl_set_cur(fsl_ctx *ctx, int which);
  * coefficient Cs^2; mu_SGS = rho Cs^2 (dx dy dz)^(2/3) |S| as in the dynamic
  * procedure (src/turbulence.c:442).  With params.sgs = FSL_SGS_LEARNED the
  * steps use it; every `every` steps the dynamic procedure runs beside it as the
- * judge, and while the error of the plane-averaged SGS viscosity profile
- * <mu_SGS>(y) exceeds the threshold the steps fall back to the dynamic
- * procedure (the Cs^2 errors are reported too; per cell the dynamic Cs^2 is
- * dominated by cell-to-cell noise, and where |S| vanishes it does not act). */
+ * judge, and while the error of the plane-averaged SGS viscosity profile,
+ * measured against the effective viscosity mu_L + <mu_SGS,dyn>(y) (the
+ * quantity the viscous fluxes see), exceeds the threshold (default 0.02) the
+ * steps fall back to the dynamic procedure.  The Cs^2 errors and the SGS
+ * viscosity error relative to the dynamic SGS viscosity alone are reported
+ * too; per cell the dynamic Cs^2 is dominated by cell-to-cell noise, and where
+ * |S| vanishes it does not act. */
 #define FSL_CLOSURE_NPARAMS 9473 /* W1[64][16] b1 W2[64][64] b2 W3[64][64] b3 w4[64] b4 */
 
 typedef struct fsl_closure_stats {
     double profile_err;    /* last judgement: |<Cs2_mlp>(y) - <Cs2_dyn>(y)|_2 / |<Cs2_dyn>(y)|_2 */
     double cell_err;       /* last judgement: |Cs2_mlp - Cs2_dyn|_2 / |Cs2_dyn|_2 over cells */
-    double mu_profile_err; /* last judgement: the same profile error of mu_SGS (the fallback criterion) */
+    double mu_profile_err; /* last judgement: |<mu_mlp>(y) - <mu_dyn>(y)|_2 / |<mu_dyn>(y)|_2 */
+    double visc_err;       /* last judgement: |<mu_mlp>(y) - <mu_dyn>(y)|_2 / |mu_L + <mu_dyn>(y)|_2
+                              (the fallback criterion) */
     int judgements, fallbacks, using_dynamic;
     unsigned last_step;
 } fsl_closure_stats;
@@ -264,10 +270,9 @@ int fsl_closure_get_weights(fsl_ctx *ctx, float *params);
 int fsl_closure_judge(fsl_ctx *ctx, int every, double threshold);
 int fsl_closure_get_stats(fsl_ctx *ctx, fsl_closure_stats *stats);
 /* Both closures on the current U^n: Cs^2 of the MLP and of the dynamic
- * procedure (padded FP32 host arrays, either may be NULL) and the three errors
- * of fsl_closure_stats. */
-int fsl_closure_compare(fsl_ctx *ctx, float *cs2_mlp, float *cs2_dyn, double *profile_err, double *cell_err,
-                        double *mu_profile_err);
+ * procedure (padded FP32 host arrays, either may be NULL) and the four errors
+ * of one judgement in *errs (its counters are the context's). */
+int fsl_closure_compare(fsl_ctx *ctx, float *cs2_mlp, float *cs2_dyn, fsl_closure_stats *errs);
 
 /* Training on (features, dynamic Cs^2) samples harvested on the GPU. */
 typedef struct fsl_trainer fsl_trainer;

@@ -96,6 +96,26 @@ def test_params_check(fsl):
                 dict(cfl_mode=3), dict(maxCoNum=-1.0)]:
         p = fsl.default_params(**bad)
         assert lib.fsl_params_check(C.byref(p)) == -1, bad
+    # the reference has one reconstruction (README.md:9 calls it PPM); a
+    # Colella-Woodward PPM is not built and asking for it is refused
+    assert lib.fsl_params_check(C.byref(fsl.default_params(recon=fsl.RECON_PPM))) == -7
+
+
+def test_shear_statistics_tanh_profile(fsl):
+    """theta of u = dU/2 tanh(2y/delta) at uniform density is delta/4."""
+    H, nrow, dU, delta = 4000, 6, 3.0, 1.0
+    dy = 20.0 / H
+    y = (np.arange(H) + 0.5) * dy - 10.0
+    u = 0.5 * dU * np.tanh(2 * y / delta)
+    rows = np.zeros((H, 8))
+    rows[:, 0] = nrow
+    rows[:, 1] = nrow * u
+    rows[:, 4] = nrow * u * u + nrow * 0.25
+    rows[:, 7] = nrow * u * 0.1
+    st = fsl.shear_statistics(rows, nrow, dU, dy)
+    assert abs(st["theta"] - delta / 4) < 1e-6
+    np.testing.assert_allclose(st["R11"], 0.25, atol=1e-12)
+    np.testing.assert_allclose(st["R12"], 0.1 * u, atol=1e-12)
 
 
 def test_initial_states_match_oracle(fsl, oracle_lib):

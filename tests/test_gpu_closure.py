@@ -84,7 +84,7 @@ def test_features_and_forward_match_oracle(fsl):
     params = tr.weights()
     params[9472] = 0.05
     d.closure_set_weights(params)
-    pe, ce, me, cs2_mlp, cs2_dyn = d.closure_compare(fields=True)
+    _, cs2_mlp, cs2_dyn = d.closure_compare(fields=True)
     got = cs2_mlp[3:-3, 3:-3, 3:-3].ravel()
     ref = mo.cs2(params, X)
     assert np.max(np.abs(got - ref)) < 2e-3
@@ -114,9 +114,10 @@ def trained(fsl):
     loss = tr.train(epochs=40, batch=8192, lr=2e-3)
     w = tr.weights()
     d.closure_set_weights(w)
-    perr, cerr, merr = d.closure_compare()
+    st = d.closure_compare()
     return dict(p=p, dU=dU, state=d.download_state(), weights=w, var=var, loss0=loss0,
-                loss=loss, n=len(Y), perr=perr, cerr=cerr, merr=merr)
+                loss=loss, n=len(Y), perr=st.profile_err, cerr=st.cell_err, merr=st.mu_profile_err,
+                verr=st.visc_err)
 
 
 def test_training_beats_mean_predictor(trained):
@@ -124,13 +125,14 @@ def test_training_beats_mean_predictor(trained):
     the bar is the mean predictor (MSE = variance) per cell, and a small error
     of the plane-averaged Cs^2 profile, the quantity that sets the mean SGS
     dissipation and the judge's criterion."""
-    print("samples %d var %.3e loss0 %.3e loss %.3e cs2 profile %.3f cs2 cell %.3f mu profile %.3f" % (
-        trained["n"], trained["var"], trained["loss0"], trained["loss"], trained["perr"], trained["cerr"],
-        trained["merr"]))
+    print("samples %d var %.3e loss0 %.3e loss %.3e cs2 profile %.3f cs2 cell %.3f mu profile %.3f "
+          "visc %.4f" % (trained["n"], trained["var"], trained["loss0"], trained["loss"], trained["perr"],
+                         trained["cerr"], trained["merr"], trained["verr"]))
     assert trained["n"] > 50000
     assert trained["loss"] < trained["loss0"]
     assert trained["loss"] < 0.9 * trained["var"]
     assert trained["merr"] < 0.35
+    assert trained["verr"] < 0.02
 
 
 def test_fallback_is_the_dynamic_procedure(fsl, trained):
@@ -165,3 +167,4 @@ def test_learned_closure_steps(fsl, trained, prec):
     st = d.closure_stats()
     assert st.judgements == 2 and st.fallbacks == 0 and st.using_dynamic == 0
     assert np.isfinite(st.mu_profile_err) and st.mu_profile_err < 0.5
+    assert np.isfinite(st.visc_err) and st.visc_err < 0.05
