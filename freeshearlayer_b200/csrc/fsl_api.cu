@@ -534,6 +534,7 @@ int fsl_upload_state(fsl_ctx *h, const double *state)
     if (!h || !state) return FSL_ERR_ARG;
     Ctx &c = h->c;
     const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
+    c.co_valid = false;
     CK(cudaMemcpyAsync(c.stage_dev, state, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     launch_state_scatter(c, c.U, c.stage_dev);
     CKL();
@@ -560,6 +561,7 @@ int fsl_set_time(fsl_ctx *h, unsigned step, double deltaT)
     Ctx &c = h->c;
     int rc = sync_scalars(c);
     if (rc) return rc;
+    c.co_valid = false;
     c.step = step;
     c.hs->dt = deltaT;
     c.hs->dtx = deltaT / c.p.deltaX; c.hs->dty = deltaT / c.p.deltaY; c.hs->dtz = deltaT / c.p.deltaZ;
@@ -573,6 +575,7 @@ int fsl_check_courant(fsl_ctx *h, double *maxCo, double *dt)
 {
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
+    c.co_valid = false;
     launch_courant(c);
     CKL();
     int rc = sync_scalars(c);
@@ -657,6 +660,7 @@ int fsl_evolution(fsl_ctx *h, int stage)
     Ctx &c = h->c;
     int rc = ensure_faces(c);
     if (rc) return rc;
+    c.co_valid = false;
     launch_evolution(c, c.p.nStages, stage);
     CKL();
     // pointer swap of src/evolution.c:71,113,155 (and :188,228 for RK2)
@@ -669,6 +673,7 @@ int fsl_step_phased(fsl_ctx *h, int nsteps)
     if (!h || nsteps < 0) return FSL_ERR_ARG;
     Ctx &c = h->c;
     int rc;
+    c.co_valid = false;
     for (int n = 0; n < nsteps; n++) {
         launch_courant(c);
         CKL();
@@ -708,7 +713,8 @@ int fsl_step(fsl_ctx *h, int nsteps)
     if (c.p.precision == FSL_PREC_FP32) {
         if ((rc = ensure_fp32(c))) return rc;
         for (int n = 0; n < nsteps; n++) {
-            launch_courant(c);
+            if (c.co_valid) launch_courant_apply(c);
+            else launch_courant(c);
             c.step++;
             draw(c);
             launch_ghost(c, c.U);
@@ -725,13 +731,15 @@ int fsl_step(fsl_ctx *h, int nsteps)
             launch_stage32(c, 2, c.Up, c.U, c.Uq);
             launch_ghost(c, c.Uq);
             launch_bface32(c, c.Uq, c.dist);
-            launch_stage32(c, 3, c.Uq, c.U, c.U);
+            launch_stage32(c, 3, c.Uq, c.U, c.U, true);
+            c.co_valid = true;
             CKL();
         }
         return FSL_OK;
     }
     for (int n = 0; n < nsteps; n++) {
-        launch_courant(c);
+        if (c.co_valid) launch_courant_apply(c);
+        else launch_courant(c);
         c.step++;
         draw(c);
         launch_ghost(c, c.U);
@@ -747,7 +755,8 @@ int fsl_step(fsl_ctx *h, int nsteps)
         launch_stage(c, 2, c.Up, c.U, c.Uq);
         launch_ghost(c, c.Uq);
         launch_bface(c, c.Uq, c.dist);
-        launch_stage(c, 3, c.Uq, c.U, c.U);
+        launch_stage(c, 3, c.Uq, c.U, c.U, true);
+        c.co_valid = true;
         CKL();
     }
     return FSL_OK;
@@ -793,6 +802,7 @@ int fsl_set_cells(fsl_ctx *h, int which, int var, const double *in)
     double *base = which == 0 ? c.U : which == 1 ? c.Up : which == 2 ? cur_ptr(c) : c.mu;
     if (which == 3) var = 0;
     base += var * g.fstride + g.off;
+    c.co_valid = false;
     CK(cudaMemcpy2DAsync(base, g.pk * sizeof(double), in, (g.D + 2) * sizeof(double), (g.D + 2) * sizeof(double),
                          (size_t)(g.L + 2) * (g.H + 2), cudaMemcpyHostToDevice, c.stream));
     CK(cudaStreamSynchronize(c.stream));
@@ -826,6 +836,7 @@ int fsl_set_faces(fsl_ctx *h, int dir, int side, int var, const double *in)
 int fsl_set_cur(fsl_ctx *h, int which)
 {
     if (!h || which < 0 || which > 1) return FSL_ERR_ARG;
+    h->c.co_valid = false;
     h->c.cur = which;
     return FSL_OK;
 }

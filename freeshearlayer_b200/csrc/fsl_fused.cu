@@ -17,12 +17,12 @@ void launch_bface(Ctx &c, const double *cur, const Disturb &d)
     stage::launch_bface_t<double>(c, cur, d, bf64(c));
 }
 
-int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double *out)
+int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant)
 {
     switch (c.stage_tje) {
-    case 8: return stage::launch_stage_t<double, 8, 1>(c, stage, cur, un, out, c.mu, bf64(c));
-    case 12: return stage::launch_stage_t<double, 12, 1>(c, stage, cur, un, out, c.mu, bf64(c));
-    default: return stage::launch_stage_t<double, 16, 1>(c, stage, cur, un, out, c.mu, bf64(c));
+    case 8: return stage::launch_stage_t<double, 8, 1>(c, stage, cur, un, out, c.mu, bf64(c), courant);
+    case 12: return stage::launch_stage_t<double, 12, 1>(c, stage, cur, un, out, c.mu, bf64(c), courant);
+    default: return stage::launch_stage_t<double, 16, 1>(c, stage, cur, un, out, c.mu, bf64(c), courant);
     }
 }
 

@@ -35,12 +35,12 @@ void launch_mu_to_f32(Ctx &c)
     prof_end(c, FSL_K_SGS, 1);
 }
 
-int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out)
+int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant)
 {
     switch (c.stage_tje) {
-    case 8: return stage::launch_stage_t<float, 8, 2>(c, stage, cur, un, out, c.mu32, bf32(c));
-    case 12: return stage::launch_stage_t<float, 12, 1>(c, stage, cur, un, out, c.mu32, bf32(c));
-    default: return stage::launch_stage_t<float, 16, 1>(c, stage, cur, un, out, c.mu32, bf32(c));
+    case 8: return stage::launch_stage_t<float, 8, 2>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
+    case 12: return stage::launch_stage_t<float, 12, 1>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
+    default: return stage::launch_stage_t<float, 16, 1>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
     }
 }
 

@@ -45,6 +45,9 @@ struct DevScalars {
     double maxCo;
     unsigned int status; // bit 0: non-finite or non-positive Courant max; bit 1: non-positive density
     unsigned int pad;
+    // Courant maximum of the state written by the last fused stage 3 (bit
+    // pattern of a non-negative double, accumulated with atomicMax)
+    unsigned long long co_bits;
 };
 
 // Disturbance block of one step (host RNG state, src/layer2.c:152-162).
@@ -127,6 +130,8 @@ struct Ctx {
     int counter = 0;
     unsigned step = 0;
     Disturb dist{};
+    // the device Courant maximum (DevScalars::co_bits) belongs to the current U^n
+    bool co_valid = false;
     double dt_host = 0; // host copy of dt, valid after sync
     double maxco_host = 0;
     unsigned long long bytes = 0;
@@ -165,6 +170,8 @@ void launch_judge_rows(Ctx &c, const float *a, const float *b, double *rows);
 void launch_judge_rows(Ctx &c, const float *a, const double *b, double *rows);
 void launch_judge_rows(Ctx &c, const double *a, const double *b, double *rows);
 void launch_courant(Ctx &c);
+// dt update from the Courant maximum the fused stage 3 accumulated
+void launch_courant_apply(Ctx &c);
 void launch_state_scatter(Ctx &c, double *dst, const double *packed);
 void launch_state_gather(Ctx &c, const double *src, double *packed);
 void launch_sums(Ctx &c, const double *U, double *out5);
@@ -173,10 +180,10 @@ void launch_plane_sums(Ctx &c, const double *U, double *rows);
 // ---- fused path (fsl_fused.cu) ----------------------------------------------
 void launch_bface(Ctx &c, const double *cur, const Disturb &d);
 // One RK3 stage: cur (ghosts filled) -> out; un = U^n.
-int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double *out);
+int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant = false);
 // FP32-bulk variants (fsl_fused32.cu): boundary states in bf32, SGS viscosity in mu32.
 void launch_bface32(Ctx &c, const double *cur, const Disturb &d);
-int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out);
+int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant = false);
 void launch_mu_to_f32(Ctx &c); // mu (FP64) -> mu32
 
 // ---- learned closure (fsl_mlp.cu) ---------------------------------------------

@@ -80,7 +80,8 @@ struct SmemW {
     alignas(128) __nv_bfloat16 W1[64 * 16];
     alignas(128) __nv_bfloat16 W2[64 * 64];
     alignas(128) __nv_bfloat16 W3[64 * 64];
-    float b1[64], b2[64], b3[64], w4[64], b4;
+    alignas(16) float b1[64];
+    float b2[64], b3[64], w4[64], b4;
 };
 
 __device__ __forceinline__ void stage_weights(SmemW &s, const float *__restrict__ P, int t, int nt)
@@ -106,10 +107,24 @@ __device__ __forceinline__ void stage_weights(SmemW &s, const float *__restrict_
 // ---- inference -----------------------------------------------------------------
 struct SmemInfer {
     SmemW w;
-    alignas(128) __nv_bfloat16 A[128 * 64]; // activations of the current layer (K-major tile)
+    alignas(16) float hb[3][64];              // b1, b2, b3 halved (silu(z + b) = h + h tanh h, h = (z + b) / 2)
+    alignas(128) __nv_bfloat16 A0[128 * 16];  // features (K-major tile, columns 8..15 zero)
+    alignas(128) __nv_bfloat16 A[128 * 64];   // activations of the current layer (K-major tile)
     uint64_t mbar;
     uint32_t tholder;
 };
+
+// silu of two values in packed BF16 arithmetic from h = (z + b) / 2 given in
+// FP32: silu = h + h tanh(h), one MUFU operation per pair.  Result: element 0
+// in the low half (the lower k of a K-major tile row).
+__device__ __forceinline__ uint32_t silu2_bf16(float h0, float h1)
+{
+    uint32_t hp, th, y;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hp) : "f"(h1), "f"(h0));
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(hp));
+    asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(hp), "r"(th));
+    return y;
+}
 
 // one tensor-core layer: D = A W^T into TMEM, wait; returns false on timeout
 __device__ __forceinline__ bool layer_mma(uint32_t tmem, uint32_t a, uint32_t b, int K, int N, uint64_t *mbar,
@@ -130,34 +145,58 @@ __device__ __forceinline__ bool layer_mma(uint32_t tmem, uint32_t a, uint32_t b,
     return ok;
 }
 
-// bias + SiLU of a TMEM accumulator row into the next activation tile
-__device__ __forceinline__ void epilogue_to_tile(uint32_t taddr, const float *bias, __nv_bfloat16 *A, int t)
+// bias + SiLU of this thread's TMEM accumulator row (64 columns) into row t
+// of the next K = 64 activation tile, 8 BF16 (16 bytes) per shared store
+__device__ __forceinline__ void epilogue_to_tile(uint32_t taddr, const float *hb, unsigned char *A, int t)
 {
+    const uint32_t row = (uint32_t)(t >> 3) * 1024u + (uint32_t)(t & 7) * 16u;
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         float v[16];
         umma::tmem_ld16(taddr + (uint32_t)(c * 16), v);
         umma::tmem_wait_ld();
 #pragma unroll
-        for (int q = 0; q < 16; q++) {
-            const int o = c * 16 + q;
-            A[umma::tile_off(t, o, 64) / 2] = __float2bfloat16_rn(silu(v[q] + bias[o]));
+        for (int half = 0; half < 2; half++) {
+            const float4 b0 = reinterpret_cast<const float4 *>(hb)[c * 4 + half * 2];
+            const float4 b1 = reinterpret_cast<const float4 *>(hb)[c * 4 + half * 2 + 1];
+            const float *x = v + half * 8;
+            uint4 pk;
+            pk.x = silu2_bf16(fmaf(x[0], 0.5f, b0.x), fmaf(x[1], 0.5f, b0.y));
+            pk.y = silu2_bf16(fmaf(x[2], 0.5f, b0.z), fmaf(x[3], 0.5f, b0.w));
+            pk.z = silu2_bf16(fmaf(x[4], 0.5f, b1.x), fmaf(x[5], 0.5f, b1.y));
+            pk.w = silu2_bf16(fmaf(x[6], 0.5f, b1.z), fmaf(x[7], 0.5f, b1.w));
+            *reinterpret_cast<uint4 *>(A + row + (uint32_t)(c * 2 + half) * 128u) = pk;
         }
     }
 }
 
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
 // Persistent: each block (one warpgroup) walks tiles of 128 interior cells in
 // (i, j, k) order; mu = rho Cs^2 DD |S| (the reference's formula,
-// src/turbulence.c:442) with Cs^2 from the MLP clipped to [0, 0.15].
+// src/turbulence.c:442) with Cs^2 from the MLP clipped to [0, 0.15].  The
+// hidden-layer SiLU runs in packed BF16 (its results are BF16 operands of the
+// next product either way); the last layer's dot product with w4 is FP32.
 template <typename MT>
-__global__ void __launch_bounds__(128) k_closure_infer(Grid g, ClosureScales sc, const double *__restrict__ U,
-                                                       const float *__restrict__ P, MT *__restrict__ mu,
-                                                       float *__restrict__ cs2_out, int *err)
+__global__ void __launch_bounds__(128, 5) k_closure_infer(Grid g, ClosureScales sc, const double *__restrict__ U,
+                                                          const float *__restrict__ P, MT *__restrict__ mu,
+                                                          float *__restrict__ cs2_out, int *err)
 {
     extern __shared__ __align__(1024) unsigned char smraw[];
     SmemInfer &s = *reinterpret_cast<SmemInfer *>(smraw);
     const int t = threadIdx.x, wp = t >> 5;
     stage_weights(s.w, P, t, 128);
+    for (int e = t; e < 3 * 64; e += 128) s.hb[e / 64][e % 64] = 0.5f * P[(e < 64 ? kOffB1 : e < 128 ? kOffB2 : kOffB3) + e % 64];
+    unsigned char *A0 = reinterpret_cast<unsigned char *>(s.A0);
+    unsigned char *A = reinterpret_cast<unsigned char *>(s.A);
+    // feature row t: columns 0..7 at +0, zero columns 8..15 at +128
+    const uint32_t frow = (uint32_t)(t >> 3) * 256u + (uint32_t)(t & 7) * 16u;
+    *reinterpret_cast<uint4 *>(A0 + frow + 128u) = make_uint4(0u, 0u, 0u, 0u);
     if (t == 0) umma::mbar_init(&s.mbar, 1);
     if (wp == 0) umma::tmem_alloc(&s.tholder, 64);
     umma::fence_before_sync();
@@ -165,8 +204,8 @@ __global__ void __launch_bounds__(128) k_closure_infer(Grid g, ClosureScales sc,
     umma::fence_after_sync();
     const uint32_t tmem = s.tholder;
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * wp) << 16);
-    const uint32_t aA = umma::smem_u32(s.A), aW1 = umma::smem_u32(s.w.W1), aW2 = umma::smem_u32(s.w.W2),
-                   aW3 = umma::smem_u32(s.w.W3);
+    const uint32_t aA0 = umma::smem_u32(s.A0), aA = umma::smem_u32(s.A), aW1 = umma::smem_u32(s.w.W1),
+                   aW2 = umma::smem_u32(s.w.W2), aW3 = umma::smem_u32(s.w.W3);
     uint32_t phase = 0;
     bool ok = true;
     const long long ncell = (long long)g.L * g.H * g.D;
@@ -183,14 +222,14 @@ __global__ void __launch_bounds__(128) k_closure_infer(Grid g, ClosureScales sc,
             c = g.idx(i, j, k);
             cell_features(g, U, c, sc, f, rho, Smag);
         }
-#pragma unroll
-        for (int q = 0; q < 16; q++) s.A[umma::tile_off(t, q, 16) / 2] = __float2bfloat16_rn(q < 8 ? f[q] : 0.f);
-        ok = layer_mma(tmem, aA, aW1, 16, 64, &s.mbar, phase, t);
+        *reinterpret_cast<uint4 *>(A0 + frow) =
+            make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
+        ok = layer_mma(tmem, aA0, aW1, 16, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile(lane_addr, s.w.b1, s.A, t);
+        epilogue_to_tile(lane_addr, s.hb[0], A, t);
         ok = layer_mma(tmem, aA, aW2, 64, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile(lane_addr, s.w.b2, s.A, t);
+        epilogue_to_tile(lane_addr, s.hb[1], A, t);
         ok = layer_mma(tmem, aA, aW3, 64, 64, &s.mbar, phase, t);
         if (!ok) break;
         float y = s.w.b4;
@@ -200,7 +239,16 @@ __global__ void __launch_bounds__(128) k_closure_infer(Grid g, ClosureScales sc,
             umma::tmem_ld16(lane_addr + (uint32_t)(cc * 16), v);
             umma::tmem_wait_ld();
 #pragma unroll
-            for (int q = 0; q < 16; q++) y += s.w.w4[cc * 16 + q] * silu(v[q] + s.w.b3[cc * 16 + q]);
+            for (int q = 0; q < 16; q += 4) {
+                const float4 b = reinterpret_cast<const float4 *>(s.hb[2])[(cc * 16 + q) / 4];
+                const float4 w = reinterpret_cast<const float4 *>(s.w.w4)[(cc * 16 + q) / 4];
+                const uint32_t p0 = silu2_bf16(fmaf(v[q], 0.5f, b.x), fmaf(v[q + 1], 0.5f, b.y));
+                const uint32_t p1 = silu2_bf16(fmaf(v[q + 2], 0.5f, b.z), fmaf(v[q + 3], 0.5f, b.w));
+                y = fmaf(w.x, __uint_as_float(p0 << 16), y);
+                y = fmaf(w.y, __uint_as_float(p0 & 0xFFFF0000u), y);
+                y = fmaf(w.z, __uint_as_float(p1 << 16), y);
+                y = fmaf(w.w, __uint_as_float(p1 & 0xFFFF0000u), y);
+            }
         }
         const float cs2 = fminf(fmaxf(y, 0.f), 0.15f);
         if (valid) {
@@ -544,7 +592,7 @@ int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, flo
             return -1;
         attr = true;
     }
-    const int blocks = 148 * 4;
+    const int blocks = 148 * 5;
     prof_begin(c, FSL_K_SGS);
     if (mu32) mlp::k_closure_infer<float><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, P, mu32, cs2_out, err);
     else mlp::k_closure_infer<double><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, P, mu64, cs2_out, err);

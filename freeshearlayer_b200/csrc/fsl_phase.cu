@@ -351,16 +351,9 @@ __global__ void k_courant_partial(Grid g, Consts kc, const double *__restrict__ 
         const int i = (int)(r / H) + 1;
         const long long c = g.idx(i, j, k);
         const double R = U[c];
-        const double Uv = U[fs + c] / R;
-        double Co;
-        if (kc.cfl_mode == FSL_CFL_ACOUSTIC) {
-            const double V = U[2 * fs + c] / R, W = U[3 * fs + c] / R;
-            const double P = (U[4 * fs + c] - 0.5 * R * (Uv * Uv + V * V + W * W)) * 0.4;
-            const double Cs = sqrt(1.4 * P / R);
-            Co = (fabs(Uv) + Cs) * dtx + (fabs(V) + Cs) * dty + (fabs(W) + Cs) * dtz;
-        } else {
-            Co = Uv * dtx;
-        }
+        const double Co = cell_courant(kc.cfl_mode, R, U[fs + c], kc.cfl_mode == FSL_CFL_ACOUSTIC ? U[2 * fs + c] : 0.,
+                                       kc.cfl_mode == FSL_CFL_ACOUSTIC ? U[3 * fs + c] : 0.,
+                                       kc.cfl_mode == FSL_CFL_ACOUSTIC ? U[4 * fs + c] : 0., dtx, dty, dtz);
         m = (Co > m) ? Co : m;
         if (!(R > 0.0)) bad = 1;
     }
@@ -385,6 +378,21 @@ __global__ void k_courant_partial(Grid g, Consts kc, const double *__restrict__ 
     }
 }
 
+// dt rescale of src/helpers.c:47-50; clears the fused accumulator for the
+// next stage 3
+__device__ __forceinline__ void apply_courant(const Consts &kc, double maxCo, DevScalars *ds)
+{
+    double dt = ds->dt;
+    dt *= (kc.maxCoNum / maxCo);
+    ds->dt = dt;
+    ds->dtx = dt / kc.deltaX;
+    ds->dty = dt / kc.deltaY;
+    ds->dtz = dt / kc.deltaZ;
+    ds->maxCo = maxCo;
+    ds->co_bits = 0ull;
+    if (!(maxCo > 0.0) || !isfinite(maxCo) || !isfinite(dt)) ds->status |= 1u;
+}
+
 // Final reduction and the dt rescale of src/helpers.c:47-50.
 __global__ void k_courant_final(Consts kc, const double *__restrict__ partials, int np, DevScalars *ds)
 {
@@ -405,16 +413,15 @@ __global__ void k_courant_final(Consts kc, const double *__restrict__ partials, 
     if (threadIdx.x == 0) {
         m = 0.0;
         for (int q = 0; q < (int)(blockDim.x >> 5); q++) m = (sm[q] > m) ? sm[q] : m;
-        const double maxCo = m;
-        double dt = ds->dt;
-        dt *= (kc.maxCoNum / maxCo);
-        ds->dt = dt;
-        ds->dtx = dt / kc.deltaX;
-        ds->dty = dt / kc.deltaY;
-        ds->dtz = dt / kc.deltaZ;
-        ds->maxCo = maxCo;
-        if (!(maxCo > 0.0) || !isfinite(maxCo) || !isfinite(dt)) ds->status |= 1u;
+        apply_courant(kc, m, ds);
     }
+}
+
+// The same dt update from the maximum the fused stage 3 of the previous step
+// accumulated over the state it wrote (that state is this step's U^n).
+__global__ void k_courant_apply(Consts kc, DevScalars *ds)
+{
+    if (threadIdx.x == 0) apply_courant(kc, __longlong_as_double((long long)ds->co_bits), ds);
 }
 
 // ---------------------------------------------------------------------------
@@ -821,6 +828,13 @@ void launch_courant(Ctx &c)
     k_courant_partial<<<c.npartials, 256, 0, c.stream>>>(g, c.k, c.U, c.ds, c.partials, c.ds);
     k_courant_final<<<1, 1024, 0, c.stream>>>(c.k, c.partials, c.npartials, c.ds);
     prof_end(c, FSL_K_CFL, 2);
+}
+
+void launch_courant_apply(Ctx &c)
+{
+    prof_begin(c, FSL_K_CFL);
+    k_courant_apply<<<1, 32, 0, c.stream>>>(c.k, c.ds);
+    prof_end(c, FSL_K_CFL, 1);
 }
 
 void launch_state_scatter(Ctx &c, double *dst, const double *packed)

@@ -256,4 +256,23 @@ __device__ __forceinline__ void face_flux(T Rho, T P, const T *vel, const T (*g)
            uu * s0 - vv * s1 - ww * s2 + q;
 }
 
+// Courant number of one cell from its conserved variables: the reference's
+// streamwise u dt/dx (src/helpers.c:31-43) or the acoustic sum
+// dt((|u|+c)/dx + (|v|+c)/dy + (|w|+c)/dz).  Every operation is an explicitly
+// rounded FP64 intrinsic, so the value does not depend on the contraction
+// flags of the translation unit: the standalone reduction and the fused
+// stage kernels (FP64 and FP32 bulk) produce the same bits.
+__device__ __forceinline__ double cell_courant(int mode, double R, double mu, double mv, double mw, double E,
+                                               double dtx, double dty, double dtz)
+{
+    const double Uv = __ddiv_rn(mu, R);
+    if (mode != 1) return __dmul_rn(Uv, dtx);
+    const double V = __ddiv_rn(mv, R), W = __ddiv_rn(mw, R);
+    const double q = __dadd_rn(__dadd_rn(__dmul_rn(Uv, Uv), __dmul_rn(V, V)), __dmul_rn(W, W));
+    const double P = __dmul_rn(__dsub_rn(E, __dmul_rn(__dmul_rn(0.5, R), q)), 0.4);
+    const double Cs = __dsqrt_rn(__ddiv_rn(__dmul_rn(1.4, P), R));
+    return __dadd_rn(__dadd_rn(__dmul_rn(__dadd_rn(fabs(Uv), Cs), dtx), __dmul_rn(__dadd_rn(fabs(V), Cs), dty)),
+                     __dmul_rn(__dadd_rn(fabs(W), Cs), dtz));
+}
+
 } // namespace fsl

@@ -143,6 +143,8 @@ template <typename T> struct Args {
     const T *mu;
     BF<T> bf;
     const DevScalars *ds;
+    unsigned long long *co; // non-null: accumulate the Courant maximum of `out` (stage 3)
+    unsigned int *status;   // bit 1 set on a non-positive output density (with co)
     int stage;
     int seg;
 };
@@ -314,6 +316,10 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
     }
     const double dtx = a.ds->dtx, dty = a.ds->dty, dtz = a.ds->dtz;
     const double one_third = 1. / 3., two_thirds = 2. / 3.;
+    // Courant maximum of the cells this thread wrote (with a.co); in shared
+    // memory rather than registers, which the FP64 16-row tile has none left of
+    __shared__ double comax[TJE][32];
+    comax[r][l] = 0.0;
     __syncthreads();
 
     for (int i = i0; i <= i1; i++) {
@@ -461,6 +467,14 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
                 else if (a.stage == 2) o = 0.75 * unv[q] + 0.25 * (b0 + X + Y + Z);
                 else o = one_third * unv[q] + two_thirds * (b0 + X + Y + Z);
                 a.out[q * fs + c] = o;
+                base[q] = o; // the new state, for the Courant number below
+            }
+            if (a.co) {
+                // the next step's check of src/helpers.c:23-52 on this state
+                const double Co = cell_courant(kc.cfl_mode, base[0], base[1], base[2], base[3], base[4], dtx, dty, dtz);
+                const double m = comax[r][l];
+                comax[r][l] = (Co > m) ? Co : m;
+                if (!(base[0] > 0.0)) atomicOr(a.status, 2u);
             }
         }
         // (g) plane i+2 into the ring slot of plane i (all readers of plane i
@@ -474,14 +488,36 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
         mu0 = mu1;
         mu1 = mu2;
     }
+    if (a.co) {
+        __syncthreads();
+        double m = comax[r][l];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double x = __shfl_xor_sync(0xffffffffu, m, o);
+            m = (x > m) ? x : m;
+        }
+        __syncthreads();
+        if (l == 0) comax[r][0] = m;
+        __syncthreads();
+        if (r == 0 && l == 0) {
+            m = 0.0;
+#pragma unroll
+            for (int q = 0; q < TJE; q++) m = (comax[q][0] > m) ? comax[q][0] : m;
+            // non-negative doubles order like their bit patterns
+            atomicMax(a.co, (unsigned long long)__double_as_longlong(m));
+        }
+    }
 }
 
 template <typename T, int TJE, int MINB>
-int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, double *out, const T *mu, BF<T> bf)
+int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, double *out, const T *mu, BF<T> bf,
+                   bool courant)
 {
     const Grid &g = c.g;
     Args<T> a;
     a.cur = cur; a.un = un; a.out = out; a.mu = mu; a.bf = bf; a.ds = c.ds; a.stage = stage;
+    a.co = courant ? &c.ds->co_bits : nullptr;
+    a.status = &c.ds->status;
     a.seg = c.stage_seg;
     const size_t smem = sizeof(Smem<T, TJE>);
     static bool attr = false;
