@@ -319,6 +319,93 @@ def matched_error(fsl, grid, state, dU, nsteps, rows, seg):
     return out
 
 
+def ensemble_members(n, seed=20251203):
+    """The batched-ensemble workload: n temporal shear layers, grids drawn from
+    {48,64,96,128} x {32,48,64} x {32,48,64}, Mc uniform in [0.2, 0.8],
+    Re_dw0 uniform in [300, 1000], perturbation seeds 0..n-1 at 1e-3 dU,
+    FP32 bulk with FP64 accumulation, dynamic Smagorinsky."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        L = int(rng.choice([48, 64, 96, 128]))
+        H = int(rng.choice([32, 48, 64]))
+        D = int(rng.choice([32, 48, 64]))
+        Mc = float(rng.uniform(0.2, 0.8))
+        Re = float(rng.uniform(300.0, 1000.0))
+        dU = 2.0 * Mc * math.sqrt(1.4 * 1e5 / 1.0)
+        p = dict(workload_params((L, H, D), precision=1, sgs=0), mu_L=dU * DW0 / Re)
+        out.append((p, Mc, q))
+    return out
+
+
+def ensemble_block(fsl, torch, steps, n):
+    """Aggregate cell-stage updates/s of n members advanced one after another
+    (each alone, fsl_step) and as one graph-replayed ensemble (autotuned tile
+    shape), from the same initial states; the final states must agree bitwise."""
+    import numpy as np
+    members = ensemble_members(n)
+    doms, states = [], []
+    for p, Mc, sd in members:
+        st, _ = fsl.temporal_state(p, Mc, DW0, AMP, sd)
+        d = fsl.Domain(p)
+        d.upload_state(st)
+        doms.append(d)
+        states.append(st)
+    cells = sum(p["LEN"] * p["HIG"] * p["DEP"] for p, _, _ in members)
+    units = cells * STAGES * steps
+    # members one after another
+    for d in doms:
+        d.step(1)  # allocation and kernel attributes outside the timed region
+        d.sync()
+    def reset():  # same initial state and time step for both runs
+        for d, st, (p, _, _) in zip(doms, states, members):
+            d.upload_state(st)
+            d.set_time(0, p["deltaT"])
+
+    reset()
+    seq_ms = 0.0
+    for d in doms:
+        ext = torch.cuda.ExternalStream(d.stream)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        d.step(steps)
+        b.record(ext)
+        b.synchronize()
+        seq_ms += a.elapsed_time(b)
+    seq_final = [d.download_state() for d in doms]
+    # the ensemble
+    e = fsl.Ensemble(doms)
+    e.step(1)
+    rows, seg, _ = e.tune(trial_steps=5)
+    reset()
+    e.step(1)  # the warm-up step after an upload runs uncaptured
+    e.sync()
+    ext = torch.cuda.ExternalStream(e.stream)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(ext)
+    e.step(steps - 1)
+    b.record(ext)
+    b.synchronize()
+    e.sync()
+    ens_ms = a.elapsed_time(b)
+    same = all(np.array_equal(d.download_state(), f) for d, f in zip(doms, seq_final))
+    e.close()
+    for d in doms:
+        d.close()
+    ens_units = cells * STAGES * (steps - 1)
+    return {"workload": "%d temporal shear layers, grids {48,64,96,128}x{32,48,64}x{32,48,64}, Mc U[0.2,0.8], "
+                        "Re_dw0 U[300,1000], noise 1e-3 dU, FP32 bulk + FP64 accumulation, dynamic Smagorinsky"
+                        % n,
+            "members": n, "cells": cells, "steps": steps,
+            "sequential": {"value": units / (seq_ms / 1e3), "ms": seq_ms},
+            "ensemble": {"value": ens_units / (ens_ms / 1e3), "ms": ens_ms, "steps": steps - 1,
+                         "tile_rows": rows, "planes_per_block": seg, "chunk": 10},
+            "speedup": (ens_units / ens_ms) / (units / seq_ms), "bit_identical": bool(same)}
+
+
 def main_gpu(args):
     import numpy as np
     import torch
@@ -422,6 +509,11 @@ def main_gpu(args):
     if rank == 0 and args.match_steps > 0:
         match = matched_error(fsl, grid, state, dU, args.match_steps, args.rows, args.seg)
 
+    # ---- batched ensemble of small uneven layers against the same run one by one ----
+    ens = None
+    if rank == 0 and args.ens_steps > 1:
+        ens = ensemble_block(fsl, torch, args.ens_steps, args.ens_members)
+
     # ---- CPU baseline: the reference's serial solver, rank 0 at N = 1 only ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -460,6 +552,8 @@ def main_gpu(args):
             line["speedup_vs_plain_fp64"] = value / plain["value"]
         if match is not None:
             line["matched_error"] = match
+        if ens is not None:
+            line["ensemble"] = ens
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -514,6 +608,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 path beside the arm")
+    ap.add_argument("--ens-steps", type=int, default=100, help="steps of the ensemble comparison (0: skip)")
+    ap.add_argument("--ens-members", type=int, default=32)
     ap.add_argument("--match-steps", type=int, default=200,
                     help="steps of the matched-error comparison against the plain FP64 path (0: skip)")
     ap.add_argument("--traffic", type=float, default=None,

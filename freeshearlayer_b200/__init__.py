@@ -31,14 +31,15 @@ __all__ = ["Params", "Domain", "FslError", "lib", "LIB_PATH", "default_params",
            "params_from_ini", "params_from_bin", "initial_state", "temporal_state",
            "SETUP_SPATIAL", "SETUP_TEMPORAL", "CFL_STREAMWISE", "CFL_ACOUSTIC",
            "PREC_FP64", "PREC_FP32", "SGS_DYNAMIC", "SGS_LEARNED", "RECON_CHARMINMOD",
-           "RECON_PPM", "Trainer", "closure_weights", "shear_statistics"]
+           "RECON_PPM", "Trainer", "Ensemble", "closure_weights", "shear_statistics"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfsl_gpu.so")
 
 FSL_OK = 0
 ERRORS = {-1: "FSL_ERR_ARG", -2: "FSL_ERR_NOMEM", -3: "FSL_ERR_CUDA", -4: "FSL_ERR_NONFINITE",
-          -5: "FSL_ERR_TIMEOUT", -6: "FSL_ERR_IO", -7: "FSL_ERR_UNSUPPORTED", -8: "FSL_ERR_NODEVICE"}
+          -5: "FSL_ERR_TIMEOUT", -6: "FSL_ERR_IO", -7: "FSL_ERR_UNSUPPORTED", -8: "FSL_ERR_NODEVICE",
+          -9: "FSL_ERR_TOO_LARGE"}
 SETUP_SPATIAL, SETUP_TEMPORAL = 0, 1
 CFL_STREAMWISE, CFL_ACOUSTIC = 0, 1
 PREC_FP64, PREC_FP32 = 0, 1
@@ -142,6 +143,12 @@ def lib():
             "fsl_trainer_gradient": [vp, ll, fp, C.POINTER(C.c_double)], "fsl_trainer_set_loss": [vp, i],
             "fsl_trainer_train": [vp, i, ll, d, C.POINTER(C.c_double)],
         })
+        sig.update({
+            "fsl_ensemble_create": [C.POINTER(C.c_void_p), i, C.POINTER(C.c_void_p)],
+            "fsl_ensemble_destroy": [vp], "fsl_ensemble_set_chunk": [vp, i], "fsl_ensemble_step": [vp, i],
+            "fsl_ensemble_sync": [vp],
+            "fsl_ensemble_tune": [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)],
+        })
         sig["fsl_tune"] = [vp, i, i]
         sig["fsl_profile"] = [vp, i]
         sig["fsl_profile_read"] = [vp, C.POINTER(KTimes)]
@@ -153,6 +160,10 @@ def lib():
         L.fsl_last_error.restype = C.c_char_p
         L.fsl_stream.argtypes = [vp]
         L.fsl_stream.restype = C.c_void_p
+        L.fsl_ensemble_last_error.argtypes = [vp]
+        L.fsl_ensemble_last_error.restype = C.c_char_p
+        L.fsl_ensemble_stream.argtypes = [vp]
+        L.fsl_ensemble_stream.restype = C.c_void_p
         L.fsl_trainer_size.argtypes = [vp]
         L.fsl_trainer_size.restype = C.c_longlong
         _lib = L
@@ -465,6 +476,54 @@ class Trainer:
         loss = C.c_double()
         _check(lib().fsl_trainer_train(self.h, epochs, batch, lr, C.byref(loss)))
         return loss.value
+
+
+class Ensemble:
+    """Independent temporal shear layers (each a :class:`Domain`) advanced
+    together: chunks of steps of all members are captured into one CUDA graph
+    and replayed (members on their own streams, so their kernels share the
+    SMs).  Results are bit-identical to stepping each member alone."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.h for m in self.members])
+        h = C.c_void_p()
+        _check(lib().fsl_ensemble_create(arr, len(self.members), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fsl_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        if rc != FSL_OK:
+            raise FslError(rc, lib().fsl_ensemble_last_error(self.h).decode())
+
+    @property
+    def stream(self) -> int:
+        return lib().fsl_ensemble_stream(self.h)
+
+    def set_chunk(self, steps: int):
+        self._c(lib().fsl_ensemble_set_chunk(self.h, steps))
+
+    def step(self, n: int = 1):
+        self._c(lib().fsl_ensemble_step(self.h, n))
+
+    def sync(self):
+        self._c(lib().fsl_ensemble_sync(self.h))
+
+    def tune(self, trial_steps: int = 5):
+        """Autotune the fused-stage tile shape; returns (rows, seg, ms per step)."""
+        r, s, ms = C.c_int(), C.c_int(), C.c_double()
+        self._c(lib().fsl_ensemble_tune(self.h, trial_steps, C.byref(r), C.byref(s), C.byref(ms)))
+        return r.value, s.value, ms.value
 
 
 # --- shear-layer statistics ----------------------------------------------------------

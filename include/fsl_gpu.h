@@ -297,6 +297,38 @@ int fsl_trainer_gradient(fsl_trainer *tr, long long n, float *grad, double *loss
 /* Adam on shuffled mini-batches; *loss receives the final full-set MSE. */
 int fsl_trainer_train(fsl_trainer *tr, int epochs, long long batch, double lr, double *loss);
 
+/* ---- ensembles -------------------------------------------------------------
+ * No counterpart in the reference (project extension; the reference runs one
+ * domain per process).  Independent temporal shear layers -- each an ordinary
+ * context with its own grid, Mach number, Reynolds number and seed -- advance
+ * together: fsl_ensemble_step captures `chunk` fused steps of every member
+ * (each on its own stream, forked from and joined to the ensemble's stream)
+ * into one CUDA graph and replays it, so the members' kernels share the SMs
+ * and a chunk costs one launch.  Every member's result is bit-identical to
+ * stepping it alone with fsl_step.  Members: temporal setup, nStages = 3, no
+ * profiling, learned closure only with judgements off
+ * (fsl_closure_judge(ctx, 0, ...)); otherwise FSL_ERR_UNSUPPORTED.  Members
+ * stay owned by the caller and must outlive the ensemble; while an ensemble
+ * step is in flight, do not call them directly.  Each member's disturbance
+ * RNG state (unused by the temporal setup) is not advanced by replays. */
+typedef struct fsl_ensemble fsl_ensemble;
+int fsl_ensemble_create(fsl_ctx *const *members, int n, fsl_ensemble **ens);
+int fsl_ensemble_destroy(fsl_ensemble *ens);
+const char *fsl_ensemble_last_error(const fsl_ensemble *ens);
+/* The ensemble's CUDA stream (cudaStream_t); its work follows and precedes
+ * the members' own streams. */
+void *fsl_ensemble_stream(fsl_ensemble *ens);
+/* Steps captured per graph (1..1000, default 10). */
+int fsl_ensemble_set_chunk(fsl_ensemble *ens, int steps);
+int fsl_ensemble_step(fsl_ensemble *ens, int nsteps);
+int fsl_ensemble_sync(fsl_ensemble *ens);
+/* Autotuner of the fused-stage tile shape (tile rows 8/12/16 x planes per
+ * block 8/16/32/64, one shape for all members): each candidate is timed on
+ * the device over one graph replay of trial_steps ensemble steps; the
+ * fastest is kept and every member's state, time step and counters are
+ * restored, so tuning changes no result. */
+int fsl_ensemble_tune(fsl_ensemble *ens, int trial_steps, int *rows, int *seg, double *ms_per_step);
+
 /* ---- profiling ------------------------------------------------------------- */
 
 /* Kernel classes timed by the context's profiler. */

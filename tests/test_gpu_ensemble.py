@@ -1,0 +1,91 @@
+"""Ensembles: graph-replayed steps of independent shear layers give the same
+bits as stepping each member alone; the autotuner changes no result."""
+import math
+
+import numpy as np
+import pytest
+
+from tests.helpers import temporal_params
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def fsl():
+    import freeshearlayer_b200 as fsl
+    return fsl
+
+
+# uneven grids, Mach and Reynolds numbers, precisions and closures
+MEMBERS = [
+    dict(L=24, H=16, D=16, Mc=0.3, Re=400.0, precision=0, sgs=0, seed=1),
+    dict(L=32, H=12, D=24, Mc=0.5, Re=700.0, precision=1, sgs=0, seed=2),
+    dict(L=16, H=24, D=12, Mc=0.7, Re=1000.0, precision=1, sgs=1, seed=3),
+    dict(L=40, H=16, D=8, Mc=0.2, Re=300.0, precision=0, sgs=1, seed=4),
+    dict(L=24, H=20, D=36, Mc=0.6, Re=550.0, precision=1, sgs=0, seed=5),
+]
+
+
+def _member(fsl, m, amp=1e-2):
+    p = temporal_params(L=m["L"], H=m["H"], D=m["D"], Mc=m["Mc"], Re=m["Re"], precision=m["precision"],
+                        sgs=m["sgs"])
+    s, dU = fsl.temporal_state(p, m["Mc"], 1.0, amp, m["seed"])
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    if m["sgs"] == 1:
+        d.closure_set_scales(1.0 / dU, 1.0)
+        d.closure_set_weights(fsl.closure_weights())
+        d.closure_judge(0, 1.0)
+    return d
+
+
+def test_ensemble_matches_members_stepped_alone(fsl):
+    ens_m = [_member(fsl, m) for m in MEMBERS]
+    ref_m = [_member(fsl, m) for m in MEMBERS]
+    e = fsl.Ensemble(ens_m)
+    e.set_chunk(5)
+    e.step(23)  # one plain warm-up step, 4 replays of 5, a 2-step tail graph
+    e.step(10)  # 2 replays of the cached graph
+    e.sync()
+    for d, r in zip(ens_m, ref_m):
+        r.step(33)
+        a, b = d.download_state(), r.download_state()
+        assert np.all(np.isfinite(a))
+        assert np.array_equal(a, b)
+        ia, ib = d.info(), r.info()
+        assert ia.step == ib.step == 33 and ia.deltaT == ib.deltaT
+    e.close()
+
+
+def test_tuner_changes_no_result(fsl):
+    ens_m = [_member(fsl, m) for m in MEMBERS[:3]]
+    ref_m = [_member(fsl, m) for m in MEMBERS[:3]]
+    e = fsl.Ensemble(ens_m)
+    e.step(4)
+    rows, seg, ms = e.tune(trial_steps=2)
+    assert rows in (8, 12, 16) and seg in (8, 16, 32, 64) and ms > 0
+    e.step(6)
+    e.sync()
+    for d, r in zip(ens_m, ref_m):
+        r.step(10)
+        assert np.array_equal(d.download_state(), r.download_state())
+        assert d.info().step == 10
+    e.close()
+
+
+def test_unsupported_members_are_refused(fsl):
+    from tests.helpers import spatial_params
+    d = fsl.Domain(spatial_params(L=12, H=8, D=6))
+    e = fsl.Ensemble([d])
+    with pytest.raises(fsl.FslError) as ex:
+        e.step(1)
+    assert ex.value.code == -7
+    e.close()
+    m = dict(MEMBERS[2])
+    d2 = _member(fsl, m)
+    d2.closure_judge(100, 0.02)
+    e2 = fsl.Ensemble([d2])
+    with pytest.raises(fsl.FslError) as ex:
+        e2.step(1)
+    assert ex.value.code == -7
+    e2.close()
