@@ -61,6 +61,7 @@ int ensure_closure(Ctx &c)
     if (cudaMalloc((void **)&c.cd32, fs * sizeof(float)) != cudaSuccess) return FSL_ERR_NOMEM;
     if (cudaMalloc((void **)&c.cs2_32, fs * sizeof(float)) != cudaSuccess) return FSL_ERR_NOMEM;
     if (cudaMalloc((void **)&c.cl_err, sizeof(int)) != cudaSuccess) return FSL_ERR_NOMEM;
+    if (cudaMalloc((void **)&c.cl_vel, 3 * fs * sizeof(float)) != cudaSuccess) return FSL_ERR_NOMEM;
     if (cudaMalloc((void **)&c.judge_rows, 8 * (size_t)c.g.H * sizeof(double)) != cudaSuccess) return FSL_ERR_NOMEM;
     if (c.p.precision == FSL_PREC_FP32) {
         if (cudaMalloc((void **)&c.mu32_alt, fs * sizeof(float)) != cudaSuccess) return FSL_ERR_NOMEM;
@@ -72,7 +73,8 @@ int ensure_closure(Ctx &c)
     cudaMemsetAsync(c.cd32, 0, fs * sizeof(float), c.stream);
     cudaMemsetAsync(c.cs2_32, 0, fs * sizeof(float), c.stream);
     cudaMemsetAsync(c.cl_err, 0, sizeof(int), c.stream);
-    c.bytes += fs * (sizeof(float) * 3 + sizeof(double)) + kNParams * sizeof(float);
+    cudaMemsetAsync(c.cl_vel, 0, 3 * fs * sizeof(float), c.stream);
+    c.bytes += fs * (sizeof(float) * 6 + sizeof(double)) + kNParams * sizeof(float);
     c.cl_alloc = true;
     return FSL_OK;
 }
@@ -203,7 +205,7 @@ int closure_ensure(Ctx &c) { return ensure_closure(c); }
 void closure_free(Ctx &c)
 {
     if (!c.cl_alloc) return;
-    cudaFree(c.cl_params); cudaFree(c.cd32); cudaFree(c.cs2_32); cudaFree(c.cl_err); cudaFree(c.judge_rows);
+    cudaFree(c.cl_params); cudaFree(c.cd32); cudaFree(c.cs2_32); cudaFree(c.cl_err); cudaFree(c.cl_vel); cudaFree(c.judge_rows);
     cudaFree(c.mu_alt); cudaFree(c.mu32_alt);
     c.cl_alloc = false;
 }

@@ -111,6 +111,7 @@ struct Ctx {
     double *mu_alt = nullptr;   // closure mu on judgement steps (FP64 path)
     float *mu32_alt = nullptr;  // closure mu on judgement steps (FP32 path)
     int *cl_err = nullptr;      // device error flag of the tensor-core kernels
+    float *cl_vel = nullptr;    // FP32 velocities of the padded cells (closure features), 3 fields
     double *judge_rows = nullptr; // [2][HIG][4] plane sums of the judgement (Cs^2, mu_SGS)
     bool cl_alloc = false, cl_weights = false;
     int judge_every = 100;

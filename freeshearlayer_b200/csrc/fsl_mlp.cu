@@ -60,6 +60,80 @@ __device__ __forceinline__ void cell_features(const Grid &g, const double *__res
     f[7] = sc.delta_ratio;
 }
 
+// FP32 velocities of every padded cell, formed exactly as cell_features forms
+// them (rho u as float times the float of the FP64 reciprocal), so features
+// computed from this field equal cell_features bit for bit.
+__global__ void k_closure_vel(Grid g, const double *__restrict__ U, float *__restrict__ vel)
+{
+    const long long fs = g.fstride;
+    const long long n = (long long)(g.L + 2) * g.pi;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        if ((int)(t % g.pk) >= g.D + 2) continue; // row padding
+        const long long a = g.off + t;
+        const double r = U[a];
+        const float rr = (float)(1. / r);
+        vel[a] = (float)U[fs + a] * rr;
+        vel[fs + a] = (float)U[2 * fs + a] * rr;
+        vel[2 * fs + a] = (float)U[3 * fs + a] * rr;
+    }
+}
+
+// The raw inputs of one cell's features: the six neighbours' velocities and
+// the cell's density, loaded one tile ahead of their use.
+struct FeatIn {
+    float u[7], v[7], w[7];
+    double r;
+    long long c;
+    bool valid;
+};
+
+__device__ __forceinline__ void feat_load(const Grid &g, const double *__restrict__ U, const float *__restrict__ vel,
+                                          long long cell, long long ncell, FeatIn &p)
+{
+    p.valid = cell < ncell;
+    p.c = 0;
+    if (!p.valid) return;
+    const int k = (int)(cell % g.D) + 1;
+    const long long rr = cell / g.D;
+    const int j = (int)(rr % g.H) + 1, i = (int)(rr / g.H) + 1;
+    const long long c = g.idx(i, j, k), fs = g.fstride;
+    const long long off[7] = {0, g.pi, -g.pi, (long long)g.pk, -(long long)g.pk, 1, -1};
+#pragma unroll
+    for (int n = 1; n < 7; n++) {
+        const long long a = c + off[n];
+        p.u[n] = vel[a];
+        p.v[n] = vel[fs + a];
+        p.w[n] = vel[2 * fs + a];
+    }
+    p.r = U[c];
+    p.c = c;
+}
+
+__device__ __forceinline__ void cell_features_v(const FeatIn &p, const ClosureScales &sc, float *f, float &rho,
+                                                float &Smag)
+{
+    const float *u = p.u, *v = p.v, *w = p.w;
+    rho = (float)p.r;
+    const float ax = sc.r2dx, ay = sc.r2dy, az = sc.r2dz;
+    const float du_dx = (u[1] - u[2]) * ax, du_dy = (u[3] - u[4]) * ay, du_dz = (u[5] - u[6]) * az;
+    const float dv_dx = (v[1] - v[2]) * ax, dv_dy = (v[3] - v[4]) * ay, dv_dz = (v[5] - v[6]) * az;
+    const float dw_dx = (w[1] - w[2]) * ax, dw_dy = (w[3] - w[4]) * ay, dw_dz = (w[5] - w[6]) * az;
+    const float S11 = du_dx, S22 = dv_dy, S33 = dw_dz;
+    const float S12 = 0.5f * (du_dy + dv_dx), S13 = 0.5f * (du_dz + dw_dx), S23 = 0.5f * (dv_dz + dw_dy);
+    const float S = sqrtf(2.f * (S11 * S11 + S22 * S22 + S33 * S33 + 2.f * (S12 * S12 + S13 * S13 + S23 * S23)));
+    Smag = S;
+    const float inv = 1.f / (S + 1e-30f);
+    f[0] = log1pf(S * sc.t_ref);
+    f[1] = S11 * inv;
+    f[2] = S22 * inv;
+    f[3] = S12 * inv;
+    f[4] = S13 * inv;
+    f[5] = S23 * inv;
+    f[6] = rho;
+    f[7] = sc.delta_ratio;
+}
+
 // SiLU and its derivative with sigmoid(x) = 0.5 tanh(x/2) + 0.5
 __device__ __forceinline__ float tanh_fast(float x)
 {
@@ -115,12 +189,14 @@ struct SmemInfer {
 };
 
 // silu of two values in packed BF16 arithmetic from h = (z + b) / 2 given in
-// FP32: silu = h + h tanh(h), one MUFU operation per pair.  Result: element 0
-// in the low half (the lower k of a K-major tile row).
+// FP32: silu = h + h tanh(h), one MUFU operation per pair.  h is cut to BF16
+// by truncation (a byte permute on the integer pipe rather than a conversion
+// on the MUFU pipe that bounds this kernel).  Result: element 0 in the low
+// half (the lower k of a K-major tile row).
 __device__ __forceinline__ uint32_t silu2_bf16(float h0, float h1)
 {
-    uint32_t hp, th, y;
-    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hp) : "f"(h1), "f"(h0));
+    uint32_t th, y;
+    const uint32_t hp = __byte_perm(__float_as_uint(h0), __float_as_uint(h1), 0x7632);
     asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(hp));
     asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(y) : "r"(hp), "r"(th));
     return y;
@@ -184,6 +260,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // next product either way); the last layer's dot product with w4 is FP32.
 template <typename MT>
 __global__ void __launch_bounds__(128, 5) k_closure_infer(Grid g, ClosureScales sc, const double *__restrict__ U,
+                                                          const float *__restrict__ vel,
                                                           const float *__restrict__ P, MT *__restrict__ mu,
                                                           float *__restrict__ cs2_out, int *err)
 {
@@ -210,20 +287,17 @@ __global__ void __launch_bounds__(128, 5) k_closure_infer(Grid g, ClosureScales 
     bool ok = true;
     const long long ncell = (long long)g.L * g.H * g.D;
     const long long ntile = (ncell + 127) / 128;
+    FeatIn in;
+    feat_load(g, U, vel, (long long)blockIdx.x * 128 + t, ncell, in);
     for (long long tile = blockIdx.x; tile < ntile && ok; tile += gridDim.x) {
-        const long long cell = tile * 128 + t;
-        const bool valid = cell < ncell;
-        long long c = 0;
+        const bool valid = in.valid;
+        const long long c = in.c;
         float f[8] = {0, 0, 0, 0, 0, 0, 0, 0}, rho = 0.f, Smag = 0.f;
-        if (valid) {
-            const int k = (int)(cell % g.D) + 1;
-            const long long rr = cell / g.D;
-            const int j = (int)(rr % g.H) + 1, i = (int)(rr / g.H) + 1;
-            c = g.idx(i, j, k);
-            cell_features(g, U, c, sc, f, rho, Smag);
-        }
+        if (valid) cell_features_v(in, sc, f, rho, Smag);
         *reinterpret_cast<uint4 *>(A0 + frow) =
             make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
+        // the next tile's inputs load while this tile is on the tensor cores
+        feat_load(g, U, vel, (tile + gridDim.x) * 128 + t, ncell, in);
         ok = layer_mma(tmem, aA0, aW1, 16, 64, &s.mbar, phase, t);
         if (!ok) break;
         epilogue_to_tile(lane_addr, s.hb[0], A, t);
@@ -582,6 +656,9 @@ size_t closure_train_smem() { return sizeof(mlp::SmemTrain); }
 
 int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, float *cs2_out, const float *P, int *err)
 {
+    prof_begin(c, FSL_K_SGS);
+    mlp::k_closure_vel<<<148 * 8, 256, 0, c.stream>>>(c.g, U, c.cl_vel);
+    prof_end(c, FSL_K_SGS, 1);
     const size_t smem = sizeof(mlp::SmemInfer);
     static bool attr = false;
     if (!attr) {
@@ -594,8 +671,10 @@ int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, flo
     }
     const int blocks = 148 * 5;
     prof_begin(c, FSL_K_SGS);
-    if (mu32) mlp::k_closure_infer<float><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, P, mu32, cs2_out, err);
-    else mlp::k_closure_infer<double><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, P, mu64, cs2_out, err);
+    if (mu32)
+        mlp::k_closure_infer<float><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu32, cs2_out, err);
+    else
+        mlp::k_closure_infer<double><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu64, cs2_out, err);
     prof_end(c, FSL_K_SGS, 1);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -26,14 +26,16 @@ template <typename T> struct Kc {
     static constexpr T TWO_THIRDS = T(0.666666666666667);
 };
 
-// Chakravarthy-Osher minmod, compression 4 (src/reconstruction.c:17-24)
+// Chakravarthy-Osher minmod, compression 4 (src/reconstruction.c:17-24),
+// written as selects: the same comparisons on the same values, so the same
+// result, without data-dependent branches that split a warp.  (y = 0 never
+// reaches |4y|: x y = 0 returns 0 first.)
 template <typename T> __device__ __forceinline__ T minmod(T x, T y)
 {
-    T ay;
-    if (x * y <= T(0)) return T(0);
-    ay = ((y *= T(4.0)) > T(0)) ? y : -y;
-    if (x > T(0)) return (x < ay) ? x : ay;
-    return ((-x < ay) ? x : -ay);
+    const T y4 = y * T(4.0);
+    const T ay = (y4 > T(0)) ? y4 : -y4;
+    const T r = (x > T(0)) ? ((x < ay) ? x : ay) : ((-x < ay) ? x : -ay);
+    return (x * y <= T(0)) ? T(0) : r;
 }
 
 // Per-cell quantities shared by the three sweeps (src/reconstruction.c:63-88,
@@ -185,18 +187,24 @@ __device__ __forceinline__ void riemann(const T *Lm, const T *Rp, T &Rho, T &Pr,
     Un = T(0.5) * (lv[N - 1] + rv[N - 1]);
     C = T(0.5) * (_C + C_);
     C_p = Un + C; C_m = Un - C; C_o = Un;
-    if (C_p > T(0.)) { al_p = k::K_1_2 * (_jm - _jp) / _jo; J_p = _jp; }
-    else { al_p = k::K_1_2 * (jm_ - jp_) / jo_; J_p = jp_; }
-    if (C_m > T(0.)) { al_m = k::K_1_2 * (_jp - _jm) / _jo; J_m = _jm; }
-    else { al_m = k::K_1_2 * (jp_ - jm_) / jo_; J_m = jm_; }
-    if (C_o > T(0.)) { al_o = k::K05 * (_jp - _jm); al_o = -al_o * al_o; J_o = _jo; }
-    else { al_o = k::K05 * (jp_ - jm_); al_o = -al_o * al_o; J_o = jo_; }
+    // upwind choices of src/fluxes.c:90-108 as operand selects (one division
+    // each on the chosen operands: the same arithmetic as the branches)
+    const bool pp = C_p > T(0.), pm = C_m > T(0.), po = C_o > T(0.);
+    al_p = k::K_1_2 * (pp ? (_jm - _jp) : (jm_ - jp_)) / (pp ? _jo : jo_);
+    J_p = pp ? _jp : jp_;
+    al_m = k::K_1_2 * (pm ? (_jp - _jm) : (jp_ - jm_)) / (pm ? _jo : jo_);
+    J_m = pm ? _jm : jm_;
+    al_o = k::K05 * (po ? (_jp - _jm) : (jp_ - jm_));
+    al_o = -al_o * al_o;
+    J_o = po ? _jo : jo_;
     P = (J_p - J_m) / (al_p - al_m);
     Un = J_p - al_p * P;
     Rho = (J_o - P) / al_o;
     Pr = P;
-    if (Un > T(0)) { vel[0] = lv[0]; vel[1] = lv[1]; vel[2] = lv[2]; }
-    else { vel[0] = rv[0]; vel[1] = rv[1]; vel[2] = rv[2]; }
+    const bool up = Un > T(0);
+    vel[0] = up ? lv[0] : rv[0];
+    vel[1] = up ? lv[1] : rv[1];
+    vel[2] = up ? lv[2] : rv[2];
     vel[N - 1] = Un;
 }
 

@@ -454,18 +454,32 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
         if (inter) {
             const long long c = cj + (long long)i * g.pi;
             const T *Uc = s.U[u0][r + 1][l + 1];
+            (void)Uc;
 #pragma unroll
             for (int q = 0; q < 5; q++) {
-                const double X = dtx * ((double)Fxp[q] - (double)Fx[q]);
-                const double Y = dty * ((double)s.Fy[r - 1][l][q] - (double)s.Fy[r][l][q]);
-                const double Z = dtz * ((double)Fzm[q] - (double)Fz[q]);
-                // the stage state itself in FP64 (shared copy is exact for T = double)
-                const double b0 = sizeof(T) == 8 ? (double)Uc[q] : base[q];
-                if (sizeof(T) == 8 && a.stage != 1) unv[q] = a.un[q * fs + c];
                 double o;
-                if (a.stage == 1) o = b0 + X + Y + Z;
-                else if (a.stage == 2) o = 0.75 * unv[q] + 0.25 * (b0 + X + Y + Z);
-                else o = one_third * unv[q] + two_thirds * (b0 + X + Y + Z);
+                if constexpr (sizeof(T) == 8) {
+                    // the reference's order, ((b0 + X) + Y) + Z, on the stage
+                    // state itself (the shared copy is exact for T = double)
+                    const double X = dtx * ((double)Fxp[q] - (double)Fx[q]);
+                    const double Y = dty * ((double)s.Fy[r - 1][l][q] - (double)s.Fy[r][l][q]);
+                    const double Z = dtz * ((double)Fzm[q] - (double)Fz[q]);
+                    const double b0 = (double)Uc[q];
+                    if (a.stage != 1) unv[q] = a.un[q * fs + c];
+                    if (a.stage == 1) o = b0 + X + Y + Z;
+                    else if (a.stage == 2) o = 0.75 * unv[q] + 0.25 * (b0 + X + Y + Z);
+                    else o = one_third * unv[q] + two_thirds * (b0 + X + Y + Z);
+                } else {
+                    // FP32 bulk: the divergence in FP32 (one conversion), the
+                    // stage combination in FP64 on the FP64 stage state
+                    const T X = T(dtx) * (Fxp[q] - Fx[q]);
+                    const T Y = T(dty) * (s.Fy[r - 1][l][q] - s.Fy[r][l][q]);
+                    const T Z = T(dtz) * (Fzm[q] - Fz[q]);
+                    const double inc = (double)(X + Y + Z);
+                    if (a.stage == 1) o = base[q] + inc;
+                    else if (a.stage == 2) o = 0.75 * unv[q] + 0.25 * (base[q] + inc);
+                    else o = one_third * unv[q] + two_thirds * (base[q] + inc);
+                }
                 a.out[q * fs + c] = o;
                 base[q] = o; // the new state, for the Courant number below
             }
