@@ -179,20 +179,85 @@ __device__ __forceinline__ void stage_weights(SmemW &s, const float *__restrict_
 }
 
 // ---- inference -----------------------------------------------------------------
+// The inference tiles fold everything linear into the tensor-core products:
+// each layer's operand carries two constant-one columns (K = 16 for the
+// features, 80 = 64 + 16 for the hidden layers) against the bias split into a
+// BF16 high and low part, and weights and biases of the hidden layers are
+// pre-scaled by 1/2, so the accumulator holds h = (z + b) / 2 and
+// silu(z + b) = h + h tanh(h) needs no further FP32 work.  The output layer
+// (w4, b4) is a fourth product with N = 16 (row 0 live).
+constexpr int kKH = 80; // K of the hidden-layer operands
+
 struct SmemInfer {
-    SmemW w;
-    alignas(16) float hb[3][64];              // b1, b2, b3 halved (silu(z + b) = h + h tanh h, h = (z + b) / 2)
-    alignas(128) __nv_bfloat16 A0[128 * 16];  // features (K-major tile, columns 8..15 zero)
-    alignas(128) __nv_bfloat16 A[128 * 64];   // activations of the current layer (K-major tile)
+    alignas(128) __nv_bfloat16 W1[64 * 16];
+    alignas(128) __nv_bfloat16 W2[64 * kKH];
+    alignas(128) __nv_bfloat16 W3[64 * kKH];
+    alignas(128) __nv_bfloat16 W4[16 * kKH];
+    alignas(128) __nv_bfloat16 A0[128 * 16];  // features (K-major tile; columns 8, 9 one, 10..15 zero)
+    alignas(128) __nv_bfloat16 A[128 * kKH];  // activations (K-major; columns 64, 65 one, 66..79 zero)
     uint64_t mbar;
     uint32_t tholder;
 };
 
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
+{
+    hi = __float2bfloat16_rn(x);
+    lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+// element (o, i) of a K-major operand of width K
+__device__ __forceinline__ __nv_bfloat16 &tile_el(__nv_bfloat16 *T, int o, int i, int K)
+{
+    return T[umma::tile_off(o, i, K) / 2];
+}
+
+__device__ __forceinline__ void stage_infer_weights(SmemInfer &s, const float *__restrict__ P, int t, int nt)
+{
+    const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
+    for (int e = t; e < 64 * 16; e += nt) {
+        const int o = e / 16, i = e % 16;
+        __nv_bfloat16 v = z;
+        if (i < 8) v = __float2bfloat16_rn(0.5f * P[kOffW1 + o * 16 + i]);
+        tile_el(s.W1, o, i, 16) = v;
+    }
+    for (int e = t; e < 64 * kKH; e += nt) {
+        const int o = e / kKH, i = e % kKH;
+        __nv_bfloat16 v2 = z, v3 = z;
+        if (i < 64) {
+            v2 = __float2bfloat16_rn(0.5f * P[kOffW2 + o * 64 + i]);
+            v3 = __float2bfloat16_rn(0.5f * P[kOffW3 + o * 64 + i]);
+        }
+        tile_el(s.W2, o, i, kKH) = v2;
+        tile_el(s.W3, o, i, kKH) = v3;
+    }
+    for (int e = t; e < 16 * kKH; e += nt) {
+        const int o = e / kKH, i = e % kKH;
+        tile_el(s.W4, o, i, kKH) = (o == 0 && i < 64) ? __float2bfloat16_rn(P[kOffW4 + i]) : z;
+    }
+    __syncthreads(); // the bias columns below overwrite zeros written above
+    if (t < 64) {
+        __nv_bfloat16 hi, lo;
+        split_bf16(0.5f * P[kOffB1 + t], hi, lo);
+        tile_el(s.W1, t, 8, 16) = hi;
+        tile_el(s.W1, t, 9, 16) = lo;
+        split_bf16(0.5f * P[kOffB2 + t], hi, lo);
+        tile_el(s.W2, t, 64, kKH) = hi;
+        tile_el(s.W2, t, 65, kKH) = lo;
+        split_bf16(0.5f * P[kOffB3 + t], hi, lo);
+        tile_el(s.W3, t, 64, kKH) = hi;
+        tile_el(s.W3, t, 65, kKH) = lo;
+    } else if (t == 64) {
+        __nv_bfloat16 hi, lo;
+        split_bf16(P[kOffB4], hi, lo);
+        tile_el(s.W4, 0, 64, kKH) = hi;
+        tile_el(s.W4, 0, 65, kKH) = lo;
+    }
+}
+
 // silu of two values in packed BF16 arithmetic from h = (z + b) / 2 given in
 // FP32: silu = h + h tanh(h), one MUFU operation per pair.  h is cut to BF16
-// by truncation (a byte permute on the integer pipe rather than a conversion
-// on the MUFU pipe that bounds this kernel).  Result: element 0 in the low
-// half (the lower k of a K-major tile row).
+// by truncation (a byte permute on the integer pipe).  Result: element 0 in
+// the low half (the lower k of a K-major tile row).
 __device__ __forceinline__ uint32_t silu2_bf16(float h0, float h1)
 {
     uint32_t th, y;
@@ -221,11 +286,11 @@ __device__ __forceinline__ bool layer_mma(uint32_t tmem, uint32_t a, uint32_t b,
     return ok;
 }
 
-// bias + SiLU of this thread's TMEM accumulator row (64 columns) into row t
-// of the next K = 64 activation tile, 8 BF16 (16 bytes) per shared store
-__device__ __forceinline__ void epilogue_to_tile(uint32_t taddr, const float *hb, unsigned char *A, int t)
+// SiLU of this thread's TMEM accumulator row (64 columns, h = (z + b) / 2)
+// into row t of the next activation tile (K = 80), 8 BF16 per 16-byte store
+__device__ __forceinline__ void epilogue_to_tile(uint32_t taddr, unsigned char *A, int t)
 {
-    const uint32_t row = (uint32_t)(t >> 3) * 1024u + (uint32_t)(t & 7) * 16u;
+    const uint32_t row = (uint32_t)(t >> 3) * (uint32_t)(kKH * 16) + (uint32_t)(t & 7) * 16u;
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         float v[16];
@@ -233,14 +298,12 @@ __device__ __forceinline__ void epilogue_to_tile(uint32_t taddr, const float *hb
         umma::tmem_wait_ld();
 #pragma unroll
         for (int half = 0; half < 2; half++) {
-            const float4 b0 = reinterpret_cast<const float4 *>(hb)[c * 4 + half * 2];
-            const float4 b1 = reinterpret_cast<const float4 *>(hb)[c * 4 + half * 2 + 1];
             const float *x = v + half * 8;
             uint4 pk;
-            pk.x = silu2_bf16(fmaf(x[0], 0.5f, b0.x), fmaf(x[1], 0.5f, b0.y));
-            pk.y = silu2_bf16(fmaf(x[2], 0.5f, b0.z), fmaf(x[3], 0.5f, b0.w));
-            pk.z = silu2_bf16(fmaf(x[4], 0.5f, b1.x), fmaf(x[5], 0.5f, b1.y));
-            pk.w = silu2_bf16(fmaf(x[6], 0.5f, b1.z), fmaf(x[7], 0.5f, b1.w));
+            pk.x = silu2_bf16(x[0], x[1]);
+            pk.y = silu2_bf16(x[2], x[3]);
+            pk.z = silu2_bf16(x[4], x[5]);
+            pk.w = silu2_bf16(x[6], x[7]);
             *reinterpret_cast<uint4 *>(A + row + (uint32_t)(c * 2 + half) * 128u) = pk;
         }
     }
@@ -259,7 +322,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // hidden-layer SiLU runs in packed BF16 (its results are BF16 operands of the
 // next product either way); the last layer's dot product with w4 is FP32.
 template <typename MT>
-__global__ void __launch_bounds__(128, 5) k_closure_infer(Grid g, ClosureScales sc, const double *__restrict__ U,
+__global__ void __launch_bounds__(128, 4) k_closure_infer(Grid g, ClosureScales sc, const double *__restrict__ U,
                                                           const float *__restrict__ vel,
                                                           const float *__restrict__ P, MT *__restrict__ mu,
                                                           float *__restrict__ cs2_out, int *err)
@@ -267,13 +330,17 @@ __global__ void __launch_bounds__(128, 5) k_closure_infer(Grid g, ClosureScales 
     extern __shared__ __align__(1024) unsigned char smraw[];
     SmemInfer &s = *reinterpret_cast<SmemInfer *>(smraw);
     const int t = threadIdx.x, wp = t >> 5;
-    stage_weights(s.w, P, t, 128);
-    for (int e = t; e < 3 * 64; e += 128) s.hb[e / 64][e % 64] = 0.5f * P[(e < 64 ? kOffB1 : e < 128 ? kOffB2 : kOffB3) + e % 64];
+    stage_infer_weights(s, P, t, 128);
     unsigned char *A0 = reinterpret_cast<unsigned char *>(s.A0);
     unsigned char *A = reinterpret_cast<unsigned char *>(s.A);
-    // feature row t: columns 0..7 at +0, zero columns 8..15 at +128
+    const uint32_t one2 = 0x3F803F80u; // two BF16 ones
+    // feature row t: columns 0..7 at +0; columns 8..15 = (1, 1, 0, ...) at +128
     const uint32_t frow = (uint32_t)(t >> 3) * 256u + (uint32_t)(t & 7) * 16u;
-    *reinterpret_cast<uint4 *>(A0 + frow + 128u) = make_uint4(0u, 0u, 0u, 0u);
+    *reinterpret_cast<uint4 *>(A0 + frow + 128u) = make_uint4(one2, 0u, 0u, 0u);
+    // activation row t: columns 64..79 = (1, 1, 0, ...) in core-matrix groups 8, 9
+    const uint32_t arow = (uint32_t)(t >> 3) * (uint32_t)(kKH * 16) + (uint32_t)(t & 7) * 16u;
+    *reinterpret_cast<uint4 *>(A + arow + 8u * 128u) = make_uint4(one2, 0u, 0u, 0u);
+    *reinterpret_cast<uint4 *>(A + arow + 9u * 128u) = make_uint4(0u, 0u, 0u, 0u);
     if (t == 0) umma::mbar_init(&s.mbar, 1);
     if (wp == 0) umma::tmem_alloc(&s.tholder, 64);
     umma::fence_before_sync();
@@ -281,8 +348,8 @@ __global__ void __launch_bounds__(128, 5) k_closure_infer(Grid g, ClosureScales 
     umma::fence_after_sync();
     const uint32_t tmem = s.tholder;
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * wp) << 16);
-    const uint32_t aA0 = umma::smem_u32(s.A0), aA = umma::smem_u32(s.A), aW1 = umma::smem_u32(s.w.W1),
-                   aW2 = umma::smem_u32(s.w.W2), aW3 = umma::smem_u32(s.w.W3);
+    const uint32_t aA0 = umma::smem_u32(s.A0), aA = umma::smem_u32(s.A), aW1 = umma::smem_u32(s.W1),
+                   aW2 = umma::smem_u32(s.W2), aW3 = umma::smem_u32(s.W3), aW4 = umma::smem_u32(s.W4);
     uint32_t phase = 0;
     bool ok = true;
     const long long ncell = (long long)g.L * g.H * g.D;
@@ -300,31 +367,19 @@ __global__ void __launch_bounds__(128, 5) k_closure_infer(Grid g, ClosureScales 
         feat_load(g, U, vel, (tile + gridDim.x) * 128 + t, ncell, in);
         ok = layer_mma(tmem, aA0, aW1, 16, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile(lane_addr, s.hb[0], A, t);
-        ok = layer_mma(tmem, aA, aW2, 64, 64, &s.mbar, phase, t);
+        epilogue_to_tile(lane_addr, A, t);
+        ok = layer_mma(tmem, aA, aW2, kKH, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile(lane_addr, s.hb[1], A, t);
-        ok = layer_mma(tmem, aA, aW3, 64, 64, &s.mbar, phase, t);
+        epilogue_to_tile(lane_addr, A, t);
+        ok = layer_mma(tmem, aA, aW3, kKH, 64, &s.mbar, phase, t);
         if (!ok) break;
-        float y = s.w.b4;
-#pragma unroll
-        for (int cc = 0; cc < 4; cc++) {
-            float v[16];
-            umma::tmem_ld16(lane_addr + (uint32_t)(cc * 16), v);
-            umma::tmem_wait_ld();
-#pragma unroll
-            for (int q = 0; q < 16; q += 4) {
-                const float4 b = reinterpret_cast<const float4 *>(s.hb[2])[(cc * 16 + q) / 4];
-                const float4 w = reinterpret_cast<const float4 *>(s.w.w4)[(cc * 16 + q) / 4];
-                const uint32_t p0 = silu2_bf16(fmaf(v[q], 0.5f, b.x), fmaf(v[q + 1], 0.5f, b.y));
-                const uint32_t p1 = silu2_bf16(fmaf(v[q + 2], 0.5f, b.z), fmaf(v[q + 3], 0.5f, b.w));
-                y = fmaf(w.x, __uint_as_float(p0 << 16), y);
-                y = fmaf(w.y, __uint_as_float(p0 & 0xFFFF0000u), y);
-                y = fmaf(w.z, __uint_as_float(p1 << 16), y);
-                y = fmaf(w.w, __uint_as_float(p1 & 0xFFFF0000u), y);
-            }
-        }
-        const float cs2 = fminf(fmaxf(y, 0.f), 0.15f);
+        epilogue_to_tile(lane_addr, A, t);
+        ok = layer_mma(tmem, aA, aW4, kKH, 16, &s.mbar, phase, t);
+        if (!ok) break;
+        float v[16];
+        umma::tmem_ld16(lane_addr, v);
+        umma::tmem_wait_ld();
+        const float cs2 = fminf(fmaxf(v[0], 0.f), 0.15f);
         if (valid) {
             mu[c] = (MT)(rho * cs2 * sc.DD * Smag);
             if (cs2_out) cs2_out[c] = cs2;
@@ -669,7 +724,7 @@ int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, flo
             return -1;
         attr = true;
     }
-    const int blocks = 148 * 5;
+    const int blocks = 148 * 4;
     prof_begin(c, FSL_K_SGS);
     if (mu32)
         mlp::k_closure_infer<float><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu32, cs2_out, err);
@@ -718,8 +773,8 @@ namespace {
 __global__ void __launch_bounds__(128) k_umma_selftest(const float *__restrict__ A, const float *__restrict__ B,
                                                        float *__restrict__ D, int K, int N, int *err)
 {
-    __shared__ __align__(1024) __nv_bfloat16 sA[128 * 64];
-    __shared__ __align__(1024) __nv_bfloat16 sB[64 * 64];
+    __shared__ __align__(1024) __nv_bfloat16 sA[128 * 80];
+    __shared__ __align__(1024) __nv_bfloat16 sB[64 * 80];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tholder;
     const int t = threadIdx.x, w = t >> 5;
@@ -766,7 +821,7 @@ using namespace fsl;
 // BF16), K in {16, 32, 48, 64}, N in {16, 32, 48, 64}.
 extern "C" int fsl_selftest_tensor_gemm(const float *A, const float *B, float *D, int K, int N)
 {
-    if (!A || !B || !D || K < 16 || K > 64 || (K % 16) || N < 16 || N > 64 || (N % 16)) return FSL_ERR_ARG;
+    if (!A || !B || !D || K < 16 || K > 80 || (K % 16) || N < 16 || N > 64 || (N % 16)) return FSL_ERR_ARG;
     int dev = 0;
     cudaDeviceProp prop;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess ||

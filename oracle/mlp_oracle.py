@@ -6,8 +6,12 @@ the tensor-core kernels (freeshearlayer_b200/csrc/fsl_mlp.cu) hold BF16
 operands: the features, the weights W1..W3, the hidden activations a1, a2
 and the back-propagated dz of layers 3, 2, 1 that feed tensor-core products.
 Pre-activations, biases, the last layer and all accumulations stay in higher
-precision.  The GPU evaluates sigmoid through tanh.approx.f32, so agreement is
-to the few-1e-3 level, not bitwise.
+precision.  This is the training kernels' arithmetic; they evaluate sigmoid
+through tanh.approx.f32, so agreement is to the few-1e-3 level, not bitwise.
+The inference kernel is coarser still (its hidden SiLU runs in packed BF16 on
+h = (z + b)/2 cut to BF16, biases enter the tensor-core products as BF16
+high + low parts, and the output layer is a BF16 product); its tests compare
+its Cs^2 with this forward pass to 2e-3 absolute.
 
 Also: the features of one cell from the padded state, as the kernels form them.
 """

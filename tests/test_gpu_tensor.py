@@ -16,7 +16,7 @@ def bf16_round(x: np.ndarray) -> np.ndarray:
     return u.astype(np.uint32).view(np.float32)
 
 
-@pytest.mark.parametrize("K,N", [(16, 16), (16, 64), (64, 64), (32, 48), (64, 16)])
+@pytest.mark.parametrize("K,N", [(16, 16), (16, 64), (64, 64), (32, 48), (64, 16), (80, 64), (80, 16)])
 def test_tensor_gemm(K, N):
     import freeshearlayer_b200 as fsl
     fn = fsl.lib().fsl_selftest_tensor_gemm
