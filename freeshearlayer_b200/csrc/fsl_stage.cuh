@@ -285,6 +285,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             mu0 = mu[cj + (long long)i0 * g.pi];
             mu1 = mu[cj + (long long)(i0 + 1) * g.pi];
             plane_prims<T, TJE>(s, i0, r, l, mu0, mum);
+            plane_prims<T, TJE>(s, i0 + 1, r, l, mu1, mu0);
         }
         __syncthreads();
         if (inter) {
@@ -325,7 +326,8 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
     for (int i = i0; i <= i1; i++) {
         const int sm1 = (i + 2) % 3, s0 = i % 3, sp1 = (i + 1) % 3;
         const int u0 = i & 1, u1 = (i + 1) & 1;
-        // (a) issue plane i+2 loads; velocities of plane i+1
+        // (a) issue plane i+2 loads (the velocities of plane i+1 were formed
+        // at the end of the previous iteration, or in the prologue)
         plane_issue<T, TJE>(g, cu, i + 2, r, l, j, k, live, pl);
         if (inter) {
             const long long c = cj + (long long)i * g.pi;
@@ -340,12 +342,9 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
                 }
             }
         }
-        if (live) {
-            if (i + 2 <= L + 1) mu2 = mu[cj + (long long)(i + 2) * g.pi];
-            plane_prims<T, TJE>(s, i + 1, r, l, mu1, mu0);
-        }
-        __syncthreads();
-        // (b) y and z reconstruction of cell (i, j, k)
+        if (live && i + 2 <= L + 1) mu2 = mu[cj + (long long)(i + 2) * g.pi];
+        // (b) y and z reconstruction of cell (i, j, k): reads the state ring
+        // only (plane i, stored two iterations ago)
         T hy[5], hz[5], lz[5];
 #pragma unroll
         for (int q = 0; q < 5; q++) hy[q] = hz[q] = lz[q] = T(0.);
@@ -492,8 +491,11 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             }
         }
         // (g) plane i+2 into the ring slot of plane i (all readers of plane i
-        // passed the barrier above); advance the march
+        // passed the barrier above) and its velocities into the slots of
+        // planes i-1 (reciprocal ring) and i (division planes), read next
+        // after the next iteration's barrier; advance the march
         plane_store<T, TJE>(s, u0, r, l, j, k, H, D, live && i + 2 <= L + 1, pl);
+        if (live && i < i1) plane_prims<T, TJE>(s, i + 2, r, l, mu2, mu1);
 #pragma unroll
         for (int q = 0; q < 5; q++) {
             Fxp[q] = Fx[q];
