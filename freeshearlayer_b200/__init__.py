@@ -31,7 +31,7 @@ __all__ = ["Params", "Domain", "FslError", "lib", "LIB_PATH", "default_params",
            "params_from_ini", "params_from_bin", "initial_state", "temporal_state",
            "SETUP_SPATIAL", "SETUP_TEMPORAL", "CFL_STREAMWISE", "CFL_ACOUSTIC",
            "PREC_FP64", "PREC_FP32", "SGS_DYNAMIC", "SGS_LEARNED", "RECON_CHARMINMOD",
-           "RECON_PPM", "Trainer", "Ensemble", "closure_weights", "shear_statistics"]
+           "RECON_PPM", "Trainer", "Ensemble", "closure_weights", "shear_statistics", "favre_from_probes"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfsl_gpu.so")
@@ -148,6 +148,13 @@ def lib():
             "fsl_ensemble_destroy": [vp], "fsl_ensemble_set_chunk": [vp, i], "fsl_ensemble_step": [vp, i],
             "fsl_ensemble_sync": [vp],
             "fsl_ensemble_tune": [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)],
+        })
+        cs = C.c_char_p
+        sig.update({
+            "fsl_write_backup": [vp, cs, i], "fsl_read_backup": [vp, cs, i], "fsl_probe_rows": [vp, _dp],
+            "fsl_write_probes": [vp, cs, i], "fsl_favre_reset": [vp], "fsl_favre_accumulate": [vp],
+            "fsl_favre_read": [vp, _dp, C.POINTER(C.c_int)],
+            "fsl_favre_from_probes": [cs, i, i, i, i, _dp, C.POINTER(C.c_int)],
         })
         sig["fsl_tune"] = [vp, i, i]
         sig["fsl_profile"] = [vp, i]
@@ -413,6 +420,38 @@ class Domain:
         self._c(lib().fsl_plane_sums(self.h, out))
         return out.reshape(self.p.HIG, 8)
 
+    # --- driver files (real_bytes 4: the reference's float build, 8: FP64) -----------
+    def write_backup(self, path: str, real_bytes: int = 8):
+        """backup.dat as Finalize() writes it (src/finalize.c:14-35)."""
+        self._c(lib().fsl_write_backup(self.h, os.fsencode(path), real_bytes))
+
+    def read_backup(self, path: str, real_bytes: int = 8):
+        """Restore state, deltaT and step from a backup.dat (src/initialize.c:133-158)."""
+        self._c(lib().fsl_read_backup(self.h, os.fsencode(path), real_bytes))
+
+    def probe_rows(self) -> np.ndarray:
+        """rho and rho u at the three probe stations of src/probes.c: (3, 2, HIG)."""
+        out = np.empty(6 * self.p.HIG, np.float64)
+        self._c(lib().fsl_probe_rows(self.h, out))
+        return out.reshape(3, 2, self.p.HIG)
+
+    def write_probes(self, path: str, real_bytes: int = 8):
+        """Append one Probes() record (src/probes.c:13-44)."""
+        self._c(lib().fsl_write_probes(self.h, os.fsencode(path), real_bytes))
+
+    def favre_reset(self):
+        self._c(lib().fsl_favre_reset(self.h))
+
+    def favre_accumulate(self):
+        self._c(lib().fsl_favre_accumulate(self.h))
+
+    def favre_read(self):
+        """Favre-averaged u at the probe stations, (3, HIG), and the record count."""
+        out = np.empty(3 * self.p.HIG, np.float64)
+        n = C.c_int()
+        self._c(lib().fsl_favre_read(self.h, out, C.byref(n)))
+        return out.reshape(3, self.p.HIG), n.value
+
 
 class Trainer:
     """Training of the learned closure on (features, dynamic Cs^2) samples
@@ -524,6 +563,16 @@ class Ensemble:
         r, s, ms = C.c_int(), C.c_int(), C.c_double()
         self._c(lib().fsl_ensemble_tune(self.h, trial_steps, C.byref(r), C.byref(s), C.byref(ms)))
         return r.value, s.value, ms.value
+
+
+def favre_from_probes(path: str, HIG: int, real_bytes: int = 4, step_start: int = 0, step_end: int = 2**31 - 1):
+    """The reference's Favre post-processor over a probes.dat file
+    (favre-average-src/layer2_p.c:59-112; host only): u~ per station and row,
+    (3, HIG), and the number of records averaged."""
+    out = np.empty(3 * HIG, np.float64)
+    n = C.c_int()
+    _check(lib().fsl_favre_from_probes(os.fsencode(path), HIG, real_bytes, step_start, step_end, out, C.byref(n)))
+    return out.reshape(3, HIG), n.value
 
 
 # --- shear-layer statistics ----------------------------------------------------------

@@ -470,7 +470,7 @@ int fsl_destroy(fsl_ctx *h)
     Ctx &c = h->c;
     if (c.stream) cudaStreamSynchronize(c.stream);
     cudaFree(c.U); cudaFree(c.Up); cudaFree(c.Uq); cudaFree(c.mu);
-    cudaFree(c.partials); cudaFree(c.stage_dev); cudaFree(c.ds);
+    cudaFree(c.partials); cudaFree(c.stage_dev); cudaFree(c.ds); cudaFree(c.favre);
     if (c.hs) cudaFreeHost(c.hs);
     if (c.faces_alloc)
         for (int s = 0; s < 2; s++)

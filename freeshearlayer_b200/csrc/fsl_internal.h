@@ -131,6 +131,9 @@ struct Ctx {
     int counter = 0;
     unsigned step = 0;
     Disturb dist{};
+    // device sums of the probe columns (fsl_favre_*): [station][rho, rho u][HIG]
+    double *favre = nullptr;
+    int favre_count = 0;
     // the device Courant maximum (DevScalars::co_bits) belongs to the current U^n
     bool co_valid = false;
     double dt_host = 0; // host copy of dt, valid after sync

@@ -9,10 +9,14 @@
  * runs on the GPU through libfsl_gpu (include/fsl_gpu.h); this file only
  * sequences calls and does file I/O.
  *
+ * Every step appends a Probes() record to ./probes.dat (src/probes.c), as the
+ * reference's loop does (src/layer2.c:181).  Files are written in FP64.
+ *
  * Options beyond layer2.ini come from the environment:
  *   FSL_SETUP=temporal  periodic-x temporal shear layer (default: spatial)
  *   FSL_CFL=acoustic    acoustic Courant number (default: streamwise)
  *   FSL_PHASED=1        run the per-phase kernels instead of the fused step
+ *   FSL_PROBES=0        no probes.dat records
  */
 #include <signal.h>
 #include <stdio.h>
@@ -29,36 +33,6 @@ static void term_handler(int sig)
     contin_flag = 0;
 }
 
-static int write_backup(const char *path, const fsl_params *p, const double *state, double dt, unsigned step)
-{
-    /* src/finalize.c:22-32: per (i, j) the DEP rows of U1..U5, then deltaT
-     * and step, in the solver's precision (FP64 here). */
-    FILE *f = fopen(path, "wb");
-    size_t n = (size_t)p->LEN * p->HIG * 5 * p->DEP;
-    if (!f) return FSL_ERR_IO;
-    if (fwrite(state, sizeof(double), n, f) != n || fwrite(&dt, sizeof dt, 1, f) != 1 ||
-        fwrite(&step, sizeof step, 1, f) != 1) {
-        fclose(f);
-        return FSL_ERR_IO;
-    }
-    fclose(f);
-    return FSL_OK;
-}
-
-static int read_backup(const char *path, const fsl_params *p, double *state, double *dt, unsigned *step)
-{
-    FILE *f = fopen(path, "rb");
-    size_t n = (size_t)p->LEN * p->HIG * 5 * p->DEP;
-    if (!f) return FSL_ERR_IO;
-    if (fread(state, sizeof(double), n, f) != n || fread(dt, sizeof *dt, 1, f) != 1 ||
-        fread(step, sizeof *step, 1, f) != 1) {
-        fclose(f);
-        return FSL_ERR_IO;
-    }
-    fclose(f);
-    return FSL_OK;
-}
-
 int main(void)
 {
     fsl_params p;
@@ -67,7 +41,7 @@ int main(void)
     double *state;
     double X;
     const char *env;
-    int rc, phased;
+    int rc, phased, probes;
     size_t n;
 
     signal(SIGINT, term_handler);
@@ -88,6 +62,8 @@ int main(void)
     if (env && strcmp(env, "acoustic") == 0) p.cfl_mode = FSL_CFL_ACOUSTIC;
     env = getenv("FSL_PHASED");
     phased = env && atoi(env) != 0;
+    env = getenv("FSL_PROBES");
+    probes = !env || atoi(env) != 0;
 
     printf("Total number of cells in computational domain: %d\n", p.LEN * p.HIG * p.DEP);
     rc = fsl_init(&p, &ctx);
@@ -103,14 +79,12 @@ int main(void)
         return 1;
     }
     if (p.Answer) {
-        double dt;
-        unsigned step;
-        if (read_backup("backup.dat", &p, state, &dt, &step) != FSL_OK) {
-            puts("Cannot open \"backup.dat\" file to read");
+        if (fsl_read_backup(ctx, "backup.dat", 8) != FSL_OK) {
+            printf("Cannot read \"backup.dat\": %s\n", fsl_last_error(ctx));
+            free(state);
+            fsl_destroy(ctx);
             return 1;
         }
-        fsl_upload_state(ctx, state);
-        fsl_set_time(ctx, step, dt);
     } else {
         fsl_initial_state(&p, state);
         fsl_upload_state(ctx, state);
@@ -127,11 +101,11 @@ int main(void)
         }
         fsl_get_info(ctx, &info);
         printf("Timestep no.: %u, Courant max = %f, time step = %g sec.\n", info.step, info.maxCo, info.deltaT);
+        if (probes && fsl_write_probes(ctx, "probes.dat", 8) != FSL_OK)
+            puts("Cannot open probes file ");
     }
 
-    fsl_download_state(ctx, state);
-    fsl_get_info(ctx, &info);
-    if (write_backup("backup.dat", &p, state, info.deltaT, info.step) != FSL_OK)
+    if (fsl_write_backup(ctx, "backup.dat", 8) != FSL_OK)
         puts("Cannot open \"backup.dat\" file to write");
     free(state);
     fsl_destroy(ctx);

@@ -235,6 +235,33 @@ int fsl_set_faces(fsl_ctx *ctx, int dir, int side, int var, const double *faces)
 /* Point U*_ at U^n (0) or at the stage buffer (1). */
 int fsl_set_cur(fsl_ctx *ctx, int which);
 
+/* ---- driver files ------------------------------------------------------------
+ * real_bytes: 4 = the reference's shipped float `real` (src/type.h:4), 8 = FP64. */
+/* backup.dat as Finalize() writes it (src/finalize.c:14-35): per (i, j) the DEP
+ * values of U1..U5, then deltaT, then step (int).  fsl_read_backup restores
+ * state, deltaT and step; src/initialize.c:133-158 skips deltaT and reads step
+ * from its first bytes, which this reader does not copy.  FSL_ERR_IO when the
+ * file size does not match the grid. */
+int fsl_write_backup(fsl_ctx *ctx, const char *path, int real_bytes);
+int fsl_read_backup(fsl_ctx *ctx, const char *path, int real_bytes);
+/* The probe columns of Probes() (src/probes.c:21-42): stations i = LEN/2,
+ * 3 LEN/4, LEN at k = DEP/2 + 1, rows j = 1..HIG, as rows[station][rho, rho u][j]
+ * (6 HIG doubles). */
+int fsl_probe_rows(fsl_ctx *ctx, double *rows);
+/* Append one Probes() record to a probes.dat file: step, then per station HIG
+ * values of rho and of rho u. */
+int fsl_write_probes(fsl_ctx *ctx, const char *path, int real_bytes);
+/* Favre average of the probe columns accumulated on the device, without a
+ * probes file (favre-average-src/layer2_p.c:59-112): reset, accumulate the
+ * current U^n, read u~[station][j] = sum(rho u) / sum(rho) and the count. */
+int fsl_favre_reset(fsl_ctx *ctx);
+int fsl_favre_accumulate(fsl_ctx *ctx);
+int fsl_favre_read(fsl_ctx *ctx, double *u, int *count);
+/* The reference's post-processor over a probes file (host only, no device):
+ * records with step_start <= step <= step_end, u~[station][j] as above. */
+int fsl_favre_from_probes(const char *path, int HIG, int real_bytes, int step_start, int step_end, double *u,
+                          int *records);
+
 /* ---- learned subgrid closure ---------------------------------------------------
  * No counterpart in the reference (project extension).  A per-cell MLP
  * 8 -> 64 -> 64 -> 64 -> 1 (SiLU; BF16 weights and activations, FP32

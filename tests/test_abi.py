@@ -134,3 +134,32 @@ def test_no_cpu_fallback(fsl):
     with pytest.raises(fsl.FslError) as e:
         fsl.Domain(spatial_params())
     assert e.value.code == -8
+
+
+@pytest.mark.parametrize("real_bytes", [4, 8])
+def test_favre_post_processor(fsl, tmp_path, real_bytes):
+    """favre-average-src/layer2_p.c over a probes file: records inside the
+    step window summed per station and row, u~ = sum(rho u) / sum(rho); the
+    read stops past step_end and at the end of the file."""
+    H = 7
+    rng = np.random.default_rng(3)
+    dt = np.float32 if real_bytes == 4 else np.float64
+    recs = []
+    path = tmp_path / "probes.dat"
+    with open(path, "wb") as f:
+        for step in range(1, 11):
+            rho = (1.0 + 0.1 * rng.random((3, H))).astype(dt)
+            ru = (100.0 * rng.random((3, H))).astype(dt)
+            f.write(np.int32(step).tobytes())
+            for s in range(3):
+                f.write(rho[s].tobytes())
+                f.write(ru[s].tobytes())
+            recs.append((step, rho.astype(np.float64), ru.astype(np.float64)))
+    u, n = fsl.favre_from_probes(str(path), H, real_bytes, 3, 8)
+    sel = [r for r in recs if 3 <= r[0] <= 8]
+    R = sum(r[1] for r in sel)
+    RU = sum(r[2] for r in sel)
+    assert n == 6
+    np.testing.assert_allclose(u, RU / R, rtol=1e-15)
+    u_all, n_all = fsl.favre_from_probes(str(path), H, real_bytes)  # to the end of the file
+    assert n_all == 10
