@@ -191,7 +191,14 @@ double *cur_ptr(Ctx &c) { return c.cur ? c.Up : c.U; }
 } // namespace
 
 namespace fsl {
-int ensure_dyn_scratch(Ctx &c) { return ensure_dyn(c); }
+int ensure_dyn_scratch(Ctx &c)
+{
+    // the dynamic procedure's scratch and, on the FP32 path, the FP32 SGS
+    // field it writes (allocated on first use, like the fused step's buffers)
+    int rc = ensure_dyn(c);
+    if (!rc && c.p.precision == FSL_PREC_FP32) rc = ensure_fp32(c);
+    return rc;
+}
 } // namespace fsl
 
 namespace {
@@ -722,8 +729,7 @@ int fsl_step(fsl_ctx *h, int nsteps)
             if (c.p.sgs == FSL_SGS_LEARNED) {
                 if ((rc = closure_step_sgs(c))) return rc;
             } else {
-                launch_dynsmag(c, c.U);
-                launch_mu_to_f32(c);
+                launch_dynsmag32(c, c.U);
             }
             if (launch_stage32(c, 1, c.U, c.U, c.Up)) return fail(c, FSL_ERR_CUDA, "FP32 stage kernel");
             launch_ghost(c, c.Up);

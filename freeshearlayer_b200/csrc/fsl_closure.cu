@@ -129,12 +129,14 @@ int judge_now(Ctx &c)
 {
     const bool fp32 = c.p.precision == FSL_PREC_FP32;
     const int H = c.g.H;
-    launch_dynsmag(c, c.U, c.cd32);
+    // the dynamic procedure in the path's own precision: mu into c.mu / c.mu32
+    if (fp32) launch_dynsmag32(c, c.U, c.cd32);
+    else launch_dynsmag(c, c.U, c.cd32);
     if (launch_closure_infer(c, c.U, fp32 ? nullptr : c.mu_alt, fp32 ? c.mu32_alt : nullptr, c.cs2_32, c.cl_params,
                              c.cl_err))
         return FSL_ERR_CUDA;
     launch_judge_rows(c, c.cs2_32, c.cd32, c.judge_rows);
-    if (fp32) launch_judge_rows(c, c.mu32_alt, c.mu, c.judge_rows + 4 * H);
+    if (fp32) launch_judge_rows(c, c.mu32_alt, c.mu32, c.judge_rows + 4 * H);
     else launch_judge_rows(c, c.mu_alt, c.mu, c.judge_rows + 4 * H);
     std::vector<double> rows(8 * (size_t)H);
     if (cudaMemcpyAsync(rows.data(), c.judge_rows, rows.size() * sizeof(double), cudaMemcpyDeviceToHost,
@@ -181,17 +183,15 @@ int closure_step_sgs(Ctx &c)
         if (fail_ && !c.using_dynamic) c.fallbacks++;
         c.using_dynamic = fail_;
         const size_t fs = (size_t)c.g.fstride;
-        if (c.using_dynamic) {
-            if (fp32) launch_mu_to_f32(c);
-        } else {
+        if (!c.using_dynamic) {
             if (fp32) cudaMemcpyAsync(c.mu32, c.mu32_alt, fs * sizeof(float), cudaMemcpyDeviceToDevice, c.stream);
             else cudaMemcpyAsync(c.mu, c.mu_alt, fs * sizeof(double), cudaMemcpyDeviceToDevice, c.stream);
         }
         return FSL_OK;
     }
     if (c.using_dynamic) {
-        launch_dynsmag(c, c.U);
-        if (fp32) launch_mu_to_f32(c);
+        if (fp32) launch_dynsmag32(c, c.U);
+        else launch_dynsmag(c, c.U);
         return FSL_OK;
     }
     if (launch_closure_infer(c, c.U, fp32 ? nullptr : c.mu, fp32 ? c.mu32 : nullptr, nullptr, c.cl_params,

@@ -22,19 +22,6 @@ void launch_bface32(Ctx &c, const double *cur, const Disturb &d)
     stage::launch_bface_t<float>(c, cur, d, bf32(c));
 }
 
-static __global__ void k_mu_to_f32(long long n, const double *__restrict__ mu, float *__restrict__ mu32)
-{
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-        mu32[t] = (float)mu[t];
-}
-
-void launch_mu_to_f32(Ctx &c)
-{
-    prof_begin(c, FSL_K_SGS);
-    k_mu_to_f32<<<148 * 8, 256, 0, c.stream>>>(c.g.fstride, c.mu, c.mu32);
-    prof_end(c, FSL_K_SGS, 1);
-}
-
 int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant)
 {
     switch (c.stage_tje) {

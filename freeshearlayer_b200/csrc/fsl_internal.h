@@ -158,7 +158,7 @@ struct Ctx {
 void prof_begin(Ctx &c, int cls);
 void prof_end(Ctx &c, int cls, int nkernels);
 
-int ensure_dyn_scratch(Ctx &c);  // SGS scratch of the dynamic procedure (fsl_api.cu)
+int ensure_dyn_scratch(Ctx &c);  // SGS scratch of the dynamic procedure + the FP32 SGS field (fsl_api.cu)
 int closure_step_sgs(Ctx &c);    // SGS of one step under FSL_SGS_LEARNED (fsl_closure.cu)
 int closure_ensure(Ctx &c);
 void closure_free(Ctx &c);
@@ -170,6 +170,8 @@ void launch_ifbc(Ctx &c, const Disturb &d);
 void launch_fluxes(Ctx &c, const double *cur);
 void launch_evolution(Ctx &c, int nstages, int stage);
 void launch_dynsmag(Ctx &c, const double *U, float *cd = nullptr); // cd: optional Cs^2 output
+// the same procedure in FP32 (the FP32-bulk path): mu_SGS into c.mu32
+void launch_dynsmag32(Ctx &c, const double *U, float *cd = nullptr);
 void launch_judge_rows(Ctx &c, const float *a, const float *b, double *rows);
 void launch_judge_rows(Ctx &c, const float *a, const double *b, double *rows);
 void launch_judge_rows(Ctx &c, const double *a, const double *b, double *rows);
@@ -188,7 +190,6 @@ int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double 
 // FP32-bulk variants (fsl_fused32.cu): boundary states in bf32, SGS viscosity in mu32.
 void launch_bface32(Ctx &c, const double *cur, const Disturb &d);
 int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant = false);
-void launch_mu_to_f32(Ctx &c); // mu (FP64) -> mu32
 
 // ---- learned closure (fsl_mlp.cu) ---------------------------------------------
 int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, float *cs2_out, const float *P,

@@ -5,14 +5,15 @@
 // (face-state arrays between reconstruction and fluxes) so each phase can be
 // checked on its own against the CPU oracle.  Compiled with --fmad=false:
 // results equal the reference's serial FP64 code bit for bit.
+#include <algorithm>
+
+#include "fsl_dyn.cuh"
 #include "fsl_internal.h"
 #include "fsl_phys.cuh"
 
 namespace fsl {
 
 namespace {
-
-constexpr double H3 = 1. / 3.; // box test-filter weight, src/turbulence.c:113
 
 __device__ __forceinline__ long long ixf(int L, int H, int D, int i, int j, int k)
 {
@@ -424,183 +425,6 @@ __global__ void k_courant_apply(Consts kc, DevScalars *ds)
     if (threadIdx.x == 0) apply_courant(kc, __longlong_as_double((long long)ds->co_bits), ds);
 }
 
-// ---------------------------------------------------------------------------
-// A5/A6 dynamic Smagorinsky (src/turbulence.c:17-507) as seven passes.
-// The filter keeps the reference's three sweeps (y, z, x), each
-// t = 0; t += a h; t += b h; t += c h, on zero-initialised scratch whose never
-// written bands stay zero (the oracle convention for src/turbulence.c:44-45).
-// ---------------------------------------------------------------------------
-__global__ void k_dyn_vel(Grid g, const double *__restrict__ U, double *__restrict__ vel)
-{
-    const long long n = (long long)(g.L + 2) * g.pi;
-    const long long fs = g.fstride;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long c = g.off + t;
-        const double rr = 1. / U[c]; // :201-205
-        vel[c] = U[fs + c] * rr;
-        vel[fs + c] = U[2 * fs + c] * rr;
-        vel[2 * fs + c] = U[3 * fs + c] * rr;
-    }
-}
-
-// y sweep (:47-61) of u, v, w and their six products (:213-230), computed
-// on the fly; i in [0,LEN], j in [1,HIG], k in [0,DEP].
-__global__ void k_filt_y_vel(Grid g, const double *__restrict__ vel, double *__restrict__ t1)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int i = blockIdx.z;
-    if (k > g.D || j > g.H) return;
-    const long long fs = g.fstride, c = g.idx(i, j, k);
-    double a[3][3];
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        const long long s = c + (r - 1) * (long long)g.pk;
-        a[r][0] = vel[s]; a[r][1] = vel[fs + s]; a[r][2] = vel[2 * fs + s];
-    }
-    double q[3][9];
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        const double uu = a[r][0], vv = a[r][1], ww = a[r][2];
-        q[r][0] = uu; q[r][1] = vv; q[r][2] = ww;
-        q[r][3] = uu * uu; q[r][4] = uu * vv; q[r][5] = uu * ww;
-        q[r][6] = vv * vv; q[r][7] = vv * ww; q[r][8] = ww * ww;
-    }
-#pragma unroll
-    for (int m = 0; m < 9; m++) {
-        double t = 0.;
-        t += q[0][m] * H3; t += q[1][m] * H3; t += q[2][m] * H3;
-        t1[m * fs + c] = t;
-    }
-}
-
-// generic y sweep of nf fields
-__global__ void k_filt_y(Grid g, int nf, const double *__restrict__ src, double *__restrict__ t1)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int i = blockIdx.z;
-    if (k > g.D || j > g.H) return;
-    const long long fs = g.fstride, c = g.idx(i, j, k);
-    for (int m = 0; m < nf; m++) {
-        const double *s = src + m * fs;
-        double t = 0.;
-        t += s[c - g.pk] * H3; t += s[c] * H3; t += s[c + g.pk] * H3;
-        t1[m * fs + c] = t;
-    }
-}
-
-// z sweep (:63-77): i in [0,LEN], j in [0,HIG], k in [1,DEP]
-__global__ void k_filt_z(Grid g, int nf, const double *__restrict__ t1, double *__restrict__ t2)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k > g.D || j > g.H) return;
-    const long long fs = g.fstride, c = g.idx(i, j, k);
-    for (int m = 0; m < nf; m++) {
-        const double *s = t1 + m * fs;
-        double t = 0.;
-        t += s[c - 1] * H3; t += s[c] * H3; t += s[c + 1] * H3;
-        t2[m * fs + c] = t;
-    }
-}
-
-// x sweep (:80-95) back into the pass-1 buffer: i in [1,LEN], j in [0,HIG],
-// k in [0,DEP]
-__global__ void k_filt_x(Grid g, int nf, const double *__restrict__ t2, double *__restrict__ t1)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z + 1;
-    if (k > g.D || j > g.H) return;
-    const long long fs = g.fstride, c = g.idx(i, j, k);
-    for (int m = 0; m < nf; m++) {
-        const double *s = t2 + m * fs;
-        double t = 0.;
-        t += s[c - g.pi] * H3; t += s[c] * H3; t += s[c + g.pi] * H3;
-        t1[m * fs + c] = t;
-    }
-}
-
-// Interior: Leonard stress, |S|, A_ij = |S| S_ij, B_ij = |S^| S^_ij
-// (:250-382).  Field order of the symmetric tensors: 11 12 13 22 23 33.
-__global__ void k_dyn_mid(Grid g, Consts kc, const double *__restrict__ vel, const double *__restrict__ F,
-                          double *__restrict__ Lst, double *__restrict__ A, double *__restrict__ B,
-                          double *__restrict__ Smag)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int i = blockIdx.z + 1;
-    if (k > g.D || j > g.H) return;
-    const long long fs = g.fstride, c = g.idx(i, j, k);
-    const double f0 = F[c], f1 = F[fs + c], f2 = F[2 * fs + c];
-    Lst[c] = F[3 * fs + c] - f0 * f0;
-    Lst[fs + c] = F[4 * fs + c] - f0 * f1;
-    Lst[2 * fs + c] = F[5 * fs + c] - f0 * f2;
-    Lst[3 * fs + c] = F[6 * fs + c] - f1 * f1;
-    Lst[4 * fs + c] = F[7 * fs + c] - f1 * f2;
-    Lst[5 * fs + c] = F[8 * fs + c] - f2 * f2;
-    const long long dI = g.pi, dJ = g.pk;
-#pragma unroll
-    for (int pass = 0; pass < 2; pass++) {
-        const double *uu = pass ? F : vel;
-        const double *vv = uu + fs, *ww = uu + 2 * fs;
-        const double du_dx = (uu[c + dI] - uu[c - dI]) * kc.r2dx;
-        const double du_dy = (uu[c + dJ] - uu[c - dJ]) * kc.r2dy;
-        const double du_dz = (uu[c + 1] - uu[c - 1]) * kc.r2dz;
-        const double dv_dx = (vv[c + dI] - vv[c - dI]) * kc.r2dx;
-        const double dv_dy = (vv[c + dJ] - vv[c - dJ]) * kc.r2dy;
-        const double dv_dz = (vv[c + 1] - vv[c - 1]) * kc.r2dz;
-        const double dw_dx = (ww[c + dI] - ww[c - dI]) * kc.r2dx;
-        const double dw_dy = (ww[c + dJ] - ww[c - dJ]) * kc.r2dy;
-        const double dw_dz = (ww[c + 1] - ww[c - 1]) * kc.r2dz;
-        const double S11 = du_dx, S12 = 0.5 * (du_dy + dv_dx), S13 = 0.5 * (du_dz + dw_dx);
-        const double S21 = S12, S22 = dv_dy, S23 = 0.5 * (dv_dz + dw_dy);
-        const double S31 = S13, S32 = S23, S33 = dw_dz;
-        const double S = sqrt(2 * (S11 * S11 + S12 * S12 + S13 * S13 + S21 * S21 + S22 * S22 + S23 * S23 +
-                                   S31 * S31 + S32 * S32 + S33 * S33));
-        double *o = pass ? B : A;
-        o[c] = S * S11; o[fs + c] = S * S12; o[2 * fs + c] = S * S13;
-        o[3 * fs + c] = S * S22; o[4 * fs + c] = S * S23; o[5 * fs + c] = S * S33;
-        if (!pass) Smag[c] = S;
-    }
-}
-
-// M_ij, Germano-Lilly coefficient with clipping to [0, 0.15], mu_SGS
-// (:398-445).
-__global__ void k_dyn_final(Grid g, Consts kc, const double *__restrict__ rho, const double *__restrict__ Lst,
-                            const double *__restrict__ B, const double *__restrict__ Ahat,
-                            const double *__restrict__ Smag, double *__restrict__ mu, float *__restrict__ cd = nullptr)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int i = blockIdx.z + 1;
-    if (k > g.D || j > g.H) return;
-    const long long fs = g.fstride, c = g.idx(i, j, k);
-    const double DD = kc.DD;
-    const double M11 = DD * (4 * B[c] - Ahat[c]);
-    const double M12 = DD * (4 * B[fs + c] - Ahat[fs + c]);
-    const double M13 = DD * (4 * B[2 * fs + c] - Ahat[2 * fs + c]);
-    const double M22 = DD * (4 * B[3 * fs + c] - Ahat[3 * fs + c]);
-    const double M23 = DD * (4 * B[4 * fs + c] - Ahat[4 * fs + c]);
-    const double M33 = DD * (4 * B[5 * fs + c] - Ahat[5 * fs + c]);
-    double L11 = Lst[c], L12 = Lst[fs + c], L13 = Lst[2 * fs + c];
-    double L22 = Lst[3 * fs + c], L23 = Lst[4 * fs + c], L33 = Lst[5 * fs + c];
-    const double tr = -(1.0 / 3.0) * (L11 + L22 + L33);
-    L11 += tr; L22 += tr; L33 += tr;
-    const double LLMM = (L11 * M11 + L12 * M12 + L13 * M13 + L12 * M12 + L22 * M22 + L23 * M23 +
-                         L13 * M13 + L23 * M23 + L33 * M33);
-    const double MMMM = (M11 * M11 + M12 * M12 + M13 * M13 + M12 * M12 + M22 * M22 + M23 * M23 +
-                         M13 * M13 + M23 * M23 + M33 * M33);
-    double Cd = -0.5 * (LLMM / (MMMM + 1e-30));
-    if (Cd > 0.15) Cd = 0.15;
-    else if (Cd < 0.0) Cd = 0.0;
-    mu[c] = rho[c] * Cd * DD * Smag[c];
-    if (cd) cd[c] = (float)Cd; // Cs^2 for the learned closure's harvest and judgement
-}
-
 // Per y row: sums over the x-z plane of a, b, (a-b)^2 and b^2 (two padded
 // fields) -- the judgement of the learned closure, over the band two cells
 // away from every boundary (nearer, the dynamic procedure's values carry the
@@ -802,22 +626,10 @@ void launch_evolution(Ctx &c, int nstages, int stage)
 
 void launch_dynsmag(Ctx &c, const double *U, float *cd)
 {
-    const Grid &g = c.g;
-    DynScratch &s = c.dyn;
-    const long long ncell = (long long)(g.L + 2) * g.pi;
+    const DynScratch &s = c.dyn;
+    const dyn::Scratch<double> sc{s.vel, s.t1, s.t2, s.A, s.Lst, s.B, s.S};
     prof_begin(c, FSL_K_SGS);
-    k_dyn_vel<<<(unsigned)std::min<long long>((ncell + 255) / 256, 148LL * 16), 256, 0, c.stream>>>(g, U, s.vel);
-    dim3 b(32, 4, 1);
-    // velocity and product filters: y over i in [0,L] j in [1,H] k in [0,D]
-    k_filt_y_vel<<<cells_grid(g, b, g.L + 1, g.H, g.D + 1), b, 0, c.stream>>>(g, s.vel, s.t1);
-    k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, c.stream>>>(g, 9, s.t1, s.t2);
-    k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, c.stream>>>(g, 9, s.t2, s.t1);
-    k_dyn_mid<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, c.k, s.vel, s.t1, s.Lst, s.A, s.B, s.S);
-    // filter of A (pass-1 buffer reused; its zero bands are preserved)
-    k_filt_y<<<cells_grid(g, b, g.L + 1, g.H, g.D + 1), b, 0, c.stream>>>(g, 6, s.A, s.t1);
-    k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, c.stream>>>(g, 6, s.t1, s.t2);
-    k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, c.stream>>>(g, 6, s.t2, s.t1);
-    k_dyn_final<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, c.k, U, s.Lst, s.B, s.t1, s.S, c.mu, cd);
+    dyn::sequence<double>(c.g, c.k, sc, U, c.mu, cd, c.stream);
     prof_end(c, FSL_K_SGS, 9);
 }
 
@@ -923,17 +735,8 @@ void noalloc_dyn_sequence(const fsl::Grid &g, const fsl::Consts &k, const fsl::D
                           double *mu, cudaStream_t st)
 {
     using namespace fsl;
-    const long long ncell = (long long)(g.L + 2) * g.pi;
-    k_dyn_vel<<<(unsigned)std::min<long long>((ncell + 255) / 256, 148LL * 16), 256, 0, st>>>(g, U, s.vel);
-    dim3 b(32, 4, 1);
-    k_filt_y_vel<<<cells_grid(g, b, g.L + 1, g.H, g.D + 1), b, 0, st>>>(g, s.vel, s.t1);
-    k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, st>>>(g, 9, s.t1, s.t2);
-    k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, st>>>(g, 9, s.t2, s.t1);
-    k_dyn_mid<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, st>>>(g, k, s.vel, s.t1, s.Lst, s.A, s.B, s.S);
-    k_filt_y<<<cells_grid(g, b, g.L + 1, g.H, g.D + 1), b, 0, st>>>(g, 6, s.A, s.t1);
-    k_filt_z<<<cells_grid(g, b, g.L + 1, g.H + 1, g.D), b, 0, st>>>(g, 6, s.t1, s.t2);
-    k_filt_x<<<cells_grid(g, b, g.L, g.H + 1, g.D + 1), b, 0, st>>>(g, 6, s.t2, s.t1);
-    k_dyn_final<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, st>>>(g, k, U, s.Lst, s.B, s.t1, s.S, mu);
+    const dyn::Scratch<double> sc{s.vel, s.t1, s.t2, s.A, s.Lst, s.B, s.S};
+    dyn::sequence<double>(g, k, sc, U, mu, nullptr, st);
 }
 
 } // namespace

@@ -168,3 +168,21 @@ def test_learned_closure_steps(fsl, trained, prec):
     assert st.judgements == 2 and st.fallbacks == 0 and st.using_dynamic == 0
     assert np.isfinite(st.mu_profile_err) and st.mu_profile_err < 0.5
     assert np.isfinite(st.visc_err) and st.visc_err < 0.05
+
+
+def test_fp32_dynamic_procedure_matches_fp64(fsl, trained):
+    """The FP32-bulk path's dynamic procedure (filters and coefficient in FP32)
+    against the plain FP64 one on the same state: plane-averaged Cs^2 within
+    1e-2 and the cell values strongly correlated."""
+    out = []
+    for prec in (0, 1):
+        d = fsl.Domain(dict(trained["p"], sgs=1, precision=prec))
+        d.upload_state(trained["state"])
+        d.closure_set_scales(1.0 / trained["dU"], 1.0)
+        d.closure_set_weights(trained["weights"])
+        _, _, dyn = d.closure_compare(fields=True)
+        out.append(dyn[3:-3, 3:-3, 3:-3].astype(np.float64))
+    a64, a32 = out
+    prof64, prof32 = a64.mean(axis=(0, 2)), a32.mean(axis=(0, 2))
+    assert np.linalg.norm(prof32 - prof64) / np.linalg.norm(prof64) < 1e-2
+    assert np.corrcoef(a64.ravel(), a32.ravel())[0, 1] > 0.99
