@@ -130,11 +130,8 @@ int ensure_dyn(Ctx &c)
     const size_t fs = (size_t)c.g.fstride;
     int rc;
     if ((rc = dev_alloc(c, &c.dyn.vel, 3 * fs))) return rc;
-    if ((rc = dev_alloc(c, &c.dyn.t1, 9 * fs))) return rc;
-    if ((rc = dev_alloc(c, &c.dyn.t2, 9 * fs))) return rc;
+    if ((rc = dev_alloc(c, &c.dyn.F, 9 * fs))) return rc;
     if ((rc = dev_alloc(c, &c.dyn.A, 6 * fs))) return rc;
-    if ((rc = dev_alloc(c, &c.dyn.Lst, 6 * fs))) return rc;
-    if ((rc = dev_alloc(c, &c.dyn.B, 6 * fs))) return rc;
     if ((rc = dev_alloc(c, &c.dyn.S, fs))) return rc;
     c.dyn_alloc = true;
     return FSL_OK;
@@ -182,6 +179,11 @@ int ensure_fp32(Ctx &c)
     if ((rc = dev_alloc_f(c, &c.bf32.z0, nz))) return rc;
     if ((rc = dev_alloc_f(c, &c.bf32.zD, nz))) return rc;
     if ((rc = dev_alloc_f(c, &c.mu32, (size_t)g.fstride))) return rc;
+    const size_t fs = (size_t)g.fstride;
+    if ((rc = dev_alloc_f(c, &c.dyn32.vel, 3 * fs))) return rc;
+    if ((rc = dev_alloc_f(c, &c.dyn32.F, 9 * fs))) return rc;
+    if ((rc = dev_alloc_f(c, &c.dyn32.A, 6 * fs))) return rc;
+    if ((rc = dev_alloc_f(c, &c.dyn32.S, fs))) return rc;
     c.fp32_alloc = true;
     return FSL_OK;
 }
@@ -483,8 +485,7 @@ int fsl_destroy(fsl_ctx *h)
         for (int s = 0; s < 2; s++)
             for (int v = 0; v < 5; v++) { cudaFree(c.f.x[s][v]); cudaFree(c.f.y[s][v]); cudaFree(c.f.z[s][v]); }
     if (c.dyn_alloc) {
-        cudaFree(c.dyn.vel); cudaFree(c.dyn.t1); cudaFree(c.dyn.t2); cudaFree(c.dyn.A);
-        cudaFree(c.dyn.Lst); cudaFree(c.dyn.B); cudaFree(c.dyn.S);
+        cudaFree(c.dyn.vel); cudaFree(c.dyn.F); cudaFree(c.dyn.A); cudaFree(c.dyn.S);
     }
     if (c.bf_alloc) {
         cudaFree(c.bf.x0); cudaFree(c.bf.xL); cudaFree(c.bf.y0);
@@ -494,6 +495,7 @@ int fsl_destroy(fsl_ctx *h)
     if (c.fp32_alloc) {
         cudaFree(c.bf32.x0); cudaFree(c.bf32.xL); cudaFree(c.bf32.y0);
         cudaFree(c.bf32.yH); cudaFree(c.bf32.z0); cudaFree(c.bf32.zD); cudaFree(c.mu32);
+        cudaFree(c.dyn32.vel); cudaFree(c.dyn32.F); cudaFree(c.dyn32.A); cudaFree(c.dyn32.S);
     }
     for (auto &r : c.recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
     for (auto e : c.evpool) cudaEventDestroy(e);

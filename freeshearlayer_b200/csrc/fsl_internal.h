@@ -72,15 +72,15 @@ struct BFaces32 {
 };
 
 // Scratch of the dynamic Smagorinsky procedure (padded layout, FP64).
-struct DynScratch {
-    double *vel;   // 3 fields u, v, w
-    double *t1;    // 9 fields (pass-1 / filtered output)
-    double *t2;    // 9 fields (pass-2)
-    double *A;     // 6 fields |S| S_ij, ghost layer kept zero
-    double *Lst;   // 6 fields Leonard stress
-    double *B;     // 6 fields |S^| S^_ij
-    double *S;     // 1 field |S|
+// Scratch of the fused dynamic procedure (fsl_dyn.cuh, sequence_fused)
+template <typename T> struct DynFields {
+    T *vel; // 3 fields u, v, w
+    T *F;   // 9 fields: the filtered velocities and products; zero where no pass writes
+    T *A;   // 6 fields |S| S_ij, ghost layer kept zero
+    T *S;   // 1 field |S|
 };
+typedef DynFields<double> DynScratch;
+typedef DynFields<float> DynScratch32;
 
 struct Ctx {
     fsl_params p;
@@ -94,6 +94,7 @@ struct Ctx {
     Faces f{};
     bool faces_alloc = false;
     DynScratch dyn{};
+    DynScratch32 dyn32{}; // the FP32 path's own (a shared buffer would mix the two views' zero bands)
     bool dyn_alloc = false;
     BFaces bf{};
     bool bf_alloc = false;

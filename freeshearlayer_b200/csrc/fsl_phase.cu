@@ -627,10 +627,10 @@ void launch_evolution(Ctx &c, int nstages, int stage)
 void launch_dynsmag(Ctx &c, const double *U, float *cd)
 {
     const DynScratch &s = c.dyn;
-    const dyn::Scratch<double> sc{s.vel, s.t1, s.t2, s.A, s.Lst, s.B, s.S};
+    const dyn::Scratch3<double> sc{s.vel, s.F, s.A, s.S};
     prof_begin(c, FSL_K_SGS);
-    dyn::sequence<double>(c.g, c.k, sc, U, c.mu, cd, c.stream);
-    prof_end(c, FSL_K_SGS, 9);
+    dyn::sequence_fused<double>(c.g, c.k, sc, U, c.mu, cd, c.stream);
+    prof_end(c, FSL_K_SGS, 4);
 }
 
 void launch_courant(Ctx &c)
@@ -731,12 +731,10 @@ int noalloc_scratch(double **out)
 }
 
 // The launch sequence of launch_dynsmag on explicit buffers and stream.
-void noalloc_dyn_sequence(const fsl::Grid &g, const fsl::Consts &k, const fsl::DynScratch &s, const double *U,
-                          double *mu, cudaStream_t st)
+void noalloc_dyn_sequence(const fsl::Grid &g, const fsl::Consts &k, const fsl::dyn::Scratch<double> &s,
+                          const double *U, double *mu, cudaStream_t st)
 {
-    using namespace fsl;
-    const dyn::Scratch<double> sc{s.vel, s.t1, s.t2, s.A, s.Lst, s.B, s.S};
-    dyn::sequence<double>(g, k, sc, U, mu, nullptr, st);
+    fsl::dyn::sequence<double>(g, k, s, U, mu, nullptr, st);
 }
 
 } // namespace
@@ -762,7 +760,7 @@ extern "C" int fsl_dynamic_smagorinsky_noalloc(const double *U, double *mu, int 
     k.r4dx = 1. / (4 * deltaX); k.r4dy = 1. / (4 * deltaY); k.r4dz = 1. / (4 * deltaZ);
     k.r2dx = k.r4dx + k.r4dx; k.r2dy = k.r4dy + k.r4dy; k.r2dz = k.r4dz + k.r4dz;
     k.DD = pow(deltaX * deltaY * deltaZ, 0.666666666666667);
-    fsl::DynScratch d;
+    fsl::dyn::Scratch<double> d;
     d.vel = s; d.t1 = s + 3 * n; d.t2 = s + 12 * n; d.A = s + 21 * n;
     d.Lst = s + 27 * n; d.B = s + 33 * n; d.S = s + 39 * n;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
