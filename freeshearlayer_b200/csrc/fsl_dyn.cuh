@@ -233,17 +233,34 @@ __global__ void __launch_bounds__(32 * TJ) k_dyn_filter9(Grid g, int seg, const 
 #pragma unroll
     for (int m = 0; m < 9; m++) p2[m] = p1[m] = cur[m] = T(0.);
     const int ib = max(i0 - 1, 0), ie = min(i1 + 1, L + 1);
+    // the staged region (TJ+2) x 34 of a plane, at most two positions per
+    // thread; plane ip+1 is loaded into registers while plane ip is filtered
+    constexpr int NP = ((TJ + 2) * 34 + 32 * TJ - 1) / (32 * TJ);
+    T pre[NP][3];
+    auto issue = [&](int ip) {
+#pragma unroll
+        for (int s = 0; s < NP; s++) {
+            const int e = tid + s * nt;
+            const int rr = e / 34, cc = e % 34, jj = j0 - 1 + rr, kk = k0 - 1 + cc;
+            pre[s][0] = pre[s][1] = pre[s][2] = T(0.);
+            if (e < (TJ + 2) * 34 && ip <= L && jj <= H + 1 && kk >= 0 && kk <= D + 1) {
+                const long long q = g.idx(ip, jj, kk);
+                pre[s][0] = vel[q]; pre[s][1] = vel[fs + q]; pre[s][2] = vel[2 * fs + q];
+            }
+        }
+    };
+    issue(ib);
     for (int ip = ib; ip <= ie; ip++) {
         if (ip <= L) {
-            for (int e = tid; e < (TJ + 2) * 34; e += nt) {
-                const int rr = e / 34, cc = e % 34, jj = j0 - 1 + rr, kk = k0 - 1 + cc;
-                T a = T(0.), b = T(0.), c = T(0.);
-                if (jj <= H + 1 && kk >= 0 && kk <= D + 1) {
-                    const long long q = g.idx(ip, jj, kk);
-                    a = vel[q]; b = vel[fs + q]; c = vel[2 * fs + q];
+#pragma unroll
+            for (int s = 0; s < NP; s++) {
+                const int e = tid + s * nt;
+                if (e < (TJ + 2) * 34) {
+                    const int rr = e / 34, cc = e % 34;
+                    vq[rr][cc][0] = pre[s][0]; vq[rr][cc][1] = pre[s][1]; vq[rr][cc][2] = pre[s][2];
                 }
-                vq[rr][cc][0] = a; vq[rr][cc][1] = b; vq[rr][cc][2] = c;
             }
+            issue(ip + 1);
             __syncthreads();
             // pass 1 (y) of the nine fields at rows j0.., columns k0-1 .. k0+32
             for (int e = tid; e < TJ * 34; e += nt) {
@@ -363,15 +380,35 @@ __global__ void __launch_bounds__(32 * TJ)
     T p2[6], p1[6], cur[6];
 #pragma unroll
     for (int m = 0; m < 6; m++) p2[m] = p1[m] = cur[m] = T(0.);
+    constexpr int NP = ((TJ + 2) * 34 + 32 * TJ - 1) / (32 * TJ);
+    T pre[NP][6];
+    auto issue = [&](int ip) {
+#pragma unroll
+        for (int s = 0; s < NP; s++) {
+            const int e = tid + s * nt;
+            const int rr = e / 34, cc = e % 34, jj = j0 - 1 + rr, kk = k0 - 1 + cc;
+#pragma unroll
+            for (int m = 0; m < 6; m++) pre[s][m] = T(0.);
+            if (e < (TJ + 2) * 34 && ip >= 1 && ip <= L && jj <= H + 1 && kk <= D + 1) {
+                const long long q = g.idx(ip, jj, kk);
+#pragma unroll
+                for (int m = 0; m < 6; m++) pre[s][m] = A[m * fs + q];
+            }
+        }
+    };
+    issue(i0 - 1);
     for (int ip = i0 - 1; ip <= i1 + 1; ip++) {
         if (ip >= 1 && ip <= L) { // A is zero on the planes 0 and L+1
-            for (int e = tid; e < (TJ + 2) * 34; e += nt) {
-                const int rr = e / 34, cc = e % 34, jj = j0 - 1 + rr, kk = k0 - 1 + cc;
-                const bool in = jj <= H + 1 && kk <= D + 1;
-                const long long q = in ? g.idx(ip, jj, kk) : 0;
 #pragma unroll
-                for (int m = 0; m < 6; m++) qa[rr][cc][m] = in ? A[m * fs + q] : T(0.);
+            for (int s = 0; s < NP; s++) {
+                const int e = tid + s * nt;
+                if (e < (TJ + 2) * 34) {
+                    const int rr = e / 34, cc = e % 34;
+#pragma unroll
+                    for (int m = 0; m < 6; m++) qa[rr][cc][m] = pre[s][m];
+                }
             }
+            issue(ip + 1);
             __syncthreads();
             for (int e = tid; e < TJ * 34; e += nt) {
                 const int rr = e / 34, cc = e % 34, jj = j0 + rr, kk = k0 - 1 + cc;
@@ -398,6 +435,7 @@ __global__ void __launch_bounds__(32 * TJ)
         } else {
 #pragma unroll
             for (int m = 0; m < 6; m++) cur[m] = T(0.);
+            if (ip == 0) issue(1); // the march starts on plane 0 (i0 = 1)
         }
         const int io = ip - 1;
         if (io >= i0 && io <= i1 && own) {
