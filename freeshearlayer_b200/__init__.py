@@ -31,7 +31,8 @@ __all__ = ["Params", "Domain", "FslError", "lib", "LIB_PATH", "default_params",
            "params_from_ini", "params_from_bin", "initial_state", "temporal_state",
            "SETUP_SPATIAL", "SETUP_TEMPORAL", "CFL_STREAMWISE", "CFL_ACOUSTIC",
            "PREC_FP64", "PREC_FP32", "SGS_DYNAMIC", "SGS_LEARNED", "RECON_CHARMINMOD",
-           "RECON_PPM", "Trainer", "Ensemble", "closure_weights", "shear_statistics", "favre_from_probes"]
+           "RECON_PPM", "Trainer", "Ensemble", "closure_weights", "shear_statistics", "favre_from_probes",
+           "tecplot_write"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfsl_gpu.so")
@@ -155,6 +156,8 @@ def lib():
             "fsl_write_probes": [vp, cs, i], "fsl_favre_reset": [vp], "fsl_favre_accumulate": [vp],
             "fsl_favre_read": [vp, _dp, C.POINTER(C.c_int)],
             "fsl_favre_from_probes": [cs, i, i, i, i, _dp, C.POINTER(C.c_int)],
+            "fsl_output_fields": [vp, _dp], "fsl_write_tecplot": [vp, cs],
+            "fsl_tecplot_write": [cs, i, i, i, _dp],
         })
         sig["fsl_tune"] = [vp, i, i]
         sig["fsl_profile"] = [vp, i]
@@ -439,6 +442,17 @@ class Domain:
         """Append one Probes() record (src/probes.c:13-44)."""
         self._c(lib().fsl_write_probes(self.h, os.fsencode(path), real_bytes))
 
+    def output_fields(self) -> np.ndarray:
+        """Output()'s 12 values per cell (src/output.c): (DEP, HIG, LEN, 12)."""
+        p = self.p
+        out = np.empty(12 * p.LEN * p.HIG * p.DEP, np.float64)
+        self._c(lib().fsl_output_fields(self.h, out))
+        return out.reshape(p.DEP, p.HIG, p.LEN, 12)
+
+    def write_tecplot(self, path: str):
+        """The ASCII Tecplot frame Output() writes (src/output.c)."""
+        self._c(lib().fsl_write_tecplot(self.h, os.fsencode(path)))
+
     def favre_reset(self):
         self._c(lib().fsl_favre_reset(self.h))
 
@@ -563,6 +577,14 @@ class Ensemble:
         r, s, ms = C.c_int(), C.c_int(), C.c_double()
         self._c(lib().fsl_ensemble_tune(self.h, trial_steps, C.byref(r), C.byref(s), C.byref(ms)))
         return r.value, s.value, ms.value
+
+
+def tecplot_write(path: str, fields: np.ndarray):
+    """Write Output()-style values, shape (DEP, HIG, LEN, 12), as the ASCII
+    Tecplot file of src/output.c (host only)."""
+    f = np.ascontiguousarray(fields, np.float64)
+    D, H, L, _ = f.shape
+    _check(lib().fsl_tecplot_write(os.fsencode(path), L, H, D, f.ravel()))
 
 
 def favre_from_probes(path: str, HIG: int, real_bytes: int = 4, step_start: int = 0, step_end: int = 2**31 - 1):

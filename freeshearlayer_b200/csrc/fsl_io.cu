@@ -244,3 +244,104 @@ int fsl_favre_from_probes(const char *path, int HIG, int real_bytes, int step_st
 }
 
 } // extern "C"
+
+// ---- Tecplot frames (src/output.c) -------------------------------------------
+namespace {
+
+// Output()'s 12 values per interior cell in its arithmetic (FP64, compiled
+// without contraction), written in its loop order: k, then j, then i fastest.
+__global__ void k_output_fields(Grid g, Consts kc, double Cs, const double *__restrict__ Ub, double *__restrict__ out)
+{
+    const long long n = (long long)g.L * g.H * g.D;
+    const long long fs = g.fstride;
+    const double *U1 = Ub, *U2 = Ub + fs, *U3 = Ub + 2 * fs, *U4 = Ub + 3 * fs, *U5 = Ub + 4 * fs;
+    const double CsDD = Cs * kc.DD;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % g.L) + 1;
+        const long long r = t / g.L;
+        const int j = (int)(r % g.H) + 1, k = (int)(r / g.H) + 1;
+        const long long c = g.idx(i, j, k), xi = g.pi, yj = g.pk;
+        double *q = out + 12 * t;
+        q[0] = (i - 1) * kc.deltaX + 0.5 * kc.deltaX;
+        q[1] = (j - 1) * kc.deltaY + 0.5 * kc.deltaY;
+        q[2] = (k - 1) * kc.deltaZ + 0.5 * kc.deltaZ;
+        const double R = U1[c], Uu = U2[c] / R, V = U3[c] / R, W = U4[c] / R;
+        const double P = (U5[c] - 0.5 * R * (Uu * Uu + V * V + W * W)) * 0.4;
+        const double T = P / (287.10 * R);
+        const double du_dx = (U2[c + xi] / U1[c + xi] - U2[c - xi] / U1[c - xi]) * kc.r2dx;
+        const double du_dy = (U2[c + yj] / U1[c + yj] - U2[c - yj] / U1[c - yj]) * kc.r2dy;
+        const double du_dz = (U2[c + 1] / U1[c + 1] - U2[c - 1] / U1[c - 1]) * kc.r2dz;
+        const double dv_dx = (U3[c + xi] / U1[c + xi] - U3[c - xi] / U1[c - xi]) * kc.r2dx;
+        const double dv_dy = (U3[c + yj] / U1[c + yj] - U3[c - yj] / U1[c - yj]) * kc.r2dy;
+        const double dv_dz = (U3[c + 1] / U1[c + 1] - U3[c - 1] / U1[c - 1]) * kc.r2dz;
+        const double dw_dx = (U4[c + xi] / U1[c + xi] - U4[c - xi] / U1[c - xi]) * kc.r2dx;
+        const double dw_dy = (U4[c + yj] / U1[c + yj] - U4[c - yj] / U1[c - yj]) * kc.r2dy;
+        const double dw_dz = (U4[c + 1] / U1[c + 1] - U4[c - 1] / U1[c - 1]) * kc.r2dz;
+        const double ox = dw_dy - dv_dz, oy = du_dz - dw_dx, oz = dv_dx - du_dy;
+        const double Om = sqrt(ox * ox + oy * oy + oz * oz);
+        const double S12 = 0.5 * (du_dy + dv_dx), S13 = 0.5 * (du_dz + dw_dx), S23 = 0.5 * (dv_dz + dw_dy);
+        const double St =
+            sqrt(2 * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz + 2 * (S12 * S12 + S13 * S13 + S23 * S23)));
+        q[3] = R; q[4] = Uu; q[5] = V; q[6] = W; q[7] = P; q[8] = T;
+        q[9] = Om;
+        q[10] = 0.5 * (Om * Om - St * St);
+        q[11] = R * CsDD * St / kc.mu_L;
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+int fsl_output_fields(fsl_ctx *h, double *out)
+{
+    if (!h || !out) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    const size_t n = (size_t)c.g.L * c.g.H * c.g.D;
+    double *d = nullptr;
+    if (cudaMalloc((void **)&d, 12 * n * sizeof(double)) != cudaSuccess)
+        return io_fail(c, FSL_ERR_NOMEM, "output fields");
+    k_output_fields<<<148 * 8, 256, 0, c.stream>>>(c.g, c.k, c.p.Cs, c.U, d);
+    const bool ok = cudaGetLastError() == cudaSuccess &&
+                    cudaMemcpyAsync(out, d, 12 * n * sizeof(double), cudaMemcpyDeviceToHost, c.stream) == cudaSuccess &&
+                    cudaStreamSynchronize(c.stream) == cudaSuccess;
+    cudaFree(d);
+    return ok ? FSL_OK : io_fail(c, FSL_ERR_CUDA, "output fields");
+}
+
+// The ASCII Tecplot file of src/output.c:66-139 from the 12 values per cell.
+int fsl_tecplot_write(const char *path, int LEN, int HIG, int DEP, const double *fields)
+{
+    if (!path || !fields || LEN < 1 || HIG < 1 || DEP < 1) return FSL_ERR_ARG;
+    FILE *f = fopen(path, "w");
+    if (!f) return FSL_ERR_IO;
+    fprintf(f, "title     = \" 3-D compressible case \"\n");
+    fprintf(f, "variables = \" x \"\n");
+    fprintf(f, "\"y\"\n\"z\"\n\"rho\"\n\"u\"\n\"v\"\n\"w\"\n\"p\"\n\"T\"\n");
+    fprintf(f, "\"Vort. mag.\"\n\"Q-criteria.\"\n\"muSgs-mu-ratio\"\n");
+    fprintf(f, "zone t=\" \"\n");
+    fprintf(f, "i=%d, j=%d, k=%d, f=point\n", LEN, HIG, DEP);
+    const size_t n = (size_t)LEN * HIG * DEP;
+    for (size_t t = 0; t < n; t++) {
+        const double *q = fields + 12 * t;
+        fprintf(f, "%g %g %g %g %g %g %g %g %g %g %g %g\n", q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8],
+                q[9], q[10], q[11]);
+    }
+    return fclose(f) == 0 ? FSL_OK : FSL_ERR_IO;
+}
+
+// Output(): "<path>" written from the current U^n (call it after fsl_step,
+// where the reference calls Output() after the stages).
+int fsl_write_tecplot(fsl_ctx *h, const char *path)
+{
+    if (!h || !path) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    std::vector<double> q(12 * (size_t)c.g.L * c.g.H * c.g.D);
+    int rc = fsl_output_fields(h, q.data());
+    if (rc) return rc;
+    rc = fsl_tecplot_write(path, c.g.L, c.g.H, c.g.D, q.data());
+    return rc ? io_fail(c, rc, "tecplot write failed") : FSL_OK;
+}
+
+} // extern "C"

@@ -9,14 +9,17 @@
  * runs on the GPU through libfsl_gpu (include/fsl_gpu.h); this file only
  * sequences calls and does file I/O.
  *
- * Every step appends a Probes() record to ./probes.dat (src/probes.c), as the
- * reference's loop does (src/layer2.c:181).  Files are written in FP64.
+ * Every step appends a Probes() record to ./probes.dat (src/probes.c), every
+ * f_step steps and at the end it writes the Tecplot frame <step>.plt
+ * (src/output.c), as the reference's loop does (src/layer2.c:180-189).
+ * Binary files are written in FP64.
  *
  * Options beyond layer2.ini come from the environment:
  *   FSL_SETUP=temporal  periodic-x temporal shear layer (default: spatial)
  *   FSL_CFL=acoustic    acoustic Courant number (default: streamwise)
  *   FSL_PHASED=1        run the per-phase kernels instead of the fused step
  *   FSL_PROBES=0        no probes.dat records
+ *   FSL_FRAMES=0        no Tecplot frames
  */
 #include <signal.h>
 #include <stdio.h>
@@ -41,7 +44,8 @@ int main(void)
     double *state;
     double X;
     const char *env;
-    int rc, phased, probes;
+    int rc, phased, probes, frames;
+    char frame[64];
     size_t n;
 
     signal(SIGINT, term_handler);
@@ -64,6 +68,8 @@ int main(void)
     phased = env && atoi(env) != 0;
     env = getenv("FSL_PROBES");
     probes = !env || atoi(env) != 0;
+    env = getenv("FSL_FRAMES");
+    frames = !env || atoi(env) != 0;
 
     printf("Total number of cells in computational domain: %d\n", p.LEN * p.HIG * p.DEP);
     rc = fsl_init(&p, &ctx);
@@ -103,6 +109,15 @@ int main(void)
         printf("Timestep no.: %u, Courant max = %f, time step = %g sec.\n", info.step, info.maxCo, info.deltaT);
         if (probes && fsl_write_probes(ctx, "probes.dat", 8) != FSL_OK)
             puts("Cannot open probes file ");
+        if (frames && p.f_step > 0 && info.step % (unsigned)p.f_step == 0) {
+            sprintf(frame, "%u.plt", info.step);
+            if (fsl_write_tecplot(ctx, frame) != FSL_OK) fprintf(stderr, "cannot open file \"Tecplot-file\"\n");
+        }
+    }
+    fsl_get_info(ctx, &info);
+    if (frames) {
+        sprintf(frame, "%u.plt", info.step);
+        if (fsl_write_tecplot(ctx, frame) != FSL_OK) fprintf(stderr, "cannot open file \"Tecplot-file\"\n");
     }
 
     if (fsl_write_backup(ctx, "backup.dat", 8) != FSL_OK)

@@ -262,6 +262,17 @@ int fsl_favre_read(fsl_ctx *ctx, double *u, int *count);
 int fsl_favre_from_probes(const char *path, int HIG, int real_bytes, int step_start, int step_end, double *u,
                           int *records);
 
+/* Output() (src/output.c:16-141): per interior cell, in its loop order (k,
+ * then j, then i fastest), the 12 values x, y, z, rho, u, v, w, p, T,
+ * vorticity magnitude, Q criterion and rho Cs DD |S| / mu_L in the reference's
+ * arithmetic, from the current U^n with the ghost layer the last stage left
+ * (call after fsl_step, as the reference calls Output() after the stages).
+ * fsl_output_fields fills 12 LEN HIG DEP doubles; fsl_write_tecplot writes the
+ * ASCII Tecplot file; fsl_tecplot_write writes such values (host only). */
+int fsl_output_fields(fsl_ctx *ctx, double *fields);
+int fsl_write_tecplot(fsl_ctx *ctx, const char *path);
+int fsl_tecplot_write(const char *path, int LEN, int HIG, int DEP, const double *fields);
+
 /* ---- learned subgrid closure ---------------------------------------------------
  * No counterpart in the reference (project extension).  A per-cell MLP
  * 8 -> 64 -> 64 -> 64 -> 1 (SiLU; BF16 weights and activations, FP32

@@ -1095,3 +1095,54 @@ void orc_plane_sums(orc_ctx *o, double *rows)
         for (q = 0; q < 8; q++) rows[8 * (j - 1) + q] = (double)acc[q];
     }
 }
+
+/* The per-cell values Output() writes to <step>.plt (src/output.c:66-139), in
+ * its loop order (k, then j, then i fastest), 12 per cell: the cell centre,
+ * rho, u, v, w, p, T, vorticity magnitude, Q criterion and the static
+ * Smagorinsky viscosity ratio rho Cs DD |S| / mu_L.  It reads U^n with the
+ * ghost layer the last stage left, as Output() does. */
+void orc_output_fields(orc_ctx *o, double *out)
+{
+    const double *U1 = o->U[0], *U2 = o->U[1], *U3 = o->U[2], *U4 = o->U[3], *U5 = o->U[4];
+    const double dX = o->p.deltaX, dY = o->p.deltaY, dZ = o->p.deltaZ;
+    const double CsDD = o->p.Cs * o->DD, mu_L = o->p.mu_L;
+    size_t n = 0;
+    int i, j, k;
+    for (k = 1; k <= o->D; k++)
+        for (j = 1; j <= o->H; j++)
+            for (i = 1; i <= o->L; i++) {
+                const size_t c = IC(o, i, j, k), xi = o->pi, yj = o->pj;
+                double R, Uu, V, W, P, T, du_dx, du_dy, du_dz, dv_dx, dv_dy, dv_dz, dw_dx, dw_dy, dw_dz;
+                double ox, oy, oz, Om, S12, S13, S23, St, *q = out + 12 * n++;
+                q[0] = (i - 1) * dX + 0.5 * dX;
+                q[1] = (j - 1) * dY + 0.5 * dY;
+                q[2] = (k - 1) * dZ + 0.5 * dZ;
+                R = U1[c];
+                Uu = U2[c] / R;
+                V = U3[c] / R;
+                W = U4[c] / R;
+                P = (U5[c] - 0.5 * R * (Uu * Uu + V * V + W * W)) * 0.4;
+                T = P / (287.10 * R);
+                du_dx = (U2[c + xi] / U1[c + xi] - U2[c - xi] / U1[c - xi]) * o->r2dx;
+                du_dy = (U2[c + yj] / U1[c + yj] - U2[c - yj] / U1[c - yj]) * o->r2dy;
+                du_dz = (U2[c + 1] / U1[c + 1] - U2[c - 1] / U1[c - 1]) * o->r2dz;
+                dv_dx = (U3[c + xi] / U1[c + xi] - U3[c - xi] / U1[c - xi]) * o->r2dx;
+                dv_dy = (U3[c + yj] / U1[c + yj] - U3[c - yj] / U1[c - yj]) * o->r2dy;
+                dv_dz = (U3[c + 1] / U1[c + 1] - U3[c - 1] / U1[c - 1]) * o->r2dz;
+                dw_dx = (U4[c + xi] / U1[c + xi] - U4[c - xi] / U1[c - xi]) * o->r2dx;
+                dw_dy = (U4[c + yj] / U1[c + yj] - U4[c - yj] / U1[c - yj]) * o->r2dy;
+                dw_dz = (U4[c + 1] / U1[c + 1] - U4[c - 1] / U1[c - 1]) * o->r2dz;
+                ox = dw_dy - dv_dz;
+                oy = du_dz - dw_dx;
+                oz = dv_dx - du_dy;
+                Om = sqrt(ox * ox + oy * oy + oz * oz);
+                S12 = 0.5 * (du_dy + dv_dx);
+                S13 = 0.5 * (du_dz + dw_dx);
+                S23 = 0.5 * (dv_dz + dw_dy);
+                St = sqrt(2 * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz + 2 * (S12 * S12 + S13 * S13 + S23 * S23)));
+                q[3] = R; q[4] = Uu; q[5] = V; q[6] = W; q[7] = P; q[8] = T;
+                q[9] = Om;
+                q[10] = 0.5 * (Om * Om - St * St);
+                q[11] = R * CsDD * St / mu_L;
+            }
+}

@@ -101,6 +101,8 @@ int orc_temporal_state(const orc_params *p, double Mc, double delta_w0, double a
  * rho vv, rho ww, rho uv over the interior x-z plane. */
 void orc_sums(orc_ctx *o, double *sums);
 void orc_plane_sums(orc_ctx *o, double *rows);
+/* Output()'s 12 values per cell, src/output.c:66-139 (k, j, i order). */
+void orc_output_fields(orc_ctx *o, double *out);
 
 #ifdef __cplusplus
 }

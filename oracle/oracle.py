@@ -128,6 +128,7 @@ class Oracle:
                                                C.POINTER(C.c_double)]
             lib.orc_sums.argtypes = [C.c_void_p, _dp]
             lib.orc_plane_sums.argtypes = [C.c_void_p, _dp]
+            lib.orc_output_fields.argtypes = [C.c_void_p, _dp]
             cls._lib = lib
         return cls._lib
 
@@ -205,6 +206,13 @@ class Oracle:
         self.lib().orc_plane_sums(self.h, a)
         return a.reshape(self.p["HIG"], 8)
 
+    def output_fields(self) -> np.ndarray:
+        """Output()'s 12 values per cell (src/output.c), (DEP, HIG, LEN, 12)."""
+        p = self.p
+        a = np.empty(12 * p["LEN"] * p["HIG"] * p["DEP"], np.float64)
+        self.lib().orc_output_fields(self.h, a)
+        return a.reshape(p["DEP"], p["HIG"], p["LEN"], 12)
+
     # --- standalone -----------------------------------------------------
     @classmethod
     def filter(cls, p: dict, a: np.ndarray) -> np.ndarray:
@@ -256,6 +264,7 @@ class RefOracle:
             lib.refh_minmod.restype = C.c_double
             lib.refh_random.argtypes = [C.c_double]
             lib.refh_random.restype = C.c_double
+            lib.refh_output.argtypes = [C.c_char_p]
             cls._lib = lib
         return cls._lib
 
@@ -318,6 +327,7 @@ class RefOracle:
     def fluxes(self): self.lib().refh_fluxes()
     def evolution(self, nst, stage): self.lib().refh_evolution(nst, stage)
     def check_courant(self): self.lib().refh_checkco()
+    def output(self, dir: str) -> int: return self.lib().refh_output(os.fsencode(dir))
     def disturb(self): self.lib().refh_disturb()
     def step(self, n=1): self.lib().refh_step(n)
 

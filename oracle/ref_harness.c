@@ -90,6 +90,18 @@ void refh_fluxes(void) { Fluxes(); }
 void refh_evolution(int nst, int stage) { Evolution(nst, stage); }
 void refh_dynsmag(void) { DynamicSmagorinsky(U1, U2, U3, U4, mu_SGS); }
 void refh_checkco(void) { checkCoNum(); }
+/* Output() writes "<step>.plt" into `dir` (src/output.c:16-141); its header
+ * file declares nothing. */
+void Output(void);
+int refh_output(const char *dir)
+{
+    char saved[4096];
+    if (!getcwd(saved, sizeof saved)) return -1;
+    if (chdir(dir) != 0) return -2;
+    Output();
+    if (chdir(saved) != 0) return -3;
+    return 0;
+}
 
 /* ---- array access ---------------------------------------------------- */
 

@@ -110,6 +110,8 @@ def test_host_driver_run_and_restart(fsl, oracle_lib, tmp_path):
     raw = (tmp_path / "backup.dat").read_bytes()
     np.testing.assert_array_equal(np.frombuffer(raw[:8 * n], np.float64), o.state())
     assert (tmp_path / "probes.dat").stat().st_size == 4 * (4 + 6 * p["HIG"] * 8)
+    frame = (tmp_path / "4.plt").read_text().splitlines()      # the end-of-run Output() frame
+    assert len(frame) == 15 + p["LEN"] * p["HIG"] * p["DEP"] and frame[14].startswith("i=12, j=8, k=6")
     p2 = dict(p, numstep=6, Answer=1)
     (tmp_path / "layer2.ini").write_text(oracle_lib.ini_text(p2))
     r = subprocess.run([exe], input=seed, text=True, capture_output=True, cwd=tmp_path, timeout=120)
@@ -118,3 +120,22 @@ def test_host_driver_run_and_restart(fsl, oracle_lib, tmp_path):
     raw = (tmp_path / "backup.dat").read_bytes()
     np.testing.assert_array_equal(np.frombuffer(raw[:8 * n], np.float64), o.state())
     assert np.frombuffer(raw[-4:], np.int32)[0] == 6
+
+
+def test_output_frame_matches_oracle(fsl, oracle_lib, tmp_path):
+    """Output()'s values (src/output.c) from the GPU state after steps equal
+    the oracle's bit for bit, and the written Tecplot frame equals the one
+    written from the oracle's values."""
+    p = spatial_params(L=12, H=8, D=6)
+    s = oracle_lib.spatial_initial_state(p)
+    o = oracle_lib.Oracle(p)
+    o.set_state(s)
+    o.step(3)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    d.step(3)
+    a, b = d.output_fields(), o.output_fields()
+    assert np.array_equal(a, b)
+    d.write_tecplot(str(tmp_path / "gpu.plt"))
+    fsl.tecplot_write(str(tmp_path / "orc.plt"), b)
+    assert (tmp_path / "gpu.plt").read_bytes() == (tmp_path / "orc.plt").read_bytes()

@@ -119,3 +119,21 @@ def test_sgs_once_per_step_equals_every_stage(orc):
     b = orc.Oracle(p); b.set_state(s)
     a.step(4); b.step_ref_sgs(4)
     _eq(a.state(), b.state(), "once-per-step SGS")
+
+
+def test_output_frame(orc, tmp_path):
+    """Output() (src/output.c): the restatement's 12 values per cell, written
+    by the library's Tecplot writer, give the reference's <step>.plt byte for
+    byte (after steps, with the ghost layer the last stage left)."""
+    import freeshearlayer_b200 as fsl
+    p = spatial_params(L=10, H=8, D=6)
+    s = orc.spatial_initial_state(p)
+    r, o = _pair(orc, p, s)
+    r.step(3); o.step(3)
+    ref_dir = tmp_path / "ref"
+    ref_dir.mkdir()
+    assert r.output(str(ref_dir)) == 0
+    ref_file = ref_dir / "3.plt"
+    mine = tmp_path / "mine.plt"
+    fsl.tecplot_write(str(mine), o.output_fields())
+    assert mine.read_bytes() == ref_file.read_bytes()
