@@ -99,8 +99,11 @@ __global__ void k_ghost(Grid g, int setup, double *__restrict__ u)
 
 // ---------------------------------------------------------------------------
 // A2 reconstruction (src/reconstruction.c:26-345): one thread per interior
-// cell, all three sweeps, six face states written to the face arrays.
+// cell, all three sweeps, six face states written to the face arrays.  With
+// PPM, a sweep whose four neighbours exist (the cell is not next to the
+// domain boundary in that direction) uses ppm_* instead.
 // ---------------------------------------------------------------------------
+template <bool PPM>
 __global__ void __launch_bounds__(128) k_recon(Grid g, const double *__restrict__ u, Faces f)
 {
     const int L = g.L, H = g.H, D = g.D;
@@ -120,7 +123,14 @@ __global__ void __launch_bounds__(128) k_recon(Grid g, const double *__restrict_
         const long long a = c0 + g.pi, b = c0 - g.pi;
 #pragma unroll
         for (int q = 0; q < 5; q++) { fw[q] = u[q * fs + a]; bw[q] = u[q * fs + b]; }
-        recon_x(c, fw, bw, hi, lo);
+        if (PPM && i >= 2 && i <= L - 1) {
+            double m2[5], p2[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) { p2[q] = u[q * fs + a + g.pi]; m2[q] = u[q * fs + b - g.pi]; }
+            ppm_x(c, m2, bw, fw, p2, hi, lo);
+        } else {
+            recon_x(c, fw, bw, hi, lo);
+        }
         const long long fh = ixf(L, H, D, i, j - 1, k - 1), fl = ixf(L, H, D, i - 1, j - 1, k - 1);
 #pragma unroll
         for (int q = 0; q < 5; q++) { f.x[0][q][fh] = hi[q]; f.x[1][q][fl] = lo[q]; }
@@ -131,7 +141,14 @@ __global__ void __launch_bounds__(128) k_recon(Grid g, const double *__restrict_
         const int perm[5] = {0, 2, 3, 1, 4};
 #pragma unroll
         for (int q = 0; q < 5; q++) { fw[q] = u[perm[q] * fs + a]; bw[q] = u[perm[q] * fs + b]; }
-        recon_y(c, fw, bw, hi, lo);
+        if (PPM && j >= 2 && j <= H - 1) {
+            double m2[5], p2[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) { p2[q] = u[perm[q] * fs + a + g.pk]; m2[q] = u[perm[q] * fs + b - g.pk]; }
+            ppm_y(c, m2, bw, fw, p2, hi, lo);
+        } else {
+            recon_y(c, fw, bw, hi, lo);
+        }
         const long long fh = iyf(L, H, D, i - 1, j, k - 1), fl = iyf(L, H, D, i - 1, j - 1, k - 1);
 #pragma unroll
         for (int q = 0; q < 5; q++) { f.y[0][q][fh] = hi[q]; f.y[1][q][fl] = lo[q]; }
@@ -142,7 +159,14 @@ __global__ void __launch_bounds__(128) k_recon(Grid g, const double *__restrict_
         const int perm[5] = {0, 3, 1, 2, 4};
 #pragma unroll
         for (int q = 0; q < 5; q++) { fw[q] = u[perm[q] * fs + a]; bw[q] = u[perm[q] * fs + b]; }
-        recon_z(c, fw, bw, hi, lo);
+        if (PPM && k >= 2 && k <= D - 1) {
+            double m2[5], p2[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) { p2[q] = u[perm[q] * fs + a + 1]; m2[q] = u[perm[q] * fs + b - 1]; }
+            ppm_z(c, m2, bw, fw, p2, hi, lo);
+        } else {
+            recon_z(c, fw, bw, hi, lo);
+        }
         const long long fh = izf(L, H, D, i - 1, j - 1, k), fl = izf(L, H, D, i - 1, j - 1, k - 1);
 #pragma unroll
         for (int q = 0; q < 5; q++) { f.z[0][q][fh] = hi[q]; f.z[1][q][fl] = lo[q]; }
@@ -589,7 +613,8 @@ void launch_recon(Ctx &c, const double *cur)
     const Grid &g = c.g;
     dim3 b(32, 4, 1);
     prof_begin(c, FSL_K_RECON);
-    k_recon<<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, cur, c.f);
+    if (c.p.recon == FSL_RECON_PPM) k_recon<true><<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, cur, c.f);
+    else k_recon<false><<<cells_grid(g, b, g.L, g.H, g.D), b, 0, c.stream>>>(g, cur, c.f);
     prof_end(c, FSL_K_RECON, 1);
 }
 

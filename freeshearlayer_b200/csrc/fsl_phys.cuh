@@ -159,6 +159,118 @@ template <typename T> __device__ __forceinline__ void recon_z(const CellC<T> &c,
                             c.w_ee, fw, bw, hi, lo);
 }
 
+// PPM (project extension; the reference has only the scheme above): Colella
+// & Woodward (1984) on the same characteristic variables, with cell i's
+// transform (src/reconstruction.c:104-129) and inverse (:148-158).  Per
+// characteristic field: monotonised-central slopes (CW84 eq. 1.8) of cells
+// i-1, i, i+1, edge values a_{i+1/2} - a_i = 1/2 d_{i+1/2} - (da_{i+1} -
+// da_i)/6 and a_{i-1/2} - a_i = -1/2 d_{i-1/2} - (da_i - da_{i-1})/6 (eq.
+// 1.6), the monotonicity limiter (eq. 1.10); the same arithmetic as the
+// oracle's restatement.
+template <typename T> __device__ __forceinline__ T ppm_mc(T a, T b)
+{
+    T m = T(0.5) * fabs(a + b);
+    const T ta = T(2.0) * fabs(a), tb = T(2.0) * fabs(b);
+    m = (ta < m) ? ta : m;
+    m = (tb < m) ? tb : m;
+    return (a * b <= T(0.0)) ? T(0.0) : ((a > T(0.0)) ? m : -m);
+}
+
+template <typename T>
+__device__ __forceinline__ void char_fwd(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2, const T *d, T *M)
+{
+    typedef Kc<T> k;
+    const T C = c.C;
+    T S12, S41, S42, S51, S52, kk, k2, k3;
+    S41 = c.aa - (kk = C * vn);
+    S51 = c.aa + kk;
+    S12 = S42 = S52 = bn;
+    S42 += C;
+    S52 -= C;
+    kk = k::K_1 * d[4]; k2 = bt1 * d[2]; k3 = bt2 * d[3];
+    M[0] = c.S11 * d[0] + S12 * d[1] + k2 + k3 + kk;
+    M[1] = -vt1 * d[0] + d[2];
+    M[2] = -vt2 * d[0] + d[3];
+    M[3] = S41 * d[0] + S42 * d[1] + k2 + k3 + kk;
+    M[4] = S51 * d[0] + S52 * d[1] + k2 + k3 + kk;
+}
+
+template <typename T, int N, int T1, int T2>
+__device__ __forceinline__ void char_inv(const CellC<T> &c, T vn, T vt1, T vt2, T n_hh, T t1_hh, T t2_hh, T n_ee,
+                                         T t1_ee, T t2_ee, const T *q, T *out)
+{
+    typedef Kc<T> k;
+    const T *u = c.u;
+    const T mm = vn * c.ll;
+    T _S24, _S25, _S54, _S55, kk;
+    _S24 = n_ee + c.ll; _S25 = n_ee - c.ll;
+    _S54 = _S55 = c.nn + k::H_K_1;
+    _S54 += mm; _S55 -= mm;
+    kk = q[3] + q[4];
+    out[0] = u[0] + c.hh * q[0] + c.ee * kk;
+    out[N] = u[N] + n_hh * q[0] + _S24 * q[3] + _S25 * q[4];
+    out[T1] = u[T1] + t1_hh * q[0] + q[1] + t1_ee * kk;
+    out[T2] = u[T2] + t2_hh * q[0] + q[2] + t2_ee * kk;
+    out[4] = u[4] + c.gg * q[0] + vt1 * q[1] + vt2 * q[2] + _S54 * q[3] + _S55 * q[4];
+}
+
+// m2, m1, p1, p2: the neighbours at -2, -1, +1, +2 in the sweep's order
+// (rho, normal, t1, t2, E); hi, lo as recon_sweep.
+template <typename T, int N, int T1, int T2>
+__device__ __forceinline__ void ppm_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2, T n_hh,
+                                          T t1_hh, T t2_hh, T n_ee, T t1_ee, T t2_ee, const T *m2, const T *m1,
+                                          const T *p1, const T *p2, T *hi, T *lo)
+{
+    const T *u = c.u;
+    const T uc[5] = {u[0], u[N], u[T1], u[T2], u[4]};
+    T d[5], W0[5], W1[5], W2[5], W3[5], qR[5], qL[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) d[v] = m1[v] - m2[v];
+    char_fwd(c, vn, vt1, vt2, bn, bt1, bt2, d, W0);
+#pragma unroll
+    for (int v = 0; v < 5; v++) d[v] = uc[v] - m1[v];
+    char_fwd(c, vn, vt1, vt2, bn, bt1, bt2, d, W1);
+#pragma unroll
+    for (int v = 0; v < 5; v++) d[v] = p1[v] - uc[v];
+    char_fwd(c, vn, vt1, vt2, bn, bt1, bt2, d, W2);
+#pragma unroll
+    for (int v = 0; v < 5; v++) d[v] = p2[v] - p1[v];
+    char_fwd(c, vn, vt1, vt2, bn, bt1, bt2, d, W3);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        const T dm = ppm_mc(W0[v], W1[v]), d0 = ppm_mc(W1[v], W2[v]), dp = ppm_mc(W2[v], W3[v]);
+        T r = T(0.5) * W2[v] - (dp - d0) / T(6.0), l = T(-0.5) * W1[v] - (d0 - dm) / T(6.0);
+        const bool flat = r * l >= T(0.0);
+        const bool capR = !flat && fabs(r) > T(2.0) * fabs(l);
+        const bool capL = !flat && !capR && fabs(l) > T(2.0) * fabs(r);
+        const T r2 = flat ? T(0.0) : (capR ? T(-2.0) * l : r);
+        const T l2 = flat ? T(0.0) : (capL ? T(-2.0) * r : l);
+        qR[v] = r2;
+        qL[v] = l2;
+    }
+    char_inv<T, N, T1, T2>(c, vn, vt1, vt2, n_hh, t1_hh, t2_hh, n_ee, t1_ee, t2_ee, qR, hi);
+    char_inv<T, N, T1, T2>(c, vn, vt1, vt2, n_hh, t1_hh, t2_hh, n_ee, t1_ee, t2_ee, qL, lo);
+}
+
+template <typename T>
+__device__ __forceinline__ void ppm_x(const CellC<T> &c, const T *m2, const T *m1, const T *p1, const T *p2, T *hi, T *lo)
+{
+    ppm_sweep<T, 1, 2, 3>(c, c.U, c.V, c.W, c.bb, c.cc, c.dd, c.u_hh, c.v_hh, c.w_hh, c.u_ee, c.v_ee, c.w_ee, m2, m1,
+                          p1, p2, hi, lo);
+}
+template <typename T>
+__device__ __forceinline__ void ppm_y(const CellC<T> &c, const T *m2, const T *m1, const T *p1, const T *p2, T *hi, T *lo)
+{
+    ppm_sweep<T, 2, 3, 1>(c, c.V, c.W, c.U, c.cc, c.dd, c.bb, c.v_hh, c.w_hh, c.u_hh, c.v_ee, c.w_ee, c.u_ee, m2, m1,
+                          p1, p2, hi, lo);
+}
+template <typename T>
+__device__ __forceinline__ void ppm_z(const CellC<T> &c, const T *m2, const T *m1, const T *p1, const T *p2, T *hi, T *lo)
+{
+    ppm_sweep<T, 3, 1, 2>(c, c.W, c.U, c.V, c.dd, c.bb, c.cc, c.w_hh, c.u_hh, c.v_hh, c.w_ee, c.u_ee, c.w_ee, m2, m1,
+                          p1, p2, hi, lo);
+}
+
 // Linearised characteristic Riemann solve on one face (src/fluxes.c:61-113,
 // :230-282, :401-453).  N = normal direction 1..3.  Lm/Rp: minus/plus
 // conserved states.  Returns interface density, pressure and velocity (the

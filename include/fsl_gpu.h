@@ -65,7 +65,8 @@ extern "C" {
 
 /* reconstruction */
 #define FSL_RECON_CHARMINMOD 0 /* characteristic kappa=1/3 minmod(beta=4), src/reconstruction.c:26-345 */
-#define FSL_RECON_PPM 1        /* Colella-Woodward PPM: not built, fsl_init returns FSL_ERR_UNSUPPORTED */
+#define FSL_RECON_PPM 1        /* Colella-Woodward PPM on the same characteristic variables (project
+                                  extension): per-phase FP64 kernels only (fsl_step runs them) */
 
 /* Parameters: the 22 positional values of layer2.ini in file order
  * (src/initialize.c:25-58; src-par's mpi_layer2.bin holds the same 22 values
@@ -120,7 +121,7 @@ int fsl_params_from_ini(const char *path, fsl_params *p);
  * Option fields are left as for fsl_params_from_ini. */
 int fsl_params_from_bin(const char *path, fsl_params *p);
 /* Check a parameter set; FSL_OK, FSL_ERR_ARG, or FSL_ERR_UNSUPPORTED for an
- * option that is not built (FSL_RECON_PPM). */
+ * option combination that is not built (FSL_RECON_PPM with FP32 bulk). */
 int fsl_params_check(const fsl_params *p);
 
 /* ---- initial states (host arrays in the state layout) ----------------- */

@@ -323,6 +323,103 @@ static void recon_dir(const cellc *c, int n, int t1, int t2, double vn, double v
     lo[4] = u[4] - c->gg * k1 - vt1 * k2 - vt2 * k3 - _S54 * k4 - _S55 * k5;
 }
 
+/* ------------------------------------------------------------------------
+ * PPM reconstruction (project extension; the reference has none): Colella &
+ * Woodward (1984) on the characteristic variables of the reference's
+ * reconstruction (the transform of src/reconstruction.c:104-129 and its
+ * inverse, :148-158, with cell i's constants).  Per characteristic field:
+ * monotonised-central slopes (CW84 eq. 1.8) of cells i-1, i, i+1 from the
+ * four differences around cell i, edge values a_{i+1/2} - a_i =
+ * 1/2 d_{i+1/2} - (da_{i+1} - da_i)/6 and a_{i-1/2} - a_i =
+ * -1/2 d_{i-1/2} - (da_i - da_{i-1})/6 (eq. 1.6), the monotonicity limiter
+ * (eq. 1.10), and the two face states.  Cells next to a domain boundary in
+ * the sweep direction (one ghost layer: no second neighbour) use the
+ * reference's reconstruction in that direction.
+ * ------------------------------------------------------------------------ */
+static double orc_mc(double a, double b)
+{
+    double m, t;
+    if (a * b <= 0.0) return 0.0;
+    m = 0.5 * fabs(a + b);
+    t = 2.0 * fabs(a);
+    if (t < m) m = t;
+    t = 2.0 * fabs(b);
+    if (t < m) m = t;
+    return a > 0.0 ? m : -m;
+}
+
+/* d: a difference in the sweep's order (rho, normal, t1, t2, E) -> M */
+static void char_fwd(const cellc *c, double vn, double vt1, double vt2, double bn, double bt1, double bt2,
+                     const double *d, double *M)
+{
+    double S12, S41, S42, S51, S52, kk, k2, k3;
+    const double C = c->C;
+    S41 = c->aa - (kk = C * vn);
+    S51 = c->aa + kk;
+    S12 = S42 = S52 = bn;
+    S42 += C;
+    S52 -= C;
+    kk = K_1 * d[4]; k2 = bt1 * d[2]; k3 = bt2 * d[3];
+    M[0] = c->S11 * d[0] + S12 * d[1] + k2 + k3 + kk;
+    M[1] = -vt1 * d[0] + d[2];
+    M[2] = -vt2 * d[0] + d[3];
+    M[3] = S41 * d[0] + S42 * d[1] + k2 + k3 + kk;
+    M[4] = S51 * d[0] + S52 * d[1] + k2 + k3 + kk;
+}
+
+/* out = u + R q (natural variable order) */
+static void char_inv(const cellc *c, int n, int t1, int t2, double vn, double vt1, double vt2, double n_hh,
+                     double t1_hh, double t2_hh, double n_ee, double t1_ee, double t2_ee, const double *q, double *out)
+{
+    const double *u = c->u;
+    const double mm = vn * c->ll;
+    double _S24, _S25, _S54, _S55, kk;
+    _S24 = n_ee + c->ll; _S25 = n_ee - c->ll;
+    _S54 = _S55 = c->nn + H_K_1;
+    _S54 += mm; _S55 -= mm;
+    kk = q[3] + q[4];
+    out[0] = u[0] + c->hh * q[0] + c->ee * kk;
+    out[n] = u[n] + n_hh * q[0] + _S24 * q[3] + _S25 * q[4];
+    out[t1] = u[t1] + t1_hh * q[0] + q[1] + t1_ee * kk;
+    out[t2] = u[t2] + t2_hh * q[0] + q[2] + t2_ee * kk;
+    out[4] = u[4] + c->gg * q[0] + vt1 * q[1] + vt2 * q[2] + _S54 * q[3] + _S55 * q[4];
+}
+
+/* m2, m1, p1, p2: neighbours at -2, -1, +1, +2 in the sweep's order */
+static void recon_dir_ppm(const cellc *c, int n, int t1, int t2, double vn, double vt1, double vt2, double bn,
+                          double bt1, double bt2, double n_hh, double t1_hh, double t2_hh, double n_ee, double t1_ee,
+                          double t2_ee, const double *m2, const double *m1, const double *p1, const double *p2,
+                          double *hi, double *lo)
+{
+    const double *u = c->u;
+    const double uc[5] = {u[0], u[n], u[t1], u[t2], u[4]};
+    double d[4][5], W[4][5], qR[5], qL[5];
+    int v;
+    for (v = 0; v < 5; v++) {
+        d[0][v] = m1[v] - m2[v];
+        d[1][v] = uc[v] - m1[v];
+        d[2][v] = p1[v] - uc[v];
+        d[3][v] = p2[v] - p1[v];
+    }
+    for (v = 0; v < 4; v++) char_fwd(c, vn, vt1, vt2, bn, bt1, bt2, d[v], W[v]);
+    for (v = 0; v < 5; v++) {
+        const double dm = orc_mc(W[0][v], W[1][v]), d0 = orc_mc(W[1][v], W[2][v]), dp = orc_mc(W[2][v], W[3][v]);
+        double r = 0.5 * W[2][v] - (dp - d0) / 6.0, l = -0.5 * W[1][v] - (d0 - dm) / 6.0;
+        if (r * l >= 0.0) {
+            r = 0.0;
+            l = 0.0;
+        } else if (fabs(r) > 2.0 * fabs(l)) {
+            r = -2.0 * l;
+        } else if (fabs(l) > 2.0 * fabs(r)) {
+            l = -2.0 * r;
+        }
+        qR[v] = r;
+        qL[v] = l;
+    }
+    char_inv(c, n, t1, t2, vn, vt1, vt2, n_hh, t1_hh, t2_hh, n_ee, t1_ee, t2_ee, qR, hi);
+    char_inv(c, n, t1, t2, vn, vt1, vt2, n_hh, t1_hh, t2_hh, n_ee, t1_ee, t2_ee, qL, lo);
+}
+
 void orc_reconstruct(orc_ctx *o)
 {
     const int L = o->L, H = o->H, D = o->D;
@@ -358,8 +455,16 @@ void orc_reconstruct(orc_ctx *o)
                 f = IC(o, i + 1, j, k); b = IC(o, i - 1, j, k);
                 fw[0] = u[0][f]; fw[1] = u[1][f]; fw[2] = u[2][f]; fw[3] = u[3][f]; fw[4] = u[4][f];
                 bw[0] = u[0][b]; bw[1] = u[1][b]; bw[2] = u[2][b]; bw[3] = u[3][b]; bw[4] = u[4][b];
-                recon_dir(&c, 1, 2, 3, c.U, c.V, c.W, bb, cc, dd, c.u_hh, c.v_hh, c.w_hh,
-                          c.u_ee, c.v_ee, c.w_ee, fw, bw, hi, lo);
+                if (o->p.recon == 1 && i >= 2 && i <= L - 1) {
+                    double m2[5], p2[5];
+                    size_t a2 = IC(o, i + 2, j, k), b2 = IC(o, i - 2, j, k);
+                    for (v = 0; v < 5; v++) { p2[v] = u[v][a2]; m2[v] = u[v][b2]; }
+                    recon_dir_ppm(&c, 1, 2, 3, c.U, c.V, c.W, bb, cc, dd, c.u_hh, c.v_hh, c.w_hh,
+                                  c.u_ee, c.v_ee, c.w_ee, m2, bw, fw, p2, hi, lo);
+                } else {
+                    recon_dir(&c, 1, 2, 3, c.U, c.V, c.W, bb, cc, dd, c.u_hh, c.v_hh, c.w_hh,
+                              c.u_ee, c.v_ee, c.w_ee, fw, bw, hi, lo);
+                }
                 for (v = 0; v < 5; v++) {
                     o->fs[0][0][v][IX(o, i, j - 1, k - 1)] = hi[v];
                     o->fs[0][1][v][IX(o, i - 1, j - 1, k - 1)] = lo[v];
@@ -368,8 +473,17 @@ void orc_reconstruct(orc_ctx *o)
                 f = IC(o, i, j + 1, k); b = IC(o, i, j - 1, k);
                 fw[0] = u[0][f]; fw[1] = u[2][f]; fw[2] = u[3][f]; fw[3] = u[1][f]; fw[4] = u[4][f];
                 bw[0] = u[0][b]; bw[1] = u[2][b]; bw[2] = u[3][b]; bw[3] = u[1][b]; bw[4] = u[4][b];
-                recon_dir(&c, 2, 3, 1, c.V, c.W, c.U, cc, dd, bb, c.v_hh, c.w_hh, c.u_hh,
-                          c.v_ee, c.w_ee, c.u_ee, fw, bw, hi, lo);
+                if (o->p.recon == 1 && j >= 2 && j <= H - 1) {
+                    double m2[5], p2[5];
+                    size_t a2 = IC(o, i, j + 2, k), b2 = IC(o, i, j - 2, k);
+                    p2[0] = u[0][a2]; p2[1] = u[2][a2]; p2[2] = u[3][a2]; p2[3] = u[1][a2]; p2[4] = u[4][a2];
+                    m2[0] = u[0][b2]; m2[1] = u[2][b2]; m2[2] = u[3][b2]; m2[3] = u[1][b2]; m2[4] = u[4][b2];
+                    recon_dir_ppm(&c, 2, 3, 1, c.V, c.W, c.U, cc, dd, bb, c.v_hh, c.w_hh, c.u_hh,
+                                  c.v_ee, c.w_ee, c.u_ee, m2, bw, fw, p2, hi, lo);
+                } else {
+                    recon_dir(&c, 2, 3, 1, c.V, c.W, c.U, cc, dd, bb, c.v_hh, c.w_hh, c.u_hh,
+                              c.v_ee, c.w_ee, c.u_ee, fw, bw, hi, lo);
+                }
                 for (v = 0; v < 5; v++) {
                     o->fs[1][0][v][IY(o, i - 1, j, k - 1)] = hi[v];
                     o->fs[1][1][v][IY(o, i - 1, j - 1, k - 1)] = lo[v];
@@ -379,8 +493,17 @@ void orc_reconstruct(orc_ctx *o)
                 f = IC(o, i, j, k + 1); b = IC(o, i, j, k - 1);
                 fw[0] = u[0][f]; fw[1] = u[3][f]; fw[2] = u[1][f]; fw[3] = u[2][f]; fw[4] = u[4][f];
                 bw[0] = u[0][b]; bw[1] = u[3][b]; bw[2] = u[1][b]; bw[3] = u[2][b]; bw[4] = u[4][b];
-                recon_dir(&c, 3, 1, 2, c.W, c.U, c.V, dd, bb, cc, c.w_hh, c.u_hh, c.v_hh,
-                          c.w_ee, c.u_ee, c.w_ee, fw, bw, hi, lo);
+                if (o->p.recon == 1 && k >= 2 && k <= D - 1) {
+                    double m2[5], p2[5];
+                    size_t a2 = IC(o, i, j, k + 2), b2 = IC(o, i, j, k - 2);
+                    p2[0] = u[0][a2]; p2[1] = u[3][a2]; p2[2] = u[1][a2]; p2[3] = u[2][a2]; p2[4] = u[4][a2];
+                    m2[0] = u[0][b2]; m2[1] = u[3][b2]; m2[2] = u[1][b2]; m2[3] = u[2][b2]; m2[4] = u[4][b2];
+                    recon_dir_ppm(&c, 3, 1, 2, c.W, c.U, c.V, dd, bb, cc, c.w_hh, c.u_hh, c.v_hh,
+                                  c.w_ee, c.u_ee, c.w_ee, m2, bw, fw, p2, hi, lo);
+                } else {
+                    recon_dir(&c, 3, 1, 2, c.W, c.U, c.V, dd, bb, cc, c.w_hh, c.u_hh, c.v_hh,
+                              c.w_ee, c.u_ee, c.w_ee, fw, bw, hi, lo);
+                }
                 for (v = 0; v < 5; v++) {
                     o->fs[2][0][v][IZ(o, i - 1, j - 1, k)] = hi[v];
                     o->fs[2][1][v][IZ(o, i - 1, j - 1, k - 1)] = lo[v];

@@ -47,6 +47,7 @@ typedef struct orc_params {
     int setup;     /* ORC_SETUP_* */
     int cfl_mode;  /* ORC_CFL_* */
     double seed_X; /* disturbance RNG seed (the reference reads it from stdin) */
+    int recon;     /* 0: the reference's reconstruction, 1: PPM (project extension) */
 } orc_params;
 
 typedef struct orc_ctx orc_ctx;

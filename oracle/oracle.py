@@ -40,7 +40,7 @@ class OrcParams(C.Structure):
                 ("Va", C.c_double), ("Wa", C.c_double), ("Ns_min", C.c_int),
                 ("Nst", C.c_int), ("f_step", C.c_int), ("nStages", C.c_int),
                 ("maxCoNum", C.c_double), ("setup", C.c_int), ("cfl_mode", C.c_int),
-                ("seed_X", C.c_double)]
+                ("seed_X", C.c_double), ("recon", C.c_int)]
 
 
 def build(ref: bool = False) -> None:
@@ -134,7 +134,7 @@ class Oracle:
 
     def __init__(self, p: dict):
         self.p = dict(p)
-        self.cp = OrcParams(**{k: self.p[k] for k, _ in OrcParams._fields_})
+        self.cp = OrcParams(**{k: self.p.get(k, 0) for k, _ in OrcParams._fields_})
         self.h = self.lib().orc_create(C.byref(self.cp))
         if not self.h:
             raise MemoryError("orc_create failed")
@@ -216,7 +216,7 @@ class Oracle:
     # --- standalone -----------------------------------------------------
     @classmethod
     def filter(cls, p: dict, a: np.ndarray) -> np.ndarray:
-        cp = OrcParams(**{k: p[k] for k, _ in OrcParams._fields_})
+        cp = OrcParams(**{k: p.get(k, 0) for k, _ in OrcParams._fields_})
         out = np.empty_like(a)
         cls.lib().orc_filter(C.byref(cp), np.ascontiguousarray(a), out)
         return out
@@ -224,7 +224,7 @@ class Oracle:
     @classmethod
     def temporal_state(cls, p: dict, Mc: float, delta_w0: float = 1.0, amp: float = 1e-3,
                        seed: int = 20251203):
-        cp = OrcParams(**{k: p[k] for k, _ in OrcParams._fields_})
+        cp = OrcParams(**{k: p.get(k, 0) for k, _ in OrcParams._fields_})
         out = np.empty(p["LEN"] * p["HIG"] * 5 * p["DEP"], np.float64)
         dU = C.c_double()
         rc = cls.lib().orc_temporal_state(C.byref(cp), Mc, delta_w0, amp, seed, out, C.byref(dU))

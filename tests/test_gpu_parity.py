@@ -205,3 +205,24 @@ def test_sums_and_plane_sums(fsl, oracle_lib):
     o, d = _pair(fsl, oracle_lib, p, s)
     np.testing.assert_allclose(d.sums(), o.sums(), rtol=1e-13)
     np.testing.assert_allclose(d.plane_sums(), o.plane_sums(), rtol=1e-12)
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_ppm_reconstruct_and_steps(fsl, oracle_lib, setup):
+    """PPM (project extension) on the per-phase kernels: face states and whole
+    steps (fsl_step routes PPM to them) bit-identical to the oracle's
+    restatement."""
+    p = (spatial_params(L=12, H=10, D=9) if setup == 0 else temporal_params(L=16, H=10, D=12))
+    p = dict(p, recon=1)
+    s = random_state(p, 15) if setup == 0 else oracle_lib.Oracle.temporal_state(p, 0.4, amp=0.02)[0]
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.ghost(); d.ghost_bc()
+    o.recon(); d.reconstruct()
+    for dd in range(3):
+        for side in range(2):
+            for v in range(5):
+                _assert_same(d.faces(dd, side, v), o.faces(dd, side, v), "PPM face dir %d side %d var %d" % (dd, side, v))
+    o2, d2 = _pair(fsl, oracle_lib, p, s)
+    o2.step(4)
+    d2.step(4)
+    _assert_same(d2.download_state(), o2.state(), "state after 4 PPM steps")
