@@ -252,6 +252,20 @@ def time_steps(torch, d, run, steps, barrier, clocks=None):
     return ms, kt, clk
 
 
+def profiled_traffic(prec):
+    """DRAM bytes per cell of one stage-2 launch of the fused stage kernel,
+    from the committed ncu summary of the 256x128x128 capture (the line
+    'derived: ... per cell X B'), or None."""
+    import re
+    name = "k_stage_fp64_256x128x128.txt" if prec == 0 else "k_stage_fp32_256x128x128.txt"
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            m = re.search(r"per cell ([0-9.]+) B", f.read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
 def stage_roofline(kt, names, ncell, prec, peaks, traffic):
     kms = {names[i]: kt.ms[i] for i in range(8)}
     kl = {names[i]: int(kt.launches[i]) for i in range(8)}
@@ -259,10 +273,18 @@ def stage_roofline(kt, names, ncell, prec, peaks, traffic):
     alg = STAGE_BYTES[prec] * ncell
     avg_ms = kms["stage"] / launches
     achieved = alg / (avg_ms / 1e3) / 1e9
+    note = None
+    if traffic is None:
+        per_cell = profiled_traffic(prec)
+        if per_cell is not None:
+            traffic = per_cell * ncell
+            note = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-2 launch at 256x128x128 "
+                    "(%.2f B/cell; that stage's algorithmic bytes are %d B/cell), scaled by cells"
+                    % (per_cell, 128 if prec == 0 else 124))
     return {"bound": "hbm", "kernel": "k_stage<%s> (fused reconstruction + Riemann + viscous flux + "
                                        "divergence + RK stage)" % ("double" if prec == 0 else "float"),
             "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
+            "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic, "traffic_note": note,
             "peak_source": peaks["source"] + " HBM copy bandwidth (burst)",
             "alg_bytes_per_cell": round(STAGE_BYTES[prec], 2), "alg_bytes_per_launch": alg,
             "avg_launch_ms": round(avg_ms, 4), "launches": launches}, kms, kl
