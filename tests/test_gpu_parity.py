@@ -226,3 +226,20 @@ def test_ppm_reconstruct_and_steps(fsl, oracle_lib, setup):
     o2.step(4)
     d2.step(4)
     _assert_same(d2.download_state(), o2.state(), "state after 4 PPM steps")
+
+
+def test_c1_config_200_steps(fsl, oracle_lib):
+    """The CPU-runnable configuration at full size: temporal shear layer
+    64x32x32 on 2pi x pi x pi, Mc 0.4, Re_dw0 500, noise 1e-3 dU, minmod
+    characteristic reconstruction, dynamic Smagorinsky, RK3 at acoustic CFL
+    0.5, 200 fused steps: all five conserved variables bit-identical to the
+    oracle (the stated bar is 1e-10 relative L2)."""
+    p = temporal_params(L=64, H=32, D=32, Mc=0.4, Re=500.0)
+    s, _ = oracle_lib.Oracle.temporal_state(p, 0.4, amp=1e-3)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.step(200)
+    d.step(200)
+    a, b = d.download_state(), o.state()
+    errs = per_var_rel_l2(a, b, p)
+    assert max(errs) <= PARITY_RTOL, errs
+    _assert_same(a, b, "state after 200 steps")
