@@ -159,6 +159,11 @@ def lib():
             "fsl_output_fields": [vp, _dp], "fsl_write_tecplot": [vp, cs],
             "fsl_tecplot_write": [cs, i, i, i, _dp],
         })
+        sig.update({
+            "fsl_get_planes": [vp, i, i, vp], "fsl_set_planes": [vp, i, i, vp],
+            "fsl_set_courant_range": [vp, i, i], "fsl_courant_prepare": [vp],
+            "fsl_get_courant_max": [vp, C.POINTER(C.c_double)], "fsl_set_courant_max": [vp, d],
+        })
         sig["fsl_tune"] = [vp, i, i]
         sig["fsl_profile"] = [vp, i]
         sig["fsl_profile_read"] = [vp, C.POINTER(KTimes)]
@@ -174,6 +179,8 @@ def lib():
         L.fsl_ensemble_last_error.restype = C.c_char_p
         L.fsl_ensemble_stream.argtypes = [vp]
         L.fsl_ensemble_stream.restype = C.c_void_p
+        L.fsl_courant_bits.argtypes = [vp]
+        L.fsl_courant_bits.restype = C.c_void_p
         L.fsl_trainer_size.argtypes = [vp]
         L.fsl_trainer_size.restype = C.c_longlong
         _lib = L
@@ -240,6 +247,21 @@ def temporal_state(p, Mc: float, delta_w0: float = 1.0, amp: float = 1e-3,
     return out, dU.value
 
 
+def _buffer_ptr(buf, n: int) -> int:
+    """Address of a contiguous float64 buffer of at least n values (numpy
+    array or torch tensor, host or CUDA)."""
+    if isinstance(buf, np.ndarray):
+        if buf.dtype != np.float64 or not buf.flags.c_contiguous or buf.size < n:
+            raise FslError(-1, "buffer: contiguous float64 with %d values expected" % n)
+        return buf.ctypes.data
+    if hasattr(buf, "data_ptr"):
+        import torch
+        if buf.dtype != torch.float64 or not buf.is_contiguous() or buf.numel() < n:
+            raise FslError(-1, "buffer: contiguous float64 with %d values expected" % n)
+        return buf.data_ptr()
+    raise FslError(-1, "buffer: numpy array or torch tensor expected")
+
+
 class Domain:
     """One device-resident domain (an fsl_ctx) on the current CUDA device."""
 
@@ -293,6 +315,37 @@ class Domain:
 
     def set_time(self, step: int, dt: float):
         self._c(lib().fsl_set_time(self.h, step, dt))
+
+    # --- x-slabs ------------------------------------------------------------------
+    def plane_size(self) -> int:
+        return self.p.HIG * 5 * self.p.DEP
+
+    def get_planes(self, i0: int, n: int, out):
+        """Planes i0..i0+n-1 (1-based) of U^n into `out`: a contiguous float64
+        numpy array or CUDA tensor of at least n * plane_size() values."""
+        self._c(lib().fsl_get_planes(self.h, i0, n, _buffer_ptr(out, n * self.plane_size())))
+        return out
+
+    def set_planes(self, i0: int, n: int, buf):
+        self._c(lib().fsl_set_planes(self.h, i0, n, _buffer_ptr(buf, n * self.plane_size())))
+
+    def set_courant_range(self, i0: int, i1: int):
+        self._c(lib().fsl_set_courant_range(self.h, i0, i1))
+
+    def courant_prepare(self):
+        self._c(lib().fsl_courant_prepare(self.h))
+
+    def get_courant_max(self) -> float:
+        m = C.c_double()
+        self._c(lib().fsl_get_courant_max(self.h, C.byref(m)))
+        return m.value
+
+    def set_courant_max(self, m: float):
+        self._c(lib().fsl_set_courant_max(self.h, m))
+
+    def courant_bits_ptr(self) -> int:
+        """Device address of the Courant maximum's bit pattern (uint64)."""
+        return lib().fsl_courant_bits(self.h)
 
     def info(self) -> Info:
         i = Info()

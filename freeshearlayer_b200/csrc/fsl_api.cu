@@ -425,6 +425,8 @@ int fsl_init(const fsl_params *p, fsl_ctx **out)
     c.p = *p;
     c.device = dev;
     c.g = make_grid(p->LEN, p->HIG, p->DEP, 8);
+    c.co_i0 = 1;
+    c.co_i1 = p->LEN;
     // derived constants, src/initialize.c:67-94
     c.k.rdx = 1. / p->deltaX; c.k.rdy = 1. / p->deltaY; c.k.rdz = 1. / p->deltaZ;
     c.k.r4dx = 1. / (4 * p->deltaX); c.k.r4dy = 1. / (4 * p->deltaY); c.k.r4dz = 1. / (4 * p->deltaZ);
@@ -543,7 +545,7 @@ int fsl_upload_state(fsl_ctx *h, const double *state)
     const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
     c.co_valid = false;
     CK(cudaMemcpyAsync(c.stage_dev, state, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    launch_state_scatter(c, c.U, c.stage_dev);
+    launch_state_scatter(c, c.U, c.stage_dev, 1, c.p.LEN);
     CKL();
     CK(cudaStreamSynchronize(c.stream));
     c.cur = 0;
@@ -555,10 +557,102 @@ int fsl_download_state(fsl_ctx *h, double *state)
     if (!h || !state) return FSL_ERR_ARG;
     Ctx &c = h->c;
     const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
-    launch_state_gather(c, c.U, c.stage_dev);
+    launch_state_gather(c, c.U, c.stage_dev, 1, c.p.LEN);
     CKL();
     CK(cudaMemcpyAsync(state, c.stage_dev, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+// ---- x-slabs ----------------------------------------------------------------
+// A decomposed domain is a set of contexts, one per slab of x-planes (one per
+// GPU), each holding its own planes plus overlap planes copied from its
+// neighbours once per step.  These calls move planes in and out of U^n and
+// make the Courant maximum (src/helpers.c:23-52) a maximum over the owned
+// planes, to be combined across slabs before the next step.
+
+static bool planes_ok(const Ctx &c, int i0, int n)
+{
+    return i0 >= 1 && n >= 0 && i0 + n - 1 <= c.p.LEN;
+}
+
+int fsl_get_planes(fsl_ctx *h, int i0, int n, double *buf)
+{
+    if (!h || !buf || !planes_ok(h->c, i0, n)) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_get_planes: the current-stage buffer is not U^n");
+    const size_t bytes = (size_t)n * c.p.HIG * 5 * c.p.DEP * sizeof(double);
+    launch_state_gather(c, c.U, c.stage_dev, i0, n);
+    CKL();
+    if (bytes) CK(cudaMemcpyAsync(buf, c.stage_dev, bytes, cudaMemcpyDefault, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+int fsl_set_planes(fsl_ctx *h, int i0, int n, const double *buf)
+{
+    if (!h || !buf || !planes_ok(h->c, i0, n)) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_set_planes: the current-stage buffer is not U^n");
+    const size_t bytes = (size_t)n * c.p.HIG * 5 * c.p.DEP * sizeof(double);
+    // planes outside the Courant range leave the owned maximum as it is
+    if (n > 0 && i0 <= c.co_i1 && i0 + n - 1 >= c.co_i0) c.co_valid = false;
+    if (bytes) CK(cudaMemcpyAsync(c.stage_dev, buf, bytes, cudaMemcpyDefault, c.stream));
+    launch_state_scatter(c, c.U, c.stage_dev, i0, n);
+    CKL();
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+int fsl_set_courant_range(fsl_ctx *h, int i0, int i1)
+{
+    if (!h || i0 < 1 || i1 < i0 || i1 > h->c.p.LEN) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    c.co_i0 = i0;
+    c.co_i1 = i1;
+    c.co_valid = false;
+    return FSL_OK;
+}
+
+int fsl_courant_prepare(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_courant_prepare: the current-stage buffer is not U^n");
+    if (!c.co_valid) {
+        launch_courant_to_bits(c);
+        CKL();
+        c.co_valid = true;
+    }
+    return FSL_OK;
+}
+
+unsigned long long *fsl_courant_bits(fsl_ctx *h)
+{
+    return h ? &h->c.ds->co_bits : nullptr;
+}
+
+int fsl_get_courant_max(fsl_ctx *h, double *maxCo)
+{
+    if (!h || !maxCo) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    if (!c.co_valid) return fail(c, FSL_ERR_ARG, "fsl_get_courant_max: no maximum for the current state");
+    unsigned long long b = 0;
+    CK(cudaMemcpyAsync(&b, &c.ds->co_bits, sizeof b, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    memcpy(maxCo, &b, sizeof b);
+    return FSL_OK;
+}
+
+int fsl_set_courant_max(fsl_ctx *h, double maxCo)
+{
+    if (!h || !(maxCo >= 0.0)) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    unsigned long long b;
+    memcpy(&b, &maxCo, sizeof b);
+    CK(cudaMemcpyAsync(&c.ds->co_bits, &b, sizeof b, cudaMemcpyHostToDevice, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    c.co_valid = true;
     return FSL_OK;
 }
 
@@ -675,14 +769,34 @@ int fsl_evolution(fsl_ctx *h, int stage)
     return FSL_OK;
 }
 
+// An x-slab (Courant range narrower than the domain) steps one step at a
+// time, from a Courant maximum combined across the slabs; a learned closure
+// would judge on the slab alone.
+static int slab_check(Ctx &c, int nsteps)
+{
+    if (c.co_i0 == 1 && c.co_i1 == c.p.LEN) return FSL_OK;
+    if (nsteps > 1) return fail(c, FSL_ERR_ARG, "x-slab: one step per call (overlap exchange between steps)");
+    if (nsteps == 1 && !c.co_valid)
+        return fail(c, FSL_ERR_ARG, "x-slab: no combined Courant maximum (fsl_courant_prepare / fsl_set_courant_max)");
+    if (c.p.sgs == FSL_SGS_LEARNED && c.judge_every > 0)
+        return fail(c, FSL_ERR_UNSUPPORTED, "x-slab: closure judgements would differ between slabs");
+    return FSL_OK;
+}
+
+static bool is_slab(const Ctx &c)
+{
+    return c.co_i0 != 1 || c.co_i1 != c.p.LEN;
+}
+
 int fsl_step_phased(fsl_ctx *h, int nsteps)
 {
     if (!h || nsteps < 0) return FSL_ERR_ARG;
     Ctx &c = h->c;
     int rc;
-    c.co_valid = false;
+    if ((rc = slab_check(c, nsteps))) return rc;
     for (int n = 0; n < nsteps; n++) {
-        launch_courant(c);
+        if (c.co_valid) launch_courant_apply(c);
+        else launch_courant(c);
         CKL();
         c.step++;
         draw(c);
@@ -698,6 +812,13 @@ int fsl_step_phased(fsl_ctx *h, int nsteps)
             launch_evolution(c, c.p.nStages, s);
             c.cur = (s == 1 || s == 2) ? 1 : 0;
             CKL();
+        }
+        c.co_valid = false;
+        if (is_slab(c)) {
+            // the owned maximum of the new state, to be combined across slabs
+            launch_courant_to_bits(c);
+            CKL();
+            c.co_valid = true;
         }
     }
     return FSL_OK;
@@ -715,6 +836,7 @@ int fsl_step(fsl_ctx *h, int nsteps)
         return fsl_step_phased(h, nsteps);
     }
     int rc;
+    if ((rc = slab_check(c, nsteps))) return rc;
     if ((rc = ensure_dyn(c))) return rc;
     if ((rc = ensure_bf(c))) return rc;
     if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_step: the current-stage buffer is not U^n");

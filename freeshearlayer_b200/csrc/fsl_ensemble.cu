@@ -58,6 +58,8 @@ int check_member(fsl_ensemble *e, const Ctx &c)
     if (c.p.sgs == FSL_SGS_LEARNED && c.judge_every > 0)
         return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members with the learned closure need judgements off");
     if (c.prof) return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members must not be profiling");
+    if (c.co_i0 != 1 || c.co_i1 != c.p.LEN)
+        return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members must be whole domains, not x-slabs");
     return FSL_OK;
 }
 

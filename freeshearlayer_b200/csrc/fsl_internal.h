@@ -137,6 +137,9 @@ struct Ctx {
     int favre_count = 0;
     // the device Courant maximum (DevScalars::co_bits) belongs to the current U^n
     bool co_valid = false;
+    // planes (1-based) whose cells enter the Courant maximum; 1..L unless an
+    // x-slab of a decomposed domain restricts it to the planes it owns
+    int co_i0 = 1, co_i1 = 0;
     double dt_host = 0; // host copy of dt, valid after sync
     double maxco_host = 0;
     unsigned long long bytes = 0;
@@ -179,8 +182,9 @@ void launch_judge_rows(Ctx &c, const double *a, const double *b, double *rows);
 void launch_courant(Ctx &c);
 // dt update from the Courant maximum the fused stage 3 accumulated
 void launch_courant_apply(Ctx &c);
-void launch_state_scatter(Ctx &c, double *dst, const double *packed);
-void launch_state_gather(Ctx &c, const double *src, double *packed);
+void launch_state_scatter(Ctx &c, double *dst, const double *packed, int i0, int ni);
+void launch_state_gather(Ctx &c, const double *src, double *packed, int i0, int ni);
+void launch_courant_to_bits(Ctx &c);
 void launch_sums(Ctx &c, const double *U, double *out5);
 void launch_plane_sums(Ctx &c, const double *U, double *rows);
 

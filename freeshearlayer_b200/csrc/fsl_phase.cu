@@ -360,10 +360,10 @@ __global__ void k_evolution(Grid g, int mode, const DevScalars *__restrict__ ds,
 // ---------------------------------------------------------------------------
 __global__ void k_courant_partial(Grid g, Consts kc, const double *__restrict__ U,
                                   const DevScalars *__restrict__ ds, double *__restrict__ partials,
-                                  DevScalars *__restrict__ dsw)
+                                  DevScalars *__restrict__ dsw, int i0, int i1)
 {
-    const int L = g.L, H = g.H, D = g.D;
-    const long long n = (long long)L * H * D;
+    const int H = g.H, D = g.D;
+    const long long n = (long long)(i1 - i0 + 1) * H * D; // planes i0..i1
     const long long fs = g.fstride;
     const double dtx = ds->dtx, dty = ds->dty, dtz = ds->dtz;
     double m = 0.0;
@@ -373,7 +373,7 @@ __global__ void k_courant_partial(Grid g, Consts kc, const double *__restrict__ 
         const int k = (int)(t % D) + 1;
         const long long r = t / D;
         const int j = (int)(r % H) + 1;
-        const int i = (int)(r / H) + 1;
+        const int i = (int)(r / H) + i0;
         const long long c = g.idx(i, j, k);
         const double R = U[c];
         const double Co = cell_courant(kc.cfl_mode, R, U[fs + c], kc.cfl_mode == FSL_CFL_ACOUSTIC ? U[2 * fs + c] : 0.,
@@ -442,6 +442,16 @@ __global__ void k_courant_final(Consts kc, const double *__restrict__ partials, 
     }
 }
 
+// The maximum of the partials as the accumulator's bit pattern, without the
+// dt update (the Courant maximum of a slab, to be combined across slabs).
+__global__ void k_courant_to_bits(const double *__restrict__ partials, int np, DevScalars *ds)
+{
+    if (threadIdx.x != 0) return;
+    double m = 0.0;
+    for (int t = 0; t < np; t++) m = (partials[t] > m) ? partials[t] : m;
+    ds->co_bits = (unsigned long long)__double_as_longlong(m);
+}
+
 // The same dt update from the maximum the fused stage 3 of the previous step
 // accumulated over the state it wrote (that state is this step's U^n).
 __global__ void k_courant_apply(Consts kc, DevScalars *ds)
@@ -488,9 +498,9 @@ __global__ void k_judge_rows(Grid g, const TA *__restrict__ a, const TB *__restr
 // ---------------------------------------------------------------------------
 // state transfer and diagnostics
 // ---------------------------------------------------------------------------
-__global__ void k_state_scatter(Grid g, double *__restrict__ dst, const double *__restrict__ packed)
+__global__ void k_state_scatter(Grid g, double *__restrict__ dst, const double *__restrict__ packed, int i0, int ni)
 {
-    const long long n = (long long)g.L * g.H * 5 * g.D;
+    const long long n = (long long)ni * g.H * 5 * g.D;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t % g.D);
@@ -498,13 +508,14 @@ __global__ void k_state_scatter(Grid g, double *__restrict__ dst, const double *
         const int v = (int)(r % 5); r /= 5;
         const int j = (int)(r % g.H);
         const int i = (int)(r / g.H);
-        dst[v * g.fstride + g.idx(i + 1, j + 1, k + 1)] = packed[t];
+        dst[v * g.fstride + g.idx(i + i0, j + 1, k + 1)] = packed[t];
     }
 }
 
-__global__ void k_state_gather(Grid g, const double *__restrict__ src, double *__restrict__ packed)
+// planes i0 .. i0+ni-1 (1-based interior planes) in the state layout
+__global__ void k_state_gather(Grid g, const double *__restrict__ src, double *__restrict__ packed, int i0, int ni)
 {
-    const long long n = (long long)g.L * g.H * 5 * g.D;
+    const long long n = (long long)ni * g.H * 5 * g.D;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t % g.D);
@@ -512,7 +523,7 @@ __global__ void k_state_gather(Grid g, const double *__restrict__ src, double *_
         const int v = (int)(r % 5); r /= 5;
         const int j = (int)(r % g.H);
         const int i = (int)(r / g.H);
-        packed[t] = src[v * g.fstride + g.idx(i + 1, j + 1, k + 1)];
+        packed[t] = src[v * g.fstride + g.idx(i + i0, j + 1, k + 1)];
     }
 }
 
@@ -662,8 +673,16 @@ void launch_courant(Ctx &c)
 {
     const Grid &g = c.g;
     prof_begin(c, FSL_K_CFL);
-    k_courant_partial<<<c.npartials, 256, 0, c.stream>>>(g, c.k, c.U, c.ds, c.partials, c.ds);
+    k_courant_partial<<<c.npartials, 256, 0, c.stream>>>(g, c.k, c.U, c.ds, c.partials, c.ds, c.co_i0, c.co_i1);
     k_courant_final<<<1, 1024, 0, c.stream>>>(c.k, c.partials, c.npartials, c.ds);
+    prof_end(c, FSL_K_CFL, 2);
+}
+
+void launch_courant_to_bits(Ctx &c)
+{
+    prof_begin(c, FSL_K_CFL);
+    k_courant_partial<<<c.npartials, 256, 0, c.stream>>>(c.g, c.k, c.U, c.ds, c.partials, c.ds, c.co_i0, c.co_i1);
+    k_courant_to_bits<<<1, 32, 0, c.stream>>>(c.partials, c.npartials, c.ds);
     prof_end(c, FSL_K_CFL, 2);
 }
 
@@ -674,17 +693,19 @@ void launch_courant_apply(Ctx &c)
     prof_end(c, FSL_K_CFL, 1);
 }
 
-void launch_state_scatter(Ctx &c, double *dst, const double *packed)
+void launch_state_scatter(Ctx &c, double *dst, const double *packed, int i0, int ni)
 {
+    if (ni <= 0) return;
     prof_begin(c, FSL_K_OTHER);
-    k_state_scatter<<<148 * 8, 256, 0, c.stream>>>(c.g, dst, packed);
+    k_state_scatter<<<148 * 8, 256, 0, c.stream>>>(c.g, dst, packed, i0, ni);
     prof_end(c, FSL_K_OTHER, 1);
 }
 
-void launch_state_gather(Ctx &c, const double *src, double *packed)
+void launch_state_gather(Ctx &c, const double *src, double *packed, int i0, int ni)
 {
+    if (ni <= 0) return;
     prof_begin(c, FSL_K_OTHER);
-    k_state_gather<<<148 * 8, 256, 0, c.stream>>>(c.g, src, packed);
+    k_state_gather<<<148 * 8, 256, 0, c.stream>>>(c.g, src, packed, i0, ni);
     prof_end(c, FSL_K_OTHER, 1);
 }
 

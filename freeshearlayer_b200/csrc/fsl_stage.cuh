@@ -144,6 +144,7 @@ template <typename T> struct Args {
     BF<T> bf;
     const DevScalars *ds;
     unsigned long long *co; // non-null: accumulate the Courant maximum of `out` (stage 3)
+    int co_i0, co_i1;       // over planes co_i0..co_i1 only
     unsigned int *status;   // bit 1 set on a non-positive output density (with co)
     int stage;
     int seg;
@@ -482,7 +483,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
                 a.out[q * fs + c] = o;
                 base[q] = o; // the new state, for the Courant number below
             }
-            if (a.co) {
+            if (a.co && i >= a.co_i0 && i <= a.co_i1) {
                 // the next step's check of src/helpers.c:23-52 on this state
                 const double Co = cell_courant(kc.cfl_mode, base[0], base[1], base[2], base[3], base[4], dtx, dty, dtz);
                 const double m = comax[r][l];
@@ -533,6 +534,8 @@ int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, doubl
     Args<T> a;
     a.cur = cur; a.un = un; a.out = out; a.mu = mu; a.bf = bf; a.ds = c.ds; a.stage = stage;
     a.co = courant ? &c.ds->co_bits : nullptr;
+    a.co_i0 = c.co_i0;
+    a.co_i1 = c.co_i1;
     a.status = &c.ds->status;
     a.seg = c.stage_seg;
     const size_t smem = sizeof(Smem<T, TJE>);

@@ -154,6 +154,45 @@ int fsl_download_state(fsl_ctx *ctx, double *state);
 /* Set step counter and time step as a restart would (src/initialize.c:149-152). */
 int fsl_set_time(fsl_ctx *ctx, unsigned step, double deltaT);
 
+/* ---- x-slabs (replaces src-par's MPI decomposition) ------------------------
+ * A domain of LEN planes split along x into slabs, one context per slab (one
+ * per GPU).  A slab context holds its owned planes plus W overlap planes on
+ * each side (x-periodic temporal setup; in the spatial setup none before the
+ * first slab and none after the last), in ascending global order, so that a
+ * slab whose overlap wraps across the periodic seam has the seam on its own
+ * periodic boundary, as the undivided domain does.  Once per step the overlap
+ * planes are refreshed from the slabs that own them, and the Courant maximum
+ * over the owned planes is combined across slabs by a maximum
+ * (src-par/helpers.c:44, MPI_Allreduce MAX).  One step changes a plane only
+ * through planes within 7 of it (9 with PPM; measured), so W >= 8
+ * (10) keeps the owned planes bit-identical to the undivided domain.  This
+ * takes the place of the per-stage ghost-plane messages of
+ * src-par/boundCondInGhostCells.c:23-102, src-par/boundCondOnInterfaces.c:20-99
+ * and src-par/communication.c:6-93.
+ *
+ * Planes are 1-based interior x-indices; buffers hold n planes in the
+ * upload/download layout ([n][HIG][5][DEP] doubles), host or device memory
+ * (copied with cudaMemcpyDefault; the call returns with the copy done).
+ * The current-stage buffer must be U^n (between steps). */
+int fsl_get_planes(fsl_ctx *ctx, int i0, int n, double *buf);
+int fsl_set_planes(fsl_ctx *ctx, int i0, int n, const double *buf);
+/* Planes i0..i1 enter the Courant maximum (default 1..LEN).  A context with a
+ * narrower range is an x-slab: fsl_step / fsl_step_phased then take one step
+ * per call and need a combined maximum (below) before each; a learned closure
+ * must have judgements off. */
+int fsl_set_courant_range(fsl_ctx *ctx, int i0, int i1);
+/* Make the owned Courant maximum of U^n available (a reduction, unless the
+ * last step's final stage already accumulated it). */
+int fsl_courant_prepare(fsl_ctx *ctx);
+/* Read / replace that maximum (host round trip; replacing it with the
+ * maximum over all slabs lets the next step rescale deltaT as one domain). */
+int fsl_get_courant_max(fsl_ctx *ctx, double *maxCo);
+int fsl_set_courant_max(fsl_ctx *ctx, double maxCo);
+/* The same maximum in device memory as the bit pattern of the non-negative
+ * double (unsigned 64-bit; such doubles order like their bit patterns), for
+ * an in-place all-reduce MAX on the context's stream. */
+unsigned long long *fsl_courant_bits(fsl_ctx *ctx);
+
 /* ---- the driver's per-step scalar work ---------------------------------- */
 
 /* checkCoNum(), src/helpers.c:23-52: reduce the Courant maximum over U^n on

@@ -1,0 +1,230 @@
+"""x-slab decomposition on the GPU: the reach of one step, and slabs that
+must reproduce the undivided domain bit for bit (FP64; the reference
+reconstruction on the fused path, PPM on the per-phase path), with overlap
+planes staged through host or device memory, and two gloo ranks sharing the
+GPU (their kernels never wait on one another: the exchange is on the host)."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+from tests.helpers import max_ulp, random_state, spatial_params, temporal_params
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def fsl():
+    import freeshearlayer_b200 as fsl
+    return fsl
+
+
+def _same(a, b, what):
+    if not np.array_equal(a, b):
+        raise AssertionError("%s: max |d| %g, max ulp %d" % (what, np.max(np.abs(a - b)), max_ulp(a, b)))
+
+
+def _case(fsl, setup, recon=0, L=48, H=12, D=16):
+    if setup == 0:
+        p = spatial_params(L=L, H=H, D=D, recon=recon)
+        s = random_state(p, 31)
+    else:
+        p = temporal_params(L=L, H=H, D=D, recon=recon)
+        s, _ = fsl.temporal_state(fsl._as_params(p), 0.4, 1.0, 2e-2, 7)
+    return p, s
+
+
+def _whole(fsl, p, s, steps):
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    d.step(steps)
+    out = d.download_state()
+    dt = d.info().deltaT
+    d.close()
+    return out, dt
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+@pytest.mark.parametrize("recon", [0, 1])
+def test_reach_of_one_step(fsl, recon, setup):
+    """A change in one plane moves no plane farther than RADIUS in one step
+    (the Courant maximum held fixed, so that deltaT is the same)."""
+    from freeshearlayer_b200.slabs import RADIUS
+    p, s = _case(fsl, setup, recon, L=40)
+    P = p["HIG"] * 5 * p["DEP"]
+    base = s.reshape(p["LEN"], P)
+    pert = base.copy()
+    mid = 20
+    pert[mid - 1] *= 1.0 + 1e-3 * np.random.default_rng(3).random(P)
+    outs = []
+    for st in (base, pert):
+        d = fsl.Domain(p)
+        d.upload_state(st.ravel())
+        d.courant_prepare()
+        d.set_courant_max(1.0)
+        d.step(1)
+        outs.append(d.download_state().reshape(p["LEN"], P))
+        d.close()
+    changed = np.nonzero(np.any(outs[0] != outs[1], axis=1))[0] + 1
+    reach = int(np.max(np.abs(changed - mid)))
+    print("reach recon=%d setup=%d: %d" % (recon, setup, reach))
+    assert reach <= RADIUS[recon], (reach, changed)
+    assert reach >= RADIUS[recon] - 2, (reach, changed)   # the bound is not loose
+
+
+@pytest.mark.parametrize("setup", [1, 0])
+@pytest.mark.parametrize("nslabs", [2, 3])
+def test_slabs_fused_bit_identical(fsl, setup, nslabs):
+    from freeshearlayer_b200.slabs import SlabSet
+    p, s = _case(fsl, setup)
+    ref, dt = _whole(fsl, p, s, 10)
+    with SlabSet(p, nslabs) as ss:
+        ss.upload_state(s)
+        ss.step(10)
+        got = ss.download_state()
+        assert all(d.info().deltaT == dt for d in ss.domains)
+    _same(got, ref, "%d slabs after 10 steps" % nslabs)
+
+
+def test_slabs_ppm_bit_identical(fsl):
+    from freeshearlayer_b200.slabs import SlabSet
+    p, s = _case(fsl, 1, recon=1, L=44)
+    ref, _ = _whole(fsl, p, s, 6)
+    with SlabSet(p, 2) as ss:
+        ss.upload_state(s)
+        ss.step(6)
+        got = ss.download_state()
+    _same(got, ref, "PPM slabs after 6 steps")
+
+
+def test_slabs_against_the_oracle(fsl, oracle_lib):
+    """Three slabs against the CPU oracle of the undivided domain."""
+    from freeshearlayer_b200.slabs import SlabSet
+    p = temporal_params(L=36, H=8, D=8)
+    s, _ = oracle_lib.Oracle.temporal_state(p, 0.4)
+    o = oracle_lib.Oracle(p)
+    o.set_state(s)
+    o.step(5)
+    with SlabSet(p, 3) as ss:
+        ss.upload_state(s)
+        ss.step(5)
+        _same(ss.download_state(), o.state(), "3 slabs vs oracle")
+
+
+def test_slabs_device_staging(fsl):
+    """Overlap planes through CUDA tensors (device pointers through the C
+    ABI) and the Courant maximum combined in device memory."""
+    from freeshearlayer_b200.slabs import SlabSet
+    p, s = _case(fsl, 1)
+    ref, _ = _whole(fsl, p, s, 8)
+    with SlabSet(p, 3, staging="device") as ss:
+        ss.upload_state(s)
+        ss.step(8)
+        got = ss.download_state()
+    _same(got, ref, "device-staged slabs")
+
+
+def test_slabs_fp32_bulk(fsl):
+    """FP32 bulk slabs: the x-march starts at other planes than in the
+    undivided domain, so agreement is to rounding, not bitwise."""
+    from freeshearlayer_b200.slabs import SlabSet
+    p, s = _case(fsl, 1)
+    p = dict(p, precision=1)
+    ref, _ = _whole(fsl, p, s, 8)
+    with SlabSet(p, 2) as ss:
+        ss.upload_state(s)
+        ss.step(8)
+        got = ss.download_state()
+    a = got.reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    b = ref.reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    for v in (0, 4):
+        assert np.linalg.norm(a[:, :, v] - b[:, :, v]) / np.linalg.norm(b[:, :, v]) < 1e-7
+
+
+def test_slab_protocol_errors(fsl):
+    p, s = _case(fsl, 1, L=32)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    d.set_courant_range(9, 24)
+    with pytest.raises(fsl.FslError):
+        d.step(1)                   # no combined Courant maximum yet
+    d.courant_prepare()
+    with pytest.raises(fsl.FslError):
+        d.step(2)                   # one step per call
+    with pytest.raises(fsl.FslError):
+        d.set_courant_range(0, 5)
+    with pytest.raises(fsl.FslError):
+        d.get_planes(30, 5, np.empty(5 * d.plane_size()))
+    d.step(1)
+    d.close()
+    q = dict(p, precision=1, sgs=1)
+    d = fsl.Domain(q)
+    d.upload_state(s)
+    d.set_courant_range(9, 24)
+    d.courant_prepare()
+    with pytest.raises(fsl.FslError):
+        d.step(1)                   # closure judgements would differ between slabs
+    d.close()
+
+
+def test_planes_roundtrip(fsl):
+    p, s = _case(fsl, 1, L=20)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    P = d.plane_size()
+    got = d.get_planes(5, 3, np.empty(3 * P))
+    _same(got, s[4 * P:7 * P], "planes 5..7")
+    new = s.copy()
+    new[9 * P:12 * P] *= 1.01
+    d.set_planes(10, 3, np.ascontiguousarray(new[9 * P:12 * P]))
+    _same(d.download_state(), new, "after set_planes")
+    d.close()
+
+
+def _free_port() -> int:
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def _rank_main(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import freeshearlayer_b200 as fsl
+    from freeshearlayer_b200.slabs import DistributedSlab
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        p, s = _case(fsl, 1)
+        ds = DistributedSlab(p)
+        ds.upload_state(s)
+        ds.step(6)
+        full = ds.gather_state(0)
+        q.put((rank, None if full is None else full.tobytes()))
+        ds.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_distributed_slabs_gloo_one_gpu(fsl):
+    import torch.multiprocessing as mp
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    res = [q.get(timeout=300) for _ in range(world)]
+    for pr in procs:
+        pr.join(60)
+        assert pr.exitcode == 0
+    full = [r[1] for r in res if r[0] == 0][0]
+    p, s = _case(fsl, 1)
+    ref, _ = _whole(fsl, p, s, 6)
+    _same(np.frombuffer(full, np.float64), ref, "two gloo ranks")
