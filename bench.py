@@ -211,6 +211,14 @@ ARM_NAMES = {"fp32-learned": "FP32 bulk (FP64 RK accumulation), learned closure 
 #          U^(s) 40 + U^n 40 + mu 8, write 40 (128 B each)   -> 114.67 B
 #   FP32 bulk with FP64 stage buffers: mu is FP32 (4 B)    -> 110.67 B
 STAGE_BYTES = {0: (88.0 + 128.0 + 128.0) / 3.0, 1: (84.0 + 124.0 + 124.0) / 3.0}
+# Arithmetic of one cell-stage as the fused stage kernel evaluates it, counted
+# exactly by instantiating the step's arithmetic templates with a counting
+# number type (freeshearlayer_b200/csrc/flopcount.cu, built as
+# freeshearlayer_b200/_build/flopcount; the CPU tests check these numbers
+# against it).  flops = add + mul + div + sqrt.
+STAGE_OPS = {"add": 520, "mul": 539, "div": 53, "sqrt": 8, "cmp": 132}
+STAGE_FLOPS = STAGE_OPS["add"] + STAGE_OPS["mul"] + STAGE_OPS["div"] + STAGE_OPS["sqrt"]
+SMS = 148
 
 
 def make_domain(fsl, grid, arm, state, dU, rows=0, seg=0):
@@ -288,6 +296,24 @@ def stage_roofline(kt, names, ncell, prec, peaks, traffic):
             "peak_source": peaks["source"] + " HBM copy bandwidth (burst)",
             "alg_bytes_per_cell": round(STAGE_BYTES[prec], 2), "alg_bytes_per_launch": alg,
             "avg_launch_ms": round(avg_ms, 4), "launches": launches}, kms, kl
+
+
+def compute_roof(roof, prec, clk):
+    """The stage kernel's arithmetic rate against the vector (non-tensor) peak
+    of its precision: 148 SMs x 128 FP32 (64 FP64) lanes x 2 flops (an FMA)
+    per cycle at the median SM clock sampled during the timed region."""
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    lanes = 64 if prec == 0 else 128
+    peak = SMS * lanes * 2 * mhz * 1e6 / 1e12
+    cells = roof["alg_bytes_per_launch"] / roof["alg_bytes_per_cell"]
+    achieved = STAGE_FLOPS * cells / (roof["avg_launch_ms"] / 1e3) / 1e12
+    return {"bound": "fp64 vector" if prec == 0 else "fp32 vector", "flops_per_cell_stage": STAGE_FLOPS,
+            "ops_per_cell_stage": STAGE_OPS, "achieved": round(achieved, 3), "peak": round(peak, 2),
+            "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "sm_mhz": mhz,
+            "note": "nominal peak counts an FMA as 2 flops; divisions and square roots count 1 flop each "
+                    "but issue as several instructions" +
+                    ("; the FP64 path is compiled without contraction, so each add and multiply issues "
+                     "on its own (half the FMA peak is its ceiling)" if prec == 0 else "")}
 
 
 def rel_l2(a, b):
@@ -540,7 +566,7 @@ def main_gpu(args):
         proof, pkms, pkl = stage_roofline(pkt, names, ncell, 0, peaks, None)
         plain = {"path": ARM_NAMES["fp64-dynamic"], "value": whole_job_rate(ncell * STAGES * args.steps, world, pms),
                  "ms_per_step": pms / args.steps, "kernels_ms": {k: round(v, 3) for k, v in pkms.items()},
-                 "roofline": proof}
+                 "roofline": proof, "compute_roof": compute_roof(proof, 0, clk)}
         dp.close()
 
     # ---- matched error: same initial state, M steps, against the plain FP64 path ----
@@ -578,7 +604,8 @@ def main_gpu(args):
                                    ARM_NAMES[arm],
                            "l2": "inputs larger than L2 (state %.2f GB per domain)" % (state.nbytes / 1e9),
                            "parallelism": "replicas (one independent domain per GPU)"},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roof, "compute_roof": compute_roof(roof, prec, clk),
+                "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(sum(kl.values())),
                 "kernels_ms": {k: round(v, 3) for k, v in kms.items()},
                 "clocks": clk}

@@ -9,6 +9,10 @@
 
 #include <cuda_runtime.h>
 
+// Arithmetic templates callable from host code too (an instrumented
+// instantiation counts their operations; the kernels use T = double, float).
+#define FSL_HD __host__ __device__ __forceinline__
+
 namespace fsl {
 
 // gas and scheme constants, src/def.h:25-45
@@ -30,7 +34,7 @@ template <typename T> struct Kc {
 // written as selects: the same comparisons on the same values, so the same
 // result, without data-dependent branches that split a warp.  (y = 0 never
 // reaches |4y|: x y = 0 returns 0 first.)
-template <typename T> __device__ __forceinline__ T minmod(T x, T y)
+template <typename T> FSL_HD T minmod(T x, T y)
 {
     const T y4 = y * T(4.0);
     const T ay = (y4 > T(0)) ? y4 : -y4;
@@ -48,7 +52,7 @@ template <typename T> struct CellC {
     T u_hh, v_hh, w_hh, u_ee, v_ee, w_ee;
 };
 
-template <typename T> __device__ __forceinline__ void cell_consts(CellC<T> &c)
+template <typename T> FSL_HD void cell_consts(CellC<T> &c)
 {
     typedef Kc<T> k;
     T R = T(1.) / c.u[0];
@@ -85,7 +89,7 @@ template <typename T> __device__ __forceinline__ void cell_consts(CellC<T> &c)
 // reference applies to the T2 momentum (the z sweep uses w_ee for rho v,
 // src/reconstruction.c:328,340).
 template <typename T, int N, int T1, int T2>
-__device__ __forceinline__ void recon_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2,
+FSL_HD void recon_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2,
                                             T n_hh, T t1_hh, T t2_hh, T n_ee, T t1_ee, T t2_ee,
                                             const T *fw, const T *bw, T *hi, T *lo)
 {
@@ -143,17 +147,17 @@ __device__ __forceinline__ void recon_sweep(const CellC<T> &c, T vn, T vt1, T vt
 }
 
 // x, y and z sweeps with the reference's permutations.
-template <typename T> __device__ __forceinline__ void recon_x(const CellC<T> &c, const T *fw, const T *bw, T *hi, T *lo)
+template <typename T> FSL_HD void recon_x(const CellC<T> &c, const T *fw, const T *bw, T *hi, T *lo)
 {
     recon_sweep<T, 1, 2, 3>(c, c.U, c.V, c.W, c.bb, c.cc, c.dd, c.u_hh, c.v_hh, c.w_hh, c.u_ee, c.v_ee,
                             c.w_ee, fw, bw, hi, lo);
 }
-template <typename T> __device__ __forceinline__ void recon_y(const CellC<T> &c, const T *fw, const T *bw, T *hi, T *lo)
+template <typename T> FSL_HD void recon_y(const CellC<T> &c, const T *fw, const T *bw, T *hi, T *lo)
 {
     recon_sweep<T, 2, 3, 1>(c, c.V, c.W, c.U, c.cc, c.dd, c.bb, c.v_hh, c.w_hh, c.u_hh, c.v_ee, c.w_ee,
                             c.u_ee, fw, bw, hi, lo);
 }
-template <typename T> __device__ __forceinline__ void recon_z(const CellC<T> &c, const T *fw, const T *bw, T *hi, T *lo)
+template <typename T> FSL_HD void recon_z(const CellC<T> &c, const T *fw, const T *bw, T *hi, T *lo)
 {
     recon_sweep<T, 3, 1, 2>(c, c.W, c.U, c.V, c.dd, c.bb, c.cc, c.w_hh, c.u_hh, c.v_hh, c.w_ee, c.u_ee,
                             c.w_ee, fw, bw, hi, lo);
@@ -167,7 +171,7 @@ template <typename T> __device__ __forceinline__ void recon_z(const CellC<T> &c,
 // da_i)/6 and a_{i-1/2} - a_i = -1/2 d_{i-1/2} - (da_i - da_{i-1})/6 (eq.
 // 1.6), the monotonicity limiter (eq. 1.10); the same arithmetic as the
 // oracle's restatement.
-template <typename T> __device__ __forceinline__ T ppm_mc(T a, T b)
+template <typename T> FSL_HD T ppm_mc(T a, T b)
 {
     T m = T(0.5) * fabs(a + b);
     const T ta = T(2.0) * fabs(a), tb = T(2.0) * fabs(b);
@@ -177,7 +181,7 @@ template <typename T> __device__ __forceinline__ T ppm_mc(T a, T b)
 }
 
 template <typename T>
-__device__ __forceinline__ void char_fwd(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2, const T *d, T *M)
+FSL_HD void char_fwd(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2, const T *d, T *M)
 {
     typedef Kc<T> k;
     const T C = c.C;
@@ -196,7 +200,7 @@ __device__ __forceinline__ void char_fwd(const CellC<T> &c, T vn, T vt1, T vt2, 
 }
 
 template <typename T, int N, int T1, int T2>
-__device__ __forceinline__ void char_inv(const CellC<T> &c, T vn, T vt1, T vt2, T n_hh, T t1_hh, T t2_hh, T n_ee,
+FSL_HD void char_inv(const CellC<T> &c, T vn, T vt1, T vt2, T n_hh, T t1_hh, T t2_hh, T n_ee,
                                          T t1_ee, T t2_ee, const T *q, T *out)
 {
     typedef Kc<T> k;
@@ -217,7 +221,7 @@ __device__ __forceinline__ void char_inv(const CellC<T> &c, T vn, T vt1, T vt2, 
 // m2, m1, p1, p2: the neighbours at -2, -1, +1, +2 in the sweep's order
 // (rho, normal, t1, t2, E); hi, lo as recon_sweep.
 template <typename T, int N, int T1, int T2>
-__device__ __forceinline__ void ppm_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2, T n_hh,
+FSL_HD void ppm_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2, T n_hh,
                                           T t1_hh, T t2_hh, T n_ee, T t1_ee, T t2_ee, const T *m2, const T *m1,
                                           const T *p1, const T *p2, T *hi, T *lo)
 {
@@ -253,19 +257,19 @@ __device__ __forceinline__ void ppm_sweep(const CellC<T> &c, T vn, T vt1, T vt2,
 }
 
 template <typename T>
-__device__ __forceinline__ void ppm_x(const CellC<T> &c, const T *m2, const T *m1, const T *p1, const T *p2, T *hi, T *lo)
+FSL_HD void ppm_x(const CellC<T> &c, const T *m2, const T *m1, const T *p1, const T *p2, T *hi, T *lo)
 {
     ppm_sweep<T, 1, 2, 3>(c, c.U, c.V, c.W, c.bb, c.cc, c.dd, c.u_hh, c.v_hh, c.w_hh, c.u_ee, c.v_ee, c.w_ee, m2, m1,
                           p1, p2, hi, lo);
 }
 template <typename T>
-__device__ __forceinline__ void ppm_y(const CellC<T> &c, const T *m2, const T *m1, const T *p1, const T *p2, T *hi, T *lo)
+FSL_HD void ppm_y(const CellC<T> &c, const T *m2, const T *m1, const T *p1, const T *p2, T *hi, T *lo)
 {
     ppm_sweep<T, 2, 3, 1>(c, c.V, c.W, c.U, c.cc, c.dd, c.bb, c.v_hh, c.w_hh, c.u_hh, c.v_ee, c.w_ee, c.u_ee, m2, m1,
                           p1, p2, hi, lo);
 }
 template <typename T>
-__device__ __forceinline__ void ppm_z(const CellC<T> &c, const T *m2, const T *m1, const T *p1, const T *p2, T *hi, T *lo)
+FSL_HD void ppm_z(const CellC<T> &c, const T *m2, const T *m1, const T *p1, const T *p2, T *hi, T *lo)
 {
     ppm_sweep<T, 3, 1, 2>(c, c.W, c.U, c.V, c.dd, c.bb, c.cc, c.w_hh, c.u_hh, c.v_hh, c.w_ee, c.u_ee, c.w_ee, m2, m1,
                           p1, p2, hi, lo);
@@ -276,7 +280,7 @@ __device__ __forceinline__ void ppm_z(const CellC<T> &c, const T *m2, const T *m
 // conserved states.  Returns interface density, pressure and velocity (the
 // normal component from the solve, the tangential ones upwinded by its sign).
 template <typename T, int N>
-__device__ __forceinline__ void riemann(const T *Lm, const T *Rp, T &Rho, T &Pr, T *vel)
+FSL_HD void riemann(const T *Lm, const T *Rp, T &Rho, T &Pr, T *vel)
 {
     typedef Kc<T> k;
     T _R, _P, _C, _jo, _jp, _jm, RU, R_, P_, C_, jo_, jp_, jm_;
@@ -321,14 +325,14 @@ __device__ __forceinline__ void riemann(const T *Lm, const T *Rp, T &Rho, T &Pr,
 }
 
 // Velocities by reciprocal, RU = 1./rho (src/fluxes.c:124-142).
-template <typename T> __device__ __forceinline__ void vel_rcp(T r, T mu_, T mv, T mw, T *o)
+template <typename T> FSL_HD void vel_rcp(T r, T mu_, T mv, T mw, T *o)
 {
     T RU = T(1.) / r;
     o[0] = mu_ * RU; o[1] = mv * RU; o[2] = mw * RU;
 }
 
 // Velocities and temperature by division (src/fluxes.c:117-122).
-template <typename T> __device__ __forceinline__ void vel_div(T R_, T mu_, T mv, T mw, T E, T *o, T &Tt)
+template <typename T> FSL_HD void vel_div(T R_, T mu_, T mv, T mw, T E, T *o, T &Tt)
 {
     typedef Kc<T> k;
     T U_ = mu_ / R_, V_ = mv / R_, W_ = mw / R_;
@@ -342,7 +346,7 @@ template <typename T> __device__ __forceinline__ void vel_div(T R_, T mu_, T mv,
 // (src/fluxes.c:185-220, :353-391, :524-568).  N = normal direction.
 // g[a][b] = d u_a / d x_b.  fw/bw: velocities of the plus/minus cell.
 template <typename T, int N>
-__device__ __forceinline__ void face_flux(T Rho, T P, const T *vel, const T (*g)[3], const T *fw, const T *bw,
+FSL_HD void face_flux(T Rho, T P, const T *vel, const T (*g)[3], const T *fw, const T *bw,
                                           T Tp, T Tm, T mu_L, T mu_T, T lambda_L, T cp_Pr_T, T rdn, T *F)
 {
     typedef Kc<T> k;
@@ -374,6 +378,42 @@ __device__ __forceinline__ void face_flux(T Rho, T P, const T *vel, const T (*g)
     if (N == 3) F[3] = RU * vel[2] + P - s2;
     F[4] = vel[N - 1] * (k::K_K_1 * P + T(0.5) * Rho * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2])) -
            uu * s0 - vv * s1 - ww * s2 + q;
+}
+
+// Flux of one face (src/fluxes.c): Riemann state from the two face states,
+// viscous and heat flux from the two adjacent cells (vm/Tm minus side, vp/Tp
+// plus side, by division) and the eight tangential neighbours (by
+// reciprocal; P/M = plus/minus cell, h/l = +/- along the first (1) and
+// second (2) tangential axis).  kc: grid spacings and transport constants
+// (rdx.., r4dx.., mu_L, lambda_L, cp_Pr_T).
+template <typename T, int N, typename KC>
+FSL_HD void fused_face(const T *Lm, const T *Rp, const T *vm, T Tm, const T *vp, T Tp, const T *Ph1, const T *Mh1,
+                       const T *Pl1, const T *Ml1, const T *Ph2, const T *Mh2, const T *Pl2, const T *Ml2, T muT,
+                       const KC &kc, T *F)
+{
+    T Rho, P, vel[3];
+    riemann<T, N>(Lm, Rp, Rho, P, vel);
+    const int n0 = N - 1;
+    const int t1 = (N == 1) ? 1 : 0;
+    const int t2 = (N == 3) ? 1 : 2;
+    const T rdn = T(N == 1 ? kc.rdx : N == 2 ? kc.rdy : kc.rdz);
+    const T rt1 = T(N == 1 ? kc.r4dy : kc.r4dx);
+    const T rt2 = T(N == 3 ? kc.r4dy : kc.r4dz);
+    T gr[3][3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        gr[q][n0] = (vp[q] - vm[q]) * rdn;
+        gr[q][t1] = (Ph1[q] + Mh1[q] - Pl1[q] - Ml1[q]) * rt1;
+        gr[q][t2] = (Ph2[q] + Mh2[q] - Pl2[q] - Ml2[q]) * rt2;
+    }
+    face_flux<T, N>(Rho, P, vel, gr, vp, vm, Tp, Tm, T(kc.mu_L), muT, T(kc.lambda_L), T(kc.cp_Pr_T), rdn, F);
+}
+
+template <typename T> FSL_HD void vdiv(const T *U, T *o)
+{
+    T Tt;
+    vel_div(U[0], U[1], U[2], U[3], U[4], o, Tt);
+    o[3] = Tt;
 }
 
 // Courant number of one cell from its conserved variables: the reference's

@@ -150,41 +150,6 @@ template <typename T> struct Args {
     int seg;
 };
 
-// Flux of one face (src/fluxes.c): Riemann state from the two face states,
-// viscous and heat flux from the two adjacent cells (vm/Tm minus side, vp/Tp
-// plus side, by division) and the eight tangential neighbours (by
-// reciprocal; P/M = plus/minus cell, h/l = +/- along the first (1) and
-// second (2) tangential axis).
-template <typename T, int N>
-__device__ __forceinline__ void fused_face(const T *Lm, const T *Rp, const T *vm, T Tm, const T *vp, T Tp,
-                                           const T *Ph1, const T *Mh1, const T *Pl1, const T *Ml1, const T *Ph2,
-                                           const T *Mh2, const T *Pl2, const T *Ml2, T muT, const Consts &kc, T *F)
-{
-    T Rho, P, vel[3];
-    riemann<T, N>(Lm, Rp, Rho, P, vel);
-    const int n0 = N - 1;
-    const int t1 = (N == 1) ? 1 : 0;
-    const int t2 = (N == 3) ? 1 : 2;
-    const T rdn = T(N == 1 ? kc.rdx : N == 2 ? kc.rdy : kc.rdz);
-    const T rt1 = T(N == 1 ? kc.r4dy : kc.r4dx);
-    const T rt2 = T(N == 3 ? kc.r4dy : kc.r4dz);
-    T gr[3][3];
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-        gr[q][n0] = (vp[q] - vm[q]) * rdn;
-        gr[q][t1] = (Ph1[q] + Mh1[q] - Pl1[q] - Ml1[q]) * rt1;
-        gr[q][t2] = (Ph2[q] + Mh2[q] - Pl2[q] - Ml2[q]) * rt2;
-    }
-    face_flux<T, N>(Rho, P, vel, gr, vp, vm, Tp, Tm, T(kc.mu_L), muT, T(kc.lambda_L), T(kc.cp_Pr_T), rdn, F);
-}
-
-template <typename T> __device__ __forceinline__ void vdiv(const T *U, T *o)
-{
-    T Tt;
-    vel_div(U[0], U[1], U[2], U[3], U[4], o, Tt);
-    o[3] = Tt;
-}
-
 // Own column of plane `pl` (and, on the tile edge, the halo neighbour the y
 // and z sweeps need) from global memory into registers.
 // Kept in the storage type (FP64) while in flight: a conversion at load

@@ -163,3 +163,27 @@ def test_favre_post_processor(fsl, tmp_path, real_bytes):
     np.testing.assert_allclose(u, RU / R, rtol=1e-15)
     u_all, n_all = fsl.favre_from_probes(str(path), H, real_bytes)  # to the end of the file
     assert n_all == 10
+
+
+def test_stage_operation_counts():
+    """The bench's per-cell-stage arithmetic (its compute roof) is the count
+    the instrumented arithmetic templates give, for the fused kernel's
+    composition; the reference's own composition (velocities per face)
+    costs more divisions."""
+    import json
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(root, "freeshearlayer_b200", "_build", "flopcount")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-C", os.path.join(root, "freeshearlayer_b200"), exe], check=True,
+                       stdout=subprocess.DEVNULL)
+    counts = json.loads(subprocess.run([exe], check=True, capture_output=True, text=True).stdout)
+    sys.path.insert(0, root)
+    import bench
+    fused = counts["fused"]
+    assert {k: fused[k] for k in bench.STAGE_OPS} == bench.STAGE_OPS
+    assert fused["flops"] == bench.STAGE_FLOPS
+    ref = counts["reference"]
+    assert ref["div"] > fused["div"] and ref["flops"] > fused["flops"]
+    # the three face fluxes differ only in their permutation
+    assert counts["face_x"] == counts["face_y"] == counts["face_z"]
