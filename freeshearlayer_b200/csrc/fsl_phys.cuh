@@ -42,6 +42,20 @@ template <typename T> FSL_HD T minmod(T x, T y)
     return (x * y <= T(0)) ? T(0) : r;
 }
 
+// minmod(a, b) and minmod(b, a) in FP32 at once: both are 0 when a b <= 0,
+// else sign(a) min(|a|, 4|b|) and sign(b) min(|b|, 4|a|) -- exactly the
+// values of the select form above (min, |.|, x4 and the sign copy are exact),
+// with one product and one sign test for the pair.
+__host__ __device__ __forceinline__ void minmod2(float a, float b, float &ab, float &ba)
+{
+    const bool z = a * b <= 0.f;
+    const float fa = fabsf(a), fb = fabsf(b);
+    const float m1 = copysignf(fminf(fa, 4.f * fb), a);
+    const float m2 = copysignf(fminf(fb, 4.f * fa), b);
+    ab = z ? 0.f : m1;
+    ba = z ? 0.f : m2;
+}
+
 // Per-cell quantities shared by the three sweeps (src/reconstruction.c:63-88,
 // :104, :142-145).
 template <typename T> struct CellC {
@@ -121,10 +135,15 @@ FSL_HD void recon_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt
     W3 = -vt2 * w1 + w4;
     W4 = S41 * w1 + S42 * w2 + k2 + k3 + kk;
     W5 = S51 * w1 + S52 * w2 + k2 + k3 + kk;
-    _M1 = minmod(M1, W1); _M2 = minmod(M2, W2); _M3 = minmod(M3, W3);
-    _M4 = minmod(M4, W4); _M5 = minmod(M5, W5);
-    _W1 = minmod(W1, M1); _W2 = minmod(W2, M2); _W3 = minmod(W3, M3);
-    _W4 = minmod(W4, M4); _W5 = minmod(W5, M5);
+    if constexpr (sizeof(T) == 4) {
+        minmod2(M1, W1, _M1, _W1); minmod2(M2, W2, _M2, _W2); minmod2(M3, W3, _M3, _W3);
+        minmod2(M4, W4, _M4, _W4); minmod2(M5, W5, _M5, _W5);
+    } else {
+        _M1 = minmod(M1, W1); _M2 = minmod(M2, W2); _M3 = minmod(M3, W3);
+        _M4 = minmod(M4, W4); _M5 = minmod(M5, W5);
+        _W1 = minmod(W1, M1); _W2 = minmod(W2, M2); _W3 = minmod(W3, M3);
+        _W4 = minmod(W4, M4); _W5 = minmod(W5, M5);
+    }
     _S24 = n_ee + c.ll; _S25 = n_ee - c.ll;
     _S54 = _S55 = c.nn + k::H_K_1;
     _S54 += mm; _S55 -= mm;
