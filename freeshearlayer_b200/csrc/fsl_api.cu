@@ -427,6 +427,9 @@ int fsl_init(const fsl_params *p, fsl_ctx **out)
     c.g = make_grid(p->LEN, p->HIG, p->DEP, 8);
     c.co_i0 = 1;
     c.co_i1 = p->LEN;
+    // x planes per fused-stage block: 48 measured fastest for the FP32 bulk
+    // at 512x256x256 (1.6 % over 32); 32 for FP64
+    c.stage_seg = (p->precision == FSL_PREC_FP32) ? 48 : 32;
     // derived constants, src/initialize.c:67-94
     c.k.rdx = 1. / p->deltaX; c.k.rdy = 1. / p->deltaY; c.k.rdz = 1. / p->deltaZ;
     c.k.r4dx = 1. / (4 * p->deltaX); c.k.r4dy = 1. / (4 * p->deltaY); c.k.r4dz = 1. / (4 * p->deltaZ);

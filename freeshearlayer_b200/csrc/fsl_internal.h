@@ -103,7 +103,7 @@ struct Ctx {
     float *mu32 = nullptr;
     bool fp32_alloc = false;
     int stage_tje = 16; // rows per fused-stage tile (incl. the two halo rows)
-    int stage_seg = 32; // x planes per fused-stage block
+    int stage_seg = 32; // x planes per fused-stage block (fsl_init: 48 for FP32 bulk)
     // learned closure
     ClosureScales cls{};
     float *cl_params = nullptr; // FP32 parameter vector (kNParams)

@@ -261,7 +261,7 @@ int fsl_step_phased(fsl_ctx *ctx, int nsteps);
 
 /* Launch-shape knobs of the fused kernels (the results do not depend on them). */
 #define FSL_TUNE_STAGE_ROWS 1 /* rows per stage tile incl. 2 halo rows: 8, 12 or 16 */
-#define FSL_TUNE_STAGE_SEG 2  /* x planes marched per stage block */
+#define FSL_TUNE_STAGE_SEG 2  /* x planes marched per stage block (default 48 FP32 bulk, 32 FP64) */
 int fsl_tune(fsl_ctx *ctx, int key, int value);
 
 /* ---- debug / parity access ----------------------------------------------- */

@@ -67,7 +67,7 @@ def test_tuner_changes_no_result(fsl):
     e = fsl.Ensemble(ens_m)
     e.step(4)
     rows, seg, ms = e.tune(trial_steps=2)
-    assert rows in (8, 12, 16) and seg in (8, 16, 32, 64) and ms > 0
+    assert rows in (8, 12, 16) and seg in (8, 16, 32, 48, 64) and ms > 0
     e.step(6)
     e.sync()
     for d, r in zip(ens_m, ref_m):
