@@ -211,13 +211,15 @@ ARM_NAMES = {"fp32-learned": "FP32 bulk (FP64 RK accumulation), learned closure 
 #          U^(s) 40 + U^n 40 + mu 8, write 40 (128 B each)   -> 114.67 B
 #   FP32 bulk with FP64 stage buffers: mu is FP32 (4 B)    -> 110.67 B
 STAGE_BYTES = {0: (88.0 + 128.0 + 128.0) / 3.0, 1: (84.0 + 124.0 + 124.0) / 3.0}
-# Arithmetic of one cell-stage as the fused stage kernel evaluates it, counted
-# exactly by instantiating the step's arithmetic templates with a counting
-# number type (freeshearlayer_b200/csrc/flopcount.cu, built as
-# freeshearlayer_b200/_build/flopcount; the CPU tests check these numbers
-# against it).  flops = add + mul + div + sqrt.
-STAGE_OPS = {"add": 520, "mul": 539, "div": 53, "sqrt": 8, "cmp": 132}
-STAGE_FLOPS = STAGE_OPS["add"] + STAGE_OPS["mul"] + STAGE_OPS["div"] + STAGE_OPS["sqrt"]
+# Arithmetic of one cell-stage as the fused stage kernel evaluates it (per
+# precision: the FP32 bulk regroups the sweeps), counted exactly by
+# instantiating the step's arithmetic templates with a counting number type
+# (freeshearlayer_b200/csrc/flopcount.cu, built as
+# freeshearlayer_b200/_build/flopcount: "fused" and "fused_fp32"; the CPU
+# tests check these numbers against it).  flops = add + mul + div + sqrt.
+STAGE_OPS = {0: {"add": 520, "mul": 539, "div": 53, "sqrt": 8, "cmp": 132},
+             1: {"add": 481, "mul": 515, "div": 53, "sqrt": 8, "cmp": 57}}
+STAGE_FLOPS = {p: o["add"] + o["mul"] + o["div"] + o["sqrt"] for p, o in STAGE_OPS.items()}
 SMS = 148
 
 
@@ -306,9 +308,9 @@ def compute_roof(roof, prec, clk):
     lanes = 64 if prec == 0 else 128
     peak = SMS * lanes * 2 * mhz * 1e6 / 1e12
     cells = roof["alg_bytes_per_launch"] / roof["alg_bytes_per_cell"]
-    achieved = STAGE_FLOPS * cells / (roof["avg_launch_ms"] / 1e3) / 1e12
-    return {"bound": "fp64 vector" if prec == 0 else "fp32 vector", "flops_per_cell_stage": STAGE_FLOPS,
-            "ops_per_cell_stage": STAGE_OPS, "achieved": round(achieved, 3), "peak": round(peak, 2),
+    achieved = STAGE_FLOPS[prec] * cells / (roof["avg_launch_ms"] / 1e3) / 1e12
+    return {"bound": "fp64 vector" if prec == 0 else "fp32 vector", "flops_per_cell_stage": STAGE_FLOPS[prec],
+            "ops_per_cell_stage": STAGE_OPS[prec], "achieved": round(achieved, 3), "peak": round(peak, 2),
             "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "sm_mhz": mhz,
             "note": "nominal peak counts an FMA as 2 flops; divisions and square roots count 1 flop each "
                     "but issue as several instructions" +

@@ -14,7 +14,9 @@
 //    primitives twice (y/z sweeps of plane i, x sweep of plane i+1), the
 //    three sweeps, one velocity set of each form and one face viscosity
 //    average per cell (shared by the faces through on-chip memory), three
-//    face fluxes, the same combination.
+//    face fluxes, the same combination.  The plain FP64 kernel.
+//  * "fused_fp32": the same with the FP32 bulk's regrouped sweeps and paired
+//    limiter (recon_sweep_grouped, minmod2).
 // Sign flips and absolute values are operand modifiers and are not counted;
 // selects are not arithmetic.  Output: one JSON line.
 #include <cmath>
@@ -46,6 +48,8 @@ inline bool operator>=(R a, R b) { ops.cmp++; return a.v >= b.v; }
 inline bool operator<=(R a, R b) { ops.cmp++; return a.v <= b.v; }
 inline R sqrt(R a) { ops.sqrt++; return R(std::sqrt(a.v)); }
 inline R fabs(R a) { return R(std::fabs(a.v)); }
+inline R fmin(R a, R b) { ops.cmp++; return R(std::fmin(a.v, b.v)); }
+inline R copysign(R a, R b) { return R(std::copysign(a.v, b.v)); }
 
 } // namespace cnt
 
@@ -81,6 +85,23 @@ static void sweeps(int nconsts)
     fsl::recon_x(c, fw, bw, hi, lo);
     fsl::recon_y(c, fw, bw, hi, lo);
     fsl::recon_z(c, fw, bw, hi, lo);
+}
+
+// the same with the FP32 bulk's regrouped sweeps
+static void sweeps_grouped(int nconsts)
+{
+    fsl::CellC<R> c;
+    state(c.u, 0.0);
+    R fw[5], bw[5], hi[5], lo[5];
+    state(fw, 0.3);
+    state(bw, -0.2);
+    for (int n = 0; n < nconsts; n++) fsl::cell_consts(c);
+    fsl::recon_sweep_grouped<R, 1, 2, 3>(c, c.U, c.V, c.W, c.bb, c.cc, c.dd, c.u_hh, c.v_hh, c.w_hh, c.u_ee,
+                                         c.v_ee, c.w_ee, fw, bw, hi, lo);
+    fsl::recon_sweep_grouped<R, 2, 3, 1>(c, c.V, c.W, c.U, c.cc, c.dd, c.bb, c.v_hh, c.w_hh, c.u_hh, c.v_ee,
+                                         c.w_ee, c.u_ee, fw, bw, hi, lo);
+    fsl::recon_sweep_grouped<R, 3, 1, 2>(c, c.W, c.U, c.V, c.dd, c.bb, c.cc, c.w_hh, c.u_hh, c.v_hh, c.w_ee,
+                                         c.u_ee, c.w_ee, fw, bw, hi, lo);
 }
 
 // one face of normal N from precomputed velocities
@@ -136,6 +157,8 @@ int main()
     const cnt::Ops sw1 = take();
     sweeps(2);
     const cnt::Ops sw2 = take();
+    sweeps_grouped(2);
+    const cnt::Ops sw32 = take();
     face<1>();
     const cnt::Ops fx = take();
     face<2>();
@@ -154,7 +177,7 @@ int main()
     // face SGS viscosity average 0.5 (mu_a + mu_b): one add, one mul
     const cnt::Ops muavg{1, 1, 0, 0, 0};
 
-    cnt::Ops ref{0, 0, 0, 0, 0}, fus{0, 0, 0, 0, 0};
+    cnt::Ops ref{0, 0, 0, 0, 0}, fus{0, 0, 0, 0, 0}, f32{0, 0, 0, 0, 0};
     add(ref, sw1);
     add(ref, fx); add(ref, fy); add(ref, fz);
     add(ref, vref, 3.0);
@@ -165,9 +188,15 @@ int main()
     add(fus, vfus);
     add(fus, muavg);
     add(fus, comb);
+    add(f32, sw32);
+    add(f32, fx); add(f32, fy); add(f32, fz);
+    add(f32, vfus);
+    add(f32, muavg);
+    add(f32, comb);
     std::printf("{");
     print("reference", ref, true);
     print("fused", fus, true);
+    print("fused_fp32", f32, true);
     print("sweeps", sw1, true);
     print("face_x", fx, true);
     print("face_y", fy, true);

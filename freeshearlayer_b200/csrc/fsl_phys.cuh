@@ -9,6 +9,8 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 // Arithmetic templates callable from host code too (an instrumented
 // instantiation counts their operations; the kernels use T = double, float).
 #define FSL_HD __host__ __device__ __forceinline__
@@ -42,18 +44,18 @@ template <typename T> FSL_HD T minmod(T x, T y)
     return (x * y <= T(0)) ? T(0) : r;
 }
 
-// minmod(a, b) and minmod(b, a) in FP32 at once: both are 0 when a b <= 0,
+// minmod(a, b) and minmod(b, a) at once (the FP32 bulk): both are 0 when a b <= 0,
 // else sign(a) min(|a|, 4|b|) and sign(b) min(|b|, 4|a|) -- exactly the
 // values of the select form above (min, |.|, x4 and the sign copy are exact),
 // with one product and one sign test for the pair.
-__host__ __device__ __forceinline__ void minmod2(float a, float b, float &ab, float &ba)
+template <typename T> FSL_HD void minmod2(T a, T b, T &ab, T &ba)
 {
-    const bool z = a * b <= 0.f;
-    const float fa = fabsf(a), fb = fabsf(b);
-    const float m1 = copysignf(fminf(fa, 4.f * fb), a);
-    const float m2 = copysignf(fminf(fb, 4.f * fa), b);
-    ab = z ? 0.f : m1;
-    ba = z ? 0.f : m2;
+    const bool z = a * b <= T(0);
+    const T fa = fabs(a), fb = fabs(b);
+    const T m1 = copysign(fmin(fa, T(4) * fb), a);
+    const T m2 = copysign(fmin(fb, T(4) * fa), b);
+    ab = z ? T(0) : m1;
+    ba = z ? T(0) : m2;
 }
 
 // Per-cell quantities shared by the three sweeps (src/reconstruction.c:63-88,
@@ -94,6 +96,63 @@ template <typename T> FSL_HD void cell_consts(CellC<T> &c)
     c.nn = T(-0.5) * c.gg;
 }
 
+// The sweep below with its characteristic rows and face coefficients
+// regrouped, for the FP32 bulk (which does not follow the reference's
+// rounding): with d the forward (or backward) differences,
+//   A = aa d1 + bn d2 + K_1 d5 + bt1 d3 + bt2 d4,  B = C (d2 - vn d1),
+//   M1 = A - C^2 d1,  M4 = A + B,  M5 = A - B
+// (S41 = aa - C vn, S42 = bn + C, S51 = aa + C vn, S52 = bn - C, S11 = aa - C^2),
+// and on the faces n_ee (k4 + k5) + ll (k4 - k5) for _S24 k4 + _S25 k5 and
+// (nn + H_K_1)(k4 + k5) + mm (k4 - k5) for _S54 k4 + _S55 k5.  The same
+// scheme in fewer operations.
+template <typename T, int N, int T1, int T2>
+FSL_HD void recon_sweep_grouped(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2, T n_hh, T t1_hh,
+                                T t2_hh, T n_ee, T t1_ee, T t2_ee, const T *fw, const T *bw, T *hi, T *lo)
+{
+    typedef Kc<T> k;
+    const T *u = c.u;
+    const T C = c.C, C2 = c.aa - c.S11;
+    T M[5], W[5];
+    {
+        const T d1 = fw[0] - u[0], d2 = fw[1] - u[N], d3 = fw[2] - u[T1], d4 = fw[3] - u[T2], d5 = fw[4] - u[4];
+        const T A = c.aa * d1 + bn * d2 + k::K_1 * d5 + bt1 * d3 + bt2 * d4;
+        const T B = C * (d2 - vn * d1);
+        M[0] = A - C2 * d1; M[1] = d3 - vt1 * d1; M[2] = d4 - vt2 * d1; M[3] = A + B; M[4] = A - B;
+    }
+    {
+        const T d1 = u[0] - bw[0], d2 = u[N] - bw[1], d3 = u[T1] - bw[2], d4 = u[T2] - bw[3], d5 = u[4] - bw[4];
+        const T A = c.aa * d1 + bn * d2 + k::K_1 * d5 + bt1 * d3 + bt2 * d4;
+        const T B = C * (d2 - vn * d1);
+        W[0] = A - C2 * d1; W[1] = d3 - vt1 * d1; W[2] = d4 - vt2 * d1; W[3] = A + B; W[4] = A - B;
+    }
+    T Ml[5], Wl[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) minmod2(M[q], W[q], Ml[q], Wl[q]);
+    const T mm = vn * c.ll, e45 = c.nn + k::H_K_1;
+    {
+        const T k1 = Ml[0] * k::C1 + Wl[0] * k::C2, k2 = Ml[1] * k::C1 + Wl[1] * k::C2;
+        const T k3 = Ml[2] * k::C1 + Wl[2] * k::C2, k4 = Ml[3] * k::C1 + Wl[3] * k::C2;
+        const T k5 = Ml[4] * k::C1 + Wl[4] * k::C2;
+        const T ks = k4 + k5, kd = k4 - k5;
+        hi[0] = u[0] + c.hh * k1 + c.ee * ks;
+        hi[N] = u[N] + n_hh * k1 + n_ee * ks + c.ll * kd;
+        hi[T1] = u[T1] + t1_hh * k1 + k2 + t1_ee * ks;
+        hi[T2] = u[T2] + t2_hh * k1 + k3 + t2_ee * ks;
+        hi[4] = u[4] + c.gg * k1 + vt1 * k2 + vt2 * k3 + e45 * ks + mm * kd;
+    }
+    {
+        const T k1 = Ml[0] * k::C2 + Wl[0] * k::C1, k2 = Ml[1] * k::C2 + Wl[1] * k::C1;
+        const T k3 = Ml[2] * k::C2 + Wl[2] * k::C1, k4 = Ml[3] * k::C2 + Wl[3] * k::C1;
+        const T k5 = Ml[4] * k::C2 + Wl[4] * k::C1;
+        const T ks = k4 + k5, kd = k4 - k5;
+        lo[0] = u[0] - (c.hh * k1 + c.ee * ks);
+        lo[N] = u[N] - (n_hh * k1 + n_ee * ks + c.ll * kd);
+        lo[T1] = u[T1] - (t1_hh * k1 + k2 + t1_ee * ks);
+        lo[T2] = u[T2] - (t2_hh * k1 + k3 + t2_ee * ks);
+        lo[4] = u[4] - (c.gg * k1 + vt1 * k2 + vt2 * k3 + e45 * ks + mm * kd);
+    }
+}
+
 // One sweep of the characteristic reconstruction.  N = index of the normal
 // momentum in u[] (1..3); T1, T2 = tangential momenta in the reference's
 // permuted order (x: 2 3 4 -> 1 2 3; y: 3 4 2 -> 2 3 1; z: 4 2 3 -> 3 1 2).
@@ -107,6 +166,11 @@ FSL_HD void recon_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt
                                             T n_hh, T t1_hh, T t2_hh, T n_ee, T t1_ee, T t2_ee,
                                             const T *fw, const T *bw, T *hi, T *lo)
 {
+    if constexpr (std::is_same<T, float>::value) {
+        recon_sweep_grouped<T, N, T1, T2>(c, vn, vt1, vt2, bn, bt1, bt2, n_hh, t1_hh, t2_hh, n_ee, t1_ee, t2_ee,
+                                          fw, bw, hi, lo);
+        return;
+    }
     typedef Kc<T> k;
     const T *u = c.u;
     const T C = c.C;
@@ -135,15 +199,10 @@ FSL_HD void recon_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt
     W3 = -vt2 * w1 + w4;
     W4 = S41 * w1 + S42 * w2 + k2 + k3 + kk;
     W5 = S51 * w1 + S52 * w2 + k2 + k3 + kk;
-    if constexpr (sizeof(T) == 4) {
-        minmod2(M1, W1, _M1, _W1); minmod2(M2, W2, _M2, _W2); minmod2(M3, W3, _M3, _W3);
-        minmod2(M4, W4, _M4, _W4); minmod2(M5, W5, _M5, _W5);
-    } else {
-        _M1 = minmod(M1, W1); _M2 = minmod(M2, W2); _M3 = minmod(M3, W3);
-        _M4 = minmod(M4, W4); _M5 = minmod(M5, W5);
-        _W1 = minmod(W1, M1); _W2 = minmod(W2, M2); _W3 = minmod(W3, M3);
-        _W4 = minmod(W4, M4); _W5 = minmod(W5, M5);
-    }
+    _M1 = minmod(M1, W1); _M2 = minmod(M2, W2); _M3 = minmod(M3, W3);
+    _M4 = minmod(M4, W4); _M5 = minmod(M5, W5);
+    _W1 = minmod(W1, M1); _W2 = minmod(W2, M2); _W3 = minmod(W3, M3);
+    _W4 = minmod(W4, M4); _W5 = minmod(W5, M5);
     _S24 = n_ee + c.ll; _S25 = n_ee - c.ll;
     _S54 = _S55 = c.nn + k::H_K_1;
     _S54 += mm; _S55 -= mm;

@@ -180,10 +180,13 @@ def test_stage_operation_counts():
     counts = json.loads(subprocess.run([exe], check=True, capture_output=True, text=True).stdout)
     sys.path.insert(0, root)
     import bench
-    fused = counts["fused"]
-    assert {k: fused[k] for k in bench.STAGE_OPS} == bench.STAGE_OPS
-    assert fused["flops"] == bench.STAGE_FLOPS
-    ref = counts["reference"]
+    for prec, name in ((0, "fused"), (1, "fused_fp32")):
+        got = counts[name]
+        assert {k: got[k] for k in bench.STAGE_OPS[prec]} == bench.STAGE_OPS[prec], name
+        assert got["flops"] == bench.STAGE_FLOPS[prec], name
+    fused, ref = counts["fused"], counts["reference"]
     assert ref["div"] > fused["div"] and ref["flops"] > fused["flops"]
+    # the FP32 bulk's regrouped sweeps and paired limiter do less of both
+    assert counts["fused_fp32"]["flops"] < fused["flops"] and counts["fused_fp32"]["cmp"] < fused["cmp"]
     # the three face fluxes differ only in their permutation
     assert counts["face_x"] == counts["face_y"] == counts["face_z"]
