@@ -228,3 +228,44 @@ def test_distributed_slabs_gloo_one_gpu(fsl):
     p, s = _case(fsl, 1)
     ref, _ = _whole(fsl, p, s, 6)
     _same(np.frombuffer(full, np.float64), ref, "two gloo ranks")
+
+
+def _nccl_one_rank(port, q):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import freeshearlayer_b200 as fsl
+    from freeshearlayer_b200.slabs import DistributedSlab
+    torch.cuda.set_device(0)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", 0))
+    try:
+        p, s = _case(fsl, 1)
+        ds = DistributedSlab(p)
+        assert ds.on_device
+        ds.upload_state(s)
+        ds.step(4)
+        full = ds.gather_state(0)
+        q.put(full.tobytes())
+        ds.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_distributed_slab_nccl_one_rank(fsl):
+    """The NCCL branch of the driver (device buffers, the Courant maximum
+    all-reduced in device memory) on a one-rank group: the undivided domain."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    pr = ctx.Process(target=_nccl_one_rank, args=(_free_port(), q))
+    pr.start()
+    full = q.get(timeout=300)
+    pr.join(60)
+    assert pr.exitcode == 0
+    p, s = _case(fsl, 1)
+    ref, _ = _whole(fsl, p, s, 4)
+    _same(np.frombuffer(full, np.float64), ref, "one NCCL rank")
