@@ -344,8 +344,6 @@ int fsl_params_check(const fsl_params *p)
     if (p->precision != FSL_PREC_FP64 && p->precision != FSL_PREC_FP32) return FSL_ERR_ARG;
     if (p->sgs != FSL_SGS_DYNAMIC && p->sgs != FSL_SGS_LEARNED) return FSL_ERR_ARG;
     if (p->recon != FSL_RECON_CHARMINMOD && p->recon != FSL_RECON_PPM) return FSL_ERR_ARG;
-    // PPM runs on the per-phase FP64 kernels only
-    if (p->recon == FSL_RECON_PPM && p->precision != FSL_PREC_FP64) return FSL_ERR_UNSUPPORTED;
     return FSL_OK;
 }
 
@@ -833,8 +831,8 @@ int fsl_step(fsl_ctx *h, int nsteps)
 {
     if (!h || nsteps < 0) return FSL_ERR_ARG;
     Ctx &c = h->c;
-    if (c.p.nStages != 3 || c.p.recon == FSL_RECON_PPM) {
-        // the RK2 chain and PPM run on the per-phase kernels (FP64)
+    if (c.p.nStages != 3) {
+        // the RK2 chain runs on the per-phase kernels (FP64)
         if (c.p.precision != FSL_PREC_FP64) return fail(c, FSL_ERR_UNSUPPORTED, "FP32 bulk needs nStages = 3");
         return fsl_step_phased(h, nsteps);
     }

@@ -53,8 +53,6 @@ int check_member(fsl_ensemble *e, const Ctx &c)
     if (c.p.setup != FSL_SETUP_TEMPORAL)
         return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members need the temporal setup");
     if (c.p.nStages != 3) return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members need nStages = 3");
-    if (c.p.recon != FSL_RECON_CHARMINMOD)
-        return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members need the fused (reference) reconstruction");
     if (c.p.sgs == FSL_SGS_LEARNED && c.judge_every > 0)
         return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members with the learned closure need judgements off");
     if (c.prof) return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members must not be profiling");

@@ -19,6 +19,9 @@ void launch_bface(Ctx &c, const double *cur, const Disturb &d)
 
 int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant)
 {
+    // PPM: the wider stencil in one tile shape (halo 2, a ring of four planes)
+    if (c.p.recon == FSL_RECON_PPM)
+        return stage::launch_stage_t<double, 8, 1, true>(c, stage, cur, un, out, c.mu, bf64(c), courant);
     switch (c.stage_tje) {
     case 8: return stage::launch_stage_t<double, 8, 1>(c, stage, cur, un, out, c.mu, bf64(c), courant);
     case 12: return stage::launch_stage_t<double, 12, 1>(c, stage, cur, un, out, c.mu, bf64(c), courant);

@@ -59,6 +59,22 @@ __device__ __forceinline__ void recon_at(const Grid &g, const double *__restrict
     else recon_z(cc, fw, bw, hi, lo);
 }
 
+// PPM x-sweep of the padded cell c (planes c-2 .. c+2 from global memory)
+template <typename T>
+__device__ __forceinline__ void ppm_at_x(const Grid &g, const double *__restrict__ u, long long c, T *hi, T *lo)
+{
+    const long long fs = g.fstride, d = g.pi;
+    CellC<T> cc;
+    T m2[5], m1[5], p1[5], p2[5];
+    load5(u, fs, c, cc.u);
+    load5(u, fs, c - 2 * d, m2);
+    load5(u, fs, c - d, m1);
+    load5(u, fs, c + d, p1);
+    load5(u, fs, c + 2 * d, p2);
+    cell_consts(cc);
+    ppm_x(cc, m2, m1, p1, p2, hi, lo);
+}
+
 // Outer states of all domain-boundary faces (src/bounCondOnInterfaces.c:11-110).
 template <typename T>
 __global__ void k_bface(Grid g, int setup, int BL_HIG, Disturb d, const double *__restrict__ u, BF<T> bf)
@@ -128,8 +144,12 @@ __global__ void k_bface(Grid g, int setup, int BL_HIG, Disturb d, const double *
     }
 }
 
-template <typename T, int TJE> struct Smem {
-    T U[2][TJE + 2][34][5]; // current-stage state, planes i and i+1 (ring), halo 2
+template <typename T, int TJE, bool PPM = false> struct Smem {
+    static constexpr int HW = PPM ? 2 : 1; // y/z halo width of the state planes
+    static constexpr int NS = PPM ? 4 : 2; // x-planes in the state ring
+    // current-stage state: planes i, i+1 (PPM: i-1 .. i+2) as a ring, with
+    // HW halo rows and lanes
+    T U[NS][TJE + 2 * HW][32 + 2 * HW][5];
     T R[3][TJE][32][3];     // velocities by reciprocal, planes i-1, i, i+1 (ring)
     T Dv[2][TJE][32][5];    // velocities by division, temperature, mu face average, planes i, i+1
     T Lo[TJE][32][5];       // y sweep: state on the face below each cell
@@ -155,10 +175,10 @@ template <typename T> struct Args {
 // Kept in the storage type (FP64) while in flight: a conversion at load
 // time would wait on the load immediately.
 struct PlaneLoad {
-    double own[5], halo[5];
+    double own[5], halo[5], halo2[5]; // halo2: the second halo cell (PPM)
 };
 
-template <typename T, int TJE>
+template <typename T, int TJE, bool PPM>
 __device__ __forceinline__ void plane_issue(const Grid &g, const double *__restrict__ cu, int pl, int r, int l, int j,
                                             int k, bool live, PlaneLoad &p)
 {
@@ -166,36 +186,60 @@ __device__ __forceinline__ void plane_issue(const Grid &g, const double *__restr
     if (!live || pl > g.L + 1) return;
     const long long c = g.idx(pl, j, k);
     load5(cu, fs, c, p.own);
-    if (r == 0 && j >= 1) load5(cu, fs, c - g.pk, p.halo);
-    else if (r == TJE - 1 && j <= g.H) load5(cu, fs, c + g.pk, p.halo);
-    else if (l == 0 && k >= 1) load5(cu, fs, c - 1, p.halo);
-    else if (l == 31 && k <= g.D) load5(cu, fs, c + 1, p.halo);
+    if (r == 0 && j >= 1) {
+        load5(cu, fs, c - g.pk, p.halo);
+        if (PPM && j >= 2) load5(cu, fs, c - 2 * g.pk, p.halo2);
+    } else if (r == TJE - 1 && j <= g.H) {
+        load5(cu, fs, c + g.pk, p.halo);
+        if (PPM && j <= g.H - 1) load5(cu, fs, c + 2 * g.pk, p.halo2);
+    } else if (l == 0 && k >= 1) {
+        load5(cu, fs, c - 1, p.halo);
+        if (PPM && k >= 2) load5(cu, fs, c - 2, p.halo2);
+    } else if (l == 31 && k <= g.D) {
+        load5(cu, fs, c + 1, p.halo);
+        if (PPM && k <= g.D - 1) load5(cu, fs, c + 2, p.halo2);
+    }
 }
 
-template <typename T, int TJE>
-__device__ __forceinline__ void plane_store(Smem<T, TJE> &s, int slot, int r, int l, int j, int k, int H, int D,
+template <typename T, int TJE, bool PPM>
+__device__ __forceinline__ void plane_store(Smem<T, TJE, PPM> &s, int slot, int r, int l, int j, int k, int H, int D,
                                             bool live, const PlaneLoad &p)
 {
+    constexpr int HW = Smem<T, TJE, PPM>::HW;
     if (!live) return;
 #pragma unroll
-    for (int q = 0; q < 5; q++) s.U[slot][r + 1][l + 1][q] = T(p.own[q]);
-    T *h = nullptr;
-    if (r == 0 && j >= 1) h = s.U[slot][0][l + 1];
-    else if (r == TJE - 1 && j <= H) h = s.U[slot][TJE + 1][l + 1];
-    else if (l == 0 && k >= 1) h = s.U[slot][r + 1][0];
-    else if (l == 31 && k <= D) h = s.U[slot][r + 1][33];
+    for (int q = 0; q < 5; q++) s.U[slot][r + HW][l + HW][q] = T(p.own[q]);
+    T *h = nullptr, *h2 = nullptr;
+    if (r == 0 && j >= 1) {
+        h = s.U[slot][HW - 1][l + HW];
+        if (PPM && j >= 2) h2 = s.U[slot][0][l + HW];
+    } else if (r == TJE - 1 && j <= H) {
+        h = s.U[slot][TJE + HW][l + HW];
+        if (PPM && j <= H - 1) h2 = s.U[slot][TJE + HW + 1][l + HW];
+    } else if (l == 0 && k >= 1) {
+        h = s.U[slot][r + HW][HW - 1];
+        if (PPM && k >= 2) h2 = s.U[slot][r + HW][0];
+    } else if (l == 31 && k <= D) {
+        h = s.U[slot][r + HW][32 + HW];
+        if (PPM && k <= D - 1) h2 = s.U[slot][r + HW][33 + HW];
+    }
     if (h) {
 #pragma unroll
         for (int q = 0; q < 5; q++) h[q] = T(p.halo[q]);
+    }
+    if (PPM && h2) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) h2[q] = T(p.halo2[q]);
     }
 }
 
 // Velocities of plane `pl` (own column, from the shared ring) into the
 // reciprocal ring and the division plane with the face-averaged viscosity.
-template <typename T, int TJE>
-__device__ __forceinline__ void plane_prims(Smem<T, TJE> &s, int pl, int r, int l, T mu_pl, T mu_prev)
+template <typename T, int TJE, bool PPM>
+__device__ __forceinline__ void plane_prims(Smem<T, TJE, PPM> &s, int pl, int r, int l, T mu_pl, T mu_prev)
 {
-    const T *u = s.U[pl & 1][r + 1][l + 1];
+    constexpr int HW = Smem<T, TJE, PPM>::HW, NS = Smem<T, TJE, PPM>::NS;
+    const T *u = s.U[pl & (NS - 1)][r + HW][l + HW];
     vel_rcp(u[0], u[1], u[2], u[3], s.R[pl % 3][r][l]);
     T dv[4];
     vdiv(u, dv);
@@ -204,11 +248,13 @@ __device__ __forceinline__ void plane_prims(Smem<T, TJE> &s, int pl, int r, int 
     o[4] = T(0.5) * (mu_pl + mu_prev);
 }
 
-template <typename T, int TJE, int MINB>
+template <typename T, int TJE, int MINB, bool PPM>
 __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Args<T> a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    Smem<T, TJE> &s = *reinterpret_cast<Smem<T, TJE> *>(smraw);
+    typedef Smem<T, TJE, PPM> SM;
+    SM &s = *reinterpret_cast<SM *>(smraw);
+    constexpr int HW = SM::HW, NS = SM::NS;
     const int L = g.L, H = g.H, D = g.D;
     constexpr int TJ = TJE - 2;
     const int r = threadIdx.y, l = threadIdx.x;
@@ -232,42 +278,59 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
     T mu0 = 0, mu1 = 0, mu2 = 0; // mu of planes i, i+1, i+2 (own column)
     PlaneLoad pl;
 #pragma unroll
-    for (int q = 0; q < 5; q++) pl.own[q] = pl.halo[q] = 0.;
+    for (int q = 0; q < 5; q++) pl.own[q] = pl.halo[q] = pl.halo2[q] = 0.;
     double base[5], unv[5]; // FP64 operands of the stage combination, fetched early
 #pragma unroll
     for (int q = 0; q < 5; q++) base[q] = unv[q] = 0.;
 
-    // ---- prologue: planes i0-1 .. i0+1, flux of face i0 - 1/2 ----
+    // ---- prologue: planes i0-1 .. i0+1 (PPM: .. i0+2), flux of face i0 - 1/2 ----
     {
         T Um[5] = {0, 0, 0, 0, 0}, mum = 0;
-        plane_issue<T, TJE>(g, cu, i0, r, l, j, k, live, pl);
-        plane_store<T, TJE>(s, i0 & 1, r, l, j, k, H, D, live, pl);
-        plane_issue<T, TJE>(g, cu, i0 + 1, r, l, j, k, live, pl);
-        plane_store<T, TJE>(s, (i0 + 1) & 1, r, l, j, k, H, D, live, pl);
+        plane_issue<T, TJE, PPM>(g, cu, i0, r, l, j, k, live, pl);
+        plane_store<T, TJE, PPM>(s, i0 & (NS - 1), r, l, j, k, H, D, live, pl);
+        plane_issue<T, TJE, PPM>(g, cu, i0 + 1, r, l, j, k, live, pl);
+        plane_store<T, TJE, PPM>(s, (i0 + 1) & (NS - 1), r, l, j, k, H, D, live, pl);
+        if constexpr (PPM) {
+            plane_issue<T, TJE, PPM>(g, cu, i0 + 2, r, l, j, k, live, pl);
+            plane_store<T, TJE, PPM>(s, (i0 + 2) & (NS - 1), r, l, j, k, H, D, live && i0 + 2 <= L + 1, pl);
+        }
         if (live) {
             load5(cu, fs, cj + (long long)(i0 - 1) * g.pi, Um);
+            if constexpr (PPM) {
+                // plane i0-1 (own column): the x sweep of cell i0+1 reads it
+#pragma unroll
+                for (int q = 0; q < 5; q++) s.U[(i0 - 1) & (NS - 1)][r + HW][l + HW][q] = Um[q];
+            }
             vel_rcp(Um[0], Um[1], Um[2], Um[3], s.R[(i0 - 1) % 3][r][l]);
             mum = mu[cj + (long long)(i0 - 1) * g.pi];
             mu0 = mu[cj + (long long)i0 * g.pi];
             mu1 = mu[cj + (long long)(i0 + 1) * g.pi];
-            plane_prims<T, TJE>(s, i0, r, l, mu0, mum);
-            plane_prims<T, TJE>(s, i0 + 1, r, l, mu1, mu0);
+            plane_prims<T, TJE, PPM>(s, i0, r, l, mu0, mum);
+            plane_prims<T, TJE, PPM>(s, i0 + 1, r, l, mu1, mu0);
         }
         __syncthreads();
         if (inter) {
             T hm[5], lo[5], hin[5], dm[4], tmp[5];
-            const T *Uc = s.U[i0 & 1][r + 1][l + 1], *Un = s.U[(i0 + 1) & 1][r + 1][l + 1];
+            const T *Uc = s.U[i0 & (NS - 1)][r + HW][l + HW], *Un = s.U[(i0 + 1) & (NS - 1)][r + HW][l + HW];
             {
                 CellC<T> cc;
 #pragma unroll
                 for (int q = 0; q < 5; q++) cc.u[q] = Uc[q];
                 cell_consts(cc);
-                recon_x(cc, Un, Um, hin, lo);
+                if (PPM && i0 >= 2 && i0 <= L - 1) {
+                    T m2[5];
+                    load5(cu, fs, cj + (long long)(i0 - 2) * g.pi, m2);
+                    ppm_x(cc, m2, Um, Un, s.U[(i0 + 2) & (NS - 1)][r + HW][l + HW], hin, lo);
+                } else {
+                    recon_x(cc, Un, Um, hin, lo);
+                }
             }
             if (i0 == 1) {
                 const long long fo = (long long)(j - 1) * D + (k - 1);
 #pragma unroll
                 for (int q = 0; q < 5; q++) hm[q] = a.bf.x0[q * nxf + fo];
+            } else if (PPM && i0 - 1 >= 2 && i0 - 1 <= L - 1) {
+                ppm_at_x<T>(g, cu, cj + (long long)(i0 - 1) * g.pi, hm, tmp);
             } else {
                 recon_at<T, 0>(g, cu, cj + (long long)(i0 - 1) * g.pi, hm, tmp);
             }
@@ -291,10 +354,11 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
 
     for (int i = i0; i <= i1; i++) {
         const int sm1 = (i + 2) % 3, s0 = i % 3, sp1 = (i + 1) % 3;
-        const int u0 = i & 1, u1 = (i + 1) & 1;
-        // (a) issue plane i+2 loads (the velocities of plane i+1 were formed
-        // at the end of the previous iteration, or in the prologue)
-        plane_issue<T, TJE>(g, cu, i + 2, r, l, j, k, live, pl);
+        const int u0 = i & 1, u1 = (i + 1) & 1;                   // Dv ring
+        const int q0 = i & (NS - 1), q1 = (i + 1) & (NS - 1);     // state ring: planes i, i+1
+        // (a) issue plane i+2 (PPM: i+3) loads (the velocities of plane i+1
+        // were formed at the end of the previous iteration, or in the prologue)
+        plane_issue<T, TJE, PPM>(g, cu, i + (PPM ? 3 : 2), r, l, j, k, live, pl);
         if (inter) {
             const long long c = cj + (long long)i * g.pi;
             // FP32 bulk keeps only a converted copy of the state in shared
@@ -319,24 +383,40 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             const bool rz = zrow && k >= 1 && k <= D;
             if (ry || rz) {
                 CellC<T> cc;
-                const T *Uc = s.U[u0][r + 1][l + 1];
+                const T *Uc = s.U[q0][r + HW][l + HW];
 #pragma unroll
                 for (int q = 0; q < 5; q++) cc.u[q] = Uc[q];
                 cell_consts(cc);
                 T fw[5], bw[5], lo[5];
                 if (ry) {
-                    const T *a1 = s.U[u0][r + 2][l + 1], *b1 = s.U[u0][r][l + 1];
+                    const T *a1 = s.U[q0][r + HW + 1][l + HW], *b1 = s.U[q0][r + HW - 1][l + HW];
                     fw[0] = a1[0]; fw[1] = a1[2]; fw[2] = a1[3]; fw[3] = a1[1]; fw[4] = a1[4];
                     bw[0] = b1[0]; bw[1] = b1[2]; bw[2] = b1[3]; bw[3] = b1[1]; bw[4] = b1[4];
-                    recon_y(cc, fw, bw, hy, lo);
+                    if (PPM && j >= 2 && j <= H - 1) {
+                        const T *a2 = s.U[q0][r + HW + 2][l + HW], *b2 = s.U[q0][r + HW - 2][l + HW];
+                        T f2[5], b2v[5];
+                        f2[0] = a2[0]; f2[1] = a2[2]; f2[2] = a2[3]; f2[3] = a2[1]; f2[4] = a2[4];
+                        b2v[0] = b2[0]; b2v[1] = b2[2]; b2v[2] = b2[3]; b2v[3] = b2[1]; b2v[4] = b2[4];
+                        ppm_y(cc, b2v, bw, fw, f2, hy, lo);
+                    } else {
+                        recon_y(cc, fw, bw, hy, lo);
+                    }
 #pragma unroll
                     for (int q = 0; q < 5; q++) s.Lo[r][l][q] = lo[q];
                 }
                 if (rz) {
-                    const T *a1 = s.U[u0][r + 1][l + 2], *b1 = s.U[u0][r + 1][l];
+                    const T *a1 = s.U[q0][r + HW][l + HW + 1], *b1 = s.U[q0][r + HW][l + HW - 1];
                     fw[0] = a1[0]; fw[1] = a1[3]; fw[2] = a1[1]; fw[3] = a1[2]; fw[4] = a1[4];
                     bw[0] = b1[0]; bw[1] = b1[3]; bw[2] = b1[1]; bw[3] = b1[2]; bw[4] = b1[4];
-                    recon_z(cc, fw, bw, hz, lz);
+                    if (PPM && k >= 2 && k <= D - 1) {
+                        const T *a2 = s.U[q0][r + HW][l + HW + 2], *b2 = s.U[q0][r + HW][l + HW - 2];
+                        T f2[5], b2v[5];
+                        f2[0] = a2[0]; f2[1] = a2[3]; f2[2] = a2[1]; f2[3] = a2[2]; f2[4] = a2[4];
+                        b2v[0] = b2[0]; b2v[1] = b2[3]; b2v[2] = b2[1]; b2v[3] = b2[2]; b2v[4] = b2[4];
+                        ppm_z(cc, b2v, bw, fw, f2, hz, lz);
+                    } else {
+                        recon_z(cc, fw, bw, hz, lz);
+                    }
                 }
             }
             if (ycol && j == 0) {
@@ -396,14 +476,28 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             T lo[5];
             if (i + 1 <= L) {
                 CellC<T> cc;
-                const T *Un = s.U[u1][r + 1][l + 1];
+                const T *Un = s.U[q1][r + HW][l + HW];
 #pragma unroll
                 for (int q = 0; q < 5; q++) cc.u[q] = Un[q];
                 cell_consts(cc);
-                T fw2[5];
+                if constexpr (PPM) {
+                    // planes i-1 .. i+2 from the ring (own column), i+3 in flight
+                    const T *Um1 = s.U[(i - 1) & (NS - 1)][r + HW][l + HW], *U0 = s.U[q0][r + HW][l + HW];
+                    const T *Up2 = s.U[(i + 2) & (NS - 1)][r + HW][l + HW];
+                    if (i + 1 <= L - 1) {
+                        T p2[5];
 #pragma unroll
-                for (int q = 0; q < 5; q++) fw2[q] = T(pl.own[q]);
-                recon_x(cc, fw2, s.U[u0][r + 1][l + 1], hin, lo);
+                        for (int q = 0; q < 5; q++) p2[q] = T(pl.own[q]);
+                        ppm_x(cc, Um1, U0, Up2, p2, hin, lo);
+                    } else {
+                        recon_x(cc, Up2, U0, hin, lo);
+                    }
+                } else {
+                    T fw2[5];
+#pragma unroll
+                    for (int q = 0; q < 5; q++) fw2[q] = T(pl.own[q]);
+                    recon_x(cc, fw2, s.U[q0][r + HW][l + HW], hin, lo);
+                }
             } else {
                 const long long fo = (long long)(j - 1) * D + (k - 1);
 #pragma unroll
@@ -418,7 +512,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
         // (f) divergence and stage combination (src/evolution.c:29-161), FP64
         if (inter) {
             const long long c = cj + (long long)i * g.pi;
-            const T *Uc = s.U[u0][r + 1][l + 1];
+            const T *Uc = s.U[q0][r + HW][l + HW];
             (void)Uc;
 #pragma unroll
             for (int q = 0; q < 5; q++) {
@@ -460,8 +554,11 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
         // passed the barrier above) and its velocities into the slots of
         // planes i-1 (reciprocal ring) and i (division planes), read next
         // after the next iteration's barrier; advance the march
-        plane_store<T, TJE>(s, u0, r, l, j, k, H, D, live && i + 2 <= L + 1, pl);
-        if (live && i < i1) plane_prims<T, TJE>(s, i + 2, r, l, mu2, mu1);
+        if constexpr (PPM)
+            plane_store<T, TJE, PPM>(s, (i + 3) & (NS - 1), r, l, j, k, H, D, live && i + 3 <= L + 1, pl);
+        else
+            plane_store<T, TJE, PPM>(s, q0, r, l, j, k, H, D, live && i + 2 <= L + 1, pl);
+        if (live && i < i1) plane_prims<T, TJE, PPM>(s, i + 2, r, l, mu2, mu1);
 #pragma unroll
         for (int q = 0; q < 5; q++) {
             Fxp[q] = Fx[q];
@@ -491,7 +588,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
     }
 }
 
-template <typename T, int TJE, int MINB>
+template <typename T, int TJE, int MINB, bool PPM = false>
 int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, double *out, const T *mu, BF<T> bf,
                    bool courant)
 {
@@ -503,18 +600,18 @@ int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, doubl
     a.co_i1 = c.co_i1;
     a.status = &c.ds->status;
     a.seg = c.stage_seg;
-    const size_t smem = sizeof(Smem<T, TJE>);
+    const size_t smem = sizeof(Smem<T, TJE, PPM>);
     static bool attr = false;
     if (!attr) {
-        if (cudaFuncSetAttribute(k_stage<T, TJE, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
+        if (cudaFuncSetAttribute(k_stage<T, TJE, MINB, PPM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
             return -1;
         attr = true;
     }
     dim3 b(32, TJE, 1);
     dim3 gr((g.D + 29) / 30, (g.H + TJE - 3) / (TJE - 2), (g.L + a.seg - 1) / a.seg);
     prof_begin(c, FSL_K_STAGE);
-    k_stage<T, TJE, MINB><<<gr, b, smem, c.stream>>>(g, c.k, a);
+    k_stage<T, TJE, MINB, PPM><<<gr, b, smem, c.stream>>>(g, c.k, a);
     prof_end(c, FSL_K_STAGE, 1);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

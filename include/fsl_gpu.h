@@ -66,7 +66,8 @@ extern "C" {
 /* reconstruction */
 #define FSL_RECON_CHARMINMOD 0 /* characteristic kappa=1/3 minmod(beta=4), src/reconstruction.c:26-345 */
 #define FSL_RECON_PPM 1        /* Colella-Woodward PPM on the same characteristic variables (project
-                                  extension): per-phase FP64 kernels only (fsl_step runs them) */
+                                  extension): the fused step in FP64 and FP32 bulk, and the per-phase
+                                  FP64 kernels; cells next to a boundary keep the reference scheme */
 
 /* Parameters: the 22 positional values of layer2.ini in file order
  * (src/initialize.c:25-58; src-par's mpi_layer2.bin holds the same 22 values
@@ -120,8 +121,7 @@ int fsl_params_from_ini(const char *path, fsl_params *p);
  * (src-par/initialize.c:35-81, written by src-par/ini2bin/ini2bin.c:63-64).
  * Option fields are left as for fsl_params_from_ini. */
 int fsl_params_from_bin(const char *path, fsl_params *p);
-/* Check a parameter set; FSL_OK, FSL_ERR_ARG, or FSL_ERR_UNSUPPORTED for an
- * option combination that is not built (FSL_RECON_PPM with FP32 bulk). */
+/* Check a parameter set: FSL_OK or FSL_ERR_ARG. */
 int fsl_params_check(const fsl_params *p);
 
 /* ---- initial states (host arrays in the state layout) ----------------- */

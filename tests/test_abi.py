@@ -96,9 +96,10 @@ def test_params_check(fsl):
                 dict(cfl_mode=3), dict(maxCoNum=-1.0)]:
         p = fsl.default_params(**bad)
         assert lib.fsl_params_check(C.byref(p)) == -1, bad
-    # PPM runs on the FP64 per-phase kernels; with FP32 bulk it is refused
+    # PPM runs on the fused step in both precisions
     assert lib.fsl_params_check(C.byref(fsl.default_params(recon=fsl.RECON_PPM))) == 0
-    assert lib.fsl_params_check(C.byref(fsl.default_params(recon=fsl.RECON_PPM, precision=1))) == -7
+    assert lib.fsl_params_check(C.byref(fsl.default_params(recon=fsl.RECON_PPM, precision=1))) == 0
+    assert lib.fsl_params_check(C.byref(fsl.default_params(recon=2))) == -1
 
 
 def test_shear_statistics_tanh_profile(fsl):

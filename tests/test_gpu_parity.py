@@ -207,14 +207,21 @@ def test_sums_and_plane_sums(fsl, oracle_lib):
     np.testing.assert_allclose(d.plane_sums(), o.plane_sums(), rtol=1e-12)
 
 
-@pytest.mark.parametrize("setup", [0, 1])
-def test_ppm_reconstruct_and_steps(fsl, oracle_lib, setup):
-    """PPM (project extension) on the per-phase kernels: face states and whole
-    steps (fsl_step routes PPM to them) bit-identical to the oracle's
-    restatement."""
+def _ppm_case(oracle_lib, setup):
     p = (spatial_params(L=12, H=10, D=9) if setup == 0 else temporal_params(L=16, H=10, D=12))
     p = dict(p, recon=1)
     s = random_state(p, 15) if setup == 0 else oracle_lib.Oracle.temporal_state(p, 0.4, amp=0.02)[0]
+    return p, s
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_ppm_reconstruct_and_steps(fsl, oracle_lib, setup):
+    """PPM (project extension): the per-phase face states, and whole steps of
+    the fused stage kernel (fsl_step) and of the per-phase kernels, all
+    bit-identical to the oracle's restatement.  Planes per block 1, 3 and 32
+    put the x-march's prologue (the reconstruction of the cell before the
+    block's first face) at every position, boundary cells included."""
+    p, s = _ppm_case(oracle_lib, setup)
     o, d = _pair(fsl, oracle_lib, p, s)
     o.ghost(); d.ghost_bc()
     o.recon(); d.reconstruct()
@@ -222,10 +229,44 @@ def test_ppm_reconstruct_and_steps(fsl, oracle_lib, setup):
         for side in range(2):
             for v in range(5):
                 _assert_same(d.faces(dd, side, v), o.faces(dd, side, v), "PPM face dir %d side %d var %d" % (dd, side, v))
-    o2, d2 = _pair(fsl, oracle_lib, p, s)
+    o2 = oracle_lib.Oracle(p)
+    o2.set_state(s)
     o2.step(4)
-    d2.step(4)
-    _assert_same(d2.download_state(), o2.state(), "state after 4 PPM steps")
+    ref = o2.state()
+    for seg in (1, 3, 32):
+        d2 = fsl.Domain(p)
+        d2.tune(d2.TUNE_STAGE_SEG, seg)
+        d2.upload_state(s)
+        d2.step(4)
+        _assert_same(d2.download_state(), ref, "state after 4 fused PPM steps, %d planes per block" % seg)
+        d2.close()
+    d3 = fsl.Domain(p)
+    d3.upload_state(s)
+    d3.step_phased(4)
+    _assert_same(d3.download_state(), ref, "state after 4 per-phase PPM steps")
+    d3.close()
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+def test_ppm_fp32_bulk(fsl, oracle_lib, setup):
+    """PPM with the FP32 bulk against the FP64 oracle after 8 steps: rho and
+    E within FP32_RTOL relative L2, the momenta within 1e-4 of the largest
+    momentum norm (the FP32-bulk bar of the reference scheme)."""
+    p, s = _ppm_case(oracle_lib, setup)
+    o = oracle_lib.Oracle(p)
+    o.set_state(s)
+    o.step(8)
+    d = fsl.Domain(dict(p, precision=1))
+    d.upload_state(s)
+    d.step(8)
+    a = d.download_state().reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    b = o.state().reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    assert np.all(np.isfinite(a))
+    errs = per_var_rel_l2(a, b, p)
+    assert errs[0] < FP32_RTOL and errs[4] < FP32_RTOL, errs
+    mscale = max(np.linalg.norm(b[:, :, v]) for v in (1, 2, 3))
+    for v in (1, 2, 3):
+        assert np.linalg.norm(a[:, :, v] - b[:, :, v]) / mscale < 1e-4, (v, errs)
 
 
 def test_c1_config_200_steps(fsl, oracle_lib):
