@@ -223,9 +223,9 @@ STAGE_FLOPS = {p: o["add"] + o["mul"] + o["div"] + o["sqrt"] for p, o in STAGE_O
 SMS = 148
 
 
-def make_domain(fsl, grid, arm, state, dU, rows=0, seg=0):
+def make_domain(fsl, grid, arm, state, dU, rows=0, seg=0, recon=0):
     prec, sgs = ARMS[arm]
-    d = fsl.Domain(workload_params(grid, precision=prec, sgs=sgs))
+    d = fsl.Domain(workload_params(grid, precision=prec, sgs=sgs, recon=recon))
     if rows:
         d.tune(d.TUNE_STAGE_ROWS, rows)
     if seg:
@@ -570,6 +570,27 @@ def main_gpu(args):
                  "roofline": proof, "compute_roof": compute_roof(proof, 0, clk)}
         dp.close()
 
+    # ---- PPM, the configs' reconstruction as written: FP32 bulk + learned
+    # closure and plain FP64 (dynamic procedure), both with PPM, same grid ----
+    ppm = None
+    if args.ppm_steps > 0:
+        ppm = {"reconstruction": "Colella-Woodward PPM on the characteristic variables (fused stage kernel)",
+               "steps": args.ppm_steps}
+        for a2 in ("fp32-learned", "fp64-dynamic"):
+            dq = make_domain(fsl, grid, a2, state, dU, 0, 0, recon=1)
+            for _ in range(args.warmup):
+                dq.step(1)
+            dq.sync()
+            qms, qkt, _ = time_steps(torch, dq, dq.step, args.ppm_steps, barrier)
+            qms = maxr(qms)
+            qkms = {names[i]: round(qkt.ms[i], 3) for i in range(8)}
+            ppm[a2] = {"value": whole_job_rate(ncell * STAGES * args.ppm_steps, world, qms),
+                       "ms_per_step": qms / args.ppm_steps, "kernels_ms": qkms}
+            dq.close()
+        ppm["speedup_fp32_learned_vs_fp64"] = ppm["fp32-learned"]["value"] / ppm["fp64-dynamic"]["value"]
+        if plain is not None:
+            ppm["fp32_learned_ppm_vs_plain_fp64"] = ppm["fp32-learned"]["value"] / plain["value"]
+
     # ---- matched error: same initial state, M steps, against the plain FP64 path ----
     match = None
     if rank == 0 and args.match_steps > 0:
@@ -617,6 +638,8 @@ def main_gpu(args):
         if plain is not None:
             line["plain_fp64"] = plain
             line["speedup_vs_plain_fp64"] = value / plain["value"]
+        if ppm is not None:
+            line["ppm"] = ppm
         if match is not None:
             line["matched_error"] = match
         if ens is not None:
@@ -675,6 +698,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 path beside the arm")
+    ap.add_argument("--ppm-steps", type=int, default=20,
+                    help="steps timed with PPM reconstruction (FP32 + closure and FP64); 0 skips them")
     ap.add_argument("--ens-steps", type=int, default=100, help="steps of the ensemble comparison (0: skip)")
     ap.add_argument("--ens-members", type=int, default=32)
     ap.add_argument("--match-steps", type=int, default=200,

@@ -5,10 +5,14 @@
 
 c2: temporal shear layer 256x128x128, Mc 0.6, Re_dw0 1000: the plain FP64
     path (dynamic Smagorinsky, bit-identical to the CPU oracle at small
-    sizes), FP32 bulk with the FP32 dynamic procedure, and FP64 with PPM
-    reconstruction (per-phase kernels), from the same seeded state.
+    sizes), FP32 bulk with the FP32 dynamic procedure, and both again with
+    PPM reconstruction, from the same seeded state.
 c5: 512x256x256, Mc 0.7, Re_dw0 1000: the plain FP64 path against FP32 bulk +
-    the learned closure (judged every 100 steps).
+    the learned closure (judged every 100 steps), and both again with PPM.
+
+Each lower-precision arm is compared with the FP64 arm of the same
+reconstruction; FP64 PPM is also compared with the plain FP64 path (the
+difference of the schemes, not an error).
 
 Box 2pi x pi x pi, acoustic CFL 0.5, velocity noise 1e-3 dU (seed 20251203).
 Every --every steps each arm records its momentum thickness; at the end the
@@ -31,9 +35,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 CONFIGS = {
     "c2": dict(grid=(256, 128, 128), Mc=0.6, Re=1000.0, steps=2000,
-               arms=[("fp64-dynamic", 0, 0, 0), ("fp32-dynamic", 1, 0, 0), ("fp64-ppm", 0, 0, 1)]),
+               arms=[("fp64-dynamic", 0, 0, 0), ("fp32-dynamic", 1, 0, 0), ("fp64-ppm", 0, 0, 1),
+                     ("fp32-dynamic-ppm", 1, 0, 1)],
+               pairs=[("fp32-dynamic", "fp64-dynamic"), ("fp32-dynamic-ppm", "fp64-ppm"),
+                      ("fp64-ppm", "fp64-dynamic")]),
     "c5": dict(grid=(512, 256, 256), Mc=0.7, Re=1000.0, steps=5000,
-               arms=[("fp64-dynamic", 0, 0, 0), ("fp32-learned", 1, 1, 0)]),
+               arms=[("fp64-dynamic", 0, 0, 0), ("fp32-learned", 1, 1, 0), ("fp64-ppm", 0, 0, 1),
+                     ("fp32-learned-ppm", 1, 1, 1)],
+               pairs=[("fp32-learned", "fp64-dynamic"), ("fp32-learned-ppm", "fp64-ppm"),
+                      ("fp64-ppm", "fp64-dynamic")]),
 }
 
 
@@ -87,24 +97,31 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=0, help="0: the configuration's own step count")
     ap.add_argument("--every", type=int, default=100)
     ap.add_argument("--seed", type=int, default=20251203)
+    ap.add_argument("--arms", default="", help="comma-separated subset of the configuration's arms")
     args = ap.parse_args(argv)
     sys.path.insert(0, os.path.dirname(HERE))
     import freeshearlayer_b200 as fsl
 
     cfg = CONFIGS[args.config]
     steps = args.steps or cfg["steps"]
-    results = []
+    want = set(a for a in args.arms.split(",") if a)
+    results = {}
     for arm in cfg["arms"]:
+        if want and arm[0] not in want:
+            continue
         out, u, stats = run_arm(fsl, cfg, arm, steps, args.every, args.seed)
         print(json.dumps(out), flush=True)
-        results.append((out, u, stats))
-    ref_out, ref_u, ref_stats = results[0]
-    g_ref = ref_out["theta"][-1][1] - ref_out["theta"][0][1]
-    mom = float(np.sqrt(sum(np.linalg.norm(ref_u[v]) ** 2 for v in (1, 2, 3))))
+        results[arm[0]] = (out, u, stats)
+    first = next(iter(results.values()))[0]
     summary = {"config": args.config, "grid": list(cfg["grid"]), "Mc": cfg["Mc"], "Re": cfg["Re"], "steps": steps,
-               "reference_arm": ref_out["arm"], "theta0": ref_out["theta"][0][1], "theta_growth_ref": g_ref,
-               "arms": {}}
-    for out, u, stats in results[1:]:
+               "theta0": first["theta"][0][1], "arms": {}}
+    for name, against in cfg["pairs"]:
+        if name not in results or against not in results:
+            continue
+        ref_out, ref_u, ref_stats = results[against]
+        out, u, stats = results[name]
+        g_ref = ref_out["theta"][-1][1] - ref_out["theta"][0][1]
+        mom = float(np.sqrt(sum(np.linalg.norm(ref_u[v]) ** 2 for v in (1, 2, 3))))
         g = out["theta"][-1][1] - out["theta"][0][1]
         rel = {n: float(np.linalg.norm(u[v] - ref_u[v]) / np.linalg.norm(ref_u[v]))
                for n, v in (("rho", 0), ("rho_u", 1), ("rho_v", 2), ("rho_w", 3), ("E", 4))}
@@ -114,12 +131,12 @@ def main(argv=None):
             den = float(np.max(np.abs(ref_stats[comp])))
             rs[comp] = float(np.max(np.abs(stats[comp] - ref_stats[comp])) / den) if den > 0 else None
         th = np.array([t for _, t in out["theta"]]) - np.array([t for _, t in ref_out["theta"]])
-        summary["arms"][out["arm"]] = {
-            "rel_l2": rel, "momentum_l2_over_momentum_norm": mrel, "theta_growth": g,
+        summary["arms"][name + " vs " + against] = {
+            "rel_l2": rel, "momentum_l2_over_momentum_norm": mrel, "theta_growth": g, "theta_growth_against": g_ref,
             "theta_growth_rel_diff": (g - g_ref) / g_ref if g_ref else None,
             "theta_history_max_abs_diff": float(np.max(np.abs(th))),
-            "reynolds_stress_max_rel_diff": rs, "wall_s": out["wall_s"], "closure": out.get("closure")}
-    summary["reference_wall_s"] = ref_out["wall_s"]
+            "reynolds_stress_max_rel_diff": rs, "wall_s": out["wall_s"], "wall_s_against": ref_out["wall_s"],
+            "closure": out.get("closure")}
     print(json.dumps(summary), flush=True)
 
 
