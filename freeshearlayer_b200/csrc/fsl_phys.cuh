@@ -251,6 +251,11 @@ template <typename T> FSL_HD void recon_z(const CellC<T> &c, const T *fw, const 
 // oracle's restatement.
 template <typename T> FSL_HD T ppm_mc(T a, T b)
 {
+    if constexpr (std::is_same<T, float>::value) {
+        // FP32 bulk: the same value as a min and a sign copy
+        const T m = fmin(fmin(T(0.5) * fabs(a + b), T(2.0) * fabs(a)), T(2.0) * fabs(b));
+        return (a * b <= T(0.0)) ? T(0.0) : copysign(m, a);
+    }
     T m = T(0.5) * fabs(a + b);
     const T ta = T(2.0) * fabs(a), tb = T(2.0) * fabs(b);
     m = (ta < m) ? ta : m;
@@ -262,6 +267,17 @@ template <typename T>
 FSL_HD void char_fwd(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2, const T *d, T *M)
 {
     typedef Kc<T> k;
+    if constexpr (std::is_same<T, float>::value) {
+        // FP32 bulk: the rows regrouped as in recon_sweep_grouped
+        const T A = c.aa * d[0] + bn * d[1] + k::K_1 * d[4] + bt1 * d[2] + bt2 * d[3];
+        const T B = c.C * (d[1] - vn * d[0]);
+        M[0] = A - (c.aa - c.S11) * d[0];
+        M[1] = d[2] - vt1 * d[0];
+        M[2] = d[3] - vt2 * d[0];
+        M[3] = A + B;
+        M[4] = A - B;
+        return;
+    }
     const T C = c.C;
     T S12, S41, S42, S51, S52, kk, k2, k3;
     S41 = c.aa - (kk = C * vn);
@@ -283,6 +299,16 @@ FSL_HD void char_inv(const CellC<T> &c, T vn, T vt1, T vt2, T n_hh, T t1_hh, T t
 {
     typedef Kc<T> k;
     const T *u = c.u;
+    if constexpr (std::is_same<T, float>::value) {
+        // FP32 bulk: the face coefficients as sums and differences
+        const T ks = q[3] + q[4], kd = q[3] - q[4];
+        out[0] = u[0] + c.hh * q[0] + c.ee * ks;
+        out[N] = u[N] + n_hh * q[0] + n_ee * ks + c.ll * kd;
+        out[T1] = u[T1] + t1_hh * q[0] + q[1] + t1_ee * ks;
+        out[T2] = u[T2] + t2_hh * q[0] + q[2] + t2_ee * ks;
+        out[4] = u[4] + c.gg * q[0] + vt1 * q[1] + vt2 * q[2] + (c.nn + k::H_K_1) * ks + (vn * c.ll) * kd;
+        return;
+    }
     const T mm = vn * c.ll;
     T _S24, _S25, _S54, _S55, kk;
     _S24 = n_ee + c.ll; _S25 = n_ee - c.ll;
@@ -322,6 +348,15 @@ FSL_HD void ppm_sweep(const CellC<T> &c, T vn, T vt1, T vt2, T bn, T bt1, T bt2,
     for (int v = 0; v < 5; v++) {
         const T dm = ppm_mc(W0[v], W1[v]), d0 = ppm_mc(W1[v], W2[v]), dp = ppm_mc(W2[v], W3[v]);
         T r = T(0.5) * W2[v] - (dp - d0) / T(6.0), l = T(-0.5) * W1[v] - (d0 - dm) / T(6.0);
+        if constexpr (std::is_same<T, float>::value) {
+            // FP32 bulk: |r| > 2|l| and |l| > 2|r| exclude each other unless
+            // both are zero, which the flat case covers
+            const bool flat = r * l >= T(0.0);
+            const T ar = fabs(r), al = fabs(l);
+            qR[v] = flat ? T(0.0) : (ar > T(2.0) * al ? T(-2.0) * l : r);
+            qL[v] = flat ? T(0.0) : (al > T(2.0) * ar ? T(-2.0) * r : l);
+            continue;
+        }
         const bool flat = r * l >= T(0.0);
         const bool capR = !flat && fabs(r) > T(2.0) * fabs(l);
         const bool capL = !flat && !capR && fabs(l) > T(2.0) * fabs(r);
