@@ -233,12 +233,14 @@ def test_ppm_reconstruct_and_steps(fsl, oracle_lib, setup):
     o2.set_state(s)
     o2.step(4)
     ref = o2.state()
-    for seg in (1, 3, 32):
+    for rows, seg in ((16, 1), (16, 3), (16, 32), (8, 3), (12, 5)):
         d2 = fsl.Domain(p)
+        d2.tune(d2.TUNE_STAGE_ROWS, rows)
         d2.tune(d2.TUNE_STAGE_SEG, seg)
         d2.upload_state(s)
         d2.step(4)
-        _assert_same(d2.download_state(), ref, "state after 4 fused PPM steps, %d planes per block" % seg)
+        _assert_same(d2.download_state(), ref, "state after 4 fused PPM steps, %d rows, %d planes per block"
+                     % (rows, seg))
         d2.close()
     d3 = fsl.Domain(p)
     d3.upload_state(s)
@@ -247,16 +249,17 @@ def test_ppm_reconstruct_and_steps(fsl, oracle_lib, setup):
     d3.close()
 
 
-@pytest.mark.parametrize("setup", [0, 1])
-def test_ppm_fp32_bulk(fsl, oracle_lib, setup):
-    """PPM with the FP32 bulk against the FP64 oracle after 8 steps: rho and
-    E within FP32_RTOL relative L2, the momenta within 1e-4 of the largest
-    momentum norm (the FP32-bulk bar of the reference scheme)."""
+@pytest.mark.parametrize("setup,rows", [(0, 16), (1, 16), (1, 8), (1, 12)])
+def test_ppm_fp32_bulk(fsl, oracle_lib, setup, rows):
+    """PPM with the FP32 bulk (each tile shape) against the FP64 oracle after
+    8 steps: rho and E within FP32_RTOL relative L2, the momenta within 1e-4
+    of the largest momentum norm (the FP32-bulk bar of the reference scheme)."""
     p, s = _ppm_case(oracle_lib, setup)
     o = oracle_lib.Oracle(p)
     o.set_state(s)
     o.step(8)
     d = fsl.Domain(dict(p, precision=1))
+    d.tune(d.TUNE_STAGE_ROWS, rows)
     d.upload_state(s)
     d.step(8)
     a = d.download_state().reshape(p["LEN"], p["HIG"], 5, p["DEP"])
