@@ -16,19 +16,22 @@ def fsl():
     return fsl
 
 
-# uneven grids, Mach and Reynolds numbers, precisions and closures
+# uneven grids, Mach and Reynolds numbers, precisions, closures and
+# reconstructions
 MEMBERS = [
     dict(L=24, H=16, D=16, Mc=0.3, Re=400.0, precision=0, sgs=0, seed=1),
     dict(L=32, H=12, D=24, Mc=0.5, Re=700.0, precision=1, sgs=0, seed=2),
     dict(L=16, H=24, D=12, Mc=0.7, Re=1000.0, precision=1, sgs=1, seed=3),
     dict(L=40, H=16, D=8, Mc=0.2, Re=300.0, precision=0, sgs=1, seed=4),
     dict(L=24, H=20, D=36, Mc=0.6, Re=550.0, precision=1, sgs=0, seed=5),
+    dict(L=20, H=16, D=20, Mc=0.5, Re=600.0, precision=1, sgs=1, seed=6, recon=1),
+    dict(L=28, H=12, D=16, Mc=0.4, Re=450.0, precision=0, sgs=0, seed=7, recon=1),
 ]
 
 
 def _member(fsl, m, amp=1e-2):
     p = temporal_params(L=m["L"], H=m["H"], D=m["D"], Mc=m["Mc"], Re=m["Re"], precision=m["precision"],
-                        sgs=m["sgs"])
+                        sgs=m["sgs"], recon=m.get("recon", 0))
     s, dU = fsl.temporal_state(p, m["Mc"], 1.0, amp, m["seed"])
     d = fsl.Domain(p)
     d.upload_state(s)
@@ -62,8 +65,8 @@ def test_tuner_changes_no_result(fsl):
     ensemble still matches members stepped alone.  (The FP32-bulk kernels'
     last bits may depend on the tile shape: the compiler may contract a face
     flux into FMAs differently where a block's march starts.)"""
-    ens_m = [_member(fsl, m) for m in MEMBERS[:3]]
-    ref_m = [_member(fsl, m) for m in MEMBERS[:3]]
+    ens_m = [_member(fsl, m) for m in MEMBERS[:3] + MEMBERS[5:6]]
+    ref_m = [_member(fsl, m) for m in MEMBERS[:3] + MEMBERS[5:6]]
     e = fsl.Ensemble(ens_m)
     e.step(4)
     rows, seg, ms = e.tune(trial_steps=2)
