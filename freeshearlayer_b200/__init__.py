@@ -162,6 +162,7 @@ def lib():
         sig.update({
             "fsl_get_planes": [vp, i, i, vp], "fsl_set_planes": [vp, i, i, vp],
             "fsl_set_courant_range": [vp, i, i], "fsl_courant_prepare": [vp],
+            "fsl_upload_state_async": [vp, _dp], "fsl_download_state_async": [vp, _dp], "fsl_transfer_wait": [vp],
             "fsl_get_courant_max": [vp, C.POINTER(C.c_double)], "fsl_set_courant_max": [vp, d],
         })
         sig["fsl_tune"] = [vp, i, i]
@@ -315,6 +316,26 @@ class Domain:
 
     def set_time(self, step: int, dt: float):
         self._c(lib().fsl_set_time(self.h, step, dt))
+
+    def upload_state_async(self, state: np.ndarray):
+        """Queue U^n <- state (a contiguous float64 array, pinned for overlap);
+        the array must stay untouched until transfer_wait()."""
+        if state.dtype != np.float64 or not state.flags.c_contiguous or state.size != state_size(self.p):
+            raise FslError(-1, "upload_state_async: contiguous float64 of the state size expected")
+        self._c(lib().fsl_upload_state_async(self.h, state.reshape(-1)))
+        self._pending = getattr(self, "_pending", []) + [state]
+
+    def download_state_async(self, out: np.ndarray):
+        """Queue out <- U^n (contiguous float64, pinned for overlap); valid
+        after transfer_wait()."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != state_size(self.p):
+            raise FslError(-1, "download_state_async: contiguous float64 of the state size expected")
+        self._c(lib().fsl_download_state_async(self.h, out.reshape(-1)))
+        self._pending = getattr(self, "_pending", []) + [out]
+
+    def transfer_wait(self):
+        self._c(lib().fsl_transfer_wait(self.h))
+        self._pending = []
 
     # --- x-slabs ------------------------------------------------------------------
     def plane_size(self) -> int:

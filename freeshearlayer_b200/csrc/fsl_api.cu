@@ -481,6 +481,16 @@ int fsl_destroy(fsl_ctx *h)
     if (c.stream) cudaStreamSynchronize(c.stream);
     cudaFree(c.U); cudaFree(c.Up); cudaFree(c.Uq); cudaFree(c.mu);
     cudaFree(c.partials); cudaFree(c.stage_dev); cudaFree(c.ds); cudaFree(c.favre);
+    if (c.xfer_alloc) {
+        if (c.up) cudaStreamSynchronize(c.up);
+        if (c.down) cudaStreamSynchronize(c.down);
+        cudaFree(c.xin); cudaFree(c.xout);
+        cudaEvent_t *ev[4] = {&c.ev_in_ready, &c.ev_in_free, &c.ev_out_ready, &c.ev_out_free};
+        for (cudaEvent_t *e : ev)
+            if (*e) cudaEventDestroy(*e);
+        if (c.up) cudaStreamDestroy(c.up);
+        if (c.down) cudaStreamDestroy(c.down);
+    }
     if (c.hs) cudaFreeHost(c.hs);
     if (c.faces_alloc)
         for (int s = 0; s < 2; s++)
@@ -654,6 +664,84 @@ int fsl_set_courant_max(fsl_ctx *h, double maxCo)
     CK(cudaMemcpyAsync(&c.ds->co_bits, &b, sizeof b, cudaMemcpyHostToDevice, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     c.co_valid = true;
+    return FSL_OK;
+}
+
+// ---- asynchronous state transfer ----------------------------------------------
+static int ensure_xfer(Ctx &c)
+{
+    if (c.xfer_alloc) return FSL_OK;
+    const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
+    if (cudaMalloc((void **)&c.xin, n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void **)&c.xout, n * sizeof(double)) != cudaSuccess) {
+        cudaFree(c.xin); cudaFree(c.xout);
+        c.xin = c.xout = nullptr;
+        return fail(c, FSL_ERR_NOMEM, "asynchronous transfer buffers");
+    }
+    c.xfer_alloc = true;
+    c.bytes += 2 * n * sizeof(double);
+    CK(cudaStreamCreateWithFlags(&c.up, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c.down, cudaStreamNonBlocking));
+    cudaEvent_t *ev[4] = {&c.ev_in_ready, &c.ev_in_free, &c.ev_out_ready, &c.ev_out_free};
+    for (cudaEvent_t *e : ev) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    // both staging buffers start free
+    CK(cudaEventRecord(c.ev_in_free, c.stream));
+    CK(cudaEventRecord(c.ev_out_free, c.stream));
+    return FSL_OK;
+}
+
+// The H2D copy runs on its own stream as soon as the previous scatter has
+// left the staging buffer, so it overlaps the work queued before it; the
+// scatter into U^n is queued on the context's stream behind that work.
+int fsl_upload_state_async(fsl_ctx *h, const double *state)
+{
+    if (!h || !state) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = ensure_xfer(c);
+    if (rc) return rc;
+    const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
+    c.co_valid = false;
+    CK(cudaStreamWaitEvent(c.up, c.ev_in_free, 0));
+    CK(cudaMemcpyAsync(c.xin, state, n * sizeof(double), cudaMemcpyHostToDevice, c.up));
+    CK(cudaEventRecord(c.ev_in_ready, c.up));
+    CK(cudaStreamWaitEvent(c.stream, c.ev_in_ready, 0));
+    launch_state_scatter(c, c.U, c.xin, 1, c.p.LEN);
+    CKL();
+    CK(cudaEventRecord(c.ev_in_free, c.stream));
+    c.cur = 0;
+    return FSL_OK;
+}
+
+// The gather out of U^n is queued on the context's stream (once the previous
+// D2H copy has left the staging buffer); the D2H copy runs on its own stream
+// and overlaps the work queued after it.
+int fsl_download_state_async(fsl_ctx *h, double *state)
+{
+    if (!h || !state) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    int rc = ensure_xfer(c);
+    if (rc) return rc;
+    if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_download_state_async: the current-stage buffer is not U^n");
+    const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
+    CK(cudaStreamWaitEvent(c.stream, c.ev_out_free, 0));
+    launch_state_gather(c, c.U, c.xout, 1, c.p.LEN);
+    CKL();
+    CK(cudaEventRecord(c.ev_out_ready, c.stream));
+    CK(cudaStreamWaitEvent(c.down, c.ev_out_ready, 0));
+    CK(cudaMemcpyAsync(state, c.xout, n * sizeof(double), cudaMemcpyDeviceToHost, c.down));
+    CK(cudaEventRecord(c.ev_out_free, c.down));
+    return FSL_OK;
+}
+
+int fsl_transfer_wait(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    if (c.xfer_alloc) {
+        CK(cudaStreamSynchronize(c.up));
+        CK(cudaStreamSynchronize(c.down));
+    }
+    CK(cudaStreamSynchronize(c.stream));
     return FSL_OK;
 }
 

@@ -127,6 +127,13 @@ struct Ctx {
     int npartials = 0;
     double *stage_host = nullptr; // pinned staging for state transfer
     double *stage_dev = nullptr;
+    // asynchronous state transfer (fsl_*_state_async): own staging buffers,
+    // copy streams (one per direction) and the events that order them
+    // against the context's stream
+    bool xfer_alloc = false;
+    double *xin = nullptr, *xout = nullptr;
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t ev_in_ready = nullptr, ev_in_free = nullptr, ev_out_ready = nullptr, ev_out_free = nullptr;
     // host driver state
     double X = 0;
     int counter = 0;

@@ -153,6 +153,17 @@ int fsl_upload_state(fsl_ctx *ctx, const double *state);
 int fsl_download_state(fsl_ctx *ctx, double *state);
 /* Set step counter and time step as a restart would (src/initialize.c:149-152). */
 int fsl_set_time(fsl_ctx *ctx, unsigned step, double deltaT);
+/* The same transfers without blocking the host, overlapped with the device
+ * work around them: the upload's host-to-device copy and the download's
+ * device-to-host copy run on copy streams of their own (one per direction,
+ * with their own staging buffers), ordered against the context's stream by
+ * events, so that a step's upload, the previous step's download and the step
+ * itself proceed together.  `state` should be pinned host memory (pageable
+ * memory works, without overlap) and must stay untouched until
+ * fsl_transfer_wait returns. */
+int fsl_upload_state_async(fsl_ctx *ctx, const double *state);
+int fsl_download_state_async(fsl_ctx *ctx, double *state);
+int fsl_transfer_wait(fsl_ctx *ctx);
 
 /* ---- x-slabs (replaces src-par's MPI decomposition) ------------------------
  * A domain of LEN planes split along x into slabs, one context per slab (one

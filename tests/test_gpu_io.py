@@ -139,3 +139,32 @@ def test_output_frame_matches_oracle(fsl, oracle_lib, tmp_path):
     d.write_tecplot(str(tmp_path / "gpu.plt"))
     fsl.tecplot_write(str(tmp_path / "orc.plt"), b)
     assert (tmp_path / "gpu.plt").read_bytes() == (tmp_path / "orc.plt").read_bytes()
+
+
+def test_async_transfers_match_the_synchronous_ones(fsl):
+    """Pipelined fsl_upload_state_async / fsl_step / fsl_download_state_async
+    over three different inputs: every result equals that of the same
+    sequence through the synchronous calls."""
+    from tests.helpers import temporal_params
+    import torch
+    p = temporal_params(L=24, H=12, D=16)
+    states = [fsl.temporal_state(fsl._as_params(p), 0.4, 1.0, 2e-2, 11 + q)[0] for q in range(3)]
+    n = states[0].size
+    ins = [torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+    outs = [torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)]
+    for a, s in zip(ins, states):
+        a[:] = s
+    d = fsl.Domain(p)
+    for q in range(3):
+        d.upload_state_async(ins[q])
+        d.step(2)
+        d.download_state_async(outs[q])
+    d.transfer_wait()
+    d.close()
+    # the same sequence with the synchronous calls (deltaT carries over)
+    r = fsl.Domain(p)
+    for q in range(3):
+        r.upload_state(states[q])
+        r.step(2)
+        assert np.array_equal(outs[q], r.download_state()), q
+    r.close()
