@@ -145,6 +145,38 @@ def test_slabs_fp32_bulk(fsl):
         assert np.linalg.norm(a[:, :, v] - b[:, :, v]) / np.linalg.norm(b[:, :, v]) < 1e-7
 
 
+def test_slabs_fp32_learned_closure(fsl):
+    """FP32 bulk + learned closure (judgements off, which slabs require): the
+    closure's features reach one plane, so the owned planes agree with the
+    undivided domain to FP32 rounding."""
+    from freeshearlayer_b200.slabs import SlabSet
+    p, s = _case(fsl, 1)
+    p = dict(p, precision=1, sgs=1)
+    dU = 2.0 * 0.4 * (1.4 * 1e5) ** 0.5
+
+    def setup(d):
+        d.closure_set_scales(1.0 / dU, 1.0)
+        d.closure_set_weights(fsl.closure_weights())
+        d.closure_judge(0, 1.0)
+
+    d = fsl.Domain(p)
+    setup(d)
+    d.upload_state(s)
+    d.step(6)
+    ref = d.download_state()
+    d.close()
+    with SlabSet(p, 2) as ss:
+        for x in ss.domains:
+            setup(x)
+        ss.upload_state(s)
+        ss.step(6)
+        got = ss.download_state()
+    a = got.reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    b = ref.reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    for v in (0, 4):
+        assert np.linalg.norm(a[:, :, v] - b[:, :, v]) / np.linalg.norm(b[:, :, v]) < 1e-7
+
+
 def test_slab_protocol_errors(fsl):
     p, s = _case(fsl, 1, L=32)
     d = fsl.Domain(p)
