@@ -263,14 +263,17 @@ int fsl_dynamic_smagorinsky_noalloc(const double *U, double *mu, int LEN, int HI
 /* ---- whole steps ---------------------------------------------------------
  * nsteps iterations of the driver loop body without I/O (src/layer2.c:147-178):
  * Courant check and dt rescale, disturbance draw, nStages stages.  Uses the
- * fused stage kernels; the SGS viscosity is evaluated once per step (it
+ * fused stage kernels (nStages = 2 runs the per-phase kernels, FP64 only);
+ * the SGS viscosity is evaluated once per step (it
  * depends only on U^n, src/fluxes.c:53, so this equals the reference's
  * per-stage evaluation).  Asynchronous: returns after queuing the work. */
 int fsl_step(fsl_ctx *ctx, int nsteps);
 /* Same work through the per-phase entry points (reference phase order). */
 int fsl_step_phased(fsl_ctx *ctx, int nsteps);
 
-/* Launch-shape knobs of the fused kernels (the results do not depend on them). */
+/* Launch-shape knobs of the fused kernels.  FP64 results do not depend on
+ * them; FP32-bulk results may differ in the last bits (the compiler may
+ * contract a flux into FMAs differently where a block's march starts). */
 #define FSL_TUNE_STAGE_ROWS 1 /* rows per stage tile incl. 2 halo rows: 8, 12 or 16 */
 #define FSL_TUNE_STAGE_SEG 2  /* x planes marched per stage block (default 48 FP32 bulk, 32 FP64) */
 int fsl_tune(fsl_ctx *ctx, int key, int value);
@@ -394,8 +397,9 @@ int fsl_trainer_train(fsl_trainer *tr, int epochs, long long batch, double lr, d
  * (each on its own stream, forked from and joined to the ensemble's stream)
  * into one CUDA graph and replays it, so the members' kernels share the SMs
  * and a chunk costs one launch.  Every member's result is bit-identical to
- * stepping it alone with fsl_step.  Members: temporal setup, nStages = 3, no
- * profiling, learned closure only with judgements off
+ * stepping it alone with fsl_step.  Members: temporal setup, nStages = 3,
+ * either reconstruction, whole domains (not x-slabs), no profiling, learned
+ * closure only with judgements off
  * (fsl_closure_judge(ctx, 0, ...)); otherwise FSL_ERR_UNSUPPORTED.  Members
  * stay owned by the caller and must outlive the ensemble; while an ensemble
  * step is in flight, do not call them directly.  Each member's disturbance
