@@ -125,7 +125,7 @@ def lib():
             "fsl_draw_disturbance": [vp], "fsl_set_disturbance": [vp, u, u, d, d, d],
             "fsl_ghost_bc": [vp], "fsl_reconstruct": [vp], "fsl_interface_bc": [vp],
             "fsl_dynamic_smagorinsky": [vp], "fsl_fluxes": [vp], "fsl_evolution": [vp, i],
-            "fsl_step": [vp, i], "fsl_step_phased": [vp, i],
+            "fsl_step": [vp, i], "fsl_step_phased": [vp, i], "fsl_step_stage": [vp],
             "fsl_get_cells": [vp, i, i, _dp], "fsl_set_cells": [vp, i, i, _dp],
             "fsl_get_faces": [vp, i, i, i, _dp], "fsl_set_faces": [vp, i, i, i, _dp],
             "fsl_set_cur": [vp, i], "fsl_sums": [vp, _dp], "fsl_plane_sums": [vp, _dp],
@@ -397,6 +397,7 @@ class Domain:
     def evolution(self, stage: int): self._c(lib().fsl_evolution(self.h, stage))
     def step(self, n: int = 1): self._c(lib().fsl_step(self.h, n))
     def step_phased(self, n: int = 1): self._c(lib().fsl_step_phased(self.h, n))
+    def step_stage(self): self._c(lib().fsl_step_stage(self.h))
 
     # reference names (src/layer2.c:147-176)
     def checkCoNum(self): return self.check_courant()

@@ -555,6 +555,7 @@ int fsl_upload_state(fsl_ctx *h, const double *state)
     Ctx &c = h->c;
     const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
     c.co_valid = false;
+    c.stage_next = 0; // a step in progress is abandoned
     CK(cudaMemcpyAsync(c.stage_dev, state, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     launch_state_scatter(c, c.U, c.stage_dev, 1, c.p.LEN);
     CKL();
@@ -587,13 +588,20 @@ static bool planes_ok(const Ctx &c, int i0, int n)
     return i0 >= 1 && n >= 0 && i0 + n - 1 <= c.p.LEN;
 }
 
+// the buffer holding the current stage state: U^n between steps, the output
+// of stage 1 or 2 while fsl_step_stage is in the middle of a step
+static double *stage_state(Ctx &c)
+{
+    return c.stage_next == 2 ? c.Up : c.stage_next == 3 ? c.Uq : c.U;
+}
+
 int fsl_get_planes(fsl_ctx *h, int i0, int n, double *buf)
 {
     if (!h || !buf || !planes_ok(h->c, i0, n)) return FSL_ERR_ARG;
     Ctx &c = h->c;
     if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_get_planes: the current-stage buffer is not U^n");
     const size_t bytes = (size_t)n * c.p.HIG * 5 * c.p.DEP * sizeof(double);
-    launch_state_gather(c, c.U, c.stage_dev, i0, n);
+    launch_state_gather(c, stage_state(c), c.stage_dev, i0, n);
     CKL();
     if (bytes) CK(cudaMemcpyAsync(buf, c.stage_dev, bytes, cudaMemcpyDefault, c.stream));
     CK(cudaStreamSynchronize(c.stream));
@@ -607,9 +615,9 @@ int fsl_set_planes(fsl_ctx *h, int i0, int n, const double *buf)
     if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_set_planes: the current-stage buffer is not U^n");
     const size_t bytes = (size_t)n * c.p.HIG * 5 * c.p.DEP * sizeof(double);
     // planes outside the Courant range leave the owned maximum as it is
-    if (n > 0 && i0 <= c.co_i1 && i0 + n - 1 >= c.co_i0) c.co_valid = false;
+    if (c.stage_next == 0 && n > 0 && i0 <= c.co_i1 && i0 + n - 1 >= c.co_i0) c.co_valid = false;
     if (bytes) CK(cudaMemcpyAsync(c.stage_dev, buf, bytes, cudaMemcpyDefault, c.stream));
-    launch_state_scatter(c, c.U, c.stage_dev, i0, n);
+    launch_state_scatter(c, stage_state(c), c.stage_dev, i0, n);
     CKL();
     CK(cudaStreamSynchronize(c.stream));
     return FSL_OK;
@@ -701,6 +709,7 @@ int fsl_upload_state_async(fsl_ctx *h, const double *state)
     if (rc) return rc;
     const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
     c.co_valid = false;
+    c.stage_next = 0; // a step in progress is abandoned
     CK(cudaStreamWaitEvent(c.up, c.ev_in_free, 0));
     CK(cudaMemcpyAsync(c.xin, state, n * sizeof(double), cudaMemcpyHostToDevice, c.up));
     CK(cudaEventRecord(c.ev_in_ready, c.up));
@@ -863,6 +872,7 @@ int fsl_evolution(fsl_ctx *h, int stage)
 // would judge on the slab alone.
 static int slab_check(Ctx &c, int nsteps)
 {
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "a step is in progress (fsl_step_stage)");
     if (c.co_i0 == 1 && c.co_i1 == c.p.LEN) return FSL_OK;
     if (nsteps > 1) return fail(c, FSL_ERR_ARG, "x-slab: one step per call (overlap exchange between steps)");
     if (nsteps == 1 && !c.co_valid)
@@ -977,6 +987,66 @@ int fsl_step(fsl_ctx *h, int nsteps)
         c.co_valid = true;
         CKL();
     }
+    return FSL_OK;
+}
+
+// One RK stage of the fused step, the three in turn: the first begins the
+// step (Courant rescale, disturbance draw, SGS viscosity, stage 1), the third
+// completes it.  The same launches as fsl_step, so an x-slab can refresh its
+// overlap planes between stages.
+int fsl_step_stage(fsl_ctx *h)
+{
+    if (!h) return FSL_ERR_ARG;
+    Ctx &c = h->c;
+    if (c.p.nStages != 3) return fail(c, FSL_ERR_UNSUPPORTED, "fsl_step_stage: nStages = 3 only");
+    const bool fp32 = c.p.precision == FSL_PREC_FP32;
+    int rc;
+    if (c.stage_next == 0) {
+        if ((rc = slab_check(c, 1))) return rc;
+        if ((rc = ensure_dyn(c))) return rc;
+        if ((rc = ensure_bf(c))) return rc;
+        if (fp32 && (rc = ensure_fp32(c))) return rc;
+        if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_step_stage: the current-stage buffer is not U^n");
+        if (c.co_valid) launch_courant_apply(c);
+        else launch_courant(c);
+        c.step++;
+        draw(c);
+        launch_ghost(c, c.U);
+        if (fp32) launch_bface32(c, c.U, c.dist);
+        else launch_bface(c, c.U, c.dist);
+        if (c.p.sgs == FSL_SGS_LEARNED) {
+            if ((rc = closure_step_sgs(c))) return rc;
+        } else if (fp32) {
+            launch_dynsmag32(c, c.U);
+        } else {
+            launch_dynsmag(c, c.U);
+        }
+        const int e = fp32 ? launch_stage32(c, 1, c.U, c.U, c.Up) : launch_stage(c, 1, c.U, c.U, c.Up);
+        if (e) return fail(c, FSL_ERR_CUDA, "stage kernel");
+        c.stage_next = 2;
+    } else if (c.stage_next == 2) {
+        launch_ghost(c, c.Up);
+        if (fp32) {
+            launch_bface32(c, c.Up, c.dist);
+            launch_stage32(c, 2, c.Up, c.U, c.Uq);
+        } else {
+            launch_bface(c, c.Up, c.dist);
+            launch_stage(c, 2, c.Up, c.U, c.Uq);
+        }
+        c.stage_next = 3;
+    } else {
+        launch_ghost(c, c.Uq);
+        if (fp32) {
+            launch_bface32(c, c.Uq, c.dist);
+            launch_stage32(c, 3, c.Uq, c.U, c.U, true);
+        } else {
+            launch_bface(c, c.Uq, c.dist);
+            launch_stage(c, 3, c.Uq, c.U, c.U, true);
+        }
+        c.co_valid = true;
+        c.stage_next = 0;
+    }
+    CKL();
     return FSL_OK;
 }
 

@@ -147,6 +147,9 @@ struct Ctx {
     // planes (1-based) whose cells enter the Courant maximum; 1..L unless an
     // x-slab of a decomposed domain restricts it to the planes it owns
     int co_i0 = 1, co_i1 = 0;
+    // fsl_step_stage: the stage the step in progress runs next (2 or 3), or 0
+    // between steps; the current stage state is then in Up (2) or Uq (3)
+    int stage_next = 0;
     double dt_host = 0; // host copy of dt, valid after sync
     double maxco_host = 0;
     unsigned long long bytes = 0;

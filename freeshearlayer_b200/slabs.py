@@ -18,11 +18,17 @@ translation-invariant: its ghost planes wrap, but the SGS test filter keeps
 the zero bands of a domain boundary at the seam between planes LEN and 1.  A
 slab whose overlap crosses the seam therefore lists its planes in ascending
 global order, which puts the seam on its own periodic boundary and the
-discontinuity between unrelated planes inside its overlap.  Once per step each slab's overlap planes are refreshed from
-its neighbours' owned planes, and before each step the Courant maximum over
-the owned planes is combined by a maximum across slabs, so that every slab
-rescales deltaT to the same value.  One exchange per step instead of one per
-stage, at the price of 2W extra planes of work per slab.
+discontinuity between unrelated planes inside its overlap.  Once per step
+each slab's overlap planes are refreshed from its neighbours' owned planes,
+and before each step the Courant maximum over the owned planes is combined by
+a maximum across slabs, so that every slab rescales deltaT to the same value.
+One exchange per step instead of one per stage, at the price of 2W extra
+planes of work per slab.
+
+exchange="stage" refreshes the overlap after every stage instead, as the
+reference does: the stage state of every local plane is then exact when the
+next stage starts, so W need only cover one stage's reach (STAGE_RADIUS), half
+the redundant work for three exchanges per step.
 
 `SlabSet` drives several slabs from one process (one device, or one device
 per slab); `DistributedSlab` drives one slab per rank of a torch.distributed
@@ -40,6 +46,16 @@ import numpy as np
 # the first stage.  Measured by perturbing one plane: 7 for the reference
 # reconstruction and 9 for PPM; the defaults keep a plane of margin.
 RADIUS = {0: 8, 1: 10}
+
+# Overlap widths for an exchange after every stage: one stage reaches 2
+# planes (reference reconstruction) or 3 (PPM) through the x-stencil, and
+# every stage reads the step's SGS viscosity at the neighbouring planes, whose
+# own reach into U^n is 2 (velocities, the test filter and the strain), so 3
+# for the first stage.  Measured by perturbing one plane: 3 and 2 for stages 1
+# and 2 with the reference reconstruction, 3 and 3 with PPM; the defaults keep
+# a plane of margin.
+STAGE_RADIUS = {0: 4, 1: 4}
+EXCHANGES = ("step", "stage")
 
 
 @dataclass(frozen=True)
@@ -149,11 +165,19 @@ def exchange_plan(slabs: list[Slab]):
     return plan
 
 
-def _check_overlap(p, overlap):
-    W = RADIUS[p.recon] if overlap is None else int(overlap)
-    if W < RADIUS[p.recon]:
-        raise ValueError("overlap %d below the step's reach of %d planes" % (W, RADIUS[p.recon]))
+def _check_overlap(p, overlap, exchange="step"):
+    if exchange not in EXCHANGES:
+        raise ValueError("exchange: 'step' or 'stage'")
+    need = (RADIUS if exchange == "step" else STAGE_RADIUS)[p.recon]
+    W = need if overlap is None else int(overlap)
+    if W < need:
+        raise ValueError("overlap %d below the %s's reach of %d planes" % (W, exchange, need))
     return W
+
+
+def _check_phased(exchange, phased):
+    if phased and exchange == "stage":
+        raise ValueError("exchange='stage' runs the fused stages (fsl_step_stage)")
 
 
 class SlabSet:
@@ -162,15 +186,18 @@ class SlabSet:
     devices: one CUDA device index per slab (default: all on the current
     device).  staging "host" moves overlap planes through numpy arrays;
     "device" through CUDA tensors (peer copies between devices) and combines
-    the Courant maximum in device memory.  domain_factory(params) makes each
-    slab's context (default: Domain)."""
+    the Courant maximum in device memory.  exchange "step" refreshes the
+    overlap planes once per step, "stage" after every stage (a narrower
+    default overlap).  domain_factory(params) makes each slab's context
+    (default: Domain)."""
 
     def __init__(self, params, nslabs: int, overlap: int | None = None, devices=None,
-                 staging: str = "host", domain_factory=None):
+                 staging: str = "host", domain_factory=None, exchange: str = "step"):
         from . import Domain, SETUP_TEMPORAL, _as_params
         p = _as_params(params)
         self.p = p
-        self.W = _check_overlap(p, overlap)
+        self.W = _check_overlap(p, overlap, exchange)
+        self.exchange_mode = exchange
         self.slabs = layout(p.LEN, nslabs, self.W, p.setup == SETUP_TEMPORAL)
         self.plan = exchange_plan(self.slabs)
         if staging not in ("host", "device"):
@@ -282,8 +309,16 @@ class SlabSet:
         return self._bufs[key]
 
     def step(self, n: int = 1, phased: bool = False):
+        _check_phased(self.exchange_mode, phased)
         for _ in range(n):
             self.combine_courant()
+            if self.exchange_mode == "stage":
+                for _stage in range(3):
+                    for s, d in zip(self.slabs, self.domains):
+                        with self._on(s.index):
+                            d.step_stage()
+                    self.exchange()
+                continue
             for s, d in zip(self.slabs, self.domains):
                 with self._on(s.index):
                     d.step_phased(1) if phased else d.step(1)
@@ -312,10 +347,11 @@ class DistributedSlab:
     CUDA tensors; with gloo in host tensors.  Every rank takes the same
     collective steps in the same order.
 
-    domain_factory(params) makes the slab's context (default: Domain on the
-    current CUDA device)."""
+    exchange: "step" or "stage", as for SlabSet.  domain_factory(params)
+    makes the slab's context (default: Domain on the current CUDA device)."""
 
-    def __init__(self, params, group=None, overlap: int | None = None, domain_factory=None):
+    def __init__(self, params, group=None, overlap: int | None = None, domain_factory=None,
+                 exchange: str = "step"):
         import torch
         import torch.distributed as dist
         from . import Domain, SETUP_TEMPORAL, _as_params
@@ -323,7 +359,8 @@ class DistributedSlab:
         self.p, self.group = p, group
         self.rank = dist.get_rank(group)
         self.size = dist.get_world_size(group)
-        self.W = _check_overlap(p, overlap)
+        self.W = _check_overlap(p, overlap, exchange)
+        self.exchange_mode = exchange
         self.slabs = layout(p.LEN, self.size, self.W, p.setup == SETUP_TEMPORAL)
         self.slab = self.slabs[self.rank]
         self.on_device = dist.get_backend(group) == "nccl"
@@ -386,8 +423,8 @@ class DistributedSlab:
 
     def exchange(self):
         """Overlap planes from the slabs that own them, as point-to-point
-        messages (the per-stage sends of src-par/boundCondInGhostCells.c:60-73
-        become one set per step)."""
+        messages (the per-stage sends of src-par/boundCondInGhostCells.c:60-73,
+        one set per step or per stage)."""
         import torch
         import torch.distributed as dist
         if not self.plan:
@@ -409,7 +446,13 @@ class DistributedSlab:
                 self.dom.set_planes(j0, n, self._buf(self._bufs[t]))
 
     def step(self, n: int = 1, phased: bool = False):
+        _check_phased(self.exchange_mode, phased)
         for _ in range(n):
             self.combine_courant()
+            if self.exchange_mode == "stage":
+                for _stage in range(3):
+                    self.dom.step_stage()
+                    self.exchange()
+                continue
             self.dom.step_phased(1) if phased else self.dom.step(1)
             self.exchange()

@@ -184,7 +184,9 @@ int fsl_transfer_wait(fsl_ctx *ctx);
  * Planes are 1-based interior x-indices; buffers hold n planes in the
  * upload/download layout ([n][HIG][5][DEP] doubles), host or device memory
  * (copied with cudaMemcpyDefault; the call returns with the copy done).
- * The current-stage buffer must be U^n (between steps). */
+ * Between steps they access U^n; while fsl_step_stage is in the middle of a
+ * step, the current stage state (the output of stage 1 or 2), so that a slab
+ * can refresh its overlap planes after every stage. */
 int fsl_get_planes(fsl_ctx *ctx, int i0, int n, double *buf);
 int fsl_set_planes(fsl_ctx *ctx, int i0, int n, const double *buf);
 /* Planes i0..i1 enter the Courant maximum (default 1..LEN).  A context with a
@@ -270,6 +272,16 @@ int fsl_dynamic_smagorinsky_noalloc(const double *U, double *mu, int LEN, int HI
 int fsl_step(fsl_ctx *ctx, int nsteps);
 /* Same work through the per-phase entry points (reference phase order). */
 int fsl_step_phased(fsl_ctx *ctx, int nsteps);
+/* One RK stage of fsl_step's work per call, the three stages in turn (nStages
+ * = 3): the first call begins a step (Courant rescale, disturbance draw, SGS
+ * viscosity, stage 1), the third completes it.  Same launches and results as
+ * fsl_step.  Between the calls only fsl_get_planes / fsl_set_planes may touch
+ * the state (the per-stage ghost-plane exchange of
+ * src-par/boundCondInGhostCells.c:60-73); fsl_step, fsl_step_phased and the
+ * other stage calls refuse with FSL_ERR_ARG until the step is complete.  An
+ * upload abandons it (its deltaT rescale, step count and disturbance draw
+ * stand, as after a completed step). */
+int fsl_step_stage(fsl_ctx *ctx);
 
 /* Launch-shape knobs of the fused kernels.  FP64 results do not depend on
  * them; FP32-bulk results may differ in the last bits (the compiler may

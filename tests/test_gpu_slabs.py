@@ -1,8 +1,9 @@
-"""x-slab decomposition on the GPU: the reach of one step, and slabs that
-must reproduce the undivided domain bit for bit (FP64; the reference
-reconstruction on the fused path, PPM on the per-phase path), with overlap
-planes staged through host or device memory, and two gloo ranks sharing the
-GPU (their kernels never wait on one another: the exchange is on the host)."""
+"""x-slab decomposition on the GPU: the reach of one step and of one stage,
+and slabs that must reproduce the undivided domain bit for bit (FP64, both
+reconstructions), with overlap planes exchanged once per step or after every
+stage and staged through host or device memory, and two gloo ranks sharing
+the GPU (their kernels never wait on one another: the exchange is on the
+host)."""
 import os
 import socket
 import sys
@@ -99,6 +100,139 @@ def test_slabs_ppm_bit_identical(fsl):
         ss.step(6)
         got = ss.download_state()
     _same(got, ref, "PPM slabs after 6 steps")
+
+
+def _perturbed_reach(a, b, mid):
+    changed = np.nonzero(np.any(a != b, axis=1))[0] + 1
+    return int(np.max(np.abs(changed - mid)))
+
+
+@pytest.mark.parametrize("recon", [0, 1])
+def test_reach_of_one_stage(fsl, recon):
+    """A change in one plane of U^n moves no plane of the stage-1 output
+    farther than STAGE_RADIUS (through the x-stencil and the SGS viscosity),
+    and a change in one plane of the stage-1 output moves no plane of the
+    stage-2 output farther either."""
+    from freeshearlayer_b200.slabs import STAGE_RADIUS
+    p, s = _case(fsl, 1, recon, L=40)
+    P = p["HIG"] * 5 * p["DEP"]
+    L, mid = p["LEN"], 20
+    rng = np.random.default_rng(3)
+    base = s.reshape(L, P)
+    pert = base.copy()
+    pert[mid - 1] *= 1.0 + 1e-3 * rng.random(P)
+    f1 = 1.0 + 1e-3 * rng.random(P)
+    st1, st2 = [], []
+    for st in (base, pert, base):
+        d = fsl.Domain(p)
+        d.upload_state(st.ravel())
+        d.courant_prepare()
+        d.set_courant_max(1.0)
+        d.step_stage()
+        st1.append(d.get_planes(1, L, np.empty(L * P)).reshape(L, P))
+        if len(st1) == 3:           # perturb the stage state itself
+            q = d.get_planes(mid, 1, np.empty(P)) * f1
+            d.set_planes(mid, 1, q)
+        d.step_stage()
+        st2.append(d.get_planes(1, L, np.empty(L * P)).reshape(L, P))
+        d.step_stage()
+        d.close()
+    r1 = _perturbed_reach(st1[0], st1[1], mid)
+    r2 = _perturbed_reach(st2[0], st2[2], mid)
+    print("stage reach recon=%d: stage 1 %d, stage 2 %d" % (recon, r1, r2))
+    assert 2 <= r1 <= STAGE_RADIUS[recon]
+    assert 2 <= r2 <= STAGE_RADIUS[recon]
+
+
+@pytest.mark.parametrize("setup,recon,nslabs", [(1, 0, 2), (1, 0, 3), (0, 0, 3), (1, 1, 3), (0, 1, 2)])
+def test_stage_exchange_bit_identical(fsl, setup, recon, nslabs):
+    """Overlap planes refreshed after every stage (4 planes instead of 8 or
+    10): the owned planes stay bit-identical to the undivided domain."""
+    from freeshearlayer_b200.slabs import STAGE_RADIUS, SlabSet
+    p, s = _case(fsl, setup, recon, L=44)
+    ref, dt = _whole(fsl, p, s, 8)
+    with SlabSet(p, nslabs, exchange="stage") as ss:
+        assert ss.W == STAGE_RADIUS[recon]
+        ss.upload_state(s)
+        ss.step(8)
+        got = ss.download_state()
+        assert all(d.info().deltaT == dt for d in ss.domains)
+    _same(got, ref, "%d slabs, per-stage exchange, recon %d" % (nslabs, recon))
+
+
+def test_stage_exchange_device_staging_fp32(fsl):
+    """Per-stage exchange through CUDA tensors, FP32 bulk: agreement to
+    rounding (the x-march starts at other planes)."""
+    from freeshearlayer_b200.slabs import SlabSet
+    p, s = _case(fsl, 1)
+    p = dict(p, precision=1)
+    ref, _ = _whole(fsl, p, s, 8)
+    with SlabSet(p, 3, staging="device", exchange="stage") as ss:
+        ss.upload_state(s)
+        ss.step(8)
+        got = ss.download_state()
+    a = got.reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    b = ref.reshape(p["LEN"], p["HIG"], 5, p["DEP"])
+    for v in (0, 4):
+        assert np.linalg.norm(a[:, :, v] - b[:, :, v]) / np.linalg.norm(b[:, :, v]) < 1e-7
+
+
+def _closure_setup(fsl, d):
+    dU = 2.0 * 0.4 * (1.4 * 1e5) ** 0.5
+    d.closure_set_scales(1.0 / dU, 1.0)
+    d.closure_set_weights(fsl.closure_weights())
+
+
+@pytest.mark.parametrize("prec,sgs,recon", [(0, 0, 0), (0, 0, 1), (1, 0, 0), (1, 1, 0)])
+def test_step_stage_equals_step(fsl, prec, sgs, recon):
+    """Three stage calls do exactly what one fsl_step does."""
+    p, s = _case(fsl, 1, recon)
+    p = dict(p, precision=prec, sgs=sgs)
+    outs = []
+    for staged in (False, True):
+        d = fsl.Domain(p)
+        if sgs:
+            _closure_setup(fsl, d)
+        d.upload_state(s)
+        for _ in range(4):
+            if staged:
+                for _s in range(3):
+                    d.step_stage()
+            else:
+                d.step(1)
+        outs.append((d.download_state(), d.info().deltaT))
+        d.close()
+    _same(outs[1][0], outs[0][0], "stage calls vs fsl_step")
+    assert outs[1][1] == outs[0][1]
+
+
+def test_step_stage_protocol(fsl):
+    p, s = _case(fsl, 1, L=32)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    d.step_stage()
+    with pytest.raises(fsl.FslError):
+        d.step(1)                   # a step is in progress
+    with pytest.raises(fsl.FslError):
+        d.step_phased(1)
+    d.upload_state(s)               # abandons it (its dt rescale and step count stand)
+    d.step(1)
+    a = d.download_state()
+    d.close()
+    d = fsl.Domain(p)               # the same begun steps, the first one completed
+    d.upload_state(s)
+    d.step(1)
+    d.upload_state(s)
+    d.step(1)
+    ref = d.download_state()
+    d.close()
+    _same(a, ref, "after an abandoned step")
+    q = dict(p, nStages=2)
+    d = fsl.Domain(q)
+    d.upload_state(s)
+    with pytest.raises(fsl.FslError):
+        d.step_stage()              # the fused stages are RK3
+    d.close()
 
 
 def test_slabs_against_the_oracle(fsl, oracle_lib):
@@ -223,7 +357,7 @@ def _free_port() -> int:
         return so.getsockname()[1]
 
 
-def _rank_main(rank, world, port, q):
+def _rank_main(rank, world, port, q, exchange="step"):
     import datetime
 
     import torch.distributed as dist
@@ -234,7 +368,7 @@ def _rank_main(rank, world, port, q):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
         p, s = _case(fsl, 1)
-        ds = DistributedSlab(p)
+        ds = DistributedSlab(p, exchange=exchange)
         ds.upload_state(s)
         ds.step(6)
         full = ds.gather_state(0)
@@ -244,12 +378,13 @@ def _rank_main(rank, world, port, q):
         dist.destroy_process_group()
 
 
-def test_distributed_slabs_gloo_one_gpu(fsl):
+@pytest.mark.parametrize("exchange", ["step", "stage"])
+def test_distributed_slabs_gloo_one_gpu(fsl, exchange):
     import torch.multiprocessing as mp
     world, port = 2, _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, q, exchange)) for r in range(world)]
     for pr in procs:
         pr.start()
     res = [q.get(timeout=300) for _ in range(world)]

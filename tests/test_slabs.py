@@ -1,9 +1,9 @@
 """x-slab decomposition, host logic on CPU: the layout, the exchange plan and
-the per-step protocol (Courant maximum combined across slabs, overlap planes
-refreshed from the neighbours) of SlabSet and of DistributedSlab over gloo
-ranks, driven on a stand-in context whose step is an x-stencil of the same
-reach.  Every owned plane must come out bit-identical to the undivided
-domain's."""
+the per-step and per-stage protocols (Courant maximum combined across slabs,
+overlap planes refreshed from the neighbours) of SlabSet and of
+DistributedSlab over gloo ranks, driven on a stand-in context whose stages are
+x-stencils of the same reach.  Every owned plane must come out bit-identical
+to the undivided domain's."""
 import os
 import socket
 import sys
@@ -15,22 +15,31 @@ import torch.multiprocessing as mp
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+# sub-steps of the three-point stencil per stage: one stage reaches at most
+# STAGE_RADIUS planes, one step RADIUS
+TOY_STAGES = {0: (4, 2, 2), 1: (4, 3, 3)}
+
+
 class ToyDomain:
     """Stand-in for a slab context with the methods the slab drivers use.
     One step: deltaT rescaled to maxCoNum by the Courant maximum (max |u| dt,
-    over the Courant range), then RADIUS sub-steps of a three-point x stencil,
-    with the setup's x boundary (periodic in the temporal setup; an inflow
-    plane of ones and a zero-gradient outflow in the spatial one) and, like
-    the SGS filter's zero bands, a treatment of its own for the first and
-    last plane, periodic or not; after the step the maximum of the new state
-    is kept, as the fused final stage does."""
+    over the Courant range), then three stages, each a few sub-steps of a
+    three-point x stencil with the setup's x boundary (periodic in the
+    temporal setup; an inflow plane of ones and a zero-gradient outflow in the
+    spatial one) and, like the SGS filter's zero bands, a treatment of its own
+    for the first and last plane, periodic or not; stages 2 and 3 are combined
+    with U^n plane by plane like the RK stages.  After the step the maximum of
+    the new state is kept, as the fused final stage does.  get_planes /
+    set_planes act on the stage state in the middle of a step."""
 
     def __init__(self, p):
-        from freeshearlayer_b200.slabs import RADIUS
+        from freeshearlayer_b200.slabs import RADIUS, STAGE_RADIUS
         self.L, self.plane = p.LEN, p.HIG * 5 * p.DEP
         self.periodic = p.setup == 1
-        self.R = RADIUS[p.recon]
+        self.stages = TOY_STAGES[p.recon]
+        assert sum(self.stages) == RADIUS[p.recon] and max(self.stages) == STAGE_RADIUS[p.recon]
         self.u = np.zeros((self.L, self.plane))
+        self.v, self.next = None, 0
         self.dt, self.maxco = p.deltaT, p.maxCoNum
         self.co0, self.co1, self.co = 1, self.L, None
 
@@ -45,15 +54,18 @@ class ToyDomain:
 
     def upload_state(self, s):
         self.u = np.asarray(s, np.float64).reshape(self.L, self.plane).copy()
-        self.co = None
+        self.co, self.next = None, 0
+
+    def _cur(self):
+        return self.v if self.next else self.u
 
     def get_planes(self, i0, n, out):
-        out[:n * self.plane] = self.u[i0 - 1:i0 - 1 + n].ravel()
+        out[:n * self.plane] = self._cur()[i0 - 1:i0 - 1 + n].ravel()
         return out
 
     def set_planes(self, i0, n, buf):
-        self.u[i0 - 1:i0 - 1 + n] = np.asarray(buf[:n * self.plane]).reshape(n, self.plane)
-        if i0 <= self.co1 and i0 + n - 1 >= self.co0:
+        self._cur()[i0 - 1:i0 - 1 + n] = np.asarray(buf[:n * self.plane]).reshape(n, self.plane)
+        if not self.next and i0 <= self.co1 and i0 + n - 1 >= self.co0:
             self.co = None
 
     def _owned_max(self):
@@ -70,25 +82,45 @@ class ToyDomain:
     def set_courant_max(self, m):
         self.co = m
 
+    def step_stage(self):
+        slab = (self.co0, self.co1) != (1, self.L)
+        if self.next == 0:
+            if slab and self.co is None:
+                raise RuntimeError("x-slab: no combined maximum")
+            m = self.co if self.co is not None else self._owned_max()
+            self.dt = self.dt * (self.maxco / m)
+            self.v = self.u.copy()
+        s = self.next
+        v, c = self.v, self.dt
+        for _ in range(self.stages[s]):
+            g = np.empty((self.L + 2, self.plane))
+            g[1:-1] = v
+            if self.periodic:
+                g[0], g[-1] = v[-1], v[0]
+            else:
+                g[0], g[-1] = 1.0, v[-1]
+            v = v + c * (g[:-2] - 2.0 * v + g[2:])
+            v[0] *= 0.999
+            v[-1] *= 1.001
+        if s == 1:
+            v = 0.75 * self.u + 0.25 * v
+        elif s == 2:
+            v = self.u / 3.0 + 2.0 / 3.0 * v
+        if s == 2:
+            self.u, self.v, self.next = v, None, 0
+            self.co = self._owned_max()
+        else:
+            self.v, self.next = v, s + 1
+
     def step(self, n=1):
         slab = (self.co0, self.co1) != (1, self.L)
+        if self.next:
+            raise RuntimeError("a step is in progress")
         if slab and (n > 1 or self.co is None):
             raise RuntimeError("x-slab: one step per call, after a combined maximum")
         for _ in range(n):
-            m = self.co if self.co is not None else self._owned_max()
-            self.dt = self.dt * (self.maxco / m)
-            c = self.dt
-            for _ in range(self.R):
-                g = np.empty((self.L + 2, self.plane))
-                g[1:-1] = self.u
-                if self.periodic:
-                    g[0], g[-1] = self.u[-1], self.u[0]
-                else:
-                    g[0], g[-1] = 1.0, self.u[-1]
-                self.u = self.u + c * (g[:-2] - 2.0 * self.u + g[2:])
-                self.u[0] *= 0.999
-                self.u[-1] *= 1.001
-            self.co = self._owned_max()
+            for _s in range(3):
+                self.step_stage()
 
     step_phased = step
 
@@ -163,6 +195,52 @@ def test_slabset_matches_whole_domain(setup, nslabs):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("recon", [0, 1])
+@pytest.mark.parametrize("setup", [1, 0])
+@pytest.mark.parametrize("nslabs", [2, 3, 4])
+def test_stage_exchange_matches_whole_domain(setup, nslabs, recon):
+    from freeshearlayer_b200.slabs import STAGE_RADIUS, SlabSet
+    p = _params(setup, recon=recon)
+    s0 = _state(p)
+    ref, dt = _whole(p, s0, 6)
+    with SlabSet(p, nslabs, domain_factory=ToyDomain, exchange="stage") as ss:
+        assert ss.W == STAGE_RADIUS[recon]
+        ss.upload_state(s0)
+        ss.step(6)
+        got = ss.download_state()
+        assert all(d.dt == dt for d in ss.domains)
+    assert np.array_equal(got, ref)
+
+
+def test_stage_overlap_exchanged_once_per_step_goes_wrong():
+    """The check has teeth: the narrow per-stage overlap, refreshed only after
+    the whole step, is too narrow."""
+    from freeshearlayer_b200.slabs import SlabSet
+    p = _params(1)
+    s0 = _state(p)
+    ref, _ = _whole(p, s0, 3)
+    with SlabSet(p, 3, domain_factory=ToyDomain, exchange="stage") as ss:
+        ss.upload_state(s0)
+        for _ in range(3):
+            ss.combine_courant()
+            for d in ss.domains:
+                d.step(1)
+            ss.exchange()
+        assert not np.array_equal(ss.download_state(), ref)
+
+
+def test_stage_exchange_arguments():
+    from freeshearlayer_b200.slabs import SlabSet
+    with pytest.raises(ValueError):
+        SlabSet(_params(1), 2, overlap=3, domain_factory=ToyDomain, exchange="stage")
+    with pytest.raises(ValueError):
+        SlabSet(_params(1), 2, domain_factory=ToyDomain, exchange="plane")
+    with SlabSet(_params(1), 2, domain_factory=ToyDomain, exchange="stage") as ss:
+        ss.upload_state(_state(_params(1)))
+        with pytest.raises(ValueError):
+            ss.step(1, phased=True)
+
+
 def test_without_exchange_the_slabs_go_wrong():
     """The check has teeth: a slab set that skips the overlap refresh differs."""
     from freeshearlayer_b200.slabs import SlabSet
@@ -199,7 +277,7 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, setup, steps, q):
+def _rank_main(rank, world, port, setup, steps, q, exchange="step"):
     import datetime
 
     import torch.distributed as dist
@@ -211,7 +289,7 @@ def _rank_main(rank, world, port, setup, steps, q):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         p = _params(setup)
-        ds = DistributedSlab(p, domain_factory=ToyDomain)
+        ds = DistributedSlab(p, domain_factory=ToyDomain, exchange=exchange)
         ds.upload_state(_state(p))
         ds.step(steps)
         full = ds.gather_state(0)
@@ -220,13 +298,15 @@ def _rank_main(rank, world, port, setup, steps, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,setup", [(2, 1), (3, 1), (2, 0), (3, 0)])
-def test_distributed_gloo_matches_whole_domain(world, setup):
+@pytest.mark.parametrize("world,setup,exchange", [(2, 1, "step"), (3, 1, "step"), (2, 0, "step"), (3, 0, "step"),
+                                                  (3, 1, "stage"), (2, 0, "stage")])
+def test_distributed_gloo_matches_whole_domain(world, setup, exchange):
     steps = 5
     port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, setup, steps, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, setup, steps, q, exchange))
+             for r in range(world)]
     for pr in procs:
         pr.start()
     for pr in procs:
