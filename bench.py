@@ -461,6 +461,47 @@ def ensemble_block(fsl, torch, steps, n):
             "speedup": (ens_units / ens_ms) / (units / seq_ms), "bit_identical": bool(same)}
 
 
+def slab_block(fsl, torch, grid, state, dU, steps, nslabs, warmup):
+    """The FP64 domain split into x-slabs on one GPU (overlap planes through
+    device buffers), with the overlap exchanged once per step and after every
+    stage, against the undivided domain.  The exchanges synchronise with the
+    host, so all three arms are timed by the host clock around
+    torch.cuda.synchronize(); the owned planes are compared bitwise."""
+    import time
+
+    import numpy as np
+
+    from freeshearlayer_b200.slabs import SlabSet
+    p = workload_params(grid)
+    ncell = grid[0] * grid[1] * grid[2]
+    out = {"path": ARM_NAMES["fp64-dynamic"], "slabs": nslabs, "staging": "device", "steps": steps,
+           "timing": "host clock around torch.cuda.synchronize()"}
+
+    def timed(run):
+        for _ in range(warmup):
+            run(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run(steps)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3
+
+    d = make_domain(fsl, grid, "fp64-dynamic", state, dU)
+    ms = timed(d.step)
+    ref = d.download_state()
+    d.close()
+    out["whole"] = {"ms_per_step": ms / steps, "value": ncell * STAGES * steps / (ms * 1e-3)}
+    for mode in ("step", "stage"):
+        with SlabSet(p, nslabs, staging="device", exchange=mode) as ss:
+            ss.upload_state(state)
+            ms = timed(ss.step)
+            same = bool(np.array_equal(ss.download_state(), ref))
+            out[mode] = {"overlap": ss.W, "ms_per_step": ms / steps,
+                         "value": ncell * STAGES * steps / (ms * 1e-3), "bit_identical": same,
+                         "planes_stepped": int(sum(x.local_len for x in ss.slabs))}
+    return out
+
+
 def max_over_ranks(torch, dist, x, device="cuda"):
     """The job's time: the maximum of x over all ranks (x itself without a
     process group)."""
@@ -604,6 +645,11 @@ def main_gpu(args):
     if rank == 0 and args.ens_steps > 1:
         ens = ensemble_block(fsl, torch, args.ens_steps, args.ens_members)
 
+    # ---- x-slabs on one GPU: overlap exchanged per step or per stage ----
+    slabs = None
+    if rank == 0 and world == 1 and args.slab_steps > 0:
+        slabs = slab_block(fsl, torch, grid, state, dU, args.slab_steps, args.slabs, args.warmup)
+
     # ---- CPU baseline: the reference's serial solver, rank 0 at N = 1 only ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -647,6 +693,8 @@ def main_gpu(args):
             line["matched_error"] = match
         if ens is not None:
             line["ensemble"] = ens
+        if slabs is not None:
+            line["slabs"] = slabs
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -705,6 +753,9 @@ def main():
                     help="steps timed with PPM reconstruction (FP32 + closure and FP64); 0 skips them")
     ap.add_argument("--ens-steps", type=int, default=100, help="steps of the ensemble comparison (0: skip)")
     ap.add_argument("--ens-members", type=int, default=32)
+    ap.add_argument("--slab-steps", type=int, default=0,
+                    help="steps of the x-slab comparison on one GPU (0: skip)")
+    ap.add_argument("--slabs", type=int, default=2)
     ap.add_argument("--match-steps", type=int, default=200,
                     help="steps of the matched-error comparison against the plain FP64 path (0: skip)")
     ap.add_argument("--traffic", type=float, default=None,

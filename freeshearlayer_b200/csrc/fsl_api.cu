@@ -1165,7 +1165,7 @@ int fsl_sums(fsl_ctx *h, double sums[5])
     if (!h || !sums) return FSL_ERR_ARG;
     Ctx &c = h->c;
     double *d = c.partials + 4000;
-    launch_sums(c, c.U, d);
+    launch_sums(c, c.U, c.co_i0, c.co_i1 - c.co_i0 + 1, d);
     CKL();
     CK(cudaMemcpyAsync(sums, d, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
@@ -1177,7 +1177,7 @@ int fsl_plane_sums(fsl_ctx *h, double *rows)
     if (!h || !rows) return FSL_ERR_ARG;
     Ctx &c = h->c;
     double *d = c.stage_dev; // scratch: 8*HIG <= LEN*HIG*5*DEP
-    launch_plane_sums(c, c.U, d);
+    launch_plane_sums(c, c.U, c.co_i0, c.co_i1 - c.co_i0 + 1, d);
     CKL();
     CK(cudaMemcpyAsync(rows, d, 8 * (size_t)c.p.HIG * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));

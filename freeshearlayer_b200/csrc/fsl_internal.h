@@ -195,8 +195,8 @@ void launch_courant_apply(Ctx &c);
 void launch_state_scatter(Ctx &c, double *dst, const double *packed, int i0, int ni);
 void launch_state_gather(Ctx &c, const double *src, double *packed, int i0, int ni);
 void launch_courant_to_bits(Ctx &c);
-void launch_sums(Ctx &c, const double *U, double *out5);
-void launch_plane_sums(Ctx &c, const double *U, double *rows);
+void launch_sums(Ctx &c, const double *U, int i0, int ni, double *out5);
+void launch_plane_sums(Ctx &c, const double *U, int i0, int ni, double *rows);
 
 // ---- fused path (fsl_fused.cu) ----------------------------------------------
 void launch_bface(Ctx &c, const double *cur, const Disturb &d);

@@ -527,17 +527,18 @@ __global__ void k_state_gather(Grid g, const double *__restrict__ src, double *_
     }
 }
 
-// Deterministic block partial sums of the five conserved variables.
-__global__ void k_sums_partial(Grid g, const double *__restrict__ U, double *__restrict__ partials)
+// Deterministic block partial sums of the five conserved variables over
+// the interior planes i0 .. i0+ni-1.
+__global__ void k_sums_partial(Grid g, int i0, int ni, const double *__restrict__ U, double *__restrict__ partials)
 {
-    const long long n = (long long)g.L * g.H * g.D;
+    const long long n = (long long)ni * g.H * g.D;
     double s[5] = {0, 0, 0, 0, 0};
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t % g.D) + 1;
         const long long r = t / g.D;
         const int j = (int)(r % g.H) + 1;
-        const int i = (int)(r / g.H) + 1;
+        const int i = (int)(r / g.H) + i0;
         const long long c = g.idx(i, j, k);
 #pragma unroll
         for (int q = 0; q < 5; q++) s[q] += U[q * g.fstride + c];
@@ -568,16 +569,16 @@ __global__ void k_sums_final(const double *__restrict__ partials, int np, double
     }
 }
 
-// One block per y row: sums over the x-z plane of rho, rho u, rho v, rho w,
-// rho uu, rho vv, rho ww, rho uv.
-__global__ void k_plane_sums(Grid g, const double *__restrict__ U, double *__restrict__ rows)
+// One block per y row: sums over the x-z plane (interior planes i0 ..
+// i0+ni-1) of rho, rho u, rho v, rho w, rho uu, rho vv, rho ww, rho uv.
+__global__ void k_plane_sums(Grid g, int i0, int ni, const double *__restrict__ U, double *__restrict__ rows)
 {
     const int j = blockIdx.x + 1;
-    const long long n = (long long)g.L * g.D;
+    const long long n = (long long)ni * g.D;
     double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (long long t = threadIdx.x; t < n; t += blockDim.x) {
         const int k = (int)(t % g.D) + 1;
-        const int i = (int)(t / g.D) + 1;
+        const int i = (int)(t / g.D) + i0;
         const long long c = g.idx(i, j, k);
         const double r = U[c], u = U[g.fstride + c] / r, v = U[2 * g.fstride + c] / r,
                      w = U[3 * g.fstride + c] / r;
@@ -709,11 +710,11 @@ void launch_state_gather(Ctx &c, const double *src, double *packed, int i0, int 
     prof_end(c, FSL_K_OTHER, 1);
 }
 
-void launch_sums(Ctx &c, const double *U, double *out5)
+void launch_sums(Ctx &c, const double *U, int i0, int ni, double *out5)
 {
     const int nb = 148 * 4;
     prof_begin(c, FSL_K_OTHER);
-    k_sums_partial<<<nb, 256, 0, c.stream>>>(c.g, U, c.partials);
+    k_sums_partial<<<nb, 256, 0, c.stream>>>(c.g, i0, ni, U, c.partials);
     const double vol = c.p.deltaX * c.p.deltaY * c.p.deltaZ;
     k_sums_final<<<1, 32, 0, c.stream>>>(c.partials, nb, vol, out5);
     prof_end(c, FSL_K_OTHER, 2);
@@ -729,10 +730,10 @@ void launch_judge_rows(Ctx &c, const float *a, const float *b, double *rows) { j
 void launch_judge_rows(Ctx &c, const float *a, const double *b, double *rows) { judge_rows_t(c, a, b, rows); }
 void launch_judge_rows(Ctx &c, const double *a, const double *b, double *rows) { judge_rows_t(c, a, b, rows); }
 
-void launch_plane_sums(Ctx &c, const double *U, double *rows)
+void launch_plane_sums(Ctx &c, const double *U, int i0, int ni, double *rows)
 {
     prof_begin(c, FSL_K_OTHER);
-    k_plane_sums<<<c.g.H, 256, 0, c.stream>>>(c.g, U, rows);
+    k_plane_sums<<<c.g.H, 256, 0, c.stream>>>(c.g, i0, ni, U, rows);
     prof_end(c, FSL_K_OTHER, 1);
 }
 

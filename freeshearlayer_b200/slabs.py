@@ -329,6 +329,27 @@ class SlabSet:
             with self._on(s.index):
                 d.sync()
 
+    # --- integrals over the whole domain ---------------------------------------------
+    def sums(self) -> np.ndarray:
+        """Volume integrals of the conserved variables: each slab's over its
+        owned planes, added (slab order; equal to the undivided domain's to
+        rounding)."""
+        out = None
+        for s, d in zip(self.slabs, self.domains):
+            with self._on(s.index):
+                x = d.sums()
+            out = x if out is None else out + x
+        return out
+
+    def plane_sums(self) -> np.ndarray:
+        """Per y-row sums over the owned x-z planes, added across slabs."""
+        out = None
+        for s, d in zip(self.slabs, self.domains):
+            with self._on(s.index):
+                x = d.plane_sums()
+            out = x if out is None else out + x
+        return out
+
 
 def device_scalar(ptr: int, device: int):
     """A one-element int64 CUDA tensor over device memory at `ptr` (not owned)."""
@@ -410,6 +431,24 @@ class DistributedSlab:
         return out.reshape(-1)
 
     # --- one step -----------------------------------------------------------------
+    def _sum_all(self, x: np.ndarray) -> np.ndarray:
+        import torch
+        import torch.distributed as dist
+        t = torch.from_numpy(np.ascontiguousarray(x, np.float64).ravel())
+        if self.on_device:
+            t = t.cuda()
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+        return t.cpu().numpy().reshape(np.shape(x))
+
+    def sums(self) -> np.ndarray:
+        """Volume integrals of the conserved variables over the whole domain:
+        the owned planes' integrals, all-reduced with SUM on every rank."""
+        return self._sum_all(self.dom.sums())
+
+    def plane_sums(self) -> np.ndarray:
+        """Per y-row sums over all x-z planes, all-reduced with SUM."""
+        return self._sum_all(self.dom.plane_sums())
+
     def combine_courant(self):
         """The owned Courant maximum, combined by an all-reduce MAX
         (src-par/helpers.c:44)."""

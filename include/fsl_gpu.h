@@ -462,6 +462,9 @@ void *fsl_stream(fsl_ctx *ctx);
 
 /* ---- diagnostics ----------------------------------------------------------- */
 
+/* Both over the planes of the Courant range (fsl_set_courant_range): the
+ * whole interior, or an x-slab's owned planes, whose results add up across
+ * the slabs (the SUM all-reduce of the distributed variant's integrals). */
 /* Volume integrals of rho, rho u, rho v, rho w, E over the interior (FP64). */
 int fsl_sums(fsl_ctx *ctx, double sums[5]);
 /* Per y-row sums over the interior x-z plane of rho, rho u, rho v, rho w,

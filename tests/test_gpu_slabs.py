@@ -235,6 +235,26 @@ def test_step_stage_protocol(fsl):
     d.close()
 
 
+def test_slab_sums_add_up(fsl):
+    """Volume integrals and per-row sums over the owned planes, added across
+    slabs, equal the undivided domain's to rounding (another summation
+    order); an overlap plane counted twice would be off by far more."""
+    from freeshearlayer_b200.slabs import SlabSet
+    p, s = _case(fsl, 1)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    d.step(3)
+    ref_s, ref_r = d.sums(), d.plane_sums()
+    d.close()
+    with SlabSet(p, 3) as ss:
+        ss.upload_state(s)
+        ss.step(3)
+        got = ss.sums()
+        np.testing.assert_allclose(got[[0, 4]], ref_s[[0, 4]], rtol=1e-12)      # mass, energy
+        np.testing.assert_allclose(got, ref_s, rtol=0, atol=1e-12 * np.abs(ref_s).max())
+        np.testing.assert_allclose(ss.plane_sums(), ref_r, rtol=1e-12, atol=1e-12 * np.abs(ref_r).max())
+
+
 def test_slabs_against_the_oracle(fsl, oracle_lib):
     """Three slabs against the CPU oracle of the undivided domain."""
     from freeshearlayer_b200.slabs import SlabSet

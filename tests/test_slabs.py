@@ -68,6 +68,12 @@ class ToyDomain:
         if not self.next and i0 <= self.co1 and i0 + n - 1 >= self.co0:
             self.co = None
 
+    def sums(self):
+        return self.u[self.co0 - 1:self.co1].sum(axis=0)[:5]
+
+    def plane_sums(self):
+        return self.u[self.co0 - 1:self.co1].sum(axis=0).reshape(-1, 2)
+
     def _owned_max(self):
         return float(np.max(np.abs(self.u[self.co0 - 1:self.co1]) * self.dt))
 
@@ -212,6 +218,19 @@ def test_stage_exchange_matches_whole_domain(setup, nslabs, recon):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("setup", [1, 0])
+def test_slab_sums_add_up(setup):
+    from freeshearlayer_b200.slabs import SlabSet
+    p = _params(setup)
+    s0 = _state(p)
+    whole = ToyDomain(p)
+    whole.upload_state(s0)
+    with SlabSet(p, 3, domain_factory=ToyDomain) as ss:
+        ss.upload_state(s0)
+        np.testing.assert_allclose(ss.sums(), whole.sums(), rtol=1e-13)
+        np.testing.assert_allclose(ss.plane_sums(), whole.plane_sums(), rtol=1e-13)
+
+
 def test_stage_overlap_exchanged_once_per_step_goes_wrong():
     """The check has teeth: the narrow per-stage overlap, refreshed only after
     the whole step, is too narrow."""
@@ -293,7 +312,8 @@ def _rank_main(rank, world, port, setup, steps, q, exchange="step"):
         ds.upload_state(_state(p))
         ds.step(steps)
         full = ds.gather_state(0)
-        q.put((rank, ds.dom.dt, None if full is None else full.tolist()))
+        sums = ds.sums()
+        q.put((rank, ds.dom.dt, None if full is None else full.tolist(), sums.tolist()))
     finally:
         dist.destroy_process_group()
 
@@ -317,3 +337,7 @@ def test_distributed_gloo_matches_whole_domain(world, setup, exchange):
     ref, dt = _whole(p, _state(p), steps)
     assert all(r[1] == dt for r in res)
     assert np.array_equal(np.array(res[0][2]), ref)
+    whole = ToyDomain(p)
+    whole.upload_state(ref)
+    for r in res:                   # the SUM all-reduce gives every rank the whole
+        np.testing.assert_allclose(r[3], whole.sums(), rtol=1e-13)
