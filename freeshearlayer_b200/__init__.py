@@ -161,6 +161,7 @@ def lib():
         })
         sig.update({
             "fsl_get_planes": [vp, i, i, vp], "fsl_set_planes": [vp, i, i, vp],
+            "fsl_get_planes_async": [vp, i, i, vp], "fsl_set_planes_async": [vp, i, i, vp],
             "fsl_set_courant_range": [vp, i, i], "fsl_courant_prepare": [vp],
             "fsl_upload_state_async": [vp, _dp], "fsl_download_state_async": [vp, _dp], "fsl_transfer_wait": [vp],
             "fsl_get_courant_max": [vp, C.POINTER(C.c_double)], "fsl_set_courant_max": [vp, d],
@@ -349,6 +350,15 @@ class Domain:
 
     def set_planes(self, i0: int, n: int, buf):
         self._c(lib().fsl_set_planes(self.h, i0, n, _buffer_ptr(buf, n * self.plane_size())))
+
+    def get_planes_async(self, i0: int, n: int, out):
+        """get_planes queued on the domain's stream without waiting (`out`: a
+        CUDA tensor, or pinned host memory)."""
+        self._c(lib().fsl_get_planes_async(self.h, i0, n, _buffer_ptr(out, n * self.plane_size())))
+        return out
+
+    def set_planes_async(self, i0: int, n: int, buf):
+        self._c(lib().fsl_set_planes_async(self.h, i0, n, _buffer_ptr(buf, n * self.plane_size())))
 
     def set_courant_range(self, i0: int, i1: int):
         self._c(lib().fsl_set_courant_range(self.h, i0, i1))

@@ -595,7 +595,9 @@ static double *stage_state(Ctx &c)
     return c.stage_next == 2 ? c.Up : c.stage_next == 3 ? c.Uq : c.U;
 }
 
-int fsl_get_planes(fsl_ctx *h, int i0, int n, double *buf)
+// gather planes i0.. of the current stage state into buf, queued on the
+// context's stream (the one scratch buffer is reused in stream order)
+static int get_planes_q(fsl_ctx *h, int i0, int n, double *buf)
 {
     if (!h || !buf || !planes_ok(h->c, i0, n)) return FSL_ERR_ARG;
     Ctx &c = h->c;
@@ -604,11 +606,10 @@ int fsl_get_planes(fsl_ctx *h, int i0, int n, double *buf)
     launch_state_gather(c, stage_state(c), c.stage_dev, i0, n);
     CKL();
     if (bytes) CK(cudaMemcpyAsync(buf, c.stage_dev, bytes, cudaMemcpyDefault, c.stream));
-    CK(cudaStreamSynchronize(c.stream));
     return FSL_OK;
 }
 
-int fsl_set_planes(fsl_ctx *h, int i0, int n, const double *buf)
+static int set_planes_q(fsl_ctx *h, int i0, int n, const double *buf)
 {
     if (!h || !buf || !planes_ok(h->c, i0, n)) return FSL_ERR_ARG;
     Ctx &c = h->c;
@@ -619,9 +620,30 @@ int fsl_set_planes(fsl_ctx *h, int i0, int n, const double *buf)
     if (bytes) CK(cudaMemcpyAsync(c.stage_dev, buf, bytes, cudaMemcpyDefault, c.stream));
     launch_state_scatter(c, stage_state(c), c.stage_dev, i0, n);
     CKL();
+    return FSL_OK;
+}
+
+int fsl_get_planes(fsl_ctx *h, int i0, int n, double *buf)
+{
+    const int rc = get_planes_q(h, i0, n, buf);
+    if (rc) return rc;
+    Ctx &c = h->c;
     CK(cudaStreamSynchronize(c.stream));
     return FSL_OK;
 }
+
+int fsl_set_planes(fsl_ctx *h, int i0, int n, const double *buf)
+{
+    const int rc = set_planes_q(h, i0, n, buf);
+    if (rc) return rc;
+    Ctx &c = h->c;
+    CK(cudaStreamSynchronize(c.stream));
+    return FSL_OK;
+}
+
+int fsl_get_planes_async(fsl_ctx *h, int i0, int n, double *buf) { return get_planes_q(h, i0, n, buf); }
+
+int fsl_set_planes_async(fsl_ctx *h, int i0, int n, const double *buf) { return set_planes_q(h, i0, n, buf); }
 
 int fsl_set_courant_range(fsl_ctx *h, int i0, int i1)
 {

@@ -186,7 +186,10 @@ class SlabSet:
     devices: one CUDA device index per slab (default: all on the current
     device).  staging "host" moves overlap planes through numpy arrays;
     "device" through CUDA tensors (peer copies between devices) and combines
-    the Courant maximum in device memory.  exchange "step" refreshes the
+    the Courant maximum in device memory.  With device staging on one device
+    the exchange and the combination are ordered between the slabs' streams
+    by CUDA events, without waiting on the host, so the slabs' kernels may
+    also overlap one another.  exchange "step" refreshes the
     overlap planes once per step, "stage" after every stage (a narrower
     default overlap).  domain_factory(params) makes each slab's context
     (default: Domain)."""
@@ -212,6 +215,12 @@ class SlabSet:
                 self.domains.append(d)
         self.plane = p.HIG * 5 * p.DEP
         self._bufs = {}
+        self._read = {}     # per buffer: the event after the set that last read it
+        self._ordered = staging == "device" and self.devices is None
+
+    def _stream(self, r):
+        import torch
+        return torch.cuda.ExternalStream(self.domains[r].stream)
 
     def _on(self, r):
         import contextlib
@@ -254,6 +263,9 @@ class SlabSet:
         for s, d in zip(self.slabs, self.domains):
             with self._on(s.index):
                 d.courant_prepare()
+        if self._ordered:
+            self._combine_courant_ordered()
+            return
         if self.staging == "device":
             self._combine_courant_device()
             return
@@ -280,8 +292,54 @@ class SlabSet:
             t.copy_(m.to(t.device))
         torch.cuda.synchronize()
 
+    def _combine_courant_ordered(self):
+        """The maximum of the slabs' device scalars on the current stream,
+        after each slab's stream has produced its scalar and before any slab
+        stream reads the result."""
+        import torch
+        cur = torch.cuda.current_stream()
+        ts = []
+        for r, d in enumerate(self.domains):
+            ts.append(device_scalar(d.courant_bits_ptr(), torch.cuda.current_device()))
+            ev = torch.cuda.Event()
+            ev.record(self._stream(r))
+            cur.wait_event(ev)
+        # non-negative doubles order like their bit patterns (as int64)
+        m = ts[0].clone()
+        for t in ts[1:]:
+            m = torch.maximum(m, t)
+        for t in ts:
+            t.copy_(m)
+        done = torch.cuda.Event()
+        done.record(cur)
+        for r in range(len(self.domains)):
+            self._stream(r).wait_event(done)
+
+    def _exchange_ordered(self):
+        """Each overlap run: the owner's stream gathers it into a device
+        buffer, the receiver's stream waits for that and scatters it; the next
+        gather into the same buffer waits for the scatter that read it."""
+        import torch
+        for src, i0, dst, j0, n in self.plan:
+            key = (src, dst, i0, n)
+            buf = self._buffer(src, dst, i0, n)
+            ss, ds = self._stream(src), self._stream(dst)
+            if key in self._read:
+                ss.wait_event(self._read[key])
+            self.domains[src].get_planes_async(i0, n, buf)
+            filled = torch.cuda.Event()
+            filled.record(ss)
+            ds.wait_event(filled)
+            self.domains[dst].set_planes_async(j0, n, buf)
+            read = torch.cuda.Event()
+            read.record(ds)
+            self._read[key] = read
+
     def exchange(self):
         if not self.plan:
+            return
+        if self._ordered:
+            self._exchange_ordered()
             return
         staged = []
         for src, i0, dst, j0, n in self.plan:

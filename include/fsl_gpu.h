@@ -189,6 +189,13 @@ int fsl_transfer_wait(fsl_ctx *ctx);
  * can refresh its overlap planes after every stage. */
 int fsl_get_planes(fsl_ctx *ctx, int i0, int n, double *buf);
 int fsl_set_planes(fsl_ctx *ctx, int i0, int n, const double *buf);
+/* The same, queued on the context's stream without waiting (buf: device or
+ * pinned host memory, untouched by the caller until the stream has reached
+ * the copy).  Between contexts the caller orders the streams (fsl_stream and
+ * CUDA events): a set after the get that filled its buffer, the next get into
+ * a buffer after the set that read it. */
+int fsl_get_planes_async(fsl_ctx *ctx, int i0, int n, double *buf);
+int fsl_set_planes_async(fsl_ctx *ctx, int i0, int n, const double *buf);
 /* Planes i0..i1 enter the Courant maximum (default 1..LEN).  A context with a
  * narrower range is an x-slab: fsl_step / fsl_step_phased then take one step
  * per call and need a combined maximum (below) before each; a learned closure

@@ -371,6 +371,27 @@ def test_planes_roundtrip(fsl):
     d.close()
 
 
+def test_planes_async_roundtrip(fsl):
+    """The stream-ordered plane transfers: CUDA tensors, ordered on the
+    domain's stream."""
+    import torch
+    p, s = _case(fsl, 1, L=20)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    P = d.plane_size()
+    buf = torch.empty(3 * P, dtype=torch.float64, device="cuda")
+    d.get_planes_async(5, 3, buf)
+    d.sync()
+    _same(buf.cpu().numpy(), s[4 * P:7 * P], "planes 5..7, queued")
+    buf.mul_(1.01)
+    torch.cuda.synchronize()
+    d.set_planes_async(10, 3, buf)
+    new = s.copy()
+    new[9 * P:12 * P] = s[4 * P:7 * P] * 1.01
+    _same(d.download_state(), new, "after a queued set")
+    d.close()
+
+
 def _free_port() -> int:
     with socket.socket() as so:
         so.bind(("127.0.0.1", 0))
