@@ -179,7 +179,9 @@ int fsl_transfer_wait(fsl_ctx *ctx);
  * (10) keeps the owned planes bit-identical to the undivided domain.  This
  * takes the place of the per-stage ghost-plane messages of
  * src-par/boundCondInGhostCells.c:23-102, src-par/boundCondOnInterfaces.c:20-99
- * and src-par/communication.c:6-93.
+ * and src-par/communication.c:6-93.  Alternatively, as src-par does, the
+ * overlap is refreshed after every stage (fsl_step_stage): one stage reaches
+ * 3 planes (measured), so W >= 4.
  *
  * Planes are 1-based interior x-indices; buffers hold n planes in the
  * upload/download layout ([n][HIG][5][DEP] doubles), host or device memory
@@ -198,8 +200,8 @@ int fsl_get_planes_async(fsl_ctx *ctx, int i0, int n, double *buf);
 int fsl_set_planes_async(fsl_ctx *ctx, int i0, int n, const double *buf);
 /* Planes i0..i1 enter the Courant maximum (default 1..LEN).  A context with a
  * narrower range is an x-slab: fsl_step / fsl_step_phased then take one step
- * per call and need a combined maximum (below) before each; a learned closure
- * must have judgements off. */
+ * per call and, like the first fsl_step_stage of a step, need a combined
+ * maximum (below) before each; a learned closure must have judgements off. */
 int fsl_set_courant_range(fsl_ctx *ctx, int i0, int i1);
 /* Make the owned Courant maximum of U^n available (a reduction, unless the
  * last step's final stage already accumulated it). */
