@@ -438,7 +438,7 @@ def test_distributed_slabs_gloo_one_gpu(fsl, exchange):
     _same(np.frombuffer(full, np.float64), ref, "two gloo ranks")
 
 
-def _nccl_one_rank(port, q):
+def _nccl_one_rank(port, q, exchange="step"):
     import datetime
 
     import torch
@@ -452,28 +452,35 @@ def _nccl_one_rank(port, q):
                             device_id=torch.device("cuda", 0))
     try:
         p, s = _case(fsl, 1)
-        ds = DistributedSlab(p)
+        ds = DistributedSlab(p, exchange=exchange)
         assert ds.on_device
         ds.upload_state(s)
         ds.step(4)
         full = ds.gather_state(0)
-        q.put(full.tobytes())
+        q.put((full.tobytes(), ds.sums().tobytes()))
         ds.close()
     finally:
         dist.destroy_process_group()
 
 
-def test_distributed_slab_nccl_one_rank(fsl):
-    """The NCCL branch of the driver (device buffers, the Courant maximum
-    all-reduced in device memory) on a one-rank group: the undivided domain."""
+@pytest.mark.parametrize("exchange", ["step", "stage"])
+def test_distributed_slab_nccl_one_rank(fsl, exchange):
+    """The NCCL branch of the driver (device buffers, the Courant maximum and
+    the integrals all-reduced in device memory) on a one-rank group: the
+    undivided domain."""
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    pr = ctx.Process(target=_nccl_one_rank, args=(_free_port(), q))
+    pr = ctx.Process(target=_nccl_one_rank, args=(_free_port(), q, exchange))
     pr.start()
-    full = q.get(timeout=300)
+    full, sums = q.get(timeout=300)
     pr.join(60)
     assert pr.exitcode == 0
     p, s = _case(fsl, 1)
-    ref, _ = _whole(fsl, p, s, 4)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    d.step(4)
+    ref, ref_sums = d.download_state(), d.sums()
+    d.close()
     _same(np.frombuffer(full, np.float64), ref, "one NCCL rank")
+    _same(np.frombuffer(sums, np.float64), ref_sums, "integrals, one NCCL rank")
