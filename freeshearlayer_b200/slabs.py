@@ -168,6 +168,8 @@ def exchange_plan(slabs: list[Slab]):
 def _check_overlap(p, overlap, exchange="step"):
     if exchange not in EXCHANGES:
         raise ValueError("exchange: 'step' or 'stage'")
+    if exchange == "stage" and p.nStages != 3:
+        raise ValueError("exchange='stage' steps the fused RK3 stages (nStages = 3)")
     need = (RADIUS if exchange == "step" else STAGE_RADIUS)[p.recon]
     W = need if overlap is None else int(overlap)
     if W < need:

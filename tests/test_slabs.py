@@ -254,6 +254,10 @@ def test_stage_exchange_arguments():
         SlabSet(_params(1), 2, overlap=3, domain_factory=ToyDomain, exchange="stage")
     with pytest.raises(ValueError):
         SlabSet(_params(1), 2, domain_factory=ToyDomain, exchange="plane")
+    q = _params(1)
+    q.nStages = 2
+    with pytest.raises(ValueError):
+        SlabSet(q, 2, domain_factory=ToyDomain, exchange="stage")
     with SlabSet(_params(1), 2, domain_factory=ToyDomain, exchange="stage") as ss:
         ss.upload_state(_state(_params(1)))
         with pytest.raises(ValueError):
