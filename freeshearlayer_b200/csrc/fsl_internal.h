@@ -2,6 +2,7 @@
 // by the translation units of libfsl_gpu.so.  Not part of the C ABI.
 #pragma once
 
+#include <atomic>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
@@ -176,6 +177,21 @@ int ensure_dyn_scratch(Ctx &c);  // SGS scratch of the dynamic procedure + the F
 int closure_step_sgs(Ctx &c);    // SGS of one step under FSL_SGS_LEARNED (fsl_closure.cu)
 int closure_ensure(Ctx &c);
 void closure_free(Ctx &c);
+
+// A kernel's dynamic shared-memory limit, raised once per device (the
+// attribute holds for the device that is current when it is set, and one
+// process may drive several devices).  false if the runtime refuses it.
+inline bool smem_limit_once(const void *kernel, size_t smem, std::atomic<uint64_t> &done)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    const uint64_t bit = 1ull << dev;
+    if (done.load() & bit) return true;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return false;
+    done.fetch_or(bit);
+    return true;
+}
 
 // ---- launchers (fsl_phase.cu) ------------------------------------------------
 void launch_ghost(Ctx &c, double *cur);

@@ -94,9 +94,13 @@ __device__ __forceinline__ void feat_load(const Grid &g, const double *__restric
     p.valid = cell < ncell;
     p.c = 0;
     if (!p.valid) return;
-    const int k = (int)(cell % g.D) + 1;
-    const long long rr = cell / g.D;
-    const int j = (int)(rr % g.H) + 1, i = (int)(rr / g.H) + 1;
+    // 32-bit index arithmetic (the launcher refuses grids of 2^31 cells or
+    // more): an unsigned 32-bit division is a short inline sequence, a 64-bit
+    // one a long subroutine, in a kernel whose issue slots are the limit
+    const unsigned cu = (unsigned)cell, D = (unsigned)g.D, H = (unsigned)g.H;
+    const unsigned rr = cu / D, ii = rr / H;
+    const int k = (int)(cu - rr * D) + 1;
+    const int j = (int)(rr - ii * H) + 1, i = (int)ii + 1;
     const long long c = g.idx(i, j, k), fs = g.fstride;
     const long long off[7] = {0, g.pi, -g.pi, (long long)g.pk, -(long long)g.pk, 1, -1};
 #pragma unroll
@@ -711,19 +715,15 @@ size_t closure_train_smem() { return sizeof(mlp::SmemTrain); }
 
 int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, float *cs2_out, const float *P, int *err)
 {
+    if ((long long)c.g.L * c.g.H * c.g.D >= (1LL << 31)) return -1; // feat_load's 32-bit indices
     prof_begin(c, FSL_K_SGS);
     mlp::k_closure_vel<<<148 * 8, 256, 0, c.stream>>>(c.g, U, c.cl_vel);
     prof_end(c, FSL_K_SGS, 1);
     const size_t smem = sizeof(mlp::SmemInfer);
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(mlp::k_closure_infer<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess ||
-            cudaFuncSetAttribute(mlp::k_closure_infer<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return -1;
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr64{0}, attr32{0};
+    if (!smem_limit_once((const void *)mlp::k_closure_infer<double>, smem, attr64) ||
+        !smem_limit_once((const void *)mlp::k_closure_infer<float>, smem, attr32))
+        return -1;
     const int blocks = 148 * 4;
     prof_begin(c, FSL_K_SGS);
     if (mu32)
@@ -746,13 +746,8 @@ int launch_train_grad(cudaStream_t st, const float *X, const float *Y, long long
                       float *Gpart, float *loss_part, int *err, int *nblk_out, float inv_wmean)
 {
     const size_t smem = sizeof(mlp::SmemTrain);
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(mlp::k_train_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-            return -1;
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr{0};
+    if (!smem_limit_once((const void *)mlp::k_train_grad, smem, attr)) return -1;
     const long long ntile = (n + 127) / 128;
     const int nblk = (int)((ntile + tpb - 1) / tpb);
     mlp::k_train_grad<<<nblk, 128, smem, st>>>(X, Y, n, tpb, P, Gpart, loss_part, err, inv_wmean);

@@ -601,13 +601,8 @@ int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, doubl
     a.status = &c.ds->status;
     a.seg = c.stage_seg;
     const size_t smem = sizeof(Smem<T, TJE, PPM>);
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_stage<T, TJE, MINB, PPM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return -1;
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr{0};
+    if (!smem_limit_once((const void *)k_stage<T, TJE, MINB, PPM>, smem, attr)) return -1;
     dim3 b(32, TJE, 1);
     dim3 gr((g.D + 29) / 30, (g.H + TJE - 3) / (TJE - 2), (g.L + a.seg - 1) / a.seg);
     prof_begin(c, FSL_K_STAGE);
