@@ -559,6 +559,8 @@ int fsl_upload_state(fsl_ctx *h, const double *state)
     CK(cudaMemcpyAsync(c.stage_dev, state, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     launch_state_scatter(c, c.U, c.stage_dev, 1, c.p.LEN);
     CKL();
+    // a new state: the flags of the one it replaces are cleared
+    CK(cudaMemsetAsync(&c.ds->status, 0, sizeof c.ds->status, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     c.cur = 0;
     return FSL_OK;

@@ -144,7 +144,10 @@ int fsl_destroy(fsl_ctx *ctx);
 /* Message of the last error on this context (static storage, never NULL). */
 const char *fsl_last_error(const fsl_ctx *ctx);
 int fsl_get_info(fsl_ctx *ctx, fsl_info *info);
-/* Block until the context's stream is idle. */
+/* Block until the context's stream is idle.  FSL_ERR_NONFINITE when a
+ * Courant reduction since the last fsl_upload_state met a density that is not
+ * positive or a maximum that is not positive and finite (the flag is kept
+ * until the next fsl_upload_state). */
 int fsl_sync(fsl_ctx *ctx);
 
 /* Upload/download U^n (backup.dat layout; src/initialize.c:134-148 reads,
