@@ -88,6 +88,26 @@ def test_params_from_bin(fsl, tmp_path):
     assert p.deltaX == float(np.float32(0.1)) and p.maxCoNum == float(np.float32(0.5))
 
 
+def test_unreadable_inputs_are_errors(fsl, tmp_path):
+    """Missing or truncated input files return FSL_ERR_IO; text the reference's
+    atoi/atof read as zeros parses like the reference and then fails the
+    parameter check (FSL_ERR_ARG) before any device work."""
+    for fn in (fsl.params_from_ini, fsl.params_from_bin):
+        with pytest.raises(fsl.FslError) as e:
+            fn(str(tmp_path / "absent"))
+        assert e.value.code == -6
+    short = tmp_path / "short.bin"
+    short.write_bytes(struct.pack("<10f", *range(10)))
+    with pytest.raises(fsl.FslError) as e:
+        fsl.params_from_bin(str(short))
+    assert e.value.code == -6
+    junk = tmp_path / "junk.ini"
+    junk.write_text("x\n" * 22)
+    p = fsl.params_from_ini(str(junk))
+    assert (p.LEN, p.HIG, p.DEP, p.deltaX) == (0, 0, 0, 0.0)
+    assert fsl.lib().fsl_params_check(C.byref(p)) == -1
+
+
 def test_params_check(fsl):
     lib = fsl.lib()
     ok = fsl.default_params()
