@@ -551,6 +551,7 @@ int fsl_get_info(fsl_ctx *h, fsl_info *info)
 
 int fsl_upload_state(fsl_ctx *h, const double *state)
 {
+    ApiRange range_("fsl_upload_state");
     if (!h || !state) return FSL_ERR_ARG;
     Ctx &c = h->c;
     const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
@@ -568,6 +569,7 @@ int fsl_upload_state(fsl_ctx *h, const double *state)
 
 int fsl_download_state(fsl_ctx *h, double *state)
 {
+    ApiRange range_("fsl_download_state");
     if (!h || !state) return FSL_ERR_ARG;
     Ctx &c = h->c;
     const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
@@ -601,6 +603,7 @@ static double *stage_state(Ctx &c)
 // context's stream (the one scratch buffer is reused in stream order)
 static int get_planes_q(fsl_ctx *h, int i0, int n, double *buf)
 {
+    ApiRange range_("fsl_get_planes");
     if (!h || !buf || !planes_ok(h->c, i0, n)) return FSL_ERR_ARG;
     Ctx &c = h->c;
     if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_get_planes: the current-stage buffer is not U^n");
@@ -613,6 +616,7 @@ static int get_planes_q(fsl_ctx *h, int i0, int n, double *buf)
 
 static int set_planes_q(fsl_ctx *h, int i0, int n, const double *buf)
 {
+    ApiRange range_("fsl_set_planes");
     if (!h || !buf || !planes_ok(h->c, i0, n)) return FSL_ERR_ARG;
     Ctx &c = h->c;
     if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_set_planes: the current-stage buffer is not U^n");
@@ -727,6 +731,7 @@ static int ensure_xfer(Ctx &c)
 // scatter into U^n is queued on the context's stream behind that work.
 int fsl_upload_state_async(fsl_ctx *h, const double *state)
 {
+    ApiRange range_("fsl_upload_state_async");
     if (!h || !state) return FSL_ERR_ARG;
     Ctx &c = h->c;
     int rc = ensure_xfer(c);
@@ -750,6 +755,7 @@ int fsl_upload_state_async(fsl_ctx *h, const double *state)
 // and overlaps the work queued after it.
 int fsl_download_state_async(fsl_ctx *h, double *state)
 {
+    ApiRange range_("fsl_download_state_async");
     if (!h || !state) return FSL_ERR_ARG;
     Ctx &c = h->c;
     int rc = ensure_xfer(c);
@@ -913,6 +919,7 @@ static bool is_slab(const Ctx &c)
 
 int fsl_step_phased(fsl_ctx *h, int nsteps)
 {
+    ApiRange range_("fsl_step_phased");
     if (!h || nsteps < 0) return FSL_ERR_ARG;
     Ctx &c = h->c;
     int rc;
@@ -951,6 +958,7 @@ int fsl_step_phased(fsl_ctx *h, int nsteps)
 // fused stage kernel; stages ping-pong U^n -> Up -> Uq -> U^n.
 int fsl_step(fsl_ctx *h, int nsteps)
 {
+    ApiRange range_("fsl_step");
     if (!h || nsteps < 0) return FSL_ERR_ARG;
     Ctx &c = h->c;
     if (c.p.nStages != 3) {
@@ -1020,6 +1028,7 @@ int fsl_step(fsl_ctx *h, int nsteps)
 // overlap planes between stages.
 int fsl_step_stage(fsl_ctx *h)
 {
+    ApiRange range_("fsl_step_stage");
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
     if (c.p.nStages != 3) return fail(c, FSL_ERR_UNSUPPORTED, "fsl_step_stage: nStages = 3 only");

@@ -197,6 +197,7 @@ int fsl_ensemble_set_chunk(fsl_ensemble *e, int steps)
 
 int fsl_ensemble_step(fsl_ensemble *e, int nsteps)
 {
+    ApiRange range_("fsl_ensemble_step");
     if (!e || nsteps < 0) return FSL_ERR_ARG;
     if (nsteps == 0) return FSL_OK;
     int rc;

@@ -4,6 +4,7 @@
 
 #include <atomic>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 #include <string>
 #include <vector>
@@ -177,6 +178,16 @@ int ensure_dyn_scratch(Ctx &c);  // SGS scratch of the dynamic procedure + the F
 int closure_step_sgs(Ctx &c);    // SGS of one step under FSL_SGS_LEARNED (fsl_closure.cu)
 int closure_ensure(Ctx &c);
 void closure_free(Ctx &c);
+
+// An NVTX range named for a C-ABI entry point, open for the call (host side:
+// profilers attribute the call's launches to it; without a profiler attached
+// a push/pop is a check of a null hook).
+struct ApiRange {
+    explicit ApiRange(const char *name) { nvtxRangePushA(name); }
+    ~ApiRange() { nvtxRangePop(); }
+    ApiRange(const ApiRange &) = delete;
+    ApiRange &operator=(const ApiRange &) = delete;
+};
 
 // A kernel's dynamic shared-memory limit, raised once per device (the
 // attribute holds for the device that is current when it is set, and one

@@ -95,6 +95,7 @@ extern "C" {
 // step, in the solver's `real` (real_bytes 4: the shipped float build; 8: FP64).
 int fsl_write_backup(fsl_ctx *h, const char *path, int real_bytes)
 {
+    ApiRange range_("fsl_write_backup");
     if (!h || !path || (real_bytes != 4 && real_bytes != 8)) return FSL_ERR_ARG;
     Ctx &c = h->c;
     const size_t n = (size_t)c.p.LEN * c.p.HIG * 5 * c.p.DEP;
