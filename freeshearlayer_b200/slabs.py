@@ -191,10 +191,11 @@ class SlabSet:
     the Courant maximum in device memory.  With device staging on one device
     the exchange and the combination are ordered between the slabs' streams
     by CUDA events, without waiting on the host, so the slabs' kernels may
-    also overlap one another.  exchange "step" refreshes the
-    overlap planes once per step, "stage" after every stage (a narrower
-    default overlap).  domain_factory(params) makes each slab's context
-    (default: Domain)."""
+    also overlap one another.
+
+    exchange "step" refreshes the overlap planes once per step, "stage"
+    after every stage (a narrower default overlap).  domain_factory(params)
+    makes each slab's context (default: Domain)."""
 
     def __init__(self, params, nslabs: int, overlap: int | None = None, devices=None,
                  staging: str = "host", domain_factory=None, exchange: str = "step"):
@@ -233,8 +234,9 @@ class SlabSet:
 
     def close(self):
         for d in self.domains:
-            d.close()
+            d.close()       # waits for the slab's stream, which may still read a buffer
         self.domains = []
+        self._bufs, self._read = {}, {}
 
     def __enter__(self):
         return self
