@@ -58,6 +58,7 @@ int check_member(fsl_ensemble *e, const Ctx &c)
     if (c.prof) return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members must not be profiling");
     if (c.co_i0 != 1 || c.co_i1 != c.p.LEN)
         return ens_fail(e, FSL_ERR_UNSUPPORTED, "ensemble members must be whole domains, not x-slabs");
+    if (c.stage_next != 0) return ens_fail(e, FSL_ERR_ARG, "an ensemble member is in the middle of a step");
     return FSL_OK;
 }
 

@@ -424,8 +424,9 @@ int fsl_trainer_train(fsl_trainer *tr, int epochs, long long batch, double lr, d
  * stepping it alone with fsl_step.  Members: temporal setup, nStages = 3,
  * either reconstruction, whole domains (not x-slabs), no profiling, learned
  * closure only with judgements off
- * (fsl_closure_judge(ctx, 0, ...)); otherwise FSL_ERR_UNSUPPORTED.  Members
- * stay owned by the caller and must outlive the ensemble; while an ensemble
+ * (fsl_closure_judge(ctx, 0, ...)); otherwise FSL_ERR_UNSUPPORTED.  A member
+ * in the middle of a stage-wise step (fsl_step_stage) is refused with
+ * FSL_ERR_ARG.  Members stay owned by the caller and must outlive the ensemble; while an ensemble
  * step is in flight, do not call them directly.  Each member's disturbance
  * RNG state (unused by the temporal setup) is not advanced by replays. */
 typedef struct fsl_ensemble fsl_ensemble;

@@ -109,3 +109,10 @@ def test_unsupported_members_are_refused(fsl):
         e2.step(1)
     assert ex.value.code == -7
     e2.close()
+    d3 = _member(fsl, dict(MEMBERS[0]))
+    d3.step_stage()                 # in the middle of a step
+    e3 = fsl.Ensemble([d3])
+    with pytest.raises(fsl.FslError) as ex:
+        e3.step(1)
+    assert ex.value.code == -1
+    e3.close()
