@@ -51,10 +51,11 @@ def test_two_rank_aggregation():
     procs = [ctx.Process(target=_rank_main, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
+    # read before joining: a rank cannot exit while its result is unread in the pipe
+    res = sorted(q.get(timeout=120) for _ in range(world))
     for p in procs:
-        p.join(120)
+        p.join(60)
         assert p.exitcode == 0
-    res = sorted(q.get(timeout=10) for _ in range(world))
     for rank, ms, rate, out in res:
         assert ms == 20.0                       # the slowest rank's time on every rank
         assert rate == pytest.approx(1000 * 2 / 0.020)

@@ -333,10 +333,11 @@ def test_distributed_gloo_matches_whole_domain(world, setup, exchange):
              for r in range(world)]
     for pr in procs:
         pr.start()
+    # read before joining: a rank cannot exit while its result is unread in the pipe
+    res = sorted((q.get(timeout=120) for _ in range(world)), key=lambda x: x[0])
     for pr in procs:
-        pr.join(120)
+        pr.join(60)
         assert pr.exitcode == 0
-    res = sorted((q.get(timeout=10) for _ in range(world)), key=lambda x: x[0])
     p = _params(setup)
     ref, dt = _whole(p, _state(p), steps)
     assert all(r[1] == dt for r in res)

@@ -161,3 +161,56 @@ def test_oracle_slabs_overlap_bound_is_tight(oracle_lib, monkeypatch, exchange, 
         ss.upload_state(s)
         ss.step(4)
         assert np.array_equal(ss.download_state(), ref.state()) == same
+
+
+def _rank_main(rank, world, port, exchange, q):
+    import datetime
+    import os
+    import sys
+
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import freeshearlayer_b200 as fsl
+    from freeshearlayer_b200.slabs import DistributedSlab
+    from oracle import oracle as orc
+    from tests.test_slabs_oracle import OracleDomain, _case
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        p, s = _case(orc, 1, 0)
+        ds = DistributedSlab(fsl._as_params(p), domain_factory=OracleDomain, exchange=exchange)
+        ds.upload_state(s)
+        ds.step(4)
+        full = ds.gather_state(0)
+        q.put((rank, ds.dom.dt, None if full is None else full.tobytes()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("exchange", ["step", "stage"])
+def test_oracle_slabs_over_gloo_ranks(oracle_lib, exchange):
+    """The same over two gloo ranks (DistributedSlab): point-to-point overlap
+    messages and an all-reduce MAX of the Courant number."""
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, exchange, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    # read before joining: a rank cannot exit while its result is unread in the pipe
+    res = sorted((q.get(timeout=120) for _ in range(2)), key=lambda x: x[0])
+    for pr in procs:
+        pr.join(60)
+        assert pr.exitcode == 0
+    p, s = _case(oracle_lib, 1, 0)
+    ref = oracle_lib.Oracle(p)
+    ref.set_state(s)
+    ref.step(4)
+    assert np.array_equal(np.frombuffer(res[0][2], np.float64), ref.state())
+    assert res[0][1] == res[1][1] == ref.scalars()[0]
