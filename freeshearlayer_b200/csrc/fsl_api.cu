@@ -666,6 +666,7 @@ int fsl_courant_prepare(fsl_ctx *h)
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
     if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_courant_prepare: the current-stage buffer is not U^n");
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "a step is in progress (fsl_step_stage)");
     if (!c.co_valid) {
         launch_courant_to_bits(c);
         CKL();
@@ -695,6 +696,8 @@ int fsl_set_courant_max(fsl_ctx *h, double maxCo)
 {
     if (!h || !(maxCo >= 0.0)) return FSL_ERR_ARG;
     Ctx &c = h->c;
+    // the final stage of a step in progress accumulates into the same scalar
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "a step is in progress (fsl_step_stage)");
     unsigned long long b;
     memcpy(&b, &maxCo, sizeof b);
     CK(cudaMemcpyAsync(&c.ds->co_bits, &b, sizeof b, cudaMemcpyHostToDevice, c.stream));
@@ -804,6 +807,7 @@ int fsl_check_courant(fsl_ctx *h, double *maxCo, double *dt)
 {
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "a step is in progress (fsl_step_stage)");
     c.co_valid = false;
     launch_courant(c);
     CKL();

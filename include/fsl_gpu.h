@@ -289,10 +289,11 @@ int fsl_step_phased(fsl_ctx *ctx, int nsteps);
  * viscosity, stage 1), the third completes it.  Same launches and results as
  * fsl_step.  Between the calls only fsl_get_planes / fsl_set_planes may touch
  * the state (the per-stage ghost-plane exchange of
- * src-par/boundCondInGhostCells.c:60-73); fsl_step, fsl_step_phased and the
- * other stage calls refuse with FSL_ERR_ARG until the step is complete.  An
- * upload abandons it (its deltaT rescale, step count and disturbance draw
- * stand, as after a completed step). */
+ * src-par/boundCondInGhostCells.c:60-73); fsl_step, fsl_step_phased, the
+ * Courant calls (fsl_check_courant, fsl_courant_prepare,
+ * fsl_set_courant_max) and ensemble steps refuse with FSL_ERR_ARG until the
+ * step is complete.  An upload abandons it (its deltaT rescale, step count
+ * and disturbance draw stand, as after a completed step). */
 int fsl_step_stage(fsl_ctx *ctx);
 
 /* Launch-shape knobs of the fused kernels.  FP64 results do not depend on

@@ -215,6 +215,10 @@ def test_step_stage_protocol(fsl):
         d.step(1)                   # a step is in progress
     with pytest.raises(fsl.FslError):
         d.step_phased(1)
+    with pytest.raises(fsl.FslError):
+        d.set_courant_max(1.0)      # the final stage accumulates into it
+    with pytest.raises(fsl.FslError):
+        d.check_courant()
     d.upload_state(s)               # abandons it (its dt rescale and step count stand)
     d.step(1)
     a = d.download_state()
