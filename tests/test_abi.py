@@ -108,6 +108,20 @@ def test_unreadable_inputs_are_errors(fsl, tmp_path):
     assert fsl.lib().fsl_params_check(C.byref(p)) == -1
 
 
+def test_plane_buffers_are_checked(fsl):
+    """Buffers handed to the plane and transfer calls: contiguous float64 of
+    at least the needed length, numpy or torch, else an error before any
+    call into the library."""
+    import torch
+    ok = np.zeros(12)
+    assert fsl._buffer_ptr(ok, 12) == ok.ctypes.data
+    assert fsl._buffer_ptr(torch.zeros(12, dtype=torch.float64), 12) != 0
+    for bad in (np.zeros(11), np.zeros(12, np.float32), np.zeros((12, 2))[:, 0],
+                torch.zeros(12, dtype=torch.float32), [0.0] * 12):
+        with pytest.raises(fsl.FslError):
+            fsl._buffer_ptr(bad, 12)
+
+
 def test_params_check(fsl):
     lib = fsl.lib()
     ok = fsl.default_params()
