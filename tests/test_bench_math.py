@@ -1,0 +1,53 @@
+"""The bench line's derived numbers on the CPU, from fake kernel timings:
+the roofline object (algorithmic bytes of a launch over its mean CUDA-event
+time, against the HBM peak; DRAM traffic from the committed ncu summary,
+scaled by cells), the compute roof (counted flops over the same time,
+against the vector peak at the sampled clock), and the whole-job rate."""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+NAMES = ["stage", "recon", "flux", "sgs", "evol", "bc", "cfl", "other"]
+
+
+class _KT:
+    ms = [27.5, 0.0, 0.0, 25.0, 0.0, 3.3, 0.07, 0.07]
+    launches = [10, 0, 0, 20, 0, 20, 10, 2]
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_stage_roofline_and_compute_roof(prec):
+    ncell = 512 * 256 * 256
+    peaks = {"hbm_gbs": 6650.0, "source": "fallback"}
+    roof, kms, kl = bench.stage_roofline(_KT(), NAMES, ncell, prec, peaks, None)
+    avg_s = 27.5e-3 / 10
+    want = bench.STAGE_BYTES[prec] * ncell / avg_s / 1e9
+    assert roof["achieved"] == pytest.approx(want, rel=1e-4)
+    assert roof["frac"] == pytest.approx(want / 6650.0, abs=1e-4)
+    assert roof["bound"] == "hbm" and roof["unit"] == "GB/s" and roof["launches"] == 10
+    per_cell = bench.profiled_traffic(prec)
+    if per_cell is not None:
+        assert roof["traffic"] == pytest.approx(per_cell * ncell)
+        assert 100.0 < per_cell < 200.0               # near the algorithmic bytes, not re-read
+    assert kl["stage"] == 10 and kms["sgs"] == 25.0
+    cr = bench.compute_roof(roof, prec, {"sm_mhz": 1965.0})
+    lanes = 64 if prec == 0 else 128
+    assert cr["peak"] == pytest.approx(148 * lanes * 2 * 1965e6 / 1e12, abs=0.01)
+    assert cr["achieved"] == pytest.approx(bench.STAGE_FLOPS[prec] * ncell / avg_s / 1e12, rel=1e-3)
+
+
+def test_whole_job_rate_is_weak_scaling():
+    # every rank does the same units; the slowest rank's time counts
+    assert bench.whole_job_rate(1000, 4, 20.0) == pytest.approx(4 * 1000 / 0.020)
+
+
+def test_peaks_fall_back_without_the_measured_file(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.measured_peaks() == {"hbm_gbs": 6650.0, "source": "fallback"}
+    (tmp_path / "MEASURED_PEAKS.json").write_text('{"hbm_gbs": 7012.5, "bf16_tflops": 1600}')
+    assert bench.measured_peaks() == {"hbm_gbs": 7012.5, "source": "measured"}
