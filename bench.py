@@ -21,6 +21,7 @@ momentum-thickness growth and Reynolds-stress profile differences
 (matched_error).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--arm ARM]
+        (--gpus N > 1 without a launcher starts N ranks under torch.distributed.run)
     python bench.py --impl reference ...   # the reference's serial CPU solver
 
 Prints exactly one JSON line on rank 0.
@@ -318,6 +319,12 @@ def compute_roof(roof, prec, clk):
                      "on its own (half the FMA peak is its ceiling)" if prec == 0 else "")}
 
 
+# the stated accuracy bar: relative L2 of each conserved variable against the
+# FP64 path, each variable against its own norm
+L2_BAR = 1e-5
+VAR_NAMES = ["rho", "rho_u", "rho_v", "rho_w", "E"]
+
+
 def rel_l2(a, b):
     import numpy as np
     return [float(np.linalg.norm(a[v] - b[v]) / max(np.linalg.norm(b[v]), 1e-300)) for v in range(5)]
@@ -354,7 +361,13 @@ def matched_error(fsl, grid, state, dU, nsteps, rows, seg):
             den = float(np.max(np.abs(ref_s1[comp])))
             rs[comp] = float(np.max(np.abs(s1[comp] - ref_s1[comp])) / den) if den > 0 else None
         mom = float(np.sqrt(sum(np.linalg.norm(ref_u[v]) ** 2 for v in (1, 2, 3))))
-        e = {"rel_l2_vs_fp64": dict(zip(["rho", "rho_u", "rho_v", "rho_w", "E"], rel_l2(u, ref_u))),
+        rel = dict(zip(VAR_NAMES, rel_l2(u, ref_u)))
+        e = {"rel_l2_vs_fp64": rel,
+             "bar": L2_BAR,
+             "pass": {n: bool(x <= L2_BAR) for n, x in rel.items()},
+             "all_pass": bool(all(x <= L2_BAR for x in rel.values())),
+             # an extra column only: the transverse momenta over the whole
+             # momentum's norm (their own norms are the velocity noise)
              "l2_vs_fp64_over_momentum_norm": {n: float(np.linalg.norm(u[v] - ref_u[v]) / mom)
                                                for n, v in (("rho_u", 1), ("rho_v", 2), ("rho_w", 3))},
              "theta_growth": g,
@@ -734,6 +747,45 @@ def main_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def free_port() -> int:
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def launch_ranks(n: int) -> int:
+    """Run this script once per GPU under torch.distributed.run (one process
+    per GPU, rendezvous on 127.0.0.1), as the multi-GPU launch would; rank 0
+    prints the JSON line.  Returns the launcher's exit code."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(n),
+           "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.abspath(__file__)]
+    return subprocess.call(cmd + sys.argv[1:])
+
+
+def main_launcher_check(args):
+    """The multi-rank plumbing without any GPU work: every rank joins the
+    process group (backend FSL_BENCH_BACKEND, default nccl), the per-rank
+    times (10 + rank ms) are combined by the maximum over ranks, and rank 0
+    prints the fields of the line that depend on the ranks."""
+    import datetime
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    backend = os.environ.get("FSL_BENCH_BACKEND", "nccl")
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
+    ms = max_over_ranks(torch, dist, 10.0 + rank, "cpu" if backend == "gloo" else "cuda")
+    if rank == 0:
+        print(json.dumps({"n_gpus": world, "ms_max": ms, "value": whole_job_rate(1000, world, ms),
+                          "backend": backend}), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -761,10 +813,21 @@ def main():
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the dominant kernel from an ncu capture")
     ap.add_argument("--ref-worker", nargs=4, default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--launcher-check", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.ref_worker:
         n, w, slab, out = args.ref_worker
         _ref_worker_main(int(n), int(w), tuple(int(x) for x in slab.split(",")), out)
+        return
+    # one process per GPU: without a launcher's WORLD_SIZE, --gpus N > 1
+    # starts the N ranks itself; under a launcher the two must agree
+    world_env = os.environ.get("WORLD_SIZE")
+    if world_env is None and args.gpus > 1:
+        sys.exit(launch_ranks(args.gpus))
+    if world_env is not None and int(world_env) != args.gpus:
+        sys.exit("bench.py: --gpus %d, but the launcher started %s ranks (WORLD_SIZE)" % (args.gpus, world_env))
+    if args.launcher_check:
+        main_launcher_check(args)
         return
     if args.warmup < 3 and args.impl == "fsl":
         args.warmup = 3

@@ -30,7 +30,7 @@ import numpy as np
 __all__ = ["Params", "Domain", "FslError", "lib", "LIB_PATH", "default_params",
            "params_from_ini", "params_from_bin", "initial_state", "temporal_state",
            "SETUP_SPATIAL", "SETUP_TEMPORAL", "CFL_STREAMWISE", "CFL_ACOUSTIC",
-           "PREC_FP64", "PREC_FP32", "SGS_DYNAMIC", "SGS_LEARNED", "RECON_CHARMINMOD",
+           "PREC_FP64", "PREC_FP32", "SGS_DYNAMIC", "SGS_LEARNED", "SGS_STATIC", "SGS_NONE", "RECON_CHARMINMOD",
            "RECON_PPM", "Trainer", "Ensemble", "closure_weights", "shear_statistics", "favre_from_probes",
            "tecplot_write"]
 
@@ -44,7 +44,7 @@ ERRORS = {-1: "FSL_ERR_ARG", -2: "FSL_ERR_NOMEM", -3: "FSL_ERR_CUDA", -4: "FSL_E
 SETUP_SPATIAL, SETUP_TEMPORAL = 0, 1
 CFL_STREAMWISE, CFL_ACOUSTIC = 0, 1
 PREC_FP64, PREC_FP32 = 0, 1
-SGS_DYNAMIC, SGS_LEARNED = 0, 1
+SGS_DYNAMIC, SGS_LEARNED, SGS_STATIC, SGS_NONE = 0, 1, 2, 3
 RECON_CHARMINMOD, RECON_PPM = 0, 1
 
 
@@ -89,7 +89,9 @@ CLOSURE_NPARAMS = 9473
 class ClosureStats(C.Structure):
     _fields_ = [("profile_err", C.c_double), ("cell_err", C.c_double), ("mu_profile_err", C.c_double),
                 ("visc_err", C.c_double), ("judgements", C.c_int),
-                ("fallbacks", C.c_int), ("using_dynamic", C.c_int), ("last_step", C.c_uint)]
+                ("fallbacks", C.c_int), ("using_dynamic", C.c_int), ("last_step", C.c_uint),
+                ("mu_active_err", C.c_double), ("dyn_ratio", C.c_double), ("active_rows", C.c_int),
+                ("reserved_", C.c_int)]
 
 
 class KTimes(C.Structure):
@@ -135,6 +137,7 @@ def lib():
         sig.update({
             "fsl_closure_set_scales": [vp, d, d], "fsl_closure_set_weights": [vp, fp],
             "fsl_closure_get_weights": [vp, fp], "fsl_closure_judge": [vp, i, d],
+            "fsl_closure_judge_active": [vp, d, d],
             "fsl_closure_get_stats": [vp, C.POINTER(ClosureStats)],
             "fsl_closure_compare": [vp, C.c_void_p, C.c_void_p, C.POINTER(ClosureStats)],
             "fsl_trainer_create": [ll, C.c_ulonglong, C.POINTER(C.c_void_p)],
@@ -460,6 +463,11 @@ class Domain:
 
     def closure_judge(self, every: int, threshold: float):
         self._c(lib().fsl_closure_judge(self.h, every, threshold))
+
+    def closure_judge_active(self, floor: float, threshold: float):
+        """Rows whose dynamic SGS viscosity is at least floor * mu_L are judged
+        on the SGS viscosity profile itself against `threshold`."""
+        self._c(lib().fsl_closure_judge_active(self.h, floor, threshold))
 
     def closure_stats(self) -> ClosureStats:
         s = ClosureStats()

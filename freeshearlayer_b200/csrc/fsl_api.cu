@@ -342,7 +342,8 @@ int fsl_params_check(const fsl_params *p)
     // (src/bounCondOnInterfaces.c:31 writes past the array otherwise)
     if (p->setup == FSL_SETUP_SPATIAL && (p->BL_HIG < 0 || p->HIG / 2 + p->BL_HIG > p->HIG)) return FSL_ERR_ARG;
     if (p->precision != FSL_PREC_FP64 && p->precision != FSL_PREC_FP32) return FSL_ERR_ARG;
-    if (p->sgs != FSL_SGS_DYNAMIC && p->sgs != FSL_SGS_LEARNED) return FSL_ERR_ARG;
+    if (p->sgs != FSL_SGS_DYNAMIC && p->sgs != FSL_SGS_LEARNED && p->sgs != FSL_SGS_STATIC && p->sgs != FSL_SGS_NONE)
+        return FSL_ERR_ARG;
     if (p->recon != FSL_RECON_CHARMINMOD && p->recon != FSL_RECON_PPM) return FSL_ERR_ARG;
     return FSL_OK;
 }
@@ -436,6 +437,7 @@ int fsl_init(const fsl_params *p, fsl_ctx **out)
     c.k.lambda_L = p->mu_L * 717.75 * 1.4 / p->Pr_L;
     c.k.cp_Pr_T = 717.75 * 1.4 / p->Pr_T;
     c.k.DD = pow(p->deltaX * p->deltaY * p->deltaZ, 0.666666666666667);
+    c.k.CsDD = p->Cs * c.k.DD;
     c.k.maxCoNum = p->maxCoNum;
     c.k.deltaX = p->deltaX; c.k.deltaY = p->deltaY; c.k.deltaZ = p->deltaZ;
     c.k.setup = p->setup; c.k.BL_HIG = p->BL_HIG; c.k.cfl_mode = p->cfl_mode; c.k.nStages = p->nStages;
@@ -838,6 +840,7 @@ int fsl_ghost_bc(fsl_ctx *h)
 {
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "fsl_ghost_bc: a step is in progress (fsl_step_stage)");
     launch_ghost(c, cur_ptr(c));
     CKL();
     return FSL_OK;
@@ -847,6 +850,7 @@ int fsl_reconstruct(fsl_ctx *h)
 {
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "fsl_reconstruct: a step is in progress (fsl_step_stage)");
     int rc = ensure_faces(c);
     if (rc) return rc;
     launch_recon(c, cur_ptr(c));
@@ -858,6 +862,7 @@ int fsl_interface_bc(fsl_ctx *h)
 {
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "fsl_interface_bc: a step is in progress (fsl_step_stage)");
     int rc = ensure_faces(c);
     if (rc) return rc;
     launch_ifbc(c, c.dist);
@@ -869,6 +874,7 @@ int fsl_dynamic_smagorinsky(fsl_ctx *h)
 {
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "fsl_dynamic_smagorinsky: a step is in progress (fsl_step_stage)");
     int rc = ensure_dyn(c);
     if (rc) return rc;
     launch_dynsmag(c, c.U);
@@ -880,6 +886,7 @@ int fsl_fluxes(fsl_ctx *h)
 {
     if (!h) return FSL_ERR_ARG;
     Ctx &c = h->c;
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "fsl_fluxes: a step is in progress (fsl_step_stage)");
     int rc = ensure_faces(c);
     if (rc) return rc;
     launch_fluxes(c, cur_ptr(c));
@@ -891,6 +898,7 @@ int fsl_evolution(fsl_ctx *h, int stage)
 {
     if (!h || stage < 1) return FSL_ERR_ARG;
     Ctx &c = h->c;
+    if (c.stage_next != 0) return fail(c, FSL_ERR_ARG, "fsl_evolution: a step is in progress (fsl_step_stage)");
     int rc = ensure_faces(c);
     if (rc) return rc;
     c.co_valid = false;
@@ -899,6 +907,27 @@ int fsl_evolution(fsl_ctx *h, int stage)
     // pointer swap of src/evolution.c:71,113,155 (and :188,228 for RK2)
     c.cur = (stage == 1 || stage == 2) ? 1 : 0;
     return FSL_OK;
+}
+
+// The SGS viscosity of one step, on U^n with its ghost layer filled: the
+// dynamic procedure, the learned closure (judged by the dynamic procedure),
+// nothing for the static model (the stage kernels form it per face), or a
+// zero field.
+static int step_sgs(Ctx &c)
+{
+    const bool fp32 = c.p.precision == FSL_PREC_FP32;
+    switch (c.p.sgs) {
+    case FSL_SGS_LEARNED: return closure_step_sgs(c);
+    case FSL_SGS_STATIC: return FSL_OK;
+    case FSL_SGS_NONE:
+        if (fp32) CK(cudaMemsetAsync(c.mu32, 0, (size_t)c.g.fstride * sizeof(float), c.stream));
+        else CK(cudaMemsetAsync(c.mu, 0, (size_t)c.g.fstride * sizeof(double), c.stream));
+        return FSL_OK;
+    default:
+        if (fp32) launch_dynsmag32(c, c.U);
+        else launch_dynsmag(c, c.U);
+        return FSL_OK;
+    }
 }
 
 // An x-slab (Courant range narrower than the domain) steps one step at a
@@ -941,7 +970,10 @@ int fsl_step_phased(fsl_ctx *h, int nsteps)
             launch_ghost(c, cur);
             launch_recon(c, cur);
             launch_ifbc(c, c.dist);
-            if (s == 1) launch_dynsmag(c, c.U);
+            if (s == 1) {
+                if (c.p.sgs == FSL_SGS_NONE) CK(cudaMemsetAsync(c.mu, 0, (size_t)c.g.fstride * sizeof(double), c.stream));
+                else if (c.p.sgs != FSL_SGS_STATIC) launch_dynsmag(c, c.U);
+            }
             launch_fluxes(c, cur);
             launch_evolution(c, c.p.nStages, s);
             c.cur = (s == 1 || s == 2) ? 1 : 0;
@@ -984,11 +1016,7 @@ int fsl_step(fsl_ctx *h, int nsteps)
             draw(c);
             launch_ghost(c, c.U);
             launch_bface32(c, c.U, c.dist);
-            if (c.p.sgs == FSL_SGS_LEARNED) {
-                if ((rc = closure_step_sgs(c))) return rc;
-            } else {
-                launch_dynsmag32(c, c.U);
-            }
+            if ((rc = step_sgs(c))) return rc;
             if (launch_stage32(c, 1, c.U, c.U, c.Up)) return fail(c, FSL_ERR_CUDA, "FP32 stage kernel");
             launch_ghost(c, c.Up);
             launch_bface32(c, c.Up, c.dist);
@@ -1008,11 +1036,7 @@ int fsl_step(fsl_ctx *h, int nsteps)
         draw(c);
         launch_ghost(c, c.U);
         launch_bface(c, c.U, c.dist);
-        if (c.p.sgs == FSL_SGS_LEARNED) {
-            if ((rc = closure_step_sgs(c))) return rc;
-        } else {
-            launch_dynsmag(c, c.U);
-        }
+        if ((rc = step_sgs(c))) return rc;
         if (launch_stage(c, 1, c.U, c.U, c.Up)) return fail(c, FSL_ERR_CUDA, "stage kernel attribute");
         launch_ghost(c, c.Up);
         launch_bface(c, c.Up, c.dist);
@@ -1051,17 +1075,12 @@ int fsl_step_stage(fsl_ctx *h)
         launch_ghost(c, c.U);
         if (fp32) launch_bface32(c, c.U, c.dist);
         else launch_bface(c, c.U, c.dist);
-        if (c.p.sgs == FSL_SGS_LEARNED) {
-            if ((rc = closure_step_sgs(c))) return rc;
-        } else if (fp32) {
-            launch_dynsmag32(c, c.U);
-        } else {
-            launch_dynsmag(c, c.U);
-        }
+        if ((rc = step_sgs(c))) return rc;
         const int e = fp32 ? launch_stage32(c, 1, c.U, c.U, c.Up) : launch_stage(c, 1, c.U, c.U, c.Up);
         if (e) return fail(c, FSL_ERR_CUDA, "stage kernel");
         c.stage_next = 2;
     } else if (c.stage_next == 2) {
+        if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_step_stage: the current-stage buffer is not U^n");
         launch_ghost(c, c.Up);
         if (fp32) {
             launch_bface32(c, c.Up, c.dist);
@@ -1072,6 +1091,7 @@ int fsl_step_stage(fsl_ctx *h)
         }
         c.stage_next = 3;
     } else {
+        if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_step_stage: the current-stage buffer is not U^n");
         launch_ghost(c, c.Uq);
         if (fp32) {
             launch_bface32(c, c.Uq, c.dist);

@@ -2,6 +2,7 @@
 // per-step SGS selection (MLP, or the dynamic procedure as judge/fallback),
 // sample harvest and the Adam training driver.  The tensor-core kernels are
 // in fsl_mlp.cu.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -150,14 +151,34 @@ int judge_now(Ctx &c)
     judge_errors(mrows, H, &c.last_merr, &mcell);
     // rows j in [3, H-2] hold sums over the (L-4)(D-4) band cells of the plane
     const double nb = (double)(c.g.L - 4) * (c.g.D - 4);
-    double num = 0, den = 0;
+    double num = 0, den = 0, anum = 0, aden = 0, ratio = 0;
+    int active = 0;
     for (int j = 2; j <= H - 3; j++) {
         const double a = mrows[4 * j] / nb, b = mrows[4 * j + 1] / nb;
         num += (a - b) * (a - b);
         den += (c.p.mu_L + b) * (c.p.mu_L + b);
+        ratio = std::max(ratio, b / c.p.mu_L);
+        if (b >= c.judge_floor * c.p.mu_L) { // the SGS model acts on this row
+            anum += (a - b) * (a - b);
+            aden += b * b;
+            active++;
+        }
     }
     c.last_verr = den > 0 ? std::sqrt(num / den) : (num > 0 ? INFINITY : 0.0);
+    c.last_aerr = active ? std::sqrt(anum / aden) : 0.0;
+    c.last_dyn_ratio = ratio;
+    c.last_active_rows = active;
     return FSL_OK;
+}
+
+// Both criteria of a judgement: the effective viscosity over all rows, and
+// the SGS viscosity itself over the rows where the dynamic model acts.  NaN
+// errors fail.
+bool judge_passes(const Ctx &c)
+{
+    if (!(c.last_verr <= c.judge_thr)) return false;
+    if (c.last_active_rows > 0 && !(c.last_aerr <= c.judge_thr_active)) return false;
+    return true;
 }
 
 } // namespace
@@ -179,7 +200,7 @@ int closure_step_sgs(Ctx &c)
         if (rc) return rc;
         c.judgements++;
         c.last_judge_step = c.step;
-        const bool fail_ = !(c.last_verr <= c.judge_thr);
+        const bool fail_ = !judge_passes(c);
         if (fail_ && !c.using_dynamic) c.fallbacks++;
         c.using_dynamic = fail_;
         const size_t fs = (size_t)c.g.fstride;
@@ -254,10 +275,22 @@ int fsl_closure_judge(fsl_ctx *h, int every, double threshold)
     return FSL_OK;
 }
 
+int fsl_closure_judge_active(fsl_ctx *h, double floor, double threshold)
+{
+    if (!h || !(floor > 0) || !(threshold >= 0)) return FSL_ERR_ARG;
+    h->c.judge_floor = floor;
+    h->c.judge_thr_active = threshold;
+    return FSL_OK;
+}
+
 int fsl_closure_get_stats(fsl_ctx *h, fsl_closure_stats *s)
 {
     if (!h || !s) return FSL_ERR_ARG;
     const Ctx &c = h->c;
+    memset(s, 0, sizeof *s);
+    s->mu_active_err = c.last_aerr;
+    s->dyn_ratio = c.last_dyn_ratio;
+    s->active_rows = c.last_active_rows;
     s->profile_err = c.last_perr;
     s->mu_profile_err = c.last_merr;
     s->cell_err = c.last_cerr;

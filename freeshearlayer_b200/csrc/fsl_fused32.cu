@@ -22,22 +22,30 @@ void launch_bface32(Ctx &c, const double *cur, const Disturb &d)
     stage::launch_bface_t<float>(c, cur, d, bf32(c));
 }
 
-int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant)
+template <bool SST>
+static int stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant)
 {
     if (c.p.recon == FSL_RECON_PPM) {
         // PPM: halo 2, a ring of four planes; 16 rows measured fastest at
         // 512x256x256 (11.7 ms per step against 13.4 for 8 rows, two blocks per SM)
         switch (c.stage_tje) {
-        case 8: return stage::launch_stage_t<float, 8, 2, true>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
-        case 12: return stage::launch_stage_t<float, 12, 1, true>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
-        default: return stage::launch_stage_t<float, 16, 1, true>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
+        case 8: return stage::launch_stage_t<float, 8, 2, true, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
+        case 12: return stage::launch_stage_t<float, 12, 1, true, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
+        default: return stage::launch_stage_t<float, 16, 1, true, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
         }
     }
     switch (c.stage_tje) {
-    case 8: return stage::launch_stage_t<float, 8, 2>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
-    case 12: return stage::launch_stage_t<float, 12, 1>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
-    default: return stage::launch_stage_t<float, 16, 1>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
+    case 8: return stage::launch_stage_t<float, 8, 2, false, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
+    case 12: return stage::launch_stage_t<float, 12, 1, false, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
+    default: return stage::launch_stage_t<float, 16, 1, false, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
     }
+}
+
+int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant)
+{
+    // the static Smagorinsky model forms the face viscosity in the kernel
+    if (c.p.sgs == FSL_SGS_STATIC) return stage32<true>(c, stage, cur, un, out, courant);
+    return stage32<false>(c, stage, cur, un, out, courant);
 }
 
 } // namespace fsl

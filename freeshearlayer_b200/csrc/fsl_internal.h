@@ -37,6 +37,7 @@ Grid make_grid(int L, int H, int D, int elem_bytes);
 struct Consts {
     double rdx, rdy, rdz, r2dx, r2dy, r2dz, r4dx, r4dy, r4dz;
     double mu_L, lambda_L, cp_Pr_T, DD, maxCoNum;
+    double CsDD; // Cs DD, the static Smagorinsky factor (src/initialize.c:94)
     double deltaX, deltaY, deltaZ;
     int setup, BL_HIG, cfl_mode, nStages;
 };
@@ -121,7 +122,10 @@ struct Ctx {
     double judge_thr = 0.02;
     bool using_dynamic = false;
     int judgements = 0, fallbacks = 0;
+    double judge_floor = 0.1, judge_thr_active = 0.5; // SGS-active rows: <mu_dyn> >= floor mu_L
     double last_perr = -1, last_cerr = -1, last_merr = -1, last_verr = -1;
+    double last_aerr = -1, last_dyn_ratio = -1;
+    int last_active_rows = 0;
     unsigned last_judge_step = 0;
     DevScalars *ds = nullptr; // device scalars
     DevScalars *hs = nullptr; // pinned host mirror

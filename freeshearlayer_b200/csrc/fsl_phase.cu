@@ -247,9 +247,12 @@ __global__ void k_ifbc(Grid g, int setup, int BL_HIG, Disturb d, Faces f)
 // A4 fluxes (src/fluxes.c:57-571): one thread per face of direction N.
 // The flux overwrites the minus-side state array, as in the reference.
 // ---------------------------------------------------------------------------
+// sgs: FSL_SGS_STATIC forms the face viscosity from the face gradients and
+// the two cells' densities (src/fluxes.c:193-205, :362-374, :533-545),
+// FSL_SGS_NONE uses zero, any other mode the mu_SGS field.
 template <int N>
 __global__ void __launch_bounds__(128) k_flux(Grid g, Consts kc, const double *__restrict__ u,
-                                              const double *__restrict__ mu, Faces f)
+                                              const double *__restrict__ mu, Faces f, int sgs)
 {
     const int L = g.L, H = g.H, D = g.D;
     const int na = L + (N == 1), nb = H + (N == 2), nc = D + (N == 3);
@@ -307,7 +310,10 @@ __global__ void __launch_bounds__(128) k_flux(Grid g, Consts kc, const double *_
     }
     // SGS viscosity at the face: x uses the two adjacent cells (:191); the y
     // and z sweeps average the plus cell with its x-neighbour (:360, :531).
-    const double mu_T = 0.5 * (mu[plus] + mu[plus - g.pi]);
+    double mu_T;
+    if (sgs == FSL_SGS_STATIC) mu_T = static_mu_t<double>(gr, 0.5 * (u[plus] + u[minus]), kc.CsDD);
+    else if (sgs == FSL_SGS_NONE) mu_T = 0.0;
+    else mu_T = 0.5 * (mu[plus] + mu[plus - g.pi]);
     double F[5];
     face_flux<double, N>(Rho, P, vel, gr, vp, vm, Tp, Tm, kc.mu_L, mu_T, kc.lambda_L, kc.cp_Pr_T, rdn, F);
 #pragma unroll
@@ -644,9 +650,9 @@ void launch_fluxes(Ctx &c, const double *cur)
     const Grid &g = c.g;
     dim3 b(32, 4, 1);
     prof_begin(c, FSL_K_FLUX);
-    k_flux<1><<<cells_grid(g, b, g.L + 1, g.H, g.D), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f);
-    k_flux<2><<<cells_grid(g, b, g.L, g.H + 1, g.D), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f);
-    k_flux<3><<<cells_grid(g, b, g.L, g.H, g.D + 1), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f);
+    k_flux<1><<<cells_grid(g, b, g.L + 1, g.H, g.D), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f, c.p.sgs);
+    k_flux<2><<<cells_grid(g, b, g.L, g.H + 1, g.D), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f, c.p.sgs);
+    k_flux<3><<<cells_grid(g, b, g.L, g.H, g.D + 1), b, 0, c.stream>>>(g, c.k, cur, c.mu, c.f, c.p.sgs);
     prof_end(c, FSL_K_FLUX, 3);
 }
 
@@ -777,7 +783,10 @@ int noalloc_scratch(double **out)
     return FSL_OK;
 }
 
-// The launch sequence of launch_dynsmag on explicit buffers and stream.
+// The dynamic procedure's unfused nine-launch sequence (dyn::sequence: the
+// seven-pass filters and the coefficient, each field in its own scratch
+// array), on explicit buffers and stream.  The context path runs the fused
+// form (dyn::sequence_fused) on less scratch; both give the same bits.
 void noalloc_dyn_sequence(const fsl::Grid &g, const fsl::Consts &k, const fsl::dyn::Scratch<double> &s,
                           const double *U, double *mu, cudaStream_t st)
 {
@@ -791,11 +800,24 @@ extern "C" int fsl_dynamic_smagorinsky_noalloc(const double *U, double *mu, int 
 {
     if (!U || !mu || LEN < 2 || HIG < 2 || DEP < 2 || !(deltaX > 0) || !(deltaY > 0) || !(deltaZ > 0))
         return FSL_ERR_ARG;
-    const long long n = (long long)(LEN + 2) * (HIG + 2) * (DEP + 2);
+    // each extent widened before the +2, so no int arithmetic can overflow
+    const long long n = ((long long)LEN + 2) * ((long long)HIG + 2) * ((long long)DEP + 2);
+    if (n <= 0) return FSL_ERR_ARG;
     if (n > (long long)FSL_NOALLOC_MAX_CELLS) return FSL_ERR_TOO_LARGE;
+    // an error left pending by the caller's earlier work is not this call's:
+    // report it without clearing it and without starting any work
+    if (cudaPeekAtLastError() != cudaSuccess) return FSL_ERR_CUDA;
     double *s = nullptr;
     int rc = noalloc_scratch(&s);
     if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the scratch address belongs to the current device: a stream of another
+    // device would run the work against that device's copy of the array
+    if (st) {
+        int sdev = -1, dev = -1;
+        if (cudaStreamGetDevice(st, &sdev) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess) return FSL_ERR_ARG;
+        if (sdev != dev) return FSL_ERR_ARG;
+    }
     fsl::Grid g;
     g.L = LEN; g.H = HIG; g.D = DEP;
     g.pk = DEP + 2;
@@ -810,7 +832,6 @@ extern "C" int fsl_dynamic_smagorinsky_noalloc(const double *U, double *mu, int 
     fsl::dyn::Scratch<double> d;
     d.vel = s; d.t1 = s + 3 * n; d.t2 = s + 12 * n; d.A = s + 21 * n;
     d.Lst = s + 27 * n; d.B = s + 33 * n; d.S = s + 39 * n;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     // zero bands of the filter passes and the A ghost layer must start at 0;
     // the previous call left its values in the shared scratch
     if (cudaMemsetAsync(s, 0, (size_t)(40 * n) * sizeof(double), st) != cudaSuccess) return FSL_ERR_CUDA;

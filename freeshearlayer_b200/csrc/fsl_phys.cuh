@@ -493,13 +493,30 @@ FSL_HD void face_flux(T Rho, T P, const T *vel, const T (*g)[3], const T *fw, co
            uu * s0 - vv * s1 - ww * s2 + q;
 }
 
+// The static Smagorinsky viscosity of one face (the reference's
+// DynamicSmagorinskySGS 0 branch, src/fluxes.c:193-205 x, :362-374 y,
+// :533-545 z; live in src-par/def.h:47): the mean density of the two cells
+// beside the face times CsDD = Cs (dx dy dz)^(2/3) times |S| from the face
+// velocity gradients g[a][b] = d u_a / d x_b, in the reference's order.
+template <typename T> FSL_HD T static_mu_t(const T (*g)[3], T rr, T CsDD)
+{
+    const T S12 = T(0.5) * (g[0][1] + g[1][0]);
+    const T S13 = T(0.5) * (g[0][2] + g[2][0]);
+    const T S23 = T(0.5) * (g[1][2] + g[2][1]);
+    const T S = sqrt(T(2) * (g[0][0] * g[0][0] + g[1][1] * g[1][1] + g[2][2] * g[2][2] +
+                             T(2) * (S12 * S12 + S13 * S13 + S23 * S23)));
+    return rr * CsDD * S;
+}
+
 // Flux of one face (src/fluxes.c): Riemann state from the two face states,
 // viscous and heat flux from the two adjacent cells (vm/Tm minus side, vp/Tp
 // plus side, by division) and the eight tangential neighbours (by
 // reciprocal; P/M = plus/minus cell, h/l = +/- along the first (1) and
 // second (2) tangential axis).  kc: grid spacings and transport constants
-// (rdx.., r4dx.., mu_L, lambda_L, cp_Pr_T).
-template <typename T, int N, typename KC>
+// (rdx.., r4dx.., mu_L, lambda_L, cp_Pr_T, CsDD).  muT is the face's SGS
+// viscosity; with SST (static Smagorinsky) it is the mean density of the two
+// cells beside the face, and the viscosity is formed here from the gradients.
+template <typename T, int N, bool SST = false, typename KC>
 FSL_HD void fused_face(const T *Lm, const T *Rp, const T *vm, T Tm, const T *vp, T Tp, const T *Ph1, const T *Mh1,
                        const T *Pl1, const T *Ml1, const T *Ph2, const T *Mh2, const T *Pl2, const T *Ml2, T muT,
                        const KC &kc, T *F)
@@ -519,6 +536,7 @@ FSL_HD void fused_face(const T *Lm, const T *Rp, const T *vm, T Tm, const T *vp,
         gr[q][t1] = (Ph1[q] + Mh1[q] - Pl1[q] - Ml1[q]) * rt1;
         gr[q][t2] = (Ph2[q] + Mh2[q] - Pl2[q] - Ml2[q]) * rt2;
     }
+    if constexpr (SST) muT = static_mu_t<T>(gr, muT, T(kc.CsDD));
     face_flux<T, N>(Rho, P, vel, gr, vp, vm, Tp, Tm, T(kc.mu_L), muT, T(kc.lambda_L), T(kc.cp_Pr_T), rdn, F);
 }
 

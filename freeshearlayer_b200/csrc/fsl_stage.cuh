@@ -235,7 +235,7 @@ __device__ __forceinline__ void plane_store(Smem<T, TJE, PPM> &s, int slot, int 
 
 // Velocities of plane `pl` (own column, from the shared ring) into the
 // reciprocal ring and the division plane with the face-averaged viscosity.
-template <typename T, int TJE, bool PPM>
+template <typename T, int TJE, bool PPM, bool SST>
 __device__ __forceinline__ void plane_prims(Smem<T, TJE, PPM> &s, int pl, int r, int l, T mu_pl, T mu_prev)
 {
     constexpr int HW = Smem<T, TJE, PPM>::HW, NS = Smem<T, TJE, PPM>::NS;
@@ -245,10 +245,12 @@ __device__ __forceinline__ void plane_prims(Smem<T, TJE, PPM> &s, int pl, int r,
     vdiv(u, dv);
     T *o = s.Dv[pl & 1][r][l];
     o[0] = dv[0]; o[1] = dv[1]; o[2] = dv[2]; o[3] = dv[3];
-    o[4] = T(0.5) * (mu_pl + mu_prev);
+    if constexpr (!SST) o[4] = T(0.5) * (mu_pl + mu_prev);
 }
 
-template <typename T, int TJE, int MINB, bool PPM>
+// SST: static Smagorinsky (the face viscosity from the face gradients and the
+// two cells' densities; no mu field is read).
+template <typename T, int TJE, int MINB, bool PPM, bool SST>
 __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Args<T> a)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -302,11 +304,13 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
                 for (int q = 0; q < 5; q++) s.U[(i0 - 1) & (NS - 1)][r + HW][l + HW][q] = Um[q];
             }
             vel_rcp(Um[0], Um[1], Um[2], Um[3], s.R[(i0 - 1) % 3][r][l]);
-            mum = mu[cj + (long long)(i0 - 1) * g.pi];
-            mu0 = mu[cj + (long long)i0 * g.pi];
-            mu1 = mu[cj + (long long)(i0 + 1) * g.pi];
-            plane_prims<T, TJE, PPM>(s, i0, r, l, mu0, mum);
-            plane_prims<T, TJE, PPM>(s, i0 + 1, r, l, mu1, mu0);
+            if constexpr (!SST) {
+                mum = mu[cj + (long long)(i0 - 1) * g.pi];
+                mu0 = mu[cj + (long long)i0 * g.pi];
+                mu1 = mu[cj + (long long)(i0 + 1) * g.pi];
+            }
+            plane_prims<T, TJE, PPM, SST>(s, i0, r, l, mu0, mum);
+            plane_prims<T, TJE, PPM, SST>(s, i0 + 1, r, l, mu1, mu0);
         }
         __syncthreads();
         if (inter) {
@@ -337,9 +341,10 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             vdiv(Um, dm);
             const T *dc = s.Dv[i0 & 1][r][l];
             const int sb = (i0 - 1) % 3, sf = i0 % 3;
-            fused_face<T, 1>(hm, lo, dm, dm[3], dc, dc[3], s.R[sf][r + 1][l], s.R[sb][r + 1][l],
-                             s.R[sf][r - 1][l], s.R[sb][r - 1][l], s.R[sf][r][l + 1], s.R[sb][r][l + 1],
-                             s.R[sf][r][l - 1], s.R[sb][r][l - 1], dc[4], kc, Fxp);
+            const T m_f = SST ? T(0.5) * (Uc[0] + Um[0]) : dc[4];
+            fused_face<T, 1, SST>(hm, lo, dm, dm[3], dc, dc[3], s.R[sf][r + 1][l], s.R[sb][r + 1][l],
+                                  s.R[sf][r - 1][l], s.R[sb][r - 1][l], s.R[sf][r][l + 1], s.R[sb][r][l + 1],
+                                  s.R[sf][r][l - 1], s.R[sb][r][l - 1], m_f, kc, Fxp);
 #pragma unroll
             for (int q = 0; q < 5; q++) hix[q] = hin[q];
         }
@@ -372,7 +377,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
                 }
             }
         }
-        if (live && i + 2 <= L + 1) mu2 = mu[cj + (long long)(i + 2) * g.pi];
+        if (!SST && live && i + 2 <= L + 1) mu2 = mu[cj + (long long)(i + 2) * g.pi];
         // (b) y and z reconstruction of cell (i, j, k): reads the state ring
         // only (plane i, stored two iterations ago)
         T hy[5], hz[5], lz[5];
@@ -445,9 +450,10 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
         if (ycol && r <= TJE - 2 && j <= H) {
             T F[5];
             const T *vm = s.Dv[u0][r][l], *vp = s.Dv[u0][r + 1][l];
-            fused_face<T, 2>(hy, s.Lo[r + 1][l], vm, vm[3], vp, vp[3], s.R[sp1][r + 1][l], s.R[sp1][r][l],
-                             s.R[sm1][r + 1][l], s.R[sm1][r][l], s.R[s0][r + 1][l + 1], s.R[s0][r][l + 1],
-                             s.R[s0][r + 1][l - 1], s.R[s0][r][l - 1], vp[4], kc, F);
+            const T m_f = SST ? T(0.5) * (s.U[q0][r + 1 + HW][l + HW][0] + s.U[q0][r + HW][l + HW][0]) : vp[4];
+            fused_face<T, 2, SST>(hy, s.Lo[r + 1][l], vm, vm[3], vp, vp[3], s.R[sp1][r + 1][l], s.R[sp1][r][l],
+                                  s.R[sm1][r + 1][l], s.R[sm1][r][l], s.R[s0][r + 1][l + 1], s.R[s0][r][l + 1],
+                                  s.R[s0][r + 1][l - 1], s.R[s0][r][l - 1], m_f, kc, F);
 #pragma unroll
             for (int q = 0; q < 5; q++) s.Fy[r][l][q] = F[q];
         }
@@ -461,9 +467,10 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             for (int q = 0; q < 5; q++) Fz[q] = T(0.);
             if (zrow && l <= 30 && k <= D) {
                 const T *vm = s.Dv[u0][r][l], *vp = s.Dv[u0][r][l + 1];
-                fused_face<T, 3>(hz, lzn, vm, vm[3], vp, vp[3], s.R[sp1][r][l + 1], s.R[sp1][r][l],
-                                 s.R[sm1][r][l + 1], s.R[sm1][r][l], s.R[s0][r + 1][l + 1], s.R[s0][r + 1][l],
-                                 s.R[s0][r - 1][l + 1], s.R[s0][r - 1][l], vp[4], kc, Fz);
+                const T m_f = SST ? T(0.5) * (s.U[q0][r + HW][l + 1 + HW][0] + s.U[q0][r + HW][l + HW][0]) : vp[4];
+                fused_face<T, 3, SST>(hz, lzn, vm, vm[3], vp, vp[3], s.R[sp1][r][l + 1], s.R[sp1][r][l],
+                                      s.R[sm1][r][l + 1], s.R[sm1][r][l], s.R[s0][r + 1][l + 1], s.R[s0][r + 1][l],
+                                      s.R[s0][r - 1][l + 1], s.R[s0][r - 1][l], m_f, kc, Fz);
             }
 #pragma unroll
             for (int q = 0; q < 5; q++) Fzm[q] = __shfl_up_sync(0xffffffffu, Fz[q], 1);
@@ -504,9 +511,10 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
                 for (int q = 0; q < 5; q++) lo[q] = a.bf.xL[q * nxf + fo];
             }
             const T *dc = s.Dv[u0][r][l], *dn = s.Dv[u1][r][l];
-            fused_face<T, 1>(hix, lo, dc, dc[3], dn, dn[3], s.R[sp1][r + 1][l], s.R[s0][r + 1][l],
-                             s.R[sp1][r - 1][l], s.R[s0][r - 1][l], s.R[sp1][r][l + 1], s.R[s0][r][l + 1],
-                             s.R[sp1][r][l - 1], s.R[s0][r][l - 1], dn[4], kc, Fx);
+            const T m_f = SST ? T(0.5) * (s.U[q1][r + HW][l + HW][0] + s.U[q0][r + HW][l + HW][0]) : dn[4];
+            fused_face<T, 1, SST>(hix, lo, dc, dc[3], dn, dn[3], s.R[sp1][r + 1][l], s.R[s0][r + 1][l],
+                                  s.R[sp1][r - 1][l], s.R[s0][r - 1][l], s.R[sp1][r][l + 1], s.R[s0][r][l + 1],
+                                  s.R[sp1][r][l - 1], s.R[s0][r][l - 1], m_f, kc, Fx);
         }
         __syncthreads();
         // (f) divergence and stage combination (src/evolution.c:29-161), FP64
@@ -558,7 +566,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             plane_store<T, TJE, PPM>(s, (i + 3) & (NS - 1), r, l, j, k, H, D, live && i + 3 <= L + 1, pl);
         else
             plane_store<T, TJE, PPM>(s, q0, r, l, j, k, H, D, live && i + 2 <= L + 1, pl);
-        if (live && i < i1) plane_prims<T, TJE, PPM>(s, i + 2, r, l, mu2, mu1);
+        if (live && i < i1) plane_prims<T, TJE, PPM, SST>(s, i + 2, r, l, mu2, mu1);
 #pragma unroll
         for (int q = 0; q < 5; q++) {
             Fxp[q] = Fx[q];
@@ -588,7 +596,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
     }
 }
 
-template <typename T, int TJE, int MINB, bool PPM = false>
+template <typename T, int TJE, int MINB, bool PPM = false, bool SST = false>
 int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, double *out, const T *mu, BF<T> bf,
                    bool courant)
 {
@@ -602,11 +610,11 @@ int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, doubl
     a.seg = c.stage_seg;
     const size_t smem = sizeof(Smem<T, TJE, PPM>);
     static std::atomic<uint64_t> attr{0};
-    if (!smem_limit_once((const void *)k_stage<T, TJE, MINB, PPM>, smem, attr)) return -1;
+    if (!smem_limit_once((const void *)k_stage<T, TJE, MINB, PPM, SST>, smem, attr)) return -1;
     dim3 b(32, TJE, 1);
     dim3 gr((g.D + 29) / 30, (g.H + TJE - 3) / (TJE - 2), (g.L + a.seg - 1) / a.seg);
     prof_begin(c, FSL_K_STAGE);
-    k_stage<T, TJE, MINB, PPM><<<gr, b, smem, c.stream>>>(g, c.k, a);
+    k_stage<T, TJE, MINB, PPM, SST><<<gr, b, smem, c.stream>>>(g, c.k, a);
     prof_end(c, FSL_K_STAGE, 1);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -62,6 +62,10 @@ extern "C" {
 /* subgrid closure */
 #define FSL_SGS_DYNAMIC 0 /* dynamic Smagorinsky (Germano-Lilly), src/turbulence.c:103-507 */
 #define FSL_SGS_LEARNED 1 /* per-cell MLP Cs^2 with the dynamic procedure as judge */
+#define FSL_SGS_STATIC 2  /* static Smagorinsky, rho_face Cs DD |S|_face per face: the reference's
+                             DynamicSmagorinskySGS 0 branch (src/fluxes.c:193-205, :362-374,
+                             :533-545), live in src-par (src-par/def.h:47); Cs from layer2.ini */
+#define FSL_SGS_NONE 3    /* no SGS viscosity (mu_SGS = 0) */
 
 /* reconstruction */
 #define FSL_RECON_CHARMINMOD 0 /* characteristic kappa=1/3 minmod(beta=4), src/reconstruction.c:26-345 */
@@ -255,7 +259,10 @@ int fsl_evolution(fsl_ctx *ctx, int stage); /* Evolution(nStages, Stage), src/ev
  * pointer to four consecutive (LEN+2)(HIG+2)(DEP+2) double arrays rho, rho u,
  * rho v, rho w (k fastest, ghost layer filled, e.g. by fsl_ghost_bc); mu:
  * device pointer to one such array, fully written (interior values, ghost
- * layer 0).  stream: a cudaStream_t, or NULL for the legacy default stream.
+ * layer 0).  stream: a cudaStream_t of the current device (another device's
+ * stream returns FSL_ERR_ARG), or NULL for the legacy default stream.  A CUDA
+ * error left pending by earlier work returns FSL_ERR_CUDA before any work and
+ * stays pending for its owner.
  *
  * Scratch is a fixed static device array of FSL_NOALLOC_SCRATCH_BYTES that
  * every GPU loading the library holds until process exit; it needs
@@ -361,13 +368,21 @@ int fsl_tecplot_write(const char *path, int LEN, int HIG, int DEP, const double 
  * coefficient Cs^2; mu_SGS = rho Cs^2 (dx dy dz)^(2/3) |S| as in the dynamic
  * procedure (src/turbulence.c:442).  With params.sgs = FSL_SGS_LEARNED the
  * steps use it; every `every` steps the dynamic procedure runs beside it as the
- * judge, and while the error of the plane-averaged SGS viscosity profile,
- * measured against the effective viscosity mu_L + <mu_SGS,dyn>(y) (the
- * quantity the viscous fluxes see), exceeds the threshold (default 0.02) the
- * steps fall back to the dynamic procedure.  The Cs^2 errors and the SGS
- * viscosity error relative to the dynamic SGS viscosity alone are reported
- * too; per cell the dynamic Cs^2 is dominated by cell-to-cell noise, and where
- * |S| vanishes it does not act. */
+ * judge, on the plane-averaged SGS viscosity profiles <mu>(y) of both closures
+ * over the cells at least two from every boundary.  The steps fall back to the
+ * dynamic procedure while either criterion fails:
+ *   - effective viscosity: |<mu_mlp> - <mu_dyn>|_2 / |mu_L + <mu_dyn>|_2 over
+ *     all rows exceeds `threshold` (fsl_closure_judge, default 0.02) -- what
+ *     the viscous fluxes see;
+ *   - SGS viscosity where the model acts: over the rows whose <mu_dyn> is at
+ *     least `floor` mu_L (fsl_closure_judge_active, default floor 0.1),
+ *     |<mu_mlp> - <mu_dyn>|_2 / |<mu_dyn>|_2 exceeds `threshold` (default
+ *     0.5).  Where the dynamic procedure gives SGS viscosity comparable to the
+ *     molecular one, a network that predicts too little (or nothing) fails
+ *     here even when the first criterion, dominated by mu_L, would pass.
+ * The Cs^2 errors and the SGS viscosity error relative to the dynamic SGS
+ * viscosity alone are reported too; per cell the dynamic Cs^2 is dominated by
+ * cell-to-cell noise, and where |S| vanishes it does not act. */
 #define FSL_CLOSURE_NPARAMS 9473 /* W1[64][16] b1 W2[64][64] b2 W3[64][64] b3 w4[64] b4 */
 
 typedef struct fsl_closure_stats {
@@ -378,13 +393,22 @@ typedef struct fsl_closure_stats {
                               (the fallback criterion) */
     int judgements, fallbacks, using_dynamic;
     unsigned last_step;
+    double mu_active_err;  /* last judgement: |<mu_mlp> - <mu_dyn>|_2 / |<mu_dyn>|_2 over the rows whose
+                              <mu_dyn> >= floor mu_L (0 when there are none) */
+    double dyn_ratio;      /* last judgement: max over rows of <mu_dyn>(y) / mu_L */
+    int active_rows;       /* last judgement: rows in mu_active_err */
+    int reserved_;
 } fsl_closure_stats;
 
 /* Feature scales: t_ref = delta_w0 / dU (time scale of |S|), len_ref = delta_w0. */
 int fsl_closure_set_scales(fsl_ctx *ctx, double t_ref, double len_ref);
 int fsl_closure_set_weights(fsl_ctx *ctx, const float *params);
 int fsl_closure_get_weights(fsl_ctx *ctx, float *params);
+/* Judge every `every` steps (0: never) with the effective-viscosity threshold. */
 int fsl_closure_judge(fsl_ctx *ctx, int every, double threshold);
+/* The second criterion: rows with <mu_dyn> >= floor mu_L are judged on the
+ * SGS viscosity profile itself, with `threshold` (floor > 0, threshold >= 0). */
+int fsl_closure_judge_active(fsl_ctx *ctx, double floor, double threshold);
 int fsl_closure_get_stats(fsl_ctx *ctx, fsl_closure_stats *stats);
 /* Both closures on the current U^n: Cs^2 of the MLP and of the dynamic
  * procedure (padded FP32 host arrays, either may be NULL) and the four errors

@@ -828,6 +828,32 @@ static void vel_div(double **u, size_t c, double *out, double *T)
     out[0] = U_; out[1] = V_; out[2] = W_;
 }
 
+/* The dynamic procedure computes mu_SGS unless the static model or none is
+ * selected (any other value, the learned closure's included, is the dynamic
+ * procedure here: the oracle has no learned closure). */
+static int sgs_dynamic(const orc_ctx *o) { return o->p.sgs != ORC_SGS_STATIC && o->p.sgs != ORC_SGS_NONE; }
+
+/* SGS viscosity of one face.  Dynamic: the average of mu_SGS over the plus
+ * cell and its x-neighbour (:191, and the reference's x-average on the y and
+ * z faces, :360, :531).  Static (the reference's DynamicSmagorinskySGS 0
+ * branch, src/fluxes.c:193-205 x, :362-374 y, :533-545 z): the mean density
+ * of the two cells beside the face times CsDD times |S| from the face
+ * velocity gradients. */
+static double face_mu_t(const orc_ctx *o, const double *mu, size_t plus, size_t xnb, double rp, double rm,
+                        double du_dx, double dv_dx, double dw_dx, double du_dy, double dv_dy, double dw_dy,
+                        double du_dz, double dv_dz, double dw_dz)
+{
+    double rr, S12, S13, S23, S;
+    if (o->p.sgs == ORC_SGS_NONE) return 0.0;
+    if (o->p.sgs != ORC_SGS_STATIC) return 0.5 * (mu[plus] + mu[xnb]);
+    rr = 0.5 * (rp + rm);
+    S12 = 0.5 * (du_dy + dv_dx);
+    S13 = 0.5 * (du_dz + dw_dx);
+    S23 = 0.5 * (dv_dz + dw_dy);
+    S = sqrt(2 * (du_dx * du_dx + dv_dy * dv_dy + dw_dz * dw_dz + 2 * (S12 * S12 + S13 * S13 + S23 * S23)));
+    return rr * (o->p.Cs * o->DD) * S;
+}
+
 void orc_fluxes_only(orc_ctx *o)
 {
     const int L = o->L, H = o->H, D = o->D;
@@ -865,7 +891,9 @@ void orc_fluxes_only(orc_ctx *o)
                 dv_dz = (Uk[1] + uk[1] - kU[1] - ku[1]) * o->r4dz;
                 dw_dz = (Uk[2] + uk[2] - kU[2] - ku[2]) * o->r4dz;
                 uu = 0.5 * (fw[0] + bw[0]); vv = 0.5 * (fw[1] + bw[1]); ww = 0.5 * (fw[2] + bw[2]);
-                mu_T = 0.5 * (mu[IC(o, i + 1, j + 1, k + 1)] + mu[IC(o, i, j + 1, k + 1)]); /* :191 */
+                mu_T = face_mu_t(o, mu, IC(o, i + 1, j + 1, k + 1), IC(o, i, j + 1, k + 1), u[0][IC(o, i + 1, j + 1, k + 1)],
+                                 u[0][IC(o, i, j + 1, k + 1)], du_dx, dv_dx, dw_dx, du_dy, dv_dy, dw_dy, du_dz, dv_dz,
+                                 dw_dz); /* :189-205 */
                 mu_E = o->p.mu_L + mu_T;
                 sxx = TWO_THIRDS * mu_E * (du_dx + du_dx - dv_dy - dw_dz);
                 sxy = mu_E * (du_dy + dv_dx);
@@ -911,7 +939,9 @@ void orc_fluxes_only(orc_ctx *o)
                 dv_dz = (Uk[1] + uk[1] - kU[1] - ku[1]) * o->r4dz;
                 dw_dz = (Uk[2] + uk[2] - kU[2] - ku[2]) * o->r4dz;
                 uu = 0.5 * (up[0] + lw[0]); vv = 0.5 * (up[1] + lw[1]); ww = 0.5 * (up[2] + lw[2]);
-                mu_T = 0.5 * (mu[IC(o, i + 1, j + 1, k + 1)] + mu[IC(o, i, j + 1, k + 1)]); /* :360 */
+                mu_T = face_mu_t(o, mu, IC(o, i + 1, j + 1, k + 1), IC(o, i, j + 1, k + 1), u[0][IC(o, i + 1, j + 1, k + 1)],
+                                 u[0][IC(o, i + 1, j, k + 1)], du_dx, dv_dx, dw_dx, du_dy, dv_dy, dw_dy, du_dz, dv_dz,
+                                 dw_dz); /* :358-374 */
                 mu_E = o->p.mu_L + mu_T;
                 syx = mu_E * (dv_dx + du_dy);
                 syy = TWO_THIRDS * mu_E * (dv_dy + dv_dy - du_dx - dw_dz);
@@ -957,7 +987,9 @@ void orc_fluxes_only(orc_ctx *o)
                 dv_dz = (nr[1] - fr[1]) * o->rdz;
                 dw_dz = (nr[2] - fr[2]) * o->rdz;
                 uu = 0.5 * (nr[0] + fr[0]); vv = 0.5 * (nr[1] + fr[1]); ww = 0.5 * (nr[2] + fr[2]);
-                mu_T = 0.5 * (mu[IC(o, i + 1, j + 1, k + 1)] + mu[IC(o, i, j + 1, k + 1)]); /* :531 */
+                mu_T = face_mu_t(o, mu, IC(o, i + 1, j + 1, k + 1), IC(o, i, j + 1, k + 1), u[0][IC(o, i + 1, j + 1, k + 1)],
+                                 u[0][IC(o, i + 1, j + 1, k)], du_dx, dv_dx, dw_dx, du_dy, dv_dy, dw_dy, du_dz, dv_dz,
+                                 dw_dz); /* :529-545 */
                 mu_E = o->p.mu_L + mu_T;
                 szx = mu_E * (dw_dx + du_dz);
                 szy = mu_E * (dw_dy + dv_dz);
@@ -976,7 +1008,7 @@ void orc_fluxes_only(orc_ctx *o)
 
 void orc_fluxes(orc_ctx *o)
 {
-    orc_dynamic_smagorinsky(o); /* src/fluxes.c:52-54 */
+    if (sgs_dynamic(o)) orc_dynamic_smagorinsky(o); /* src/fluxes.c:52-54 */
     orc_fluxes_only(o);
 }
 
@@ -1116,7 +1148,7 @@ static void step_impl(orc_ctx *o, int nsteps, int every_stage)
             orc_ghost_bc(o);
             orc_reconstruct(o);
             orc_interface_bc(o);
-            if (s == 1 || every_stage) orc_dynamic_smagorinsky(o);
+            if ((s == 1 || every_stage) && sgs_dynamic(o)) orc_dynamic_smagorinsky(o);
             orc_fluxes_only(o);
             orc_evolution(o, o->p.nStages, s);
         }

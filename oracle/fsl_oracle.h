@@ -48,7 +48,15 @@ typedef struct orc_params {
     int cfl_mode;  /* ORC_CFL_* */
     double seed_X; /* disturbance RNG seed (the reference reads it from stdin) */
     int recon;     /* 0: the reference's reconstruction, 1: PPM (project extension) */
+    int sgs;       /* ORC_SGS_*: the SGS viscosity the face fluxes use */
 } orc_params;
+
+/* SGS models (values as FSL_SGS_* of the product's C ABI).  DYNAMIC is the
+ * reference's hardcoded choice (src/def.h:47, DynamicSmagorinskySGS 1);
+ * STATIC is its other branch, rho_face Cs DD |S|_face per face
+ * (src/fluxes.c:193-205, :362-374, :533-545), live in src-par/def.h:47;
+ * NONE sets the SGS viscosity to zero. */
+enum { ORC_SGS_DYNAMIC = 0, ORC_SGS_STATIC = 2, ORC_SGS_NONE = 3 };
 
 typedef struct orc_ctx orc_ctx;
 

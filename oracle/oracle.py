@@ -19,7 +19,6 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_ORACLE = os.path.join(HERE, "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libfslref.so")
-REF_SRC = "/root/reference/src"
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
@@ -40,14 +39,15 @@ class OrcParams(C.Structure):
                 ("Va", C.c_double), ("Wa", C.c_double), ("Ns_min", C.c_int),
                 ("Nst", C.c_int), ("f_step", C.c_int), ("nStages", C.c_int),
                 ("maxCoNum", C.c_double), ("setup", C.c_int), ("cfl_mode", C.c_int),
-                ("seed_X", C.c_double), ("recon", C.c_int)]
+                ("seed_X", C.c_double), ("recon", C.c_int), ("sgs", C.c_int)]
 
 
 def build(ref: bool = False) -> None:
-    """Build liboracle.so (and, with ref=True and the reference present, _ref)."""
+    """Build liboracle.so (and, with ref=True and the reference sources present
+    -- FSL_REF_SRC, or a `reference` checkout beside the repository -- _ref)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and os.path.isdir(REF_SRC):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
 
 
 def ref_available() -> bool:
@@ -265,6 +265,7 @@ class RefOracle:
             lib.refh_random.argtypes = [C.c_double]
             lib.refh_random.restype = C.c_double
             lib.refh_output.argtypes = [C.c_char_p]
+            lib.refh_set_static.argtypes = [C.c_int]
             cls._lib = lib
         return cls._lib
 
@@ -279,6 +280,9 @@ class RefOracle:
         if rc != 0:
             raise RuntimeError("refh_init failed: %d" % rc)
         self.lib().refh_seed(p["seed_X"])
+        # the SGS model: the dynamic procedure (src/def.h:47) or, with
+        # sgs = 2, the static Smagorinsky branch of src/fluxes.c
+        self.lib().refh_set_static(1 if p.get("sgs", 0) == 2 else 0)
 
     def cells(self, which: int, var: int = 0) -> np.ndarray:
         a = np.empty(padded_shape(self.p), np.float64)
@@ -325,6 +329,7 @@ class RefOracle:
     def ifbc(self): self.lib().refh_ifbc()
     def dynsmag(self): self.lib().refh_dynsmag()
     def fluxes(self): self.lib().refh_fluxes()
+    def fluxes_static(self): self.lib().refh_fluxes_static()
     def evolution(self, nst, stage): self.lib().refh_evolution(nst, stage)
     def check_courant(self): self.lib().refh_checkco()
     def output(self, dir: str) -> int: return self.lib().refh_output(os.fsencode(dir))

@@ -34,6 +34,13 @@ void Evolution(int numStages, int Stage);
 /* the driver's block-period counter (a local of main() at src/layer2.c:120) */
 static int refh_counter = 0;
 
+/* src/fluxes.c compiled a second time with its static Smagorinsky branch
+ * live (DynamicSmagorinskySGS 0, as src-par/def.h:47 sets it; see
+ * ref_static.h).  refh_set_static(1) makes refh_step use it. */
+void Fluxes_static(void);
+static int refh_static = 0;
+void refh_set_static(int on) { refh_static = on; }
+
 /* Run Initialize() (src/initialize.c:14-192) with `dir` as the working
  * directory, so that it reads dir/layer2.ini (and dir/backup.dat on restart). */
 int refh_init(const char *dir)
@@ -77,7 +84,8 @@ void refh_step(int n)
             BounCondInGhostCells();
             Reconstruction();
             BounCondOnInterfaces();
-            Fluxes();
+            if (refh_static) Fluxes_static();
+            else Fluxes();
             Evolution(nStages, s);
         }
     }
@@ -87,6 +95,7 @@ void refh_ghost(void) { BounCondInGhostCells(); }
 void refh_recon(void) { Reconstruction(); }
 void refh_ifbc(void) { BounCondOnInterfaces(); }
 void refh_fluxes(void) { Fluxes(); }
+void refh_fluxes_static(void) { Fluxes_static(); }
 void refh_evolution(int nst, int stage) { Evolution(nst, stage); }
 void refh_dynsmag(void) { DynamicSmagorinsky(U1, U2, U3, U4, mu_SGS); }
 void refh_checkco(void) { checkCoNum(); }

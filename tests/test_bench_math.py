@@ -51,3 +51,31 @@ def test_peaks_fall_back_without_the_measured_file(tmp_path, monkeypatch):
     assert bench.measured_peaks() == {"hbm_gbs": 6650.0, "source": "fallback"}
     (tmp_path / "MEASURED_PEAKS.json").write_text('{"hbm_gbs": 7012.5, "bf16_tflops": 1600}')
     assert bench.measured_peaks() == {"hbm_gbs": 7012.5, "source": "measured"}
+
+
+def test_gpus_flag_starts_that_many_ranks():
+    """`bench.py --gpus 2` without a launcher starts two ranks under
+    torch.distributed.run (gloo here, no GPU work): the line's n_gpus is 2 and
+    its time the maximum over the ranks."""
+    import json
+    import subprocess
+    env = dict(os.environ, FSL_BENCH_BACKEND="gloo", OMP_NUM_THREADS="1")
+    env.pop("WORLD_SIZE", None)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--launcher-check"],
+                       capture_output=True, text=True, timeout=180, env=env, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    line = json.loads(lines[0])
+    assert line["n_gpus"] == 2 and line["ms_max"] == 11.0
+    assert line["value"] == pytest.approx(2 * 1000 / 11e-3)
+
+
+def test_gpus_flag_must_match_the_launcher():
+    """Under a launcher that started another number of ranks, bench.py fails
+    loudly instead of timing the wrong job."""
+    import subprocess
+    env = dict(os.environ, WORLD_SIZE="2", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "4", "--launcher-check"],
+                       capture_output=True, text=True, timeout=60, env=env, cwd=ROOT)
+    assert r.returncode != 0 and "WORLD_SIZE" in r.stderr

@@ -186,3 +186,60 @@ def test_fp32_dynamic_procedure_matches_fp64(fsl, trained):
     prof64, prof32 = a64.mean(axis=(0, 2)), a32.mean(axis=(0, 2))
     assert np.linalg.norm(prof32 - prof64) / np.linalg.norm(prof64) < 1e-2
     assert np.corrcoef(a64.ravel(), a32.ravel())[0, 1] > 0.99
+
+
+def _active_state(fsl, oracle_lib):
+    """A temporal layer whose velocity noise (5e-2 dU) at a high Reynolds
+    number (2e4) makes the dynamic procedure's SGS viscosity comparable to the
+    molecular one (plane averages up to several mu_L)."""
+    p = temporal_params(L=48, H=32, D=32, Mc=0.5, Re=20000.0)
+    s, dU = oracle_lib.Oracle.temporal_state(p, 0.5, amp=0.05)
+    return p, s, dU
+
+
+def _weights(fsl, kind):
+    w = fsl.closure_weights().copy()
+    if kind == "zero":
+        return np.zeros_like(w)
+    rng = np.random.default_rng(17)
+    for a, b in GROUPS.values():  # every parameter group permuted within itself
+        w[a:b] = rng.permutation(w[a:b])
+    return w
+
+
+@pytest.mark.parametrize("kind", ["zero", "shuffled"])
+def test_useless_weights_fall_back(fsl, oracle_lib, kind):
+    """The judge at its default thresholds catches a useless network: with the
+    shipped parameters zeroed, or permuted within each layer, on a state where
+    the dynamic SGS viscosity reaches more than 0.1 mu_L, the first judgement
+    (step 1) falls back, and the step is then exactly the dynamic procedure's."""
+    p, s, dU = _active_state(fsl, oracle_lib)
+    d = fsl.Domain(dict(p, sgs=1))
+    d.upload_state(s)
+    d.closure_set_scales(1.0 / dU, 1.0)
+    d.closure_set_weights(_weights(fsl, kind))
+    d.step(1)
+    st = d.closure_stats()
+    print("%s: dyn_ratio %.3f active rows %d mu_active_err %.3f visc_err %.4f" %
+          (kind, st.dyn_ratio, st.active_rows, st.mu_active_err, st.visc_err))
+    assert st.dyn_ratio > 0.1 and st.active_rows > 0
+    assert st.judgements == 1 and st.fallbacks >= 1 and st.using_dynamic == 1
+    ref = fsl.Domain(p)
+    ref.upload_state(s)
+    ref.step(1)
+    assert np.array_equal(d.download_state(), ref.download_state())
+
+
+def test_shipped_weights_on_an_active_state(fsl, oracle_lib):
+    """The shipped parameters judged on the same state: the errors are
+    reported; both criteria are computed on the rows where the model acts."""
+    p, s, dU = _active_state(fsl, oracle_lib)
+    d = fsl.Domain(dict(p, sgs=1))
+    d.upload_state(s)
+    d.closure_set_scales(1.0 / dU, 1.0)
+    d.closure_set_weights(fsl.closure_weights())
+    st = d.closure_compare()
+    print("shipped: dyn_ratio %.3f active rows %d mu_active_err %.3f mu_profile_err %.3f visc_err %.4f "
+          "cs2_profile_err %.3f" % (st.dyn_ratio, st.active_rows, st.mu_active_err, st.mu_profile_err,
+                                    st.visc_err, st.profile_err))
+    assert st.active_rows > 0 and np.isfinite(st.mu_active_err)

@@ -287,3 +287,63 @@ def test_c1_config_200_steps(fsl, oracle_lib):
     errs = per_var_rel_l2(a, b, p)
     assert max(errs) <= PARITY_RTOL, errs
     _assert_same(a, b, "state after 200 steps")
+
+
+@pytest.mark.parametrize("setup", [0, 1])
+@pytest.mark.parametrize("sgs", [2, 3])
+def test_steps_static_smagorinsky_and_no_sgs(fsl, oracle_lib, setup, sgs):
+    """The static Smagorinsky model (sgs = 2: the reference's
+    DynamicSmagorinskySGS 0 branch, rho_face Cs DD |S|_face per face,
+    src/fluxes.c:193-205, :362-374, :533-545) and no SGS model (sgs = 3):
+    whole fused steps (each tile shape) and per-phase steps bit-identical to
+    the oracle, whose static branch is pinned to the reference's own
+    (tests/test_oracle_vs_ref.py)."""
+    if setup == 0:
+        p = spatial_params(L=20, H=10, D=12, sgs=sgs)
+        from oracle.oracle import spatial_initial_state
+        s = spatial_initial_state(p)
+    else:
+        p = temporal_params(L=24, H=12, D=16, sgs=sgs, Re=20000.0)
+        s, _ = oracle_lib.Oracle.temporal_state(p, 0.4, amp=0.05)
+    o = oracle_lib.Oracle(p)
+    o.set_state(s)
+    o.step(6)
+    ref = o.state()
+    for rows in (16, 12, 8):
+        d = fsl.Domain(p)
+        d.tune(d.TUNE_STAGE_ROWS, rows)
+        d.upload_state(s)
+        d.step(6)
+        _assert_same(d.download_state(), ref, "fused steps, sgs %d, %d rows" % (sgs, rows))
+        d.close()
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    d.step_phased(6)
+    _assert_same(d.download_state(), ref, "per-phase steps, sgs %d" % sgs)
+    d.close()
+    # the model matters: the dynamic procedure's steps differ
+    q = oracle_lib.Oracle(dict(p, sgs=0))
+    q.set_state(s)
+    q.step(6)
+    assert not np.array_equal(q.state(), ref)
+
+
+def test_static_smagorinsky_ppm_and_fp32(fsl, oracle_lib):
+    """Static Smagorinsky with PPM reconstruction (bit-identical to the
+    oracle's restatement) and in the FP32 bulk (rho and E within FP32_RTOL of
+    the FP64 oracle after 8 steps)."""
+    p = temporal_params(L=16, H=10, D=12, sgs=2, Re=20000.0, recon=1)
+    s, _ = oracle_lib.Oracle.temporal_state(p, 0.4, amp=0.02)
+    o, d = _pair(fsl, oracle_lib, p, s)
+    o.step(4)
+    d.step(4)
+    _assert_same(d.download_state(), o.state(), "static Smagorinsky + PPM, 4 steps")
+    p32 = dict(p, recon=0)
+    o = oracle_lib.Oracle(p32)
+    o.set_state(s)
+    o.step(8)
+    d = fsl.Domain(dict(p32, precision=1))
+    d.upload_state(s)
+    d.step(8)
+    errs = per_var_rel_l2(d.download_state(), o.state(), p32)
+    assert errs[0] < FP32_RTOL and errs[4] < FP32_RTOL, errs

@@ -239,6 +239,28 @@ def test_step_stage_protocol(fsl):
     d.close()
 
 
+def test_per_phase_calls_refused_mid_step(fsl):
+    """While fsl_step_stage is in the middle of a step, the per-phase entry
+    points (which would overwrite the stage buffers the step holds) refuse,
+    and the step then completes as if they had not been called."""
+    p, s = _case(fsl, 1, L=32)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    d.step_stage()
+    for call in (d.ghost_bc, d.reconstruct, d.interface_bc, d.dynamic_smagorinsky, d.fluxes,
+                 lambda: d.evolution(1)):
+        with pytest.raises(fsl.FslError):
+            call()
+    d.step_stage()
+    d.step_stage()
+    ref = fsl.Domain(p)
+    ref.upload_state(s)
+    ref.step(1)
+    _same(d.download_state(), ref.download_state(), "a step with refused per-phase calls in between")
+    d.close()
+    ref.close()
+
+
 def test_slab_sums_add_up(fsl):
     """Volume integrals and per-row sums over the owned planes, added across
     slabs, equal the undivided domain's to rounding (another summation

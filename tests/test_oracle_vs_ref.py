@@ -137,3 +137,57 @@ def test_output_frame(orc, tmp_path):
     mine = tmp_path / "mine.plt"
     fsl.tecplot_write(str(mine), o.output_fields())
     assert mine.read_bytes() == ref_file.read_bytes()
+
+
+def test_static_smagorinsky_fluxes(orc):
+    """The static Smagorinsky branch of the reference's Fluxes()
+    (src/fluxes.c:193-205, :362-374, :533-545; dead in src, which hardcodes
+    the dynamic procedure, live in src-par/def.h:47) compiled in place with
+    the macro set to 0, against the restatement's sgs = 2: every face flux
+    bit-identical, and not equal to the dynamic procedure's."""
+    p = spatial_params(L=8, H=6, D=5, sgs=2)
+    s = random_state(p, 25)
+    r, o = _pair(orc, p, s)
+    r.set_disturbance(0, 3, 5.0, 1.0, -2.0)
+    o.set_disturbance(0, 3, 5.0, 1.0, -2.0)
+    for stage in (1, 2, 3):
+        r.ghost(); o.ghost()
+        r.recon(); o.recon()
+        r.ifbc(); o.ifbc()
+        r.fluxes_static(); o.fluxes()
+        for d in range(3):
+            for v in range(5):
+                _eq(o.faces(d, 0, v), r.faces(d, 0, v), "static flux %d %d stage %d" % (d, v, stage))
+        r.evolution(3, stage); o.evolution(3, stage)
+        for v in range(5):
+            _eq(o.cells(0, v), r.cells(0, v), "U%d stage %d" % (v + 1, stage))
+    # the dynamic procedure gives other fluxes on the same state
+    q = orc.Oracle(dict(p, sgs=0))
+    q.set_state(s)
+    q.set_disturbance(0, 3, 5.0, 1.0, -2.0)
+    q.ghost(); q.recon(); q.ifbc(); q.fluxes()
+    o2 = orc.Oracle(p)
+    o2.set_state(s)
+    o2.set_disturbance(0, 3, 5.0, 1.0, -2.0)
+    o2.ghost(); o2.recon(); o2.ifbc(); o2.fluxes()
+    assert not np.array_equal(q.faces(0, 0, 1), o2.faces(0, 0, 1))
+
+
+def test_static_smagorinsky_whole_steps(orc):
+    """Whole driver steps with the static branch (Courant rescale, disturbance
+    draw, three stages): the restatement equals the reference bit for bit."""
+    p = spatial_params(L=16, H=8, D=8, sgs=2)
+    s = orc.spatial_initial_state(p)
+    r, o = _pair(orc, p, s)
+    r.step(8); o.step(8)
+    _eq(o.state(), r.state(), "static SGS state after 8 steps")
+
+
+def test_no_sgs_is_static_with_zero_constant(orc):
+    """sgs = 3 (no SGS viscosity) equals the static model with Cs = 0."""
+    p = spatial_params(L=12, H=8, D=6)
+    s = random_state(p, 26)
+    a = orc.Oracle(dict(p, sgs=3)); a.set_state(s)
+    b = orc.Oracle(dict(p, sgs=2, Cs=0.0)); b.set_state(s)
+    a.step(3); b.step(3)
+    _eq(a.state(), b.state(), "no SGS vs Cs = 0")

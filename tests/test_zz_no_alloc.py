@@ -40,7 +40,9 @@ def _context_mu(fsl, p, state):
 
 
 @pytest.mark.parametrize("make_p", [lambda: spatial_params(L=24, H=16, D=12),
-                                    lambda: temporal_params(L=32, H=16, D=16)])
+                                    lambda: temporal_params(L=32, H=16, D=16),
+                                    # near the size limit, non-cubic: 66 x 34 x 34 padded cells
+                                    lambda: temporal_params(L=64, H=32, D=32)])
 def test_noalloc_matches_context_two_calls(make_p):
     import torch
     import freeshearlayer_b200 as fsl
@@ -69,3 +71,31 @@ def test_noalloc_rejects_oversize():
     # (LEN+2)(HIG+2)(DEP+2) above FSL_NOALLOC_MAX_CELLS: rejected before any device work
     rc = fn(buf.data_ptr(), buf.data_ptr(), 128, 64, 64, 1.0, 1.0, 1.0, None)
     assert rc == -9
+
+
+def test_noalloc_leaves_a_pending_error_to_its_owner():
+    """A CUDA error left pending by the caller's earlier work (here a refused
+    host-side allocation request, which touches no device) is reported as
+    FSL_ERR_CUDA before any work starts, and stays pending for its owner."""
+    import torch
+    import freeshearlayer_b200 as fsl
+    fn = _bind(fsl.lib())
+    rt = C.CDLL("libcudart.so.12")  # the runtime instance the library shares
+    rt.cudaMalloc.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
+    rt.cudaGetLastError.restype = C.c_int
+    rt.cudaPeekAtLastError.restype = C.c_int
+    p = temporal_params(L=16, H=8, D=8)
+    U = torch.zeros(4 * 18 * 10 * 10, dtype=torch.float64, device="cuda")
+    mu = torch.full((18 * 10 * 10,), 7.0, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    assert rt.cudaGetLastError() == 0
+    ptr = C.c_void_p()
+    assert rt.cudaMalloc(C.byref(ptr), 1 << 62) != 0  # far beyond any device: refused
+    pending = rt.cudaPeekAtLastError()
+    assert pending != 0
+    rc = fn(U.data_ptr(), mu.data_ptr(), p["LEN"], p["HIG"], p["DEP"], p["deltaX"], p["deltaY"],
+            p["deltaZ"], None)
+    assert rc == -3
+    assert rt.cudaGetLastError() == pending  # still the caller's, now cleared by its owner
+    torch.cuda.synchronize()
+    assert bool(torch.all(mu == 7.0))       # no work was queued
