@@ -653,6 +653,17 @@ def main_gpu(args):
     if rank == 0 and args.match_steps > 0:
         match = matched_error(fsl, grid, state, dU, args.match_steps, args.rows, args.seg)
 
+    # ---- what the learned closure gains, in a layer that turns turbulent ----
+    gain = None
+    if rank == 0 and args.gain_steps > 0:
+        from freeshearlayer_b200 import closure_gain
+        g = tuple(int(x) for x in args.gain_grid.split("x"))
+        gain = closure_gain.run(fsl, grid=g, steps=args.gain_steps, every=500)
+        for e in gain["arms"].values():  # the histories stay in validate's output
+            e.pop("theta_history", None)
+            e.pop("r12_max_history", None)
+        gain["apriori"] = gain["apriori"][-3:]
+
     # ---- batched ensemble of small uneven layers against the same run one by one ----
     ens = None
     if rank == 0 and args.ens_steps > 1:
@@ -704,6 +715,8 @@ def main_gpu(args):
             line["ppm"] = ppm
         if match is not None:
             line["matched_error"] = match
+        if gain is not None:
+            line["closure_gain"] = gain
         if ens is not None:
             line["ensemble"] = ens
         if slabs is not None:
@@ -810,6 +823,9 @@ def main():
     ap.add_argument("--slabs", type=int, default=2)
     ap.add_argument("--match-steps", type=int, default=200,
                     help="steps of the matched-error comparison against the plain FP64 path (0: skip)")
+    ap.add_argument("--gain-steps", type=int, default=10000,
+                    help="steps of the turbulent comparison of SGS models (0: skip)")
+    ap.add_argument("--gain-grid", default="128x64x64")
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the dominant kernel from an ncu capture")
     ap.add_argument("--ref-worker", nargs=4, default=None, help=argparse.SUPPRESS)

@@ -423,12 +423,16 @@ int fsl_init(const fsl_params *p, fsl_ctx **out)
     Ctx &c = h->c;
     c.p = *p;
     c.device = dev;
+    c.sms = prop.multiProcessorCount > 0 ? prop.multiProcessorCount : 1;
     c.g = make_grid(p->LEN, p->HIG, p->DEP, 8);
     c.co_i0 = 1;
     c.co_i1 = p->LEN;
     // x planes per fused-stage block: 48 measured fastest for the FP32 bulk
     // at 512x256x256 (1.6 % over 32); 32 for FP64
     c.stage_seg = (p->precision == FSL_PREC_FP32) ? 48 : 32;
+    // the FP32 bulk's reference-scheme stages run the full-lane persistent
+    // tile (rows 0); FP64 and PPM stages the ring tiles (rows 16)
+    c.stage_tje = (p->precision == FSL_PREC_FP32) ? 0 : 16;
     // derived constants, src/initialize.c:67-94
     c.k.rdx = 1. / p->deltaX; c.k.rdy = 1. / p->deltaY; c.k.rdz = 1. / p->deltaZ;
     c.k.r4dx = 1. / (4 * p->deltaX); c.k.r4dy = 1. / (4 * p->deltaY); c.k.r4dz = 1. / (4 * p->deltaZ);
@@ -1113,12 +1117,16 @@ int fsl_tune(fsl_ctx *h, int key, int value)
     Ctx &c = h->c;
     switch (key) {
     case FSL_TUNE_STAGE_ROWS:
-        if (value != 8 && value != 12 && value != 16) return FSL_ERR_ARG;
+        if (value != 0 && value != 8 && value != 12 && value != 16) return FSL_ERR_ARG;
         c.stage_tje = value;
         return FSL_OK;
     case FSL_TUNE_STAGE_SEG:
         if (value < 1 || value > 1 << 20) return FSL_ERR_ARG;
         c.stage_seg = value;
+        return FSL_OK;
+    case FSL_TUNE_INFER_TILES:
+        if (value != 1 && value != 2) return FSL_ERR_ARG;
+        c.infer_tiles = value;
         return FSL_OK;
     default:
         return FSL_ERR_ARG;

@@ -272,14 +272,16 @@ int fsl_ensemble_tune(fsl_ensemble *e, int trial_steps, int *rows_out, int *seg_
     std::vector<Snapshot> snap(e->m.size());
     for (size_t q = 0; q < e->m.size(); q++)
         if ((rc = take(e->m[q]->c, snap[q]))) return ens_fail(e, rc, "tuner snapshot");
-    const int rows_c[3] = {8, 12, 16}, seg_c[5] = {8, 16, 32, 48, 64};
+    // rows 0: the full-lane persistent tile (FP32 bulk, reference scheme;
+    // it balances its own planes, so one planes-per-block value is tried)
+    const int rows_c[4] = {0, 8, 12, 16}, seg_c[5] = {8, 16, 32, 48, 64};
     int best_r = e->m[0]->c.stage_tje, best_s = e->m[0]->c.stage_seg;
     double best = 1e300;
     cudaEvent_t a = nullptr, b = nullptr;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    for (int ri = 0; ri < 3 && !rc; ri++)
-        for (int si = 0; si < 5 && !rc; si++) {
+    for (int ri = 0; ri < 4 && !rc; ri++)
+        for (int si = 0; si < (rows_c[ri] == 0 ? 1 : 5) && !rc; si++) {
             for (fsl_ctx *h : e->m) {
                 h->c.stage_tje = rows_c[ri];
                 h->c.stage_seg = seg_c[si];

@@ -7,6 +7,7 @@
 // state, converts it once to FP32 in shared memory, and adds the FP32 flux
 // divergence to the FP64 state in FP64.
 #include "fsl_stage.cuh"
+#include "fsl_stage_wide.cuh"
 
 namespace fsl {
 
@@ -35,6 +36,7 @@ static int stage32(Ctx &c, int stage, const double *cur, const double *un, doubl
         }
     }
     switch (c.stage_tje) {
+    case 0: return wide::launch_wide<SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
     case 8: return stage::launch_stage_t<float, 8, 2, false, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
     case 12: return stage::launch_stage_t<float, 12, 1, false, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
     default: return stage::launch_stage_t<float, 16, 1, false, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);

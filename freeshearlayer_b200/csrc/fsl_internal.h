@@ -91,6 +91,7 @@ struct Ctx {
     Grid g;
     cudaStream_t stream = nullptr;
     int device = 0;
+    int sms = 148; // streaming multiprocessors of the device
     // cell fields (FP64): U^n, stage buffer, second stage buffer, mu_SGS
     double *U = nullptr, *Up = nullptr, *Uq = nullptr, *mu = nullptr;
     int cur = 0; // 0: U*_ = U, 1: U*_ = Up
@@ -105,7 +106,7 @@ struct Ctx {
     BFaces32 bf32{};
     float *mu32 = nullptr;
     bool fp32_alloc = false;
-    int stage_tje = 16; // rows per fused-stage tile (incl. the two halo rows)
+    int stage_tje = 16; // rows per fused-stage ring tile (incl. the two halo rows); 0: full-lane tile (FP32)
     int stage_seg = 32; // x planes per fused-stage block (fsl_init: 48 for FP32 bulk)
     // learned closure
     ClosureScales cls{};
@@ -118,6 +119,7 @@ struct Ctx {
     float *cl_vel = nullptr;    // FP32 velocities of the padded cells (closure features), 3 fields
     double *judge_rows = nullptr; // [2][HIG][4] plane sums of the judgement (Cs^2, mu_SGS)
     bool cl_alloc = false, cl_weights = false;
+    int infer_tiles = 2;        // closure inference: tiles in flight per block (1 or 2)
     int judge_every = 100;
     double judge_thr = 0.02;
     bool using_dynamic = false;

@@ -1,0 +1,565 @@
+// fsl_stage_wide.cuh -- the FP32-bulk fused RK3 stage kernel with a full-lane
+// tile, for the reference reconstruction (src/reconstruction.c:26-345).
+//
+// The ring-tile kernel (fsl_stage.cuh) gives each of its 32 x TJE threads a
+// cell of a tile that includes its own one-cell halo ring: the ring threads
+// load and reconstruct, then idle through the x sweep, the three face fluxes
+// and the stage combination, and a 30-wide tile leaves lanes empty where the
+// domain's DEP is a multiple of 32.  Here every thread owns an interior
+// column: a block of 16 warps x 32 lanes owns a 16 (y) x 32 (z) tile and the
+// halo ring's work is handed out as whole-warp tasks:
+//   - loads of the state halo (two rows and two columns on each side) and the
+//     velocities of the one-cell ring: threads 0..195, one cell each;
+//   - the y sweeps of the two halo rows and the z sweeps of the two halo
+//     columns (warps 13, 14, 15), before the first barrier of a plane;
+//   - the fluxes of the tile's bottom y faces and left z faces (warps 12
+//     and 11), between the two barriers.
+// The tile's own faces (the y face above each cell, the z face beyond it,
+// the x face ahead of it) are computed once each, as in the ring-tile kernel;
+// the z faces exchange states and fluxes between neighbouring lanes by warp
+// shuffles.  Arithmetic, boundary rules and the march along x (planes i+2 in
+// flight while plane i is computed, two barriers per plane) are those of the
+// ring-tile kernel.
+//
+// The grid is persistent: one block per SM (or fewer for small domains) takes
+// an equal share of the domain's (tile, plane) pairs, i.e. at most two
+// x-segments of tiles, so every SM gets the same number of planes and there is
+// no tail wave.
+#pragma once
+
+#include "fsl_stage.cuh"
+
+namespace fsl {
+namespace wide {
+
+using stage::Args;
+using stage::BF;
+using stage::load5;
+using stage::recon_at;
+
+constexpr int WJ = 16;  // tile rows (warps)
+constexpr int WK = 32;  // tile columns (lanes)
+constexpr int NT = WJ * WK;
+constexpr int NHALO = 196; // state halo cells loaded per plane (see halo_cell)
+
+template <typename T> struct Smem {
+    T U[2][WJ + 4][WK + 4][5];  // state of planes i, i+1: rows -2..17, cols -2..33
+    T R[3][WJ + 2][WK + 2][3];  // velocities by reciprocal, planes i-1, i, i+1: rows -1..16, cols -1..32
+    T Dv[2][WJ + 2][WK + 2][5]; // velocities by division, T, face-averaged mu: planes i, i+1
+    T Lo[WJ + 1][WK][5];        // y sweep, state on the face below: rows 0..16
+    T Fy[WJ + 1][WK][5];        // y flux of the face below row r (r = 0..16: faces j0-1/2 .. j0+15+1/2)
+    T HyB[WK][5];               // y sweep of halo row -1, state on the face above it
+    T HzL[WJ][5];               // z sweep of halo column -1, state on the face beyond it
+    T LzR[WJ][5];               // z sweep of halo column 32, state on the face before it
+    T Lz0[WJ][5];               // z sweep of column 0, state on the face before it
+    T FzL[WJ][5];               // z flux of the face before column 0
+    double comax[WJ][WK];       // Courant maxima of the cells written
+};
+
+// Ring coordinates of state-halo cell h (0..195) of a tile: rows -2, -1, 16,
+// 17 over the 32 columns (h < 128), columns -2, -1, 32, 33 over the 16 rows
+// (h < 192), and the four corners of the one-cell ring (h < 196).  The
+// velocity ring's halo (rows -1 and 16 over columns -1..32, columns -1 and
+// 32 over rows 0..15) is the subset h in [32, 96) U [144, 176) U [192, 196).
+__device__ __forceinline__ void halo_cell(int h, int &hr, int &hc)
+{
+    if (h < 128) {
+        const int row = h >> 5;
+        hr = row == 0 ? -2 : row == 1 ? -1 : row == 2 ? WJ : WJ + 1;
+        hc = h & 31;
+    } else if (h < 192) {
+        const int col = (h - 128) >> 4;
+        hc = col == 0 ? -2 : col == 1 ? -1 : col == 2 ? WK : WK + 1;
+        hr = (h - 128) & 15;
+    } else {
+        const int q = h - 192;
+        hr = (q & 1) ? WJ : -1;
+        hc = (q & 2) ? WK : -1;
+    }
+}
+
+__device__ __forceinline__ bool halo_has_velocity(int h)
+{
+    return (h >= 32 && h < 96) || (h >= 144 && h < 176) || (h >= 192 && h < NHALO);
+}
+
+// velocities of one cell of the state ring into the velocity rings
+template <typename T, bool SST>
+__device__ __forceinline__ void cell_prims(Smem<T> &s, int pl, int rr, int cc, T mu_pl, T mu_prev)
+{
+    const T *u = s.U[pl & 1][rr + 2][cc + 2];
+    vel_rcp(u[0], u[1], u[2], u[3], s.R[pl % 3][rr + 1][cc + 1]);
+    T dv[4];
+    vdiv(u, dv);
+    T *o = s.Dv[pl & 1][rr + 1][cc + 1];
+    o[0] = dv[0]; o[1] = dv[1]; o[2] = dv[2]; o[3] = dv[3];
+    if constexpr (!SST) o[4] = T(0.5) * (mu_pl + mu_prev);
+}
+
+template <typename T> __device__ __forceinline__ void store5(T *dst, const double *v)
+{
+#pragma unroll
+    for (int q = 0; q < 5; q++) dst[q] = T(v[q]);
+}
+
+// The y sweep of ring cell (rr, cc) of plane slot q: hi (face above) and lo
+// (face below), from the state ring.
+template <typename T>
+__device__ __forceinline__ void sweep_y(const Smem<T> &s, int q, int rr, int cc, T *hi, T *lo)
+{
+    CellC<T> c;
+    const T *Uc = s.U[q][rr + 2][cc + 2];
+#pragma unroll
+    for (int v = 0; v < 5; v++) c.u[v] = Uc[v];
+    cell_consts(c);
+    const T *a1 = s.U[q][rr + 3][cc + 2], *b1 = s.U[q][rr + 1][cc + 2];
+    T fw[5] = {a1[0], a1[2], a1[3], a1[1], a1[4]};
+    T bw[5] = {b1[0], b1[2], b1[3], b1[1], b1[4]};
+    recon_y(c, fw, bw, hi, lo);
+}
+
+template <typename T>
+__device__ __forceinline__ void sweep_z(const Smem<T> &s, int q, int rr, int cc, T *hi, T *lo)
+{
+    CellC<T> c;
+    const T *Uc = s.U[q][rr + 2][cc + 2];
+#pragma unroll
+    for (int v = 0; v < 5; v++) c.u[v] = Uc[v];
+    cell_consts(c);
+    const T *a1 = s.U[q][rr + 2][cc + 3], *b1 = s.U[q][rr + 2][cc + 1];
+    T fw[5] = {a1[0], a1[3], a1[1], a1[2], a1[4]};
+    T bw[5] = {b1[0], b1[3], b1[1], b1[2], b1[4]};
+    recon_z(c, fw, bw, hi, lo);
+}
+
+// y flux of the face between ring rows rr and rr+1 at column cc, plane i
+// (velocity slots: s0 plane i, sm1 plane i-1, sp1 plane i+1; u0 Dv of plane i)
+template <typename T, bool SST>
+__device__ __forceinline__ void face_y(const Smem<T> &s, const Consts &kc, int q0, int u0, int sm1, int s0, int sp1,
+                                       int rr, int cc, const T *Lm, const T *Rp, T *F)
+{
+    const int a = rr + 1, b = cc + 1;
+    const T *vm = s.Dv[u0][a][b], *vp = s.Dv[u0][a + 1][b];
+    const T m_f = SST ? T(0.5) * (s.U[q0][rr + 3][cc + 2][0] + s.U[q0][rr + 2][cc + 2][0]) : vp[4];
+    fused_face<T, 2, SST>(Lm, Rp, vm, vm[3], vp, vp[3], s.R[sp1][a + 1][b], s.R[sp1][a][b], s.R[sm1][a + 1][b],
+                          s.R[sm1][a][b], s.R[s0][a + 1][b + 1], s.R[s0][a][b + 1], s.R[s0][a + 1][b - 1],
+                          s.R[s0][a][b - 1], m_f, kc, F);
+}
+
+// z flux of the face between ring columns cc and cc+1 at row rr, plane i
+template <typename T, bool SST>
+__device__ __forceinline__ void face_z(const Smem<T> &s, const Consts &kc, int q0, int u0, int sm1, int s0, int sp1,
+                                       int rr, int cc, const T *Lm, const T *Rp, T *F)
+{
+    const int a = rr + 1, b = cc + 1;
+    const T *vm = s.Dv[u0][a][b], *vp = s.Dv[u0][a][b + 1];
+    const T m_f = SST ? T(0.5) * (s.U[q0][rr + 2][cc + 3][0] + s.U[q0][rr + 2][cc + 2][0]) : vp[4];
+    fused_face<T, 3, SST>(Lm, Rp, vm, vm[3], vp, vp[3], s.R[sp1][a][b + 1], s.R[sp1][a][b], s.R[sm1][a][b + 1],
+                          s.R[sm1][a][b], s.R[s0][a + 1][b + 1], s.R[s0][a + 1][b], s.R[s0][a - 1][b + 1],
+                          s.R[s0][a - 1][b], m_f, kc, F);
+}
+
+template <typename T, bool SST>
+__global__ void __launch_bounds__(NT, 1) k_stage_wide(Grid g, Consts kc, Args<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Smem<T> &s = *reinterpret_cast<Smem<T> *>(smraw);
+    const int L = g.L, H = g.H, D = g.D;
+    const int t = threadIdx.x, r = t >> 5, l = t & 31;
+    const long long fs = g.fstride;
+    const double *__restrict__ cu = a.cur;
+    const T *__restrict__ mu = a.mu;
+    const long long nxf = (long long)H * D, nyf = (long long)L * D, nzf = (long long)L * H;
+    const double dtx = a.ds->dtx, dty = a.ds->dty, dtz = a.ds->dtz;
+    const double one_third = 1. / 3., two_thirds = 2. / 3.;
+    // this thread's halo cell (threads 0..195)
+    int hr = 0, hc = 0;
+    const bool hthread = t < NHALO;
+    if (hthread) halo_cell(t, hr, hc);
+    const bool hvel = hthread && halo_has_velocity(t);
+    s.comax[r][l] = 0.0;
+
+    const int ntk = (D + WK - 1) / WK, ntj = (H + WJ - 1) / WJ;
+    const long long total = (long long)ntk * ntj * L;
+    long long pos = total * blockIdx.x / gridDim.x;
+    const long long end = total * (blockIdx.x + 1) / gridDim.x;
+    while (pos < end) {
+        const long long tile = pos / L;
+        const int i0 = (int)(pos % L) + 1;
+        const int i1 = (int)min((long long)L, (long long)i0 + (end - pos) - 1);
+        pos += i1 - i0 + 1;
+        const int k0 = (int)(tile % ntk) * WK + 1, j0 = (int)(tile / ntk) * WJ + 1;
+        const int j = j0 + r, k = k0 + l;
+        const bool own = j <= H && k <= D;               // interior cell of this thread
+        const bool live = j <= H + 1 && k <= D + 1;      // cell in the padded array
+        const long long cj = g.idx(0, j, k);
+        // halo cell of this thread (padded indices)
+        const int hj = j0 + hr, hk = k0 + hc;
+        const bool hlive = hthread && hj >= 0 && hj <= H + 1 && hk >= 0 && hk <= D + 1;
+        const bool hvlive = hvel && hlive;
+        const long long hcj = g.idx(0, hj, hk);
+        const bool ybot = j0 > 1, ytop = j0 + WJ <= H, zlft = k0 > 1, zrgt = k0 + WK <= D;
+
+        T hix[5], Fxp[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) hix[q] = Fxp[q] = T(0.);
+        T mu0 = 0, mu1 = 0, mu2 = 0, hmu0 = 0, hmu1 = 0, hmu2 = 0;
+        double pown[5], phal[5], base[5], unv[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) pown[q] = phal[q] = base[q] = unv[q] = 0.;
+
+        __syncthreads(); // the previous segment's readers of the rings are done
+        // ---- prologue: planes i0, i0+1 into the state ring, velocities of
+        // planes i0-1 .. i0+1, the flux of face i0 - 1/2 ----
+        {
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+                const int pl = i0 + p;
+                if (live && pl <= L + 1) {
+                    load5(cu, fs, cj + (long long)pl * g.pi, pown);
+                    store5(s.U[pl & 1][r + 2][l + 2], pown);
+                }
+                if (hlive && pl <= L + 1) {
+                    load5(cu, fs, hcj + (long long)pl * g.pi, phal);
+                    store5(s.U[pl & 1][hr + 2][hc + 2], phal);
+                }
+            }
+            T Um[5] = {0, 0, 0, 0, 0}, mum = 0, hmum = 0;
+            if (live) {
+                load5(cu, fs, cj + (long long)(i0 - 1) * g.pi, Um);
+                vel_rcp(Um[0], Um[1], Um[2], Um[3], s.R[(i0 - 1) % 3][r + 1][l + 1]);
+                if constexpr (!SST) {
+                    mum = mu[cj + (long long)(i0 - 1) * g.pi];
+                    mu0 = mu[cj + (long long)i0 * g.pi];
+                    mu1 = mu[cj + (long long)(i0 + 1) * g.pi];
+                }
+                cell_prims<T, SST>(s, i0, r, l, mu0, mum);
+                cell_prims<T, SST>(s, i0 + 1, r, l, mu1, mu0);
+            }
+            if (hvlive) {
+                T Hm[5];
+                load5(cu, fs, hcj + (long long)(i0 - 1) * g.pi, Hm);
+                vel_rcp(Hm[0], Hm[1], Hm[2], Hm[3], s.R[(i0 - 1) % 3][hr + 1][hc + 1]);
+                if constexpr (!SST) {
+                    hmum = mu[hcj + (long long)(i0 - 1) * g.pi];
+                    hmu0 = mu[hcj + (long long)i0 * g.pi];
+                    hmu1 = mu[hcj + (long long)(i0 + 1) * g.pi];
+                }
+                cell_prims<T, SST>(s, i0, hr, hc, hmu0, hmum);
+                cell_prims<T, SST>(s, i0 + 1, hr, hc, hmu1, hmu0);
+            }
+            __syncthreads();
+            if (own) {
+                T hm[5], lo[5], hin[5], dm[4], tmp[5];
+                const T *Uc = s.U[i0 & 1][r + 2][l + 2], *Un = s.U[(i0 + 1) & 1][r + 2][l + 2];
+                {
+                    CellC<T> cc;
+#pragma unroll
+                    for (int q = 0; q < 5; q++) cc.u[q] = Uc[q];
+                    cell_consts(cc);
+                    recon_x(cc, Un, Um, hin, lo);
+                }
+                if (i0 == 1) {
+                    const long long fo = (long long)(j - 1) * D + (k - 1);
+#pragma unroll
+                    for (int q = 0; q < 5; q++) hm[q] = a.bf.x0[q * nxf + fo];
+                } else {
+                    recon_at<T, 0>(g, cu, cj + (long long)(i0 - 1) * g.pi, hm, tmp);
+                }
+                vdiv(Um, dm);
+                const T *dc = s.Dv[i0 & 1][r + 1][l + 1];
+                const int sb = (i0 - 1) % 3, sf = i0 % 3;
+                const T m_f = SST ? T(0.5) * (Uc[0] + Um[0]) : dc[4];
+                fused_face<T, 1, SST>(hm, lo, dm, dm[3], dc, dc[3], s.R[sf][r + 2][l + 1], s.R[sb][r + 2][l + 1],
+                                      s.R[sf][r][l + 1], s.R[sb][r][l + 1], s.R[sf][r + 1][l + 2],
+                                      s.R[sb][r + 1][l + 2], s.R[sf][r + 1][l], s.R[sb][r + 1][l], m_f, kc, Fxp);
+#pragma unroll
+                for (int q = 0; q < 5; q++) hix[q] = hin[q];
+            }
+        }
+
+        for (int i = i0; i <= i1; i++) {
+            const int sm1 = (i + 2) % 3, s0 = i % 3, sp1 = (i + 1) % 3;
+            const int q0 = i & 1, q1 = (i + 1) & 1;
+            // (a) plane i+2 in flight; the FP64 operands of the combination
+            if (live && i + 2 <= L + 1) load5(cu, fs, cj + (long long)(i + 2) * g.pi, pown);
+            if (hlive && i + 2 <= L + 1) load5(cu, fs, hcj + (long long)(i + 2) * g.pi, phal);
+            if (own) {
+                const long long c = cj + (long long)i * g.pi;
+#pragma unroll
+                for (int q = 0; q < 5; q++) base[q] = cu[q * fs + c];
+                if (a.stage != 1) {
+#pragma unroll
+                    for (int q = 0; q < 5; q++) unv[q] = a.un[q * fs + c];
+                }
+            }
+            if constexpr (!SST) {
+                if (live && i + 2 <= L + 1) mu2 = mu[cj + (long long)(i + 2) * g.pi];
+                if (hvlive && i + 2 <= L + 1) hmu2 = mu[hcj + (long long)(i + 2) * g.pi];
+            }
+            // (b) y and z sweeps of the own cell, the boundary outer states,
+            // and the halo sweeps (warps 13..15)
+            T hy[5], hz[5], lz[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) hy[q] = hz[q] = lz[q] = T(0.);
+            if (own) {
+                CellC<T> cc;
+                const T *Uc = s.U[q0][r + 2][l + 2];
+#pragma unroll
+                for (int q = 0; q < 5; q++) cc.u[q] = Uc[q];
+                cell_consts(cc);
+                T lo[5];
+                {
+                    const T *a1 = s.U[q0][r + 3][l + 2], *b1 = s.U[q0][r + 1][l + 2];
+                    T fw[5] = {a1[0], a1[2], a1[3], a1[1], a1[4]};
+                    T bw[5] = {b1[0], b1[2], b1[3], b1[1], b1[4]};
+                    recon_y(cc, fw, bw, hy, lo);
+                }
+#pragma unroll
+                for (int q = 0; q < 5; q++) s.Lo[r][l][q] = lo[q];
+                {
+                    const T *a1 = s.U[q0][r + 2][l + 3], *b1 = s.U[q0][r + 2][l + 1];
+                    T fw[5] = {a1[0], a1[3], a1[1], a1[2], a1[4]};
+                    T bw[5] = {b1[0], b1[3], b1[1], b1[2], b1[4]};
+                    recon_z(cc, fw, bw, hz, lz);
+                }
+                if (l == 0) {
+#pragma unroll
+                    for (int q = 0; q < 5; q++) s.Lz0[r][q] = lz[q];
+                }
+            } else if (j == H + 1 && k <= D) {
+                // the face below this ghost row: the top boundary's outer state
+                const long long fo = (long long)(i - 1) * D + (k - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) s.Lo[r][l][q] = a.bf.yH[q * nyf + fo];
+            } else if (k == D + 1 && j <= H) {
+                // beyond the last column: the far z boundary's outer state (shuffled to lane l-1)
+                const long long fo = (long long)(i - 1) * H + (j - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) lz[q] = a.bf.zD[q * nzf + fo];
+            }
+            if (r == WJ - 3) {
+                // halo row -1: its state on the face above (the tile's bottom faces)
+                if (k <= D) {
+                    T hb[5], tmp[5];
+                    if (ybot) {
+                        sweep_y(s, q0, -1, l, hb, tmp);
+                    } else {
+                        const long long fo = (long long)(i - 1) * D + (k - 1);
+#pragma unroll
+                        for (int q = 0; q < 5; q++) hb[q] = a.bf.y0[q * nyf + fo];
+                    }
+#pragma unroll
+                    for (int q = 0; q < 5; q++) s.HyB[l][q] = hb[q];
+                }
+            } else if (r == WJ - 2) {
+                // halo row 16: its state on the face below (the tile's top
+                // faces), or the top boundary's outer state when row 16 is
+                // the ghost row
+                if (k <= D) {
+                    if (ytop) {
+                        T lo[5], tmp[5];
+                        sweep_y(s, q0, WJ, l, tmp, lo);
+#pragma unroll
+                        for (int q = 0; q < 5; q++) s.Lo[WJ][l][q] = lo[q];
+                    } else if (j0 + WJ == H + 1) {
+                        const long long fo = (long long)(i - 1) * D + (k - 1);
+#pragma unroll
+                        for (int q = 0; q < 5; q++) s.Lo[WJ][l][q] = a.bf.yH[q * nyf + fo];
+                    }
+                }
+            } else if (r == WJ - 1) {
+                // halo columns -1 (lanes 0..15) and 32 (lanes 16..31)
+                const int rr = l & 15, jr = j0 + rr;
+                if (jr <= H) {
+                    T hv[5], lv[5];
+                    if (l < 16) {
+                        if (zlft) {
+                            sweep_z(s, q0, rr, -1, hv, lv);
+                        } else {
+                            const long long fo = (long long)(i - 1) * H + (jr - 1);
+#pragma unroll
+                            for (int q = 0; q < 5; q++) hv[q] = a.bf.z0[q * nzf + fo];
+                        }
+#pragma unroll
+                        for (int q = 0; q < 5; q++) s.HzL[rr][q] = hv[q];
+                    } else if (k0 + WK - 1 <= D) {
+                        if (zrgt) {
+                            sweep_z(s, q0, rr, WK, hv, lv);
+                        } else {
+                            const long long fo = (long long)(i - 1) * H + (jr - 1);
+#pragma unroll
+                            for (int q = 0; q < 5; q++) lv[q] = a.bf.zD[q * nzf + fo];
+                        }
+#pragma unroll
+                        for (int q = 0; q < 5; q++) s.LzR[rr][q] = lv[q];
+                    }
+                }
+            }
+            __syncthreads();
+            // (c) the own faces: y above, z beyond, x ahead; the tile's bottom
+            // y faces (warp 12) and left z faces (warp 11)
+            T Fz[5], Fx[5], hin[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) Fz[q] = Fx[q] = hin[q] = T(0.);
+            {
+                T lzn[5];
+#pragma unroll
+                for (int q = 0; q < 5; q++) lzn[q] = __shfl_down_sync(0xffffffffu, lz[q], 1);
+                if (own) {
+                    if (l == WK - 1) {
+#pragma unroll
+                        for (int q = 0; q < 5; q++) lzn[q] = s.LzR[r][q];
+                    }
+                    face_z<T, SST>(s, kc, q0, q0, sm1, s0, sp1, r, l, hz, lzn, Fz);
+                    T F[5];
+                    face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, r, l, hy, s.Lo[r + 1][l], F);
+#pragma unroll
+                    for (int q = 0; q < 5; q++) s.Fy[r + 1][l][q] = F[q];
+                }
+            }
+            if (r == WJ - 4 && k <= D && j0 <= H) {
+                T F[5];
+                face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, -1, l, s.HyB[l], s.Lo[0][l], F);
+#pragma unroll
+                for (int q = 0; q < 5; q++) s.Fy[0][l][q] = F[q];
+            }
+            if (r == WJ - 5 && l < WJ && j0 + l <= H && k0 <= D) {
+                T F[5];
+                face_z<T, SST>(s, kc, q0, q0, sm1, s0, sp1, l, -1, s.HzL[l], s.Lz0[l], F);
+#pragma unroll
+                for (int q = 0; q < 5; q++) s.FzL[l][q] = F[q];
+            }
+            if (own) {
+                T lo[5];
+                if (i + 1 <= L) {
+                    CellC<T> cc;
+                    const T *Un = s.U[q1][r + 2][l + 2];
+#pragma unroll
+                    for (int q = 0; q < 5; q++) cc.u[q] = Un[q];
+                    cell_consts(cc);
+                    T fw2[5];
+#pragma unroll
+                    for (int q = 0; q < 5; q++) fw2[q] = T(pown[q]);
+                    recon_x(cc, fw2, s.U[q0][r + 2][l + 2], hin, lo);
+                } else {
+                    const long long fo = (long long)(j - 1) * D + (k - 1);
+#pragma unroll
+                    for (int q = 0; q < 5; q++) lo[q] = a.bf.xL[q * nxf + fo];
+                }
+                const T *dc = s.Dv[q0][r + 1][l + 1], *dn = s.Dv[q1][r + 1][l + 1];
+                const T m_f = SST ? T(0.5) * (s.U[q1][r + 2][l + 2][0] + s.U[q0][r + 2][l + 2][0]) : dn[4];
+                fused_face<T, 1, SST>(hix, lo, dc, dc[3], dn, dn[3], s.R[sp1][r + 2][l + 1], s.R[s0][r + 2][l + 1],
+                                      s.R[sp1][r][l + 1], s.R[s0][r][l + 1], s.R[sp1][r + 1][l + 2],
+                                      s.R[s0][r + 1][l + 2], s.R[sp1][r + 1][l], s.R[s0][r + 1][l], m_f, kc, Fx);
+            }
+            T Fzm[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) Fzm[q] = __shfl_up_sync(0xffffffffu, Fz[q], 1);
+            __syncthreads();
+            // (d) divergence and stage combination (src/evolution.c:29-161):
+            // the divergence in FP32, the combination in FP64
+            if (own) {
+                if (l == 0) {
+#pragma unroll
+                    for (int q = 0; q < 5; q++) Fzm[q] = s.FzL[r][q];
+                }
+                const long long c = cj + (long long)i * g.pi;
+#pragma unroll
+                for (int q = 0; q < 5; q++) {
+                    const T X = T(dtx) * (Fxp[q] - Fx[q]);
+                    const T Y = T(dty) * (s.Fy[r][l][q] - s.Fy[r + 1][l][q]);
+                    const T Z = T(dtz) * (Fzm[q] - Fz[q]);
+                    const double inc = (double)(X + Y + Z);
+                    double o;
+                    if (a.stage == 1) o = base[q] + inc;
+                    else if (a.stage == 2) o = 0.75 * unv[q] + 0.25 * (base[q] + inc);
+                    else o = one_third * unv[q] + two_thirds * (base[q] + inc);
+                    a.out[q * fs + c] = o;
+                    base[q] = o;
+                }
+                if (a.co && i >= a.co_i0 && i <= a.co_i1) {
+                    const double Co = cell_courant(kc.cfl_mode, base[0], base[1], base[2], base[3], base[4], dtx, dty, dtz);
+                    const double m = s.comax[r][l];
+                    s.comax[r][l] = (Co > m) ? Co : m;
+                    if (!(base[0] > 0.0)) atomicOr(a.status, 2u);
+                }
+            }
+            // (e) plane i+2 into the state ring slot of plane i and its
+            // velocities into the slots of planes i-1 (reciprocal) and i
+            // (division); advance the march
+            if (i < i1) {
+                if (live && i + 2 <= L + 1) {
+                    store5(s.U[q0][r + 2][l + 2], pown);
+                    cell_prims<T, SST>(s, i + 2, r, l, mu2, mu1);
+                }
+                if (hlive && i + 2 <= L + 1) {
+                    store5(s.U[q0][hr + 2][hc + 2], phal);
+                    if (hvel) cell_prims<T, SST>(s, i + 2, hr, hc, hmu2, hmu1);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                Fxp[q] = Fx[q];
+                hix[q] = hin[q];
+            }
+            mu0 = mu1;
+            mu1 = mu2;
+            hmu0 = hmu1;
+            hmu1 = hmu2;
+        }
+    }
+    if (a.co) {
+        __syncthreads();
+        double m = s.comax[r][l];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double x = __shfl_xor_sync(0xffffffffu, m, o);
+            m = (x > m) ? x : m;
+        }
+        __syncthreads();
+        if (l == 0) s.comax[r][0] = m;
+        __syncthreads();
+        if (t == 0) {
+            m = 0.0;
+#pragma unroll
+            for (int q = 0; q < WJ; q++) m = (s.comax[q][0] > m) ? s.comax[q][0] : m;
+            // non-negative doubles order like their bit patterns
+            atomicMax(a.co, (unsigned long long)__double_as_longlong(m));
+        }
+    }
+}
+
+// Blocks of the persistent grid: one per SM, fewer when the domain has fewer
+// than 16 planes of tiles per SM (each block then marches at least that far).
+inline int wide_blocks(const Grid &g, int sms)
+{
+    const long long ntiles = (long long)((g.D + WK - 1) / WK) * ((g.H + WJ - 1) / WJ);
+    const long long units = ntiles * g.L;
+    const long long want = (units + 15) / 16;
+    return (int)std::max(1LL, std::min((long long)sms, want));
+}
+
+template <bool SST>
+int launch_wide(Ctx &c, int stage, const double *cur, const double *un, double *out, const float *mu,
+                BF<float> bf, bool courant)
+{
+    const Grid &g = c.g;
+    Args<float> a;
+    a.cur = cur; a.un = un; a.out = out; a.mu = mu; a.bf = bf; a.ds = c.ds; a.stage = stage;
+    a.co = courant ? &c.ds->co_bits : nullptr;
+    a.co_i0 = c.co_i0;
+    a.co_i1 = c.co_i1;
+    a.status = &c.ds->status;
+    a.seg = 0;
+    const size_t smem = sizeof(Smem<float>);
+    static std::atomic<uint64_t> attr{0};
+    if (!smem_limit_once((const void *)k_stage_wide<float, SST>, smem, attr)) return -1;
+    prof_begin(c, FSL_K_STAGE);
+    k_stage_wide<float, SST><<<wide_blocks(g, c.sms), NT, smem, c.stream>>>(g, c.k, a);
+    prof_end(c, FSL_K_STAGE, 1);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+} // namespace wide
+} // namespace fsl

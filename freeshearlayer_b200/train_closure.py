@@ -3,15 +3,19 @@
     python -m freeshearlayer_b200.train_closure --out freeshearlayer_b200/closure_weights.f32
 
 Runs temporal shear layers on the GPU (FP32 bulk, dynamic Smagorinsky) at
-convective Mach 0.3, 0.5 and 0.7 (box 2pi x pi x pi, Re_dw0 1000), each
-GRID:AMP:STEPS entry of --runs once per Mach number: velocity noise of 1e-3 dU
-(the laminar-to-transitional phase the production runs start in) and 5e-2 dU
-(small scales within a few hundred steps), on a 256x128x128 and a 512x256x256
-grid.  Every 50 steps it harvests (features, dynamic Cs^2) samples, with a
-cell stride per grid that spreads the --samples budget over all snapshots,
-trains the MLP with Adam on the tensor-core kernels and writes the FP32
-parameter vector (FSL_CLOSURE_NPARAMS little-endian floats).  Finally it
-judges the trained closure on fresh runs and prints one JSON log line.
+convective Mach 0.3, 0.5 and 0.7 (box 2pi x pi x pi), each
+GRID:AMP:STEPS:RE entry of --runs once per Mach number:
+  - velocity noise of 1e-3 dU at Re_dw0 1000 on the 256x128x128 and the
+    512x256x256 grid (the laminar phase the production runs start in);
+  - noise of 5e-2 dU at Re_dw0 2e4 on a 128x64x64 and a 256x128x128 grid,
+    run through the roll-up into turbulence, where the dynamic SGS viscosity
+    reaches and passes the molecular one.
+Every 50 steps it harvests (features, dynamic Cs^2) samples, with a cell
+stride per run that spreads the --samples budget over all snapshots, trains
+the MLP with Adam on the tensor-core kernels and writes the FP32 parameter
+vector (FSL_CLOSURE_NPARAMS little-endian floats).  Finally it judges the
+trained closure on fresh runs (another Mach number and seed) and prints one
+JSON log line.
 """
 from __future__ import annotations
 
@@ -45,8 +49,8 @@ def load_weights(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
     return w
 
 
-def judge(fsl, w, grid, Mc, amp, steps, seed):
-    p, dU = shear_params(grid, Mc)
+def judge(fsl, w, grid, Mc, amp, steps, seed, Re=1000.0):
+    p, dU = shear_params(grid, Mc, Re)
     state, _ = fsl.temporal_state(p, Mc, 1.0, amp, seed)
     d = fsl.Domain(p)
     d.upload_state(state)
@@ -56,15 +60,16 @@ def judge(fsl, w, grid, Mc, amp, steps, seed):
         d.step(steps)
     st = d.closure_compare()
     d.close()
-    return {"grid": list(grid), "Mc": Mc, "amp": amp, "steps": steps, "cs2_profile_err": st.profile_err,
-            "cs2_cell_err": st.cell_err, "mu_profile_err": st.mu_profile_err, "visc_err": st.visc_err}
+    return {"grid": list(grid), "Mc": Mc, "Re": Re, "amp": amp, "steps": steps, "cs2_profile_err": st.profile_err,
+            "cs2_cell_err": st.cell_err, "mu_profile_err": st.mu_profile_err, "visc_err": st.visc_err,
+            "mu_active_err": st.mu_active_err, "dyn_ratio": st.dyn_ratio, "active_rows": st.active_rows}
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
-    ap.add_argument("--runs", default="256x128x128:0.001:2000,256x128x128:0.05:300,"
-                                      "512x256x256:0.001:1000,512x256x256:0.05:300")
+    ap.add_argument("--runs", default="256x128x128:0.001:2000:1000,512x256x256:0.001:600:1000,"
+                                      "128x64x64:0.05:12000:20000,256x128x128:0.05:20000:20000")
     ap.add_argument("--mach", default="0.3,0.5,0.7")
     ap.add_argument("--every", type=int, default=50)
     ap.add_argument("--samples", type=float, default=2e8, help="target number of harvested samples")
@@ -78,19 +83,20 @@ def main(argv=None):
 
     runs = []
     for r in args.runs.split(","):
-        g, amp, steps = r.split(":")
-        runs.append((tuple(int(x) for x in g.split("x")), float(amp), int(steps)))
+        f = r.split(":")
+        runs.append((tuple(int(x) for x in f[0].split("x")), float(f[1]), int(f[2]),
+                     float(f[3]) if len(f) > 3 else 1000.0))
     machs = [float(m) for m in args.mach.split(",")]
-    nsnap = sum(len(machs) * (steps // args.every + 1) for _, _, steps in runs)
+    nsnap = sum(len(machs) * (steps // args.every + 1) for _, _, steps, _ in runs)
     per_snap = args.samples / nsnap
     tr = fsl.Trainer(int(args.samples * 1.1) + 1, seed=args.seed)
     log = {"runs": []}
     t0 = time.time()
-    for grid, amp, steps in runs:
+    for grid, amp, steps, Re in runs:
         band = (grid[0] - 4) * (grid[1] - 4) * (grid[2] - 4)
         stride = max(1, int(math.ceil(band / per_snap)))
         for Mc in machs:
-            p, dU = shear_params(grid, Mc)
+            p, dU = shear_params(grid, Mc, Re)
             state, _ = fsl.temporal_state(p, Mc, 1.0, amp, args.seed + int(Mc * 10) + int(amp * 1e4))
             d = fsl.Domain(p)
             d.upload_state(state)
@@ -99,10 +105,10 @@ def main(argv=None):
             for _ in range(steps // args.every):
                 d.step(args.every)
                 tr.harvest(d, stride)
-            log["runs"].append({"grid": list(grid), "Mc": Mc, "amp": amp, "steps": steps, "stride": stride,
-                                "samples": tr.size})
-            print("harvest %s Mc %.1f amp %g stride %d -> %d samples (%.0f s)" % (
-                grid, Mc, amp, stride, tr.size, time.time() - t0), flush=True)
+            log["runs"].append({"grid": list(grid), "Mc": Mc, "Re": Re, "amp": amp, "steps": steps,
+                                "stride": stride, "samples": tr.size})
+            print("harvest %s Mc %.1f Re %g amp %g stride %d -> %d samples (%.0f s)" % (
+                grid, Mc, Re, amp, stride, tr.size, time.time() - t0), flush=True)
             d.close()
     X, Y = tr.samples(min(tr.size, 1 << 20))
     p0 = tr.weights()
@@ -120,8 +126,8 @@ def main(argv=None):
     # the trained closure against the dynamic procedure on fresh runs
     s = args.seed + 99
     log["judge"] = [judge(fsl, w, (512, 256, 256), 0.7, 1e-3, 0, s), judge(fsl, w, (512, 256, 256), 0.7, 1e-3, 300, s)]
-    for Mc in machs:
-        log["judge"] += [judge(fsl, w, (256, 128, 128), Mc, 1e-3, 1000, s), judge(fsl, w, (256, 128, 128), Mc, 0.05, 300, s)]
+    for steps in (0, 4000, 8000, 10000):  # Mc 0.6: not a training Mach number
+        log["judge"].append(judge(fsl, w, (128, 64, 64), 0.6, 0.05, steps, s, Re=20000.0))
     print(json.dumps(log), flush=True)
 
 

@@ -9,6 +9,9 @@ c2: temporal shear layer 256x128x128, Mc 0.6, Re_dw0 1000: the plain FP64
     PPM reconstruction, from the same seeded state.
 c5: 512x256x256, Mc 0.7, Re_dw0 1000: the plain FP64 path against FP32 bulk +
     the learned closure (judged every 100 steps), and both again with PPM.
+turb: 256x128x128, Mc 0.6, Re_dw0 2e4, noise 5e-2 dU, 20000 steps through
+    the roll-up into turbulence: the SGS models against each other
+    (freeshearlayer_b200/closure_gain.py).
 
 Each lower-precision arm is compared with the FP64 arm of the same
 reconstruction; FP64 PPM is also compared with the plain FP64 path (the
@@ -93,7 +96,7 @@ def run_arm(fsl, cfg, arm, steps, every, seed):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
+    ap.add_argument("--config", choices=sorted(CONFIGS) + ["turb"], default="c2")
     ap.add_argument("--steps", type=int, default=0, help="0: the configuration's own step count")
     ap.add_argument("--every", type=int, default=100)
     ap.add_argument("--seed", type=int, default=20251203)
@@ -102,6 +105,13 @@ def main(argv=None):
     sys.path.insert(0, os.path.dirname(HERE))
     import freeshearlayer_b200 as fsl
 
+    if args.config == "turb":
+        # the SGS models in a layer that turns turbulent (closure_gain)
+        from freeshearlayer_b200 import closure_gain
+        out = closure_gain.run(fsl, grid=(256, 128, 128), Mc=0.6, Re=2e4, amp=0.05,
+                               steps=args.steps or 20000, every=args.every * 5, seed=args.seed)
+        print(json.dumps(out), flush=True)
+        return
     cfg = CONFIGS[args.config]
     steps = args.steps or cfg["steps"]
     want = set(a for a in args.arms.split(",") if a)

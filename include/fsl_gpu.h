@@ -306,8 +306,12 @@ int fsl_step_stage(fsl_ctx *ctx);
 /* Launch-shape knobs of the fused kernels.  FP64 results do not depend on
  * them; FP32-bulk results may differ in the last bits (the compiler may
  * contract a flux into FMAs differently where a block's march starts). */
-#define FSL_TUNE_STAGE_ROWS 1 /* rows per stage tile incl. 2 halo rows: 8, 12 or 16 */
+#define FSL_TUNE_STAGE_ROWS 1 /* rows per ring stage tile incl. 2 halo rows: 8, 12 or 16; or 0, the
+                                 full-lane persistent 16 x 32 tile (the FP32 bulk's default with the
+                                 reference reconstruction; elsewhere 0 runs 16) */
 #define FSL_TUNE_STAGE_SEG 2  /* x planes marched per stage block (default 48 FP32 bulk, 32 FP64) */
+#define FSL_TUNE_INFER_TILES 3 /* learned-closure inference: 128-cell tiles in flight per block, 1 or
+                                  2 (default 2: one tile's SiLU overlaps the other's products) */
 int fsl_tune(fsl_ctx *ctx, int key, int value);
 
 /* ---- debug / parity access ----------------------------------------------- */

@@ -168,3 +168,44 @@ def test_async_transfers_match_the_synchronous_ones(fsl):
         r.step(2)
         assert np.array_equal(outs[q], r.download_state()), q
     r.close()
+
+
+def test_host_driver_headline_path(fsl, oracle_lib, tmp_path):
+    """The ANSI-C driver runs the FP32 bulk with the learned closure (weights
+    file, feature scales, judgements every 2 steps) from the optional
+    layer2_gpu.ini beside an unchanged layer2.ini, starting from the temporal
+    shear layer: its backup.dat equals the same steps through the library."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(fsl.__file__), "layer2_gpu")
+    if not os.path.exists(exe):
+        pytest.skip("layer2_gpu not built")
+    from tests.helpers import temporal_params
+    p = temporal_params(L=24, H=16, D=16, Mc=0.5, Re=2000.0, numstep=5, Answer=0)
+    (tmp_path / "layer2.ini").write_text(oracle_lib.ini_text(p))
+    dU = 2.0 * 0.5 * np.sqrt(1.4e5)
+    (tmp_path / "layer2_gpu.ini").write_text(
+        "# the headline path\nprecision = fp32\nsgs = learned   \nsetup = temporal\ncfl = acoustic\n"
+        "closure_weights = %s\nclosure_t_ref = %.17g\nclosure_len_ref = 1\njudge_every = 2\n"
+        "judge_threshold = 0.02\ntemporal_state = 0.5 1.0 0.02 7\n" % (fsl.CLOSURE_WEIGHTS, 1.0 / dU))
+    r = subprocess.run([exe], input="%.12f\n" % p["seed_X"], text=True, capture_output=True, cwd=tmp_path,
+                       env=dict(os.environ, FSL_FRAMES="0", FSL_PROBES="0"), timeout=120)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    q = dict(p, precision=1, sgs=1)
+    s, dU2 = fsl.temporal_state(q, 0.5, 1.0, 0.02, 7)
+    d = fsl.Domain(q)
+    d.upload_state(s)
+    d.closure_set_scales(1.0 / dU, 1.0)
+    d.closure_set_weights(fsl.closure_weights())
+    d.closure_judge(2, 0.02)
+    for _ in range(5):
+        d.step(1)
+        d.sync()
+    n = p["LEN"] * p["HIG"] * 5 * p["DEP"]
+    raw = (tmp_path / "backup.dat").read_bytes()
+    np.testing.assert_array_equal(np.frombuffer(raw[:8 * n], np.float64), d.download_state())
+    assert d.closure_stats().judgements == 3
+    # an unknown option is refused with the line it came from
+    (tmp_path / "layer2_gpu.ini").write_text("precision = fp16\n")
+    r = subprocess.run([exe], input="0.3\n", text=True, capture_output=True, cwd=tmp_path, timeout=60)
+    assert r.returncode != 0 and "layer2_gpu.ini:1" in r.stdout

@@ -347,3 +347,44 @@ def test_static_smagorinsky_ppm_and_fp32(fsl, oracle_lib):
     d.step(8)
     errs = per_var_rel_l2(d.download_state(), o.state(), p32)
     assert errs[0] < FP32_RTOL and errs[4] < FP32_RTOL, errs
+
+
+@pytest.mark.parametrize("setup,grid", [(1, (24, 12, 16)), (1, (40, 20, 40)), (1, (33, 17, 33)),
+                                        (1, (20, 16, 32)), (0, (20, 10, 12)), (0, (18, 33, 35))])
+@pytest.mark.parametrize("sgs", [0, 2])
+def test_fp32_full_lane_tile_matches_ring_tile(fsl, oracle_lib, setup, grid, sgs):
+    """The FP32 bulk's full-lane persistent stage kernel (rows 0, the default)
+    against the ring-tile kernel (rows 16) on grids whose extents are and are
+    not multiples of the 16 x 32 tile (partial tiles, a ghost row or column
+    as the halo, tiles narrower than the halo work), in both setups, with the
+    dynamic and the static SGS model: the same steps to FP32 rounding, and
+    both within FP32_RTOL of the FP64 oracle for rho and E."""
+    L, H, D = grid
+    if setup == 0:
+        p = spatial_params(L=L, H=H, D=D, sgs=sgs)
+        from oracle.oracle import spatial_initial_state
+        s = spatial_initial_state(p)
+    else:
+        p = temporal_params(L=L, H=H, D=D, sgs=sgs, Re=5000.0)
+        s, _ = oracle_lib.Oracle.temporal_state(p, 0.4, amp=0.02)
+    o = oracle_lib.Oracle(p)
+    o.set_state(s)
+    o.step(6)
+    ref = o.state()
+    out = {}
+    for rows in (0, 16):
+        d = fsl.Domain(dict(p, precision=1))
+        d.tune(d.TUNE_STAGE_ROWS, rows)
+        d.upload_state(s)
+        d.step(6)
+        out[rows] = d.download_state()
+        d.close()
+        errs = per_var_rel_l2(out[rows], ref, p)
+        assert errs[0] < FP32_RTOL and errs[4] < FP32_RTOL, (rows, errs)
+    diff = per_var_rel_l2(out[0], out[16], p)
+    assert max(diff[0], diff[1], diff[4]) < 1e-6, diff
+    a = out[0].reshape(L, H, 5, D)
+    b = out[16].reshape(L, H, 5, D)
+    mscale = max(np.linalg.norm(b[:, :, v]) for v in (1, 2, 3))
+    for v in (2, 3):
+        assert np.linalg.norm(a[:, :, v] - b[:, :, v]) / mscale < 1e-6, (v, diff)
