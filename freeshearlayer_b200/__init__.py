@@ -32,6 +32,7 @@ __all__ = ["Params", "Domain", "FslError", "lib", "LIB_PATH", "default_params",
            "SETUP_SPATIAL", "SETUP_TEMPORAL", "CFL_STREAMWISE", "CFL_ACOUSTIC",
            "PREC_FP64", "PREC_FP32", "SGS_DYNAMIC", "SGS_LEARNED", "SGS_STATIC", "SGS_NONE", "RECON_CHARMINMOD",
            "RECON_PPM", "Trainer", "Ensemble", "closure_weights", "shear_statistics", "favre_from_probes",
+           "favre_profiles",
            "tecplot_write"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -159,6 +160,7 @@ def lib():
             "fsl_write_probes": [vp, cs, i], "fsl_favre_reset": [vp], "fsl_favre_accumulate": [vp],
             "fsl_favre_read": [vp, _dp, C.POINTER(C.c_int)],
             "fsl_favre_from_probes": [cs, i, i, i, i, _dp, C.POINTER(C.c_int)],
+            "fsl_favre_profiles": [cs, i, i, i, cs, C.POINTER(C.c_int)],
             "fsl_output_fields": [vp, _dp], "fsl_write_tecplot": [vp, cs],
             "fsl_tecplot_write": [cs, i, i, i, _dp],
         })
@@ -688,6 +690,16 @@ def favre_from_probes(path: str, HIG: int, real_bytes: int = 4, step_start: int 
     n = C.c_int()
     _check(lib().fsl_favre_from_probes(os.fsencode(path), HIG, real_bytes, step_start, step_end, out, C.byref(n)))
     return out.reshape(3, HIG), n.value
+
+
+def favre_profiles(path: str, HIG: int, step_start: int, step_end: int, out_dir: str) -> int:
+    """The reference's post-processor (favre-average-src/layer2_p.c) on a
+    float probes file: writes out_dir/probe1.dat .. probe3.dat (float sums,
+    its text format); returns the number of records summed (host only)."""
+    n = C.c_int()
+    _check(lib().fsl_favre_profiles(os.fsencode(path), HIG, step_start, step_end, os.fsencode(out_dir),
+                                    C.byref(n)))
+    return n.value
 
 
 # --- shear-layer statistics ----------------------------------------------------------

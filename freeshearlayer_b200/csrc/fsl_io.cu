@@ -4,6 +4,7 @@
 // reference's post-processor over a probes file and accumulated on the device.
 #include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "fsl_internal.h"
@@ -240,6 +241,52 @@ int fsl_favre_from_probes(const char *path, int HIG, int real_bytes, int step_st
     }
     fclose(f);
     for (size_t q = 0; q < R.size(); q++) u[q] = RU[q] / R[q];
+    if (records) *records = n;
+    return FSL_OK;
+}
+
+// The reference post-processor's whole job on a float probes file
+// (favre-average-src/layer2_p.c:30-146): per station, the records with
+// step_start <= step <= step_end summed in float in file order, u~ = sum(rho
+// u) / sum(rho) in float, and the three profile files probe1.dat ..
+// probe3.dat in its text format.  Unlike the reference's reader, which
+// re-adds its last record for ever when the file ends before a step beyond
+// step_end, reading stops at the end of the file.
+int fsl_favre_profiles(const char *path, int HIG, int step_start, int step_end, const char *dir, int *records)
+{
+    if (!path || HIG < 1 || !dir) return FSL_ERR_ARG;
+    FILE *f = fopen(path, "rb");
+    if (!f) return FSL_ERR_IO;
+    std::vector<float> R(3 * (size_t)HIG, 0.f), RU(3 * (size_t)HIG, 0.f), pr(HIG), pu(HIG);
+    unsigned step = 0;
+    int n = 0;
+    for (;;) {
+        if (fread(&step, sizeof step, 1, f) != 1) break;
+        if (step > (unsigned)step_end) break;
+        bool ok = true;
+        for (int st = 0; st < 3 && ok; st++) {
+            ok = fread(pr.data(), sizeof(float) * HIG, 1, f) == 1 && fread(pu.data(), sizeof(float) * HIG, 1, f) == 1;
+            if (!ok || step < (unsigned)step_start) continue;
+            for (int j = 0; j < HIG; j++) {
+                R[st * HIG + j] += pr[j];
+                RU[st * HIG + j] += pu[j];
+            }
+        }
+        if (!ok) break;
+        if (step >= (unsigned)step_start) n++;
+    }
+    fclose(f);
+    for (size_t q = 0; q < RU.size(); q++) RU[q] /= R[q];
+    for (int st = 0; st < 3; st++) {
+        const std::string name = std::string(dir) + "/probe" + std::to_string(st + 1) + ".dat";
+        FILE *o = fopen(name.c_str(), "w");
+        if (!o) return FSL_ERR_IO;
+        fprintf(o, "%d\n1\n", HIG + 2);
+        fprintf(o, "%f %3.2f \n", -0.00001, 0.);
+        for (int j = 0; j < HIG; j++) fprintf(o, "%d %3.2f \n", j, RU[st * HIG + j]);
+        fprintf(o, "%f %3.2f \n", HIG - 1 + 0.00001, 210.);
+        fclose(o);
+    }
     if (records) *records = n;
     return FSL_OK;
 }

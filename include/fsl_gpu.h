@@ -351,6 +351,14 @@ int fsl_favre_read(fsl_ctx *ctx, double *u, int *count);
  * records with step_start <= step <= step_end, u~[station][j] as above. */
 int fsl_favre_from_probes(const char *path, int HIG, int real_bytes, int step_start, int step_end, double *u,
                           int *records);
+/* The reference post-processor itself (favre-average-src/layer2_p.c:30-146,
+ * host only): a probes file of float records (fsl_write_probes with
+ * real_bytes 4, the reference's format), the records with step_start <= step
+ * <= step_end summed in float, u~ = sum(rho u) / sum(rho) in float, written as
+ * dir/probe1.dat .. dir/probe3.dat in its text format; *records (may be
+ * NULL) receives the number summed.  Reading stops at the end of the file
+ * (the reference's loop re-adds its last record there until killed). */
+int fsl_favre_profiles(const char *path, int HIG, int step_start, int step_end, const char *dir, int *records);
 
 /* Output() (src/output.c:16-141): per interior cell, in its loop order (k,
  * then j, then i fastest), the 12 values x, y, z, rho, u, v, w, p, T,

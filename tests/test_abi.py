@@ -200,6 +200,43 @@ def test_favre_post_processor(fsl, tmp_path, real_bytes):
     assert n_all == 10
 
 
+def _write_float_probes(path, H, steps, seed):
+    rng = np.random.default_rng(seed)
+    with open(path, "wb") as f:
+        for step in steps:
+            f.write(np.int32(step).tobytes())
+            for _ in range(3):
+                f.write((1.0 + 0.1 * rng.random(H)).astype(np.float32).tobytes())
+                f.write((50.0 + 150.0 * rng.random(H)).astype(np.float32).tobytes())
+
+
+@pytest.mark.parametrize("window", [(1, 9), (4, 7), (12, 12)])
+def test_favre_profiles_equal_the_reference_program(fsl, oracle_lib, tmp_path, window):
+    """The reference's own post-processor (favre-average-src/layer2_p.c,
+    compiled unchanged into oracle/_ref/layer2_p) and fsl_favre_profiles on
+    the same float probes file: probe1.dat .. probe3.dat byte for byte (float
+    sums in file order, its text format).  The window ends before the file's
+    last record: the reference's loop ends only on a step beyond step_end."""
+    exe = os.path.join(os.path.dirname(oracle_lib.__file__), "_ref", "layer2_p")
+    if not os.path.exists(exe):
+        pytest.skip("the reference post-processor is not built (reference sources absent)")
+    H = 9
+    _write_float_probes(tmp_path / "probes.dat", H, list(range(1, 11)) + [13, 14], seed=5)
+    ref_dir, mine = tmp_path / "ref", tmp_path / "mine"
+    ref_dir.mkdir()
+    mine.mkdir()
+    (ref_dir / "probes.dat").write_bytes((tmp_path / "probes.dat").read_bytes())
+    r = subprocess.run([exe], input="%d\n%d\n%d\n" % (window[0], window[1], H), text=True,
+                       capture_output=True, cwd=ref_dir, timeout=30)
+    assert r.returncode == 0, r.stdout[-500:]
+    n = fsl.favre_profiles(str(tmp_path / "probes.dat"), H, window[0], window[1], str(mine))
+    assert n == sum(1 for s in list(range(1, 11)) + [13, 14] if window[0] <= s <= window[1])
+    for st in (1, 2, 3):
+        a = (mine / ("probe%d.dat" % st)).read_bytes()
+        assert a == (ref_dir / ("probe%d.dat" % st)).read_bytes(), st
+        assert a.startswith(b"%d\n1\n" % (H + 2))
+
+
 def test_stage_operation_counts():
     """The bench's per-cell-stage arithmetic (its compute roof) is the count
     the instrumented arithmetic templates give, for the fused kernel's

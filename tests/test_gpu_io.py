@@ -209,3 +209,33 @@ def test_host_driver_headline_path(fsl, oracle_lib, tmp_path):
     (tmp_path / "layer2_gpu.ini").write_text("precision = fp16\n")
     r = subprocess.run([exe], input="0.3\n", text=True, capture_output=True, cwd=tmp_path, timeout=60)
     assert r.returncode != 0 and "layer2_gpu.ini:1" in r.stdout
+
+
+def test_favre_profiles_from_gpu_probes_equal_the_reference_program(fsl, oracle_lib, tmp_path):
+    """Probes records written from the GPU state in the reference's float
+    format (fsl_write_probes, real_bytes 4) over 8 steps, post-processed by
+    the reference's own program (favre-average-src/layer2_p.c) and by
+    fsl_favre_profiles: the three profile files are byte-identical."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(oracle_lib.__file__), "_ref", "layer2_p")
+    if not os.path.exists(exe):
+        pytest.skip("the reference post-processor is not built")
+    p = spatial_params(L=16, H=10, D=8)
+    d = fsl.Domain(p)
+    d.upload_state(oracle_lib.spatial_initial_state(p))
+    path = tmp_path / "probes.dat"
+    for _ in range(8):
+        d.step(1)
+        d.write_probes(str(path), 4)
+    d.close()
+    ref_dir, mine = tmp_path / "ref", tmp_path / "mine"
+    ref_dir.mkdir()
+    mine.mkdir()
+    (ref_dir / "probes.dat").write_bytes(path.read_bytes())
+    r = subprocess.run([exe], input="2\n7\n%d\n" % p["HIG"], text=True, capture_output=True, cwd=ref_dir,
+                       timeout=30)
+    assert r.returncode == 0
+    assert fsl.favre_profiles(str(path), p["HIG"], 2, 7, str(mine)) == 6
+    for st in (1, 2, 3):
+        assert (mine / ("probe%d.dat" % st)).read_bytes() == (ref_dir / ("probe%d.dat" % st)).read_bytes()
