@@ -92,7 +92,7 @@ class ClosureStats(C.Structure):
                 ("visc_err", C.c_double), ("judgements", C.c_int),
                 ("fallbacks", C.c_int), ("using_dynamic", C.c_int), ("last_step", C.c_uint),
                 ("mu_active_err", C.c_double), ("dyn_ratio", C.c_double), ("active_rows", C.c_int),
-                ("reserved_", C.c_int)]
+                ("dynamic_steps", C.c_int)]
 
 
 class KTimes(C.Structure):
@@ -487,7 +487,7 @@ class Domain:
                                           b.ctypes.data if fields else None, C.byref(st)))
         return (st, a, b) if fields else st
 
-    TUNE_STAGE_ROWS, TUNE_STAGE_SEG, TUNE_INFER_TILES = 1, 2, 3
+    TUNE_STAGE_ROWS, TUNE_STAGE_SEG = 1, 2
 
     def tune(self, key: int, value: int):
         """Launch-shape knob of the fused kernels (results do not depend on it)."""

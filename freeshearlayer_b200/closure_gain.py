@@ -12,7 +12,9 @@ same state by five arms:
   of any comparison (in a turbulent flow two runs that differ only in
   rounding decorrelate too);
 * ``fp32-learned``: the FP32 bulk with the learned closure (judged every 100
-  steps, the default);
+  steps, the default; while a judgement fails the steps run the dynamic
+  procedure, and ``closure_steps`` counts the steps the network served);
+* ``fp32-learned-only``: the network alone, judgements off;
 * ``fp32-static``: the FP32 bulk with the reference's static Smagorinsky
   model (src/fluxes.c:193-205, Cs from the parameters, 0.01 as in
   layer2.ini);
@@ -38,8 +40,8 @@ import time
 
 import numpy as np
 
-ARMS = [("fp64-dynamic", 0, 0), ("fp32-dynamic", 1, 0), ("fp32-learned", 1, 1), ("fp32-static", 1, 2),
-        ("fp32-none", 1, 3)]
+ARMS = [("fp64-dynamic", 0, 0), ("fp32-dynamic", 1, 0), ("fp32-learned", 1, 1), ("fp32-learned-only", 1, 1),
+        ("fp32-static", 1, 2), ("fp32-none", 1, 3)]
 
 
 def layer_params(grid, Mc, Re, precision=0, sgs=0, Cs=0.01):
@@ -106,6 +108,8 @@ def run(fsl, grid=(128, 64, 64), Mc=0.6, Re=2e4, amp=0.05, steps=10000, every=50
         d.upload_state(state)
         d.closure_set_scales(1.0 / dU, 1.0)
         d.closure_set_weights(w)
+        if name == "fp32-learned-only":
+            d.closure_judge(0, 0.05)
         th, r12, t0 = [], [], time.time()
         done = 0
         while True:
@@ -130,7 +134,8 @@ def run(fsl, grid=(128, 64, 64), Mc=0.6, Re=2e4, amp=0.05, steps=10000, every=50
         if sgs == 1:
             cs = d.closure_stats()
             info["closure"] = {"judgements": int(cs.judgements), "fallbacks": int(cs.fallbacks),
-                               "using_dynamic": int(cs.using_dynamic)}
+                               "using_dynamic": int(cs.using_dynamic), "dynamic_steps": int(cs.dynamic_steps),
+                               "closure_steps": steps - int(cs.dynamic_steps)}
         hist[name] = (info, final)
         d.close()
     ref, ref_final = hist["fp64-dynamic"]
@@ -160,10 +165,11 @@ def run(fsl, grid=(128, 64, 64), Mc=0.6, Re=2e4, amp=0.05, steps=10000, every=50
 
     out["apriori_mean"] = {k: mean(k) for k in ("learned_active", "static_active", "learned_all", "static_all")}
     a = out["arms"]
-    if "fp32-learned" in a and "fp32-static" in a:
-        out["learned_beats_static"] = {
-            "apriori_mu_profile": (out["apriori_mean"]["learned_active"] or 1e9)
-            < (out["apriori_mean"]["static_active"] or 1e9),
-            "theta_history": a["fp32-learned"]["theta_history_err"] < a["fp32-static"]["theta_history_err"],
-            "r12_history": a["fp32-learned"]["r12_history_err"] < a["fp32-static"]["r12_history_err"]}
+    for arm in ("fp32-learned", "fp32-learned-only"):
+        if arm in a and "fp32-static" in a:
+            out[arm.replace("fp32-", "").replace("-", "_") + "_beats_static"] = {
+                "apriori_mu_profile": (out["apriori_mean"]["learned_active"] or 1e9)
+                < (out["apriori_mean"]["static_active"] or 1e9),
+                "theta_history": a[arm]["theta_history_err"] < a["fp32-static"]["theta_history_err"],
+                "r12_history": a[arm]["r12_history_err"] < a["fp32-static"]["r12_history_err"]}
     return out

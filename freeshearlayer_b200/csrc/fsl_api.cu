@@ -1124,10 +1124,6 @@ int fsl_tune(fsl_ctx *h, int key, int value)
         if (value < 1 || value > 1 << 20) return FSL_ERR_ARG;
         c.stage_seg = value;
         return FSL_OK;
-    case FSL_TUNE_INFER_TILES:
-        if (value != 1 && value != 2) return FSL_ERR_ARG;
-        c.infer_tiles = value;
-        return FSL_OK;
     default:
         return FSL_ERR_ARG;
     }

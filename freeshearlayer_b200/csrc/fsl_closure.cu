@@ -203,6 +203,7 @@ int closure_step_sgs(Ctx &c)
         const bool fail_ = !judge_passes(c);
         if (fail_ && !c.using_dynamic) c.fallbacks++;
         c.using_dynamic = fail_;
+        if (fail_) c.dynamic_steps++; // judge_now left the dynamic viscosity in place
         const size_t fs = (size_t)c.g.fstride;
         if (!c.using_dynamic) {
             if (fp32) cudaMemcpyAsync(c.mu32, c.mu32_alt, fs * sizeof(float), cudaMemcpyDeviceToDevice, c.stream);
@@ -213,6 +214,7 @@ int closure_step_sgs(Ctx &c)
     if (c.using_dynamic) {
         if (fp32) launch_dynsmag32(c, c.U);
         else launch_dynsmag(c, c.U);
+        c.dynamic_steps++;
         return FSL_OK;
     }
     if (launch_closure_infer(c, c.U, fp32 ? nullptr : c.mu, fp32 ? c.mu32 : nullptr, nullptr, c.cl_params,
@@ -291,6 +293,7 @@ int fsl_closure_get_stats(fsl_ctx *h, fsl_closure_stats *s)
     s->mu_active_err = c.last_aerr;
     s->dyn_ratio = c.last_dyn_ratio;
     s->active_rows = c.last_active_rows;
+    s->dynamic_steps = c.dynamic_steps;
     s->profile_err = c.last_perr;
     s->mu_profile_err = c.last_merr;
     s->cell_err = c.last_cerr;

@@ -119,12 +119,11 @@ struct Ctx {
     float *cl_vel = nullptr;    // FP32 velocities of the padded cells (closure features), 3 fields
     double *judge_rows = nullptr; // [2][HIG][4] plane sums of the judgement (Cs^2, mu_SGS)
     bool cl_alloc = false, cl_weights = false;
-    int infer_tiles = 2;        // closure inference: tiles in flight per block (1 or 2)
     int judge_every = 100;
-    double judge_thr = 0.02;
+    double judge_thr = 0.05;
     bool using_dynamic = false;
-    int judgements = 0, fallbacks = 0;
-    double judge_floor = 0.1, judge_thr_active = 0.5; // SGS-active rows: <mu_dyn> >= floor mu_L
+    int judgements = 0, fallbacks = 0, dynamic_steps = 0;
+    double judge_floor = 0.1, judge_thr_active = 0.4; // SGS-active rows: <mu_dyn> >= floor mu_L
     double last_perr = -1, last_cerr = -1, last_merr = -1, last_verr = -1;
     double last_aerr = -1, last_dyn_ratio = -1;
     int last_active_rows = 0;

@@ -215,8 +215,7 @@ __device__ __forceinline__ __nv_bfloat16 &tile_el(__nv_bfloat16 *T, int o, int i
     return T[umma::tile_off(o, i, K) / 2];
 }
 
-template <typename S>
-__device__ __forceinline__ void stage_infer_weights(S &s, const float *__restrict__ P, int t, int nt)
+__device__ __forceinline__ void stage_infer_weights(SmemInfer &s, const float *__restrict__ P, int t, int nt)
 {
     const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
     for (int e = t; e < 64 * 16; e += nt) {
@@ -397,163 +396,6 @@ __global__ void __launch_bounds__(128, 4) k_closure_infer(Grid g, ClosureScales 
     umma::fence_before_sync();
     __syncthreads();
     if (wp == 0) umma::tmem_free(tmem, 64);
-}
-
-// Two tiles in flight per block: while the tensor cores run one tile's layer,
-// the warps apply SiLU to the other tile's previous layer, so neither the
-// products nor their completion waits stall the MUFU work.  Each tile has its
-// own activation operands, TMEM columns (64 each) and mbarrier; the weights
-// are shared.  72.5 KB of shared memory: three blocks (six tiles) per SM.
-struct SmemInfer2 {
-    alignas(128) __nv_bfloat16 W1[64 * 16];
-    alignas(128) __nv_bfloat16 W2[64 * kKH];
-    alignas(128) __nv_bfloat16 W3[64 * kKH];
-    alignas(128) __nv_bfloat16 W4[16 * kKH];
-    alignas(128) __nv_bfloat16 A0[2][128 * 16];
-    alignas(128) __nv_bfloat16 A[2][128 * kKH];
-    uint64_t mbar[2];
-    uint32_t tholder;
-};
-
-// Issue D = A W^T for tile slot `sl` after every thread's operand rows are
-// written (all threads call; thread 0 issues and commits to the slot's barrier).
-__device__ __forceinline__ void issue_layer(uint32_t tmem, uint32_t a, uint32_t b, int K, int N, uint64_t *mbar,
-                                            int t)
-{
-    umma::fence_async_smem();
-    umma::fence_before_sync();
-    __syncthreads();
-    umma::fence_after_sync();
-    if (t == 0) {
-        umma::gemm_issue(tmem, a, b, K, N, false);
-        umma::commit(mbar);
-    }
-}
-
-// Wait for a slot's product; on success the slot's parity advances and it
-// has nothing in flight.  On a timeout (every thread sees the same outcome)
-// both stay as they were, so the clean-up waits for the same completion.
-__device__ __forceinline__ bool wait_layer(uint64_t *mbar, uint32_t &phase, bool &pending)
-{
-    bool ok = umma::mbar_wait(mbar, phase, kWaitLimit);
-    ok = __syncthreads_and(ok) != 0;
-    umma::fence_after_sync();
-    if (ok) {
-        phase ^= 1u;
-        pending = false;
-    }
-    return ok;
-}
-
-template <typename MT>
-__global__ void __launch_bounds__(128, 3) k_closure_infer2(Grid g, ClosureScales sc, const double *__restrict__ U,
-                                                           const float *__restrict__ vel,
-                                                           const float *__restrict__ P, MT *__restrict__ mu,
-                                                           float *__restrict__ cs2_out, int *err)
-{
-    extern __shared__ __align__(1024) unsigned char smraw[];
-    SmemInfer2 &s = *reinterpret_cast<SmemInfer2 *>(smraw);
-    const int t = threadIdx.x, wp = t >> 5;
-    stage_infer_weights(s, P, t, 128);
-    const uint32_t one2 = 0x3F803F80u; // two BF16 ones
-    const uint32_t frow = (uint32_t)(t >> 3) * 256u + (uint32_t)(t & 7) * 16u;
-    const uint32_t arow = (uint32_t)(t >> 3) * (uint32_t)(kKH * 16) + (uint32_t)(t & 7) * 16u;
-    unsigned char *A0[2], *A[2];
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-        A0[q] = reinterpret_cast<unsigned char *>(s.A0[q]);
-        A[q] = reinterpret_cast<unsigned char *>(s.A[q]);
-        *reinterpret_cast<uint4 *>(A0[q] + frow + 128u) = make_uint4(one2, 0u, 0u, 0u);
-        *reinterpret_cast<uint4 *>(A[q] + arow + 8u * 128u) = make_uint4(one2, 0u, 0u, 0u);
-        *reinterpret_cast<uint4 *>(A[q] + arow + 9u * 128u) = make_uint4(0u, 0u, 0u, 0u);
-    }
-    if (t == 0) {
-        umma::mbar_init(&s.mbar[0], 1);
-        umma::mbar_init(&s.mbar[1], 1);
-    }
-    if (wp == 0) umma::tmem_alloc(&s.tholder, 128);
-    umma::fence_before_sync();
-    __syncthreads();
-    umma::fence_after_sync();
-    const uint32_t tmem = s.tholder;
-    const uint32_t tm[2] = {tmem, tmem + 64u};
-    const uint32_t lane = (uint32_t)(32 * wp) << 16;
-    const uint32_t aA0[2] = {umma::smem_u32(s.A0[0]), umma::smem_u32(s.A0[1])};
-    const uint32_t aA[2] = {umma::smem_u32(s.A[0]), umma::smem_u32(s.A[1])};
-    const uint32_t aW1 = umma::smem_u32(s.W1), aW2 = umma::smem_u32(s.W2), aW3 = umma::smem_u32(s.W3),
-                   aW4 = umma::smem_u32(s.W4);
-    const uint32_t aW[3] = {aW2, aW3, aW4};
-    uint32_t phase[2] = {0u, 0u};
-    bool pending[2] = {false, false};
-    bool ok = true;
-    const long long ncell = (long long)g.L * g.H * g.D;
-    const long long ntile = (ncell + 127) / 128;
-    const long long G = gridDim.x;
-    FeatIn in[2];
-    feat_load(g, U, vel, (long long)blockIdx.x * 128 + t, ncell, in[0]);
-    feat_load(g, U, vel, ((long long)blockIdx.x + G) * 128 + t, ncell, in[1]);
-    for (long long tile = blockIdx.x; tile < ntile && ok; tile += 2 * G) {
-        const bool two = tile + G < ntile; // block-uniform
-        bool valid[2];
-        long long c[2];
-        float rho[2], Smag[2];
-#pragma unroll
-        for (int q = 0; q < 2; q++) {
-            valid[q] = in[q].valid;
-            c[q] = in[q].c;
-            float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            rho[q] = 0.f;
-            Smag[q] = 0.f;
-            if (valid[q]) cell_features_v(in[q], sc, f, rho[q], Smag[q]);
-            *reinterpret_cast<uint4 *>(A0[q] + frow) = make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]),
-                                                                  pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
-        }
-        // the next pair's inputs load while this pair is on the tensor cores
-        feat_load(g, U, vel, (tile + 2 * G) * 128 + t, ncell, in[0]);
-        feat_load(g, U, vel, (tile + 3 * G) * 128 + t, ncell, in[1]);
-        issue_layer(tm[0], aA0[0], aW1, 16, 64, &s.mbar[0], t);
-        pending[0] = true;
-        if (two) {
-            issue_layer(tm[1], aA0[1], aW1, 16, 64, &s.mbar[1], t);
-            pending[1] = true;
-        }
-        for (int layer = 0; layer < 3 && ok; layer++) {
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                if (q == 1 && !two) break;
-                ok = wait_layer(&s.mbar[q], phase[q], pending[q]);
-                if (!ok) break;
-                epilogue_to_tile(tm[q] + lane, A[q], t);
-                issue_layer(tm[q], aA[q], aW[layer], kKH, layer == 2 ? 16 : 64, &s.mbar[q], t);
-                pending[q] = true;
-            }
-        }
-        if (!ok) break;
-#pragma unroll
-        for (int q = 0; q < 2; q++) {
-            if (q == 1 && !two) break;
-            ok = wait_layer(&s.mbar[q], phase[q], pending[q]);
-            if (!ok) break;
-            float v[16];
-            umma::tmem_ld16(tm[q] + lane, v);
-            umma::tmem_wait_ld();
-            const float cs2 = fminf(fmaxf(v[0], 0.f), 0.15f);
-            if (valid[q]) {
-                mu[c[q]] = (MT)(rho[q] * cs2 * sc.DD * Smag[q]);
-                if (cs2_out) cs2_out[c[q]] = cs2;
-            }
-        }
-    }
-    if (!ok) {
-        atomicExch(err, 1);
-        // products still in flight complete (bounded) before TMEM is released
-#pragma unroll
-        for (int q = 0; q < 2; q++)
-            if (pending[q]) umma::mbar_wait(&s.mbar[q], phase[q], kWaitLimit);
-    }
-    umma::fence_before_sync();
-    __syncthreads();
-    if (wp == 0) umma::tmem_free(tmem, 128);
 }
 
 // ---- harvest -------------------------------------------------------------------
@@ -877,24 +719,6 @@ int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, flo
     prof_begin(c, FSL_K_SGS);
     mlp::k_closure_vel<<<148 * 8, 256, 0, c.stream>>>(c.g, U, c.cl_vel);
     prof_end(c, FSL_K_SGS, 1);
-    if (c.infer_tiles == 2) {
-        // two tiles in flight per block, three blocks per SM
-        const size_t smem = sizeof(mlp::SmemInfer2);
-        static std::atomic<uint64_t> attr64{0}, attr32{0};
-        if (!smem_limit_once((const void *)mlp::k_closure_infer2<double>, smem, attr64) ||
-            !smem_limit_once((const void *)mlp::k_closure_infer2<float>, smem, attr32))
-            return -1;
-        const int blocks = c.sms * 3;
-        prof_begin(c, FSL_K_SGS);
-        if (mu32)
-            mlp::k_closure_infer2<float><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu32, cs2_out,
-                                                                          err);
-        else
-            mlp::k_closure_infer2<double><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu64,
-                                                                           cs2_out, err);
-        prof_end(c, FSL_K_SGS, 1);
-        return cudaGetLastError() == cudaSuccess ? 0 : -1;
-    }
     const size_t smem = sizeof(mlp::SmemInfer);
     static std::atomic<uint64_t> attr64{0}, attr32{0};
     if (!smem_limit_once((const void *)mlp::k_closure_infer<double>, smem, attr64) ||

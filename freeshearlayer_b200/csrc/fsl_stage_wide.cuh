@@ -22,9 +22,13 @@
 // ring-tile kernel.
 //
 // The grid is persistent: one block per SM (or fewer for small domains) takes
-// an equal share of the domain's (tile, plane) pairs, i.e. at most two
-// x-segments of tiles, so every SM gets the same number of planes and there is
-// no tail wave.
+// an equal share of the domain's (tile, plane) pairs, so every SM gets the
+// same number of planes and there is no tail wave.  The pairs are ordered
+// heads first: the first Hd = total / blocks planes of every tile, tile after
+// tile, then the remaining planes of every tile.  When there are more blocks
+// than tiles, the blocks that start on heads start on neighbouring tiles at
+// nearly the same plane and march in step, so the halo planes one block
+// reads were read by its neighbours moments before and come from L2.
 #pragma once
 
 #include "fsl_stage.cuh"
@@ -180,13 +184,26 @@ __global__ void __launch_bounds__(NT, 1) k_stage_wide(Grid g, Consts kc, Args<T>
     s.comax[r][l] = 0.0;
 
     const int ntk = (D + WK - 1) / WK, ntj = (H + WJ - 1) / WJ;
-    const long long total = (long long)ntk * ntj * L;
+    const long long ntiles = (long long)ntk * ntj, total = ntiles * L;
+    // heads: planes 1..Hd of every tile; tails: planes Hd+1..L of every tile
+    const long long Hd = min((long long)L, total / gridDim.x);
+    const long long Lt = L - Hd, nhead = ntiles * Hd;
     long long pos = total * blockIdx.x / gridDim.x;
     const long long end = total * (blockIdx.x + 1) / gridDim.x;
     while (pos < end) {
-        const long long tile = pos / L;
-        const int i0 = (int)(pos % L) + 1;
-        const int i1 = (int)min((long long)L, (long long)i0 + (end - pos) - 1);
+        long long tile, run;
+        int i0;
+        if (pos < nhead) {
+            tile = pos / Hd;
+            i0 = (int)(pos % Hd) + 1;
+            run = Hd - (pos % Hd);
+        } else {
+            const long long v = pos - nhead;
+            tile = v / Lt;
+            i0 = (int)(Hd + v % Lt) + 1;
+            run = Lt - (v % Lt);
+        }
+        const int i1 = i0 + (int)min(run, end - pos) - 1;
         pos += i1 - i0 + 1;
         const int k0 = (int)(tile % ntk) * WK + 1, j0 = (int)(tile / ntk) * WJ + 1;
         const int j = j0 + r, k = k0 + l;

@@ -310,8 +310,6 @@ int fsl_step_stage(fsl_ctx *ctx);
                                  full-lane persistent 16 x 32 tile (the FP32 bulk's default with the
                                  reference reconstruction; elsewhere 0 runs 16) */
 #define FSL_TUNE_STAGE_SEG 2  /* x planes marched per stage block (default 48 FP32 bulk, 32 FP64) */
-#define FSL_TUNE_INFER_TILES 3 /* learned-closure inference: 128-cell tiles in flight per block, 1 or
-                                  2 (default 2: one tile's SiLU overlaps the other's products) */
 int fsl_tune(fsl_ctx *ctx, int key, int value);
 
 /* ---- debug / parity access ----------------------------------------------- */
@@ -384,12 +382,12 @@ int fsl_tecplot_write(const char *path, int LEN, int HIG, int DEP, const double 
  * over the cells at least two from every boundary.  The steps fall back to the
  * dynamic procedure while either criterion fails:
  *   - effective viscosity: |<mu_mlp> - <mu_dyn>|_2 / |mu_L + <mu_dyn>|_2 over
- *     all rows exceeds `threshold` (fsl_closure_judge, default 0.02) -- what
+ *     all rows exceeds `threshold` (fsl_closure_judge, default 0.05) -- what
  *     the viscous fluxes see;
  *   - SGS viscosity where the model acts: over the rows whose <mu_dyn> is at
  *     least `floor` mu_L (fsl_closure_judge_active, default floor 0.1),
  *     |<mu_mlp> - <mu_dyn>|_2 / |<mu_dyn>|_2 exceeds `threshold` (default
- *     0.5).  Where the dynamic procedure gives SGS viscosity comparable to the
+ *     0.4).  Where the dynamic procedure gives SGS viscosity comparable to the
  *     molecular one, a network that predicts too little (or nothing) fails
  *     here even when the first criterion, dominated by mu_L, would pass.
  * The Cs^2 errors and the SGS viscosity error relative to the dynamic SGS
@@ -409,7 +407,7 @@ typedef struct fsl_closure_stats {
                               <mu_dyn> >= floor mu_L (0 when there are none) */
     double dyn_ratio;      /* last judgement: max over rows of <mu_dyn>(y) / mu_L */
     int active_rows;       /* last judgement: rows in mu_active_err */
-    int reserved_;
+    int dynamic_steps;     /* steps whose SGS viscosity came from the dynamic procedure (fallback) */
 } fsl_closure_stats;
 
 /* Feature scales: t_ref = delta_w0 / dU (time scale of |S|), len_ref = delta_w0. */

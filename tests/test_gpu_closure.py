@@ -243,29 +243,3 @@ def test_shipped_weights_on_an_active_state(fsl, oracle_lib):
           "cs2_profile_err %.3f" % (st.dyn_ratio, st.active_rows, st.mu_active_err, st.mu_profile_err,
                                     st.visc_err, st.profile_err))
     assert st.active_rows > 0 and np.isfinite(st.mu_active_err)
-
-
-@pytest.mark.parametrize("grid", [(24, 12, 16), (40, 20, 24), (64, 32, 32)])
-def test_inference_two_tiles_in_flight_equals_one(fsl, oracle_lib, grid):
-    """The inference kernel that keeps two 128-cell tiles in flight per block
-    (the default) gives the same Cs^2 and SGS viscosity, bit for bit, as the
-    one-tile kernel: the same products on the same operands, only
-    interleaved (grids with an odd tile count per block exercise the
-    single-tile tail)."""
-    L, H, D = grid
-    p = temporal_params(L=L, H=H, D=D, Mc=0.5, Re=20000.0, sgs=1, precision=1)
-    s, dU = oracle_lib.Oracle.temporal_state(p, 0.5, amp=0.05)
-    out = []
-    for tiles in (1, 2):
-        d = fsl.Domain(p)
-        d.tune(d.TUNE_INFER_TILES, tiles)
-        d.upload_state(s)
-        d.closure_set_scales(1.0 / dU, 1.0)
-        d.closure_set_weights(fsl.closure_weights())
-        d.closure_judge(0, 0.02)
-        _, cm, _ = d.closure_compare(fields=True)
-        d.step(3)
-        out.append((cm, d.download_state()))
-        d.close()
-    assert np.array_equal(out[0][0], out[1][0])
-    assert np.array_equal(out[0][1], out[1][1])
