@@ -151,7 +151,8 @@ def lib():
         sig.update({
             "fsl_ensemble_create": [C.POINTER(C.c_void_p), i, C.POINTER(C.c_void_p)],
             "fsl_ensemble_destroy": [vp], "fsl_ensemble_set_chunk": [vp, i], "fsl_ensemble_step": [vp, i],
-            "fsl_ensemble_sync": [vp],
+            "fsl_ensemble_sync": [vp], "fsl_ensemble_persistent": [vp],
+            "fsl_ensemble_set_barrier_limit": [vp, C.c_uint],
             "fsl_ensemble_tune": [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)],
         })
         cs = C.c_char_p
@@ -666,6 +667,14 @@ class Ensemble:
 
     def sync(self):
         self._c(lib().fsl_ensemble_sync(self.h))
+
+    def persistent(self) -> int:
+        """1 when a step's stages run as one cooperative launch for all members."""
+        return lib().fsl_ensemble_persistent(self.h)
+
+    def set_barrier_limit(self, polls: int):
+        """Polls a grid barrier of the persistent launch waits before giving up."""
+        self._c(lib().fsl_ensemble_set_barrier_limit(self.h, polls))
 
     def tune(self, trial_steps: int = 5):
         """Autotune the fused-stage tile shape; returns (rows, seg, ms per step)."""

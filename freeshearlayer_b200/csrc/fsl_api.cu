@@ -934,6 +934,29 @@ static int step_sgs(Ctx &c)
     }
 }
 
+} // extern "C"
+
+namespace fsl {
+// The part of an FP32-bulk fused step before its stages, for the persistent
+// multi-domain stage launch (which runs the three stages, with the ghost
+// layers and boundary faces between them): the same launches fsl_step makes
+// before its first stage.
+int step_prelude32(Ctx &c)
+{
+    int rc;
+    if ((rc = ensure_dyn(c)) || (rc = ensure_bf(c)) || (rc = ensure_fp32(c))) return rc;
+    if (c.co_valid) launch_courant_apply(c);
+    else launch_courant(c);
+    c.step++;
+    draw(c);
+    launch_ghost(c, c.U);
+    launch_bface32(c, c.U, c.dist);
+    return step_sgs(c);
+}
+} // namespace fsl
+
+extern "C" {
+
 // An x-slab (Courant range narrower than the domain) steps one step at a
 // time, from a Courant maximum combined across the slabs; a learned closure
 // would judge on the slab alone.

@@ -31,6 +31,14 @@ struct fsl_ensemble {
     unsigned long long gen = 0, exec_gen = ~0ull; // member configuration generation
     int chunk = 10;
     std::string err;
+    // the persistent path: the members' three stages of a step in one
+    // cooperative launch (all members FP32 bulk, reference reconstruction,
+    // full-lane tiles); otherwise each member's fused steps
+    WidePlan *plan = nullptr;
+    unsigned long long plan_gen = ~0ull;
+    bool persistent_off = false; // the persistent path could not be captured here
+    unsigned barrier_limit = 1u << 24;
+    std::string why_not;
 };
 
 namespace {
@@ -62,10 +70,80 @@ int check_member(fsl_ensemble *e, const Ctx &c)
     return FSL_OK;
 }
 
+// The persistent plan for the current members, when they all qualify.
+void refresh_plan(fsl_ensemble *e)
+{
+    if (e->plan && e->plan_gen == e->gen) return;
+    wide_plan_free(e->plan);
+    e->plan = nullptr;
+    if (e->persistent_off) return;
+    std::vector<Ctx *> ms;
+    for (fsl_ctx *h : e->m) ms.push_back(&h->c);
+    WidePlan *p = nullptr;
+    if (wide_plan_build(ms, &p, e->why_not) == FSL_OK) {
+        wide_plan_set_limit(p, e->barrier_limit);
+        e->plan = p;
+        e->why_not.clear();
+    }
+    e->plan_gen = e->gen;
+}
+
+// Capture `steps` persistent-path steps: per step the members' work before
+// their first stage (each on its own stream), then one cooperative launch
+// of all members' three stages.
+int capture_persistent(fsl_ensemble *e, int steps)
+{
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return ens_fail(e, FSL_ERR_CUDA, "cudaStreamBeginCapture");
+    int rc = FSL_OK;
+    for (int t = 0; t < steps && !rc; t++) {
+        cudaEventRecord(e->cap_fork[0], e->stream);
+        for (size_t q = 0; q < e->m.size(); q++) {
+            Ctx &c = e->m[q]->c;
+            cudaStreamWaitEvent(c.stream, e->cap_fork[0], 0);
+            if (!rc) rc = step_prelude32(c);
+            cudaEventRecord(e->cap_join[q], c.stream);
+            cudaStreamWaitEvent(e->stream, e->cap_join[q], 0);
+        }
+        if (!rc) rc = wide_plan_launch(e->plan, e->stream);
+        for (fsl_ctx *h : e->m) h->c.co_valid = true;
+    }
+    const cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+    for (fsl_ctx *h : e->m) h->c.step -= (unsigned)steps;
+    if (rc || ce != cudaSuccess || !graph) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError(); // a refused capture leaves no sticky state
+        return rc ? rc : FSL_ERR_CUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&e->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+        e->exec = nullptr;
+        cudaGetLastError();
+        return FSL_ERR_CUDA;
+    }
+    e->exec_steps = steps;
+    e->exec_gen = e->gen;
+    return FSL_OK;
+}
+
 // Capture `steps` fused steps of every member into one graph.
 int capture(fsl_ensemble *e, int steps)
 {
     drop_graph(e);
+    refresh_plan(e);
+    if (e->plan) {
+        const int rc = capture_persistent(e, steps);
+        if (rc == FSL_OK) return FSL_OK;
+        // the cooperative launch could not be captured: the members' fused
+        // steps instead, from now on
+        drop_graph(e);
+        e->persistent_off = true;
+        wide_plan_free(e->plan);
+        e->plan = nullptr;
+        e->why_not = "the cooperative stage launch could not be captured in a graph";
+    }
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return ens_fail(e, FSL_ERR_CUDA, "cudaStreamBeginCapture");
@@ -176,6 +254,7 @@ int fsl_ensemble_destroy(fsl_ensemble *e)
     if (!e) return FSL_ERR_ARG;
     if (e->stream) cudaStreamSynchronize(e->stream);
     drop_graph(e);
+    wide_plan_free(e->plan);
     for (auto *v : {&e->fork, &e->join, &e->cap_fork, &e->cap_join})
         for (cudaEvent_t ev : *v)
             if (ev) cudaEventDestroy(ev);
@@ -187,6 +266,22 @@ int fsl_ensemble_destroy(fsl_ensemble *e)
 const char *fsl_ensemble_last_error(const fsl_ensemble *e) { return e ? e->err.c_str() : "no ensemble"; }
 
 void *fsl_ensemble_stream(fsl_ensemble *e) { return e ? (void *)e->stream : nullptr; }
+
+int fsl_ensemble_persistent(fsl_ensemble *e)
+{
+    if (!e) return FSL_ERR_ARG;
+    refresh_plan(e);
+    return e->plan ? 1 : 0;
+}
+
+int fsl_ensemble_set_barrier_limit(fsl_ensemble *e, unsigned polls)
+{
+    if (!e) return FSL_ERR_ARG;
+    drop_graph(e); // the limit is a launch argument
+    e->barrier_limit = polls;
+    if (e->plan) wide_plan_set_limit(e->plan, polls);
+    return FSL_OK;
+}
 
 int fsl_ensemble_set_chunk(fsl_ensemble *e, int steps)
 {
@@ -251,6 +346,10 @@ int fsl_ensemble_sync(fsl_ensemble *e)
 {
     if (!e) return FSL_ERR_ARG;
     if (cudaStreamSynchronize(e->stream) != cudaSuccess) return ens_fail(e, FSL_ERR_CUDA, "ensemble stream");
+    if (e->plan) {
+        const int brc = wide_plan_check(e->plan, e->stream);
+        if (brc) return ens_fail(e, brc, "a grid barrier of the persistent stage launch gave up");
+    }
     for (fsl_ctx *h : e->m) {
         int rc = fsl_sync(h);
         if (rc) return ens_fail(e, rc, fsl_last_error(h));

@@ -180,6 +180,7 @@ void prof_begin(Ctx &c, int cls);
 void prof_end(Ctx &c, int cls, int nkernels);
 
 int ensure_dyn_scratch(Ctx &c);  // SGS scratch of the dynamic procedure + the FP32 SGS field (fsl_api.cu)
+int step_prelude32(Ctx &c);      // an FP32-bulk step up to its first stage (fsl_api.cu)
 int closure_step_sgs(Ctx &c);    // SGS of one step under FSL_SGS_LEARNED (fsl_closure.cu)
 int closure_ensure(Ctx &c);
 void closure_free(Ctx &c);
@@ -237,6 +238,14 @@ int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double 
 // FP32-bulk variants (fsl_fused32.cu): boundary states in bf32, SGS viscosity in mu32.
 void launch_bface32(Ctx &c, const double *cur, const Disturb &d);
 int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant = false);
+// The three stages of an FP32-bulk step of several domains in one persistent
+// cooperative launch (fsl_fused32.cu); opaque plan built per member set.
+struct WidePlan;
+int wide_plan_build(const std::vector<Ctx *> &members, WidePlan **plan, std::string &why);
+void wide_plan_free(WidePlan *plan);
+int wide_plan_launch(WidePlan *plan, cudaStream_t st);
+int wide_plan_set_limit(WidePlan *plan, unsigned polls);
+int wide_plan_check(WidePlan *plan, cudaStream_t st); // FSL_ERR_TIMEOUT (and reset) after a barrier gave up
 
 // ---- learned closure (fsl_mlp.cu) ---------------------------------------------
 int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, float *cs2_out, const float *P,

@@ -75,12 +75,15 @@ __device__ __forceinline__ void ppm_at_x(const Grid &g, const double *__restrict
     ppm_x(cc, m2, m1, p1, p2, hi, lo);
 }
 
-// Outer states of all domain-boundary faces (src/bounCondOnInterfaces.c:11-110).
+// Outer states of one domain-boundary face (src/bounCondOnInterfaces.c:11-110):
+// face t of the x (HIG DEP), y (LEN DEP) and z (LEN HIG) boundary lists.
+// Not inlined: the boundary pass and the persistent multi-domain stage
+// kernel run this one compiled body, so their FP32 results agree bit for bit.
 template <typename T>
-__global__ void k_bface(Grid g, int setup, int BL_HIG, Disturb d, const double *__restrict__ u, BF<T> bf)
+__device__ __noinline__ void bface_one(Grid g, int setup, int BL_HIG, Disturb d, const double *__restrict__ u,
+                                       BF<T> bf, long long t)
 {
     const int L = g.L, H = g.H, D = g.D;
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nx = (long long)H * D, ny = (long long)L * D, nz = (long long)L * H;
     const bool spatial = (setup == FSL_SETUP_SPATIAL);
     typedef Kc<T> kc;
@@ -142,6 +145,14 @@ __global__ void k_bface(Grid g, int setup, int BL_HIG, Disturb d, const double *
 #pragma unroll
         for (int q = 0; q < 5; q++) bf.zD[q * nz + t] = lo[q];
     }
+}
+
+template <typename T>
+__global__ void k_bface(Grid g, int setup, int BL_HIG, Disturb d, const double *__restrict__ u, BF<T> bf)
+{
+    const long long n = (long long)g.H * g.D + (long long)g.L * g.D + (long long)g.L * g.H;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) bface_one<T>(g, setup, BL_HIG, d, u, bf, t);
 }
 
 template <typename T, int TJE, bool PPM = false> struct Smem {

@@ -163,11 +163,12 @@ __device__ __forceinline__ void face_z(const Smem<T> &s, const Consts &kc, int q
                           s.R[s0][a - 1][b], m_f, kc, F);
 }
 
+// Block b of a domain's stage launch of nb blocks: its share of the
+// (tile, plane) pairs, and with a.co the Courant maximum of what it wrote.
 template <typename T, bool SST>
-__global__ void __launch_bounds__(NT, 1) k_stage_wide(Grid g, Consts kc, Args<T> a)
+__device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Consts &kc, const Args<T> &a, int b,
+                                           int nb)
 {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    Smem<T> &s = *reinterpret_cast<Smem<T> *>(smraw);
     const int L = g.L, H = g.H, D = g.D;
     const int t = threadIdx.x, r = t >> 5, l = t & 31;
     const long long fs = g.fstride;
@@ -186,10 +187,10 @@ __global__ void __launch_bounds__(NT, 1) k_stage_wide(Grid g, Consts kc, Args<T>
     const int ntk = (D + WK - 1) / WK, ntj = (H + WJ - 1) / WJ;
     const long long ntiles = (long long)ntk * ntj, total = ntiles * L;
     // heads: planes 1..Hd of every tile; tails: planes Hd+1..L of every tile
-    const long long Hd = min((long long)L, total / gridDim.x);
+    const long long Hd = min((long long)L, total / nb);
     const long long Lt = L - Hd, nhead = ntiles * Hd;
-    long long pos = total * blockIdx.x / gridDim.x;
-    const long long end = total * (blockIdx.x + 1) / gridDim.x;
+    long long pos = total * b / nb;
+    const long long end = total * (b + 1) / nb;
     while (pos < end) {
         long long tile, run;
         int i0;
@@ -544,6 +545,192 @@ __global__ void __launch_bounds__(NT, 1) k_stage_wide(Grid g, Consts kc, Args<T>
             // non-negative doubles order like their bit patterns
             atomicMax(a.co, (unsigned long long)__double_as_longlong(m));
         }
+        __syncthreads(); // comax is reset by the next block's work
+    }
+}
+
+// One domain of a (multi-domain) persistent stage launch: its grid, constants
+// and buffers.  Stage s reads st[s-1] and writes out[s-1] (U -> Up -> Uq -> U);
+// nb is the number of blocks of the domain's own launch, whose split of the
+// (tile, plane) pairs a multi-domain launch keeps, so a domain's results do
+// not depend on the other domains it is stepped with.
+struct WideMember {
+    Grid g;
+    Consts kc;
+    const double *st[3];
+    double *out[3];
+    const double *un;
+    const float *mu;
+    BF<float> bf;
+    const DevScalars *ds;
+    unsigned long long *co; // stage 3 Courant maximum (device scalar)
+    unsigned int *status;
+    int co_i0, co_i1;
+    int nb;
+    int setup, BL_HIG;
+    Disturb dist;
+};
+
+// A grid-wide barrier with a bounded wait: false (and *err set) when the
+// other blocks did not all arrive within `limit` polls.  Only for launches
+// whose blocks are all resident (cooperative launches).
+struct GridBarrier {
+    unsigned *count, *gen;
+    int *err;
+    unsigned limit;
+};
+
+__device__ __forceinline__ bool grid_sync(const GridBarrier &gb, unsigned nblocks)
+{
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = gb.gen;
+        const unsigned g0 = *gen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(gb.count, 1u) + 1u == nblocks) {
+            atomicExch(gb.count, 0u);
+            __threadfence();
+            atomicAdd(gb.gen, 1u);
+        } else {
+            unsigned n = 0;
+            while (*gen == g0) {
+                if (++n > gb.limit) {
+                    ok = 0;
+                    atomicExch(gb.err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok_s = ok && *(volatile int *)gb.err == 0;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// The ghost layer of a temporal-setup state (periodic x and z, zero-gradient
+// y; the copies of the ghost-cell pass, src/boundCondInGhostCells.c:58-94
+// with the periodic x rule): ghost cell t of the x, y and z boundary lists.
+__device__ __forceinline__ void ghost_temporal(const Grid &g, double *__restrict__ u, long long t)
+{
+    const int L = g.L, H = g.H, D = g.D;
+    const long long nx = 2LL * (H + 2) * (D + 2), ny = 2LL * L * (D + 2);
+    int i, j, k;
+    if (t < nx) {
+        const long long q = (long long)(H + 2) * (D + 2);
+        i = (t / q) ? L + 1 : 0;
+        const long long rr = t % q;
+        j = (int)(rr / (D + 2));
+        k = (int)(rr % (D + 2));
+    } else if ((t -= nx) < ny) {
+        const long long q = (long long)L * (D + 2);
+        j = (t / q) ? H + 1 : 0;
+        const long long rr = t % q;
+        i = 1 + (int)(rr / (D + 2));
+        k = (int)(rr % (D + 2));
+    } else {
+        t -= ny;
+        const long long q = (long long)L * H;
+        k = (t / q) ? D + 1 : 0;
+        const long long rr = t % q;
+        i = 1 + (int)(rr / H);
+        j = 1 + (int)(rr % H);
+    }
+    const int jj = j == 0 ? 1 : j == H + 1 ? H : j;
+    const int kk = k == 0 ? D : k == D + 1 ? 1 : k;
+    const int si = i == 0 ? L : i == L + 1 ? 1 : i;
+    const long long src = g.idx(si, jj, kk), dst = g.idx(i, j, k), fs = g.fstride;
+#pragma unroll
+    for (int q = 0; q < 5; q++) u[q * fs + dst] = u[q * fs + src];
+}
+
+__device__ __forceinline__ long long ghost_count(const Grid &g)
+{
+    return 2LL * (g.H + 2) * (g.D + 2) + 2LL * g.L * (g.D + 2) + 2LL * g.L * g.H;
+}
+
+__device__ __forceinline__ long long bface_count(const Grid &g)
+{
+    return (long long)g.H * g.D + (long long)g.L * g.D + (long long)g.L * g.H;
+}
+
+// The work of one persistent launch: stages s_begin .. s_end of nmem domains
+// (m0 alone when mem is null).  With items, block x runs the (domain, block)
+// pairs items[start[x] .. start[x+1]); without, block x is block x of the
+// single domain.  Between two stages of one launch the blocks meet at a grid
+// barrier and fill the new state's ghost layer and boundary faces (temporal
+// setup), so a whole step of many domains is one launch.
+struct WideWork {
+    WideMember m0;
+    const WideMember *mem;
+    int nmem;
+    const int2 *items;
+    const int *start;
+    int s_begin, s_end;
+    int courant; // stage 3 accumulates the Courant maximum
+    GridBarrier bar;
+};
+
+__device__ __forceinline__ Args<float> member_args(const WideMember &M, int st, bool courant)
+{
+    Args<float> a;
+    a.cur = M.st[st - 1];
+    a.un = M.un;
+    a.out = M.out[st - 1];
+    a.mu = M.mu;
+    a.bf = M.bf;
+    a.ds = M.ds;
+    a.co = (st == 3 && courant) ? M.co : nullptr;
+    a.co_i0 = M.co_i0;
+    a.co_i1 = M.co_i1;
+    a.status = M.status;
+    a.stage = st;
+    a.seg = 0;
+    return a;
+}
+
+// MULTI = false: one stage of the domain w.m0, block x its block x (its
+// descriptor stays in the parameter space).  MULTI = true: the work list.
+// Both instantiate the same block code (wide_block), so a domain stepped
+// alone and in a multi-domain launch computes the same values.
+template <bool SST, bool MULTI>
+__global__ void __launch_bounds__(NT, 1) k_wide(WideWork w)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Smem<float> &s = *reinterpret_cast<Smem<float> *>(smraw);
+    if constexpr (!MULTI) {
+        wide_block<float, SST>(s, w.m0.g, w.m0.kc, member_args(w.m0, w.s_begin, w.courant != 0), blockIdx.x,
+                               w.m0.nb);
+    } else {
+    for (int st = w.s_begin; st <= w.s_end; st++) {
+        const int i0 = w.start[blockIdx.x], i1 = w.start[blockIdx.x + 1];
+        for (int it = i0; it < i1; it++) {
+            const int2 x = w.items[it];
+            const int mi = x.x, b = x.y;
+            const WideMember &M = w.mem[mi];
+            wide_block<float, SST>(s, M.g, M.kc, member_args(M, st, w.courant != 0), b, M.nb);
+        }
+        if (st == w.s_end) break;
+        // the new state's ghost layer, then its boundary faces, all domains
+        const long long nthr = (long long)gridDim.x * NT, t0 = (long long)blockIdx.x * NT + threadIdx.x;
+        if (!grid_sync(w.bar, gridDim.x)) return;
+        for (int m = 0; m < w.nmem; m++) {
+            const WideMember &M = w.mem[m];
+            const long long n = ghost_count(M.g);
+            for (long long t = t0; t < n; t += nthr) ghost_temporal(M.g, M.out[st - 1], t);
+        }
+        if (!grid_sync(w.bar, gridDim.x)) return;
+        for (int m = 0; m < w.nmem; m++) {
+            const WideMember &M = w.mem[m];
+            const long long n = bface_count(M.g);
+            for (long long t = t0; t < n; t += nthr)
+                stage::bface_one<float>(M.g, M.setup, M.BL_HIG, M.dist, M.out[st - 1], M.bf, t);
+        }
+        if (!grid_sync(w.bar, gridDim.x)) return;
+    }
     }
 }
 
@@ -557,23 +744,53 @@ inline int wide_blocks(const Grid &g, int sms)
     return (int)std::max(1LL, std::min((long long)sms, want));
 }
 
+// The single-domain member descriptor of a context (FP32 buffers).
+inline WideMember wide_member(const Ctx &c, const float *mu, BF<float> bf, int sms)
+{
+    WideMember m;
+    m.g = c.g;
+    m.kc = c.k;
+    m.st[0] = c.U; m.st[1] = c.Up; m.st[2] = c.Uq;
+    m.out[0] = c.Up; m.out[1] = c.Uq; m.out[2] = c.U;
+    m.un = c.U;
+    m.mu = mu;
+    m.bf = bf;
+    m.ds = c.ds;
+    m.co = &c.ds->co_bits;
+    m.status = &c.ds->status;
+    m.co_i0 = c.co_i0;
+    m.co_i1 = c.co_i1;
+    m.nb = wide_blocks(c.g, sms);
+    m.setup = c.k.setup;
+    m.BL_HIG = c.k.BL_HIG;
+    m.dist = c.dist;
+    return m;
+}
+
+template <bool SST, bool MULTI> inline bool wide_attr()
+{
+    static std::atomic<uint64_t> attr{0};
+    return smem_limit_once((const void *)k_wide<SST, MULTI>, sizeof(Smem<float>), attr);
+}
+
+// One stage of one domain (the FP32 bulk's fused stage with the reference
+// reconstruction).  The buffers are the context's fixed stage sequence.
 template <bool SST>
 int launch_wide(Ctx &c, int stage, const double *cur, const double *un, double *out, const float *mu,
                 BF<float> bf, bool courant)
 {
-    const Grid &g = c.g;
-    Args<float> a;
-    a.cur = cur; a.un = un; a.out = out; a.mu = mu; a.bf = bf; a.ds = c.ds; a.stage = stage;
-    a.co = courant ? &c.ds->co_bits : nullptr;
-    a.co_i0 = c.co_i0;
-    a.co_i1 = c.co_i1;
-    a.status = &c.ds->status;
-    a.seg = 0;
-    const size_t smem = sizeof(Smem<float>);
-    static std::atomic<uint64_t> attr{0};
-    if (!smem_limit_once((const void *)k_stage_wide<float, SST>, smem, attr)) return -1;
+    (void)cur; (void)un; (void)out; // always U -> Up -> Uq -> U with U^n = U
+    if (!wide_attr<SST, false>()) return -1;
+    WideWork w{};
+    w.m0 = wide_member(c, mu, bf, c.sms);
+    w.mem = nullptr;
+    w.nmem = 1;
+    w.items = nullptr;
+    w.start = nullptr;
+    w.s_begin = w.s_end = stage;
+    w.courant = courant ? 1 : 0;
     prof_begin(c, FSL_K_STAGE);
-    k_stage_wide<float, SST><<<wide_blocks(g, c.sms), NT, smem, c.stream>>>(g, c.k, a);
+    k_wide<SST, false><<<w.m0.nb, NT, sizeof(Smem<float>), c.stream>>>(w);
     prof_end(c, FSL_K_STAGE, 1);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

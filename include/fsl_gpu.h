@@ -475,6 +475,21 @@ void *fsl_ensemble_stream(fsl_ensemble *ens);
 int fsl_ensemble_set_chunk(fsl_ensemble *ens, int steps);
 int fsl_ensemble_step(fsl_ensemble *ens, int nsteps);
 int fsl_ensemble_sync(fsl_ensemble *ens);
+/* 1 when the ensemble steps on the persistent path: all members FP32 bulk,
+ * reference reconstruction, full-lane tiles (FSL_TUNE_STAGE_ROWS 0).  A step
+ * is then the members' work before their first stage, each on its own
+ * stream, and ONE cooperative launch that runs the three stages of every
+ * member, balanced over one block per SM, with grid barriers between the
+ * stages (where the blocks also fill the new states' ghost layers and
+ * boundary faces).  A member keeps the split of its planes into blocks that
+ * its own launches use, so its results are bit-identical to stepping it
+ * alone.  0: each member's fused steps, replayed from a CUDA graph. */
+int fsl_ensemble_persistent(fsl_ensemble *e);
+/* Polls (64 ns sleeps) a grid barrier of the persistent launch waits for the
+ * other blocks before it gives up (default 2^24).  A barrier that gives up
+ * ends the launch early and fsl_ensemble_sync returns FSL_ERR_TIMEOUT; the
+ * members' states of that step are then incomplete (upload them again). */
+int fsl_ensemble_set_barrier_limit(fsl_ensemble *e, unsigned polls);
 /* Autotuner of the fused-stage tile shape (tile rows 8/12/16 x planes per
  * block 8/16/32/64, one shape for all members): each candidate is timed on
  * the device over one graph replay of trial_steps ensemble steps; the
