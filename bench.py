@@ -461,16 +461,40 @@ def ensemble_block(fsl, torch, steps, n):
     for d in doms:
         d.step(steps)
     same = all(np.array_equal(d.download_state(), f) for d, f in zip(doms, ens_final))
+    ens_units = cells * STAGES * (steps - 1)
+    # the persistent path (one cooperative launch of every member's stages
+    # per step) when the tuner chose another shape
+    pers = None
+    if rows != 0:
+        reset()
+        for d in doms:
+            d.tune(d.TUNE_STAGE_ROWS, 0)
+        e = fsl.Ensemble(doms)
+        e.step(1)
+        e.sync()
+        if e.persistent():
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            ext = torch.cuda.ExternalStream(e.stream)
+            a.record(ext)
+            e.step(steps - 1)
+            b.record(ext)
+            b.synchronize()
+            e.sync()
+            pms = a.elapsed_time(b)
+            pers = {"value": ens_units / (pms / 1e3), "ms": pms, "steps": steps - 1}
+        e.close()
     for d in doms:
         d.close()
-    ens_units = cells * STAGES * (steps - 1)
     return {"workload": "%d temporal shear layers, grids {48,64,96,128}x{32,48,64}x{32,48,64}, Mc U[0.2,0.8], "
                         "Re_dw0 U[300,1000], noise 1e-3 dU, FP32 bulk + FP64 accumulation, dynamic Smagorinsky"
                         % n,
             "members": n, "cells": cells, "steps": steps,
             "sequential": {"value": units / (seq_ms / 1e3), "ms": seq_ms},
             "ensemble": {"value": ens_units / (ens_ms / 1e3), "ms": ens_ms, "steps": steps - 1,
-                         "tile_rows": rows, "planes_per_block": seg, "chunk": 10},
+                         "tile_rows": rows, "planes_per_block": seg, "chunk": 10,
+                         "persistent": rows == 0},
+            "persistent_rows0": pers,
             "speedup": (ens_units / ens_ms) / (units / seq_ms), "bit_identical": bool(same)}
 
 

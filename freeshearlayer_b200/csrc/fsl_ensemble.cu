@@ -39,6 +39,7 @@ struct fsl_ensemble {
     bool persistent_off = false; // the persistent path could not be captured here
     unsigned barrier_limit = 1u << 24;
     std::string why_not;
+    std::vector<int> sig; // the members' launch shapes the captured work was built for
 };
 
 namespace {
@@ -291,6 +292,20 @@ int fsl_ensemble_set_chunk(fsl_ensemble *e, int steps)
     return FSL_OK;
 }
 
+// A member retuned after the ensemble captured its work invalidates it.
+static void check_shapes(fsl_ensemble *e)
+{
+    std::vector<int> sig;
+    for (fsl_ctx *h : e->m) {
+        sig.push_back(h->c.stage_tje);
+        sig.push_back(h->c.stage_seg);
+    }
+    if (sig != e->sig) {
+        e->sig = sig;
+        e->gen++;
+    }
+}
+
 int fsl_ensemble_step(fsl_ensemble *e, int nsteps)
 {
     ApiRange range_("fsl_ensemble_step");
@@ -299,6 +314,7 @@ int fsl_ensemble_step(fsl_ensemble *e, int nsteps)
     int rc;
     for (fsl_ctx *h : e->m)
         if ((rc = check_member(e, h->c))) return rc;
+    check_shapes(e);
     // a member whose Courant maximum is not on the device yet (fresh upload,
     // a per-phase call) takes one plain step first: it allocates what the
     // step needs and leaves the graph-ready device state

@@ -710,8 +710,18 @@ __global__ void __launch_bounds__(NT, 1) k_wide(WideWork w)
         for (int it = i0; it < i1; it++) {
             const int2 x = w.items[it];
             const int mi = x.x, b = x.y;
-            const WideMember &M = w.mem[mi];
-            wide_block<float, SST>(s, M.g, M.kc, member_args(M, st, w.courant != 0), b, M.nb);
+            // the member's descriptor and stage arguments in shared memory:
+            // the block code reads them where it needs them instead of
+            // holding them in registers
+            __shared__ WideMember sm;
+            __shared__ Args<float> sa;
+            __syncthreads(); // the previous item's readers are done
+            if (threadIdx.x == 0) {
+                sm = w.mem[mi];
+                sa = member_args(sm, st, w.courant != 0);
+            }
+            __syncthreads();
+            wide_block<float, SST>(s, sm.g, sm.kc, sa, b, sm.nb);
         }
         if (st == w.s_end) break;
         // the new state's ghost layer, then its boundary faces, all domains
@@ -735,12 +745,13 @@ __global__ void __launch_bounds__(NT, 1) k_wide(WideWork w)
 }
 
 // Blocks of the persistent grid: one per SM, fewer when the domain has fewer
-// than 16 planes of tiles per SM (each block then marches at least that far).
+// than 32 planes of tiles per SM (each block then marches at least that far,
+// so its prologue -- two planes loaded, one face -- stays a small share).
 inline int wide_blocks(const Grid &g, int sms)
 {
     const long long ntiles = (long long)((g.D + WK - 1) / WK) * ((g.H + WJ - 1) / WJ);
     const long long units = ntiles * g.L;
-    const long long want = (units + 15) / 16;
+    const long long want = (units + 31) / 32;
     return (int)std::max(1LL, std::min((long long)sms, want));
 }
 
