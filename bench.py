@@ -404,8 +404,11 @@ def ensemble_members(n, seed=20251203):
 
 def ensemble_block(fsl, torch, steps, n):
     """Aggregate cell-stage updates/s of n members advanced one after another
-    (each alone, fsl_step) and as one graph-replayed ensemble (autotuned tile
-    shape), from the same initial states; the final states must agree bitwise."""
+    (each alone, fsl_step) and as one graph-replayed ensemble, both with the
+    tile shape the autotuner picks for the ensemble, from the same initial
+    states; the final states must agree bitwise.  When the tuner does not pick
+    the persistent path (one cooperative launch of all members' stages per
+    step), that path is timed too."""
     import numpy as np
     members = ensemble_members(n)
     doms, states = [], []
@@ -417,15 +420,21 @@ def ensemble_block(fsl, torch, steps, n):
         states.append(st)
     cells = sum(p["LEN"] * p["HIG"] * p["DEP"] for p, _, _ in members)
     units = cells * STAGES * steps
-    # members one after another
     for d in doms:
         d.step(1)  # allocation and kernel attributes outside the timed region
         d.sync()
-    def reset():  # same initial state and time step for both runs
+    def reset():  # same initial state and time step for every run
         for d, st, (p, _, _) in zip(doms, states, members):
             d.upload_state(st)
             d.set_time(0, p["deltaT"])
 
+    # the tile shape the autotuner picks for the ensemble; the members stepped
+    # one after another use the same shape, so the ratio compares schedules
+    e = fsl.Ensemble(doms)
+    e.step(1)
+    rows, seg, _ = e.tune(trial_steps=5)
+    e.close()
+    # members one after another
     reset()
     seq_ms = 0.0
     for d in doms:
@@ -437,10 +446,8 @@ def ensemble_block(fsl, torch, steps, n):
         b.record(ext)
         b.synchronize()
         seq_ms += a.elapsed_time(b)
-    # the ensemble, with the autotuned tile shape
+    # the ensemble, with the autotuned tile shape (the members kept it)
     e = fsl.Ensemble(doms)
-    e.step(1)
-    rows, seg, _ = e.tune(trial_steps=5)
     reset()
     e.step(1)  # the warm-up step after an upload runs uncaptured
     e.sync()
@@ -455,8 +462,7 @@ def ensemble_block(fsl, torch, steps, n):
     ens_ms = a.elapsed_time(b)
     ens_final = [d.download_state() for d in doms]
     e.close()
-    # members alone with the ensemble's tile shape: the same bits (the FP32
-    # bulk kernels' last bits may depend on the tile shape)
+    # members alone with the ensemble's tile shape: the same bits
     reset()
     for d in doms:
         d.step(steps)
@@ -840,7 +846,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 path beside the arm")
     ap.add_argument("--ppm-steps", type=int, default=20,
                     help="steps timed with PPM reconstruction (FP32 + closure and FP64); 0 skips them")
-    ap.add_argument("--ens-steps", type=int, default=100, help="steps of the ensemble comparison (0: skip)")
+    ap.add_argument("--ens-steps", type=int, default=500, help="steps of the ensemble comparison (0: skip)")
     ap.add_argument("--ens-members", type=int, default=32)
     ap.add_argument("--slab-steps", type=int, default=0,
                     help="steps of the x-slab comparison on one GPU (0: skip)")
