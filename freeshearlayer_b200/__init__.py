@@ -488,7 +488,7 @@ class Domain:
                                           b.ctypes.data if fields else None, C.byref(st)))
         return (st, a, b) if fields else st
 
-    TUNE_STAGE_ROWS, TUNE_STAGE_SEG = 1, 2
+    TUNE_STAGE_ROWS, TUNE_STAGE_SEG, TUNE_CLOSURE_POLY = 1, 2, 3
 
     def tune(self, key: int, value: int):
         """Launch-shape knob of the fused kernels (results do not depend on it)."""

@@ -1147,6 +1147,10 @@ int fsl_tune(fsl_ctx *h, int key, int value)
         if (value < 1 || value > 1 << 20) return FSL_ERR_ARG;
         c.stage_seg = value;
         return FSL_OK;
+    case FSL_TUNE_CLOSURE_POLY:
+        if (value != 0 && value != 2 && value != 3 && value != 4) return FSL_ERR_ARG;
+        c.infer_poly = value;
+        return FSL_OK;
     default:
         return FSL_ERR_ARG;
     }

@@ -271,6 +271,33 @@ __device__ __forceinline__ uint32_t silu2_bf16(float h0, float h1)
     return y;
 }
 
+// silu of two values on the FMA pipe (the MUFU pipe runs the others): tanh
+// from an odd polynomial of degree 13 on [-3.3, 3.3], h clamped there,
+// coefficients this project fitted near-minimax on Chebyshev nodes with
+// Lawson's iteratively reweighted least squares (max |error| 1.4e-3,
+// including the clamp; the BF16 result rounds at 2^-9 relative), then
+// silu = h + h tanh(h) in FP32 and one rounding to BF16.
+__device__ __forceinline__ float tanh_poly(float h)
+{
+    const float x = fminf(fmaxf(h, -3.3f), 3.3f), x2 = x * x;
+    float p = 2.460764335e-06f;
+    p = fmaf(p, x2, -1.012231442e-04f);
+    p = fmaf(p, x2, 1.705276780e-03f);
+    p = fmaf(p, x2, -1.538222842e-02f);
+    p = fmaf(p, x2, 8.308345824e-02f);
+    p = fmaf(p, x2, -2.995448709e-01f);
+    p = fmaf(p, x2, 9.929457903e-01f);
+    return p * x;
+}
+
+__device__ __forceinline__ uint32_t silu2_poly(float h0, float h1)
+{
+    const float y0 = fmaf(h0, tanh_poly(h0), h0), y1 = fmaf(h1, tanh_poly(h1), h1);
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(y1), "f"(y0));
+    return r;
+}
+
 // one tensor-core layer: D = A W^T into TMEM, wait; returns false on timeout
 __device__ __forceinline__ bool layer_mma(uint32_t tmem, uint32_t a, uint32_t b, int K, int N, uint64_t *mbar,
                                           uint32_t &phase, int t)
@@ -291,7 +318,12 @@ __device__ __forceinline__ bool layer_mma(uint32_t tmem, uint32_t a, uint32_t b,
 }
 
 // SiLU of this thread's TMEM accumulator row (64 columns, h = (z + b) / 2)
-// into row t of the next activation tile (K = 80), 8 BF16 per 16-byte store
+// into row t of the next activation tile (K = 80), 8 BF16 per 16-byte store.
+// Of each chunk's 8 pairs, the first kPolyPairs take the FMA-pipe tanh and
+// the rest the MUFU one: the MUFU pipe sets the kernel's pace, and a MUFU
+// tanh of a warp's 64 values leaves ~13 issue slots free on its scheduler
+// (FSL_TUNE_CLOSURE_POLY picks the split).
+template <int kPolyPairs>
 __device__ __forceinline__ void epilogue_to_tile(uint32_t taddr, unsigned char *A, int t)
 {
     const uint32_t row = (uint32_t)(t >> 3) * (uint32_t)(kKH * 16) + (uint32_t)(t & 7) * 16u;
@@ -300,16 +332,14 @@ __device__ __forceinline__ void epilogue_to_tile(uint32_t taddr, unsigned char *
         float v[16];
         umma::tmem_ld16(taddr + (uint32_t)(c * 16), v);
         umma::tmem_wait_ld();
+        uint32_t y[8];
 #pragma unroll
-        for (int half = 0; half < 2; half++) {
-            const float *x = v + half * 8;
-            uint4 pk;
-            pk.x = silu2_bf16(x[0], x[1]);
-            pk.y = silu2_bf16(x[2], x[3]);
-            pk.z = silu2_bf16(x[4], x[5]);
-            pk.w = silu2_bf16(x[6], x[7]);
-            *reinterpret_cast<uint4 *>(A + row + (uint32_t)(c * 2 + half) * 128u) = pk;
-        }
+        for (int q = 0; q < 8; q++)
+            y[q] = q < kPolyPairs ? silu2_poly(v[2 * q], v[2 * q + 1]) : silu2_bf16(v[2 * q], v[2 * q + 1]);
+#pragma unroll
+        for (int half = 0; half < 2; half++)
+            *reinterpret_cast<uint4 *>(A + row + (uint32_t)(c * 2 + half) * 128u) =
+                make_uint4(y[4 * half], y[4 * half + 1], y[4 * half + 2], y[4 * half + 3]);
     }
 }
 
@@ -325,7 +355,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // src/turbulence.c:442) with Cs^2 from the MLP clipped to [0, 0.15].  The
 // hidden-layer SiLU runs in packed BF16 (its results are BF16 operands of the
 // next product either way); the last layer's dot product with w4 is FP32.
-template <typename MT>
+template <typename MT, int NP>
 __global__ void __launch_bounds__(128, 4) k_closure_infer(Grid g, ClosureScales sc, const double *__restrict__ U,
                                                           const float *__restrict__ vel,
                                                           const float *__restrict__ P, MT *__restrict__ mu,
@@ -371,13 +401,13 @@ __global__ void __launch_bounds__(128, 4) k_closure_infer(Grid g, ClosureScales 
         feat_load(g, U, vel, (tile + gridDim.x) * 128 + t, ncell, in);
         ok = layer_mma(tmem, aA0, aW1, 16, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile(lane_addr, A, t);
+        epilogue_to_tile<NP>(lane_addr, A, t);
         ok = layer_mma(tmem, aA, aW2, kKH, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile(lane_addr, A, t);
+        epilogue_to_tile<NP>(lane_addr, A, t);
         ok = layer_mma(tmem, aA, aW3, kKH, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile(lane_addr, A, t);
+        epilogue_to_tile<NP>(lane_addr, A, t);
         ok = layer_mma(tmem, aA, aW4, kKH, 16, &s.mbar, phase, t);
         if (!ok) break;
         float v[16];
@@ -713,25 +743,38 @@ __global__ void k_reduce_adam(const float *__restrict__ Gpart, int nblk, float *
 size_t closure_infer_smem() { return sizeof(mlp::SmemInfer); }
 size_t closure_train_smem() { return sizeof(mlp::SmemTrain); }
 
+template <int NP>
+static int infer_np(Ctx &c, const double *U, double *mu64, float *mu32, float *cs2_out, const float *P, int *err)
+{
+    const size_t smem = sizeof(mlp::SmemInfer);
+    static std::atomic<uint64_t> attr64{0}, attr32{0};
+    if (!smem_limit_once((const void *)mlp::k_closure_infer<double, NP>, smem, attr64) ||
+        !smem_limit_once((const void *)mlp::k_closure_infer<float, NP>, smem, attr32))
+        return -1;
+    const int blocks = c.sms * 4;
+    prof_begin(c, FSL_K_SGS);
+    if (mu32)
+        mlp::k_closure_infer<float, NP><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu32, cs2_out,
+                                                                         err);
+    else
+        mlp::k_closure_infer<double, NP><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu64, cs2_out,
+                                                                          err);
+    prof_end(c, FSL_K_SGS, 1);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, float *cs2_out, const float *P, int *err)
 {
     if ((long long)c.g.L * c.g.H * c.g.D >= (1LL << 31)) return -1; // feat_load's 32-bit indices
     prof_begin(c, FSL_K_SGS);
     mlp::k_closure_vel<<<148 * 8, 256, 0, c.stream>>>(c.g, U, c.cl_vel);
     prof_end(c, FSL_K_SGS, 1);
-    const size_t smem = sizeof(mlp::SmemInfer);
-    static std::atomic<uint64_t> attr64{0}, attr32{0};
-    if (!smem_limit_once((const void *)mlp::k_closure_infer<double>, smem, attr64) ||
-        !smem_limit_once((const void *)mlp::k_closure_infer<float>, smem, attr32))
-        return -1;
-    const int blocks = c.sms * 4;
-    prof_begin(c, FSL_K_SGS);
-    if (mu32)
-        mlp::k_closure_infer<float><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu32, cs2_out, err);
-    else
-        mlp::k_closure_infer<double><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu64, cs2_out, err);
-    prof_end(c, FSL_K_SGS, 1);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    switch (c.infer_poly) {
+    case 0: return infer_np<0>(c, U, mu64, mu32, cs2_out, P, err);
+    case 2: return infer_np<2>(c, U, mu64, mu32, cs2_out, P, err);
+    case 4: return infer_np<4>(c, U, mu64, mu32, cs2_out, P, err);
+    default: return infer_np<3>(c, U, mu64, mu32, cs2_out, P, err);
+    }
 }
 
 void launch_harvest(Ctx &c, const float *cd, long long stride, long long offset, float *X, float *Y, long long cap,

@@ -310,6 +310,8 @@ int fsl_step_stage(fsl_ctx *ctx);
                                  full-lane persistent 16 x 32 tile (the FP32 bulk's default with the
                                  reference reconstruction; elsewhere 0 runs 16) */
 #define FSL_TUNE_STAGE_SEG 2  /* x planes marched per stage block (default 48 FP32 bulk, 32 FP64) */
+#define FSL_TUNE_CLOSURE_POLY 3 /* learned-closure inference: of every 8 SiLU value pairs, how many take
+                                   the FMA-pipe polynomial tanh instead of the MUFU one: 0, 2, 3 or 4 */
 int fsl_tune(fsl_ctx *ctx, int key, int value);
 
 /* ---- debug / parity access ----------------------------------------------- */
