@@ -119,7 +119,7 @@ struct Ctx {
     float *cl_vel = nullptr;    // FP32 velocities of the padded cells (closure features), 3 fields
     double *judge_rows = nullptr; // [2][HIG][4] plane sums of the judgement (Cs^2, mu_SGS)
     bool cl_alloc = false, cl_weights = false;
-    int infer_poly = 3;         // closure inference: SiLU pairs of 8 on the FMA-pipe tanh (0, 2, 3, 4)
+    int infer_poly = 2;         // closure inference: SiLU pairs of 8 on the FMA-pipe tanh (0, 2, 3, 4)
     int judge_every = 100;
     double judge_thr = 0.05;
     bool using_dynamic = false;

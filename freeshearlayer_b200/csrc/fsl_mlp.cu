@@ -771,9 +771,9 @@ int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, flo
     prof_end(c, FSL_K_SGS, 1);
     switch (c.infer_poly) {
     case 0: return infer_np<0>(c, U, mu64, mu32, cs2_out, P, err);
-    case 2: return infer_np<2>(c, U, mu64, mu32, cs2_out, P, err);
+    case 3: return infer_np<3>(c, U, mu64, mu32, cs2_out, P, err);
     case 4: return infer_np<4>(c, U, mu64, mu32, cs2_out, P, err);
-    default: return infer_np<3>(c, U, mu64, mu32, cs2_out, P, err);
+    default: return infer_np<2>(c, U, mu64, mu32, cs2_out, P, err);
     }
 }
 
