@@ -913,6 +913,15 @@ int fsl_evolution(fsl_ctx *h, int stage)
     return FSL_OK;
 }
 
+// The FP32 bulk's full-lane stages on the temporal setup form the boundary
+// faces' outer states from the state itself and write the ghost cells of
+// their output: no boundary pass runs, and no ghost pass between stages.
+static bool wide_temporal(const Ctx &c)
+{
+    return c.p.precision == FSL_PREC_FP32 && c.p.recon == FSL_RECON_CHARMINMOD && c.stage_tje == 0 &&
+           c.p.setup == FSL_SETUP_TEMPORAL;
+}
+
 // The SGS viscosity of one step, on U^n with its ghost layer filled: the
 // dynamic procedure, the learned closure (judged by the dynamic procedure),
 // nothing for the static model (the stage kernels form it per face), or a
@@ -950,7 +959,7 @@ int step_prelude32(Ctx &c)
     c.step++;
     draw(c);
     launch_ghost(c, c.U);
-    launch_bface32(c, c.U, c.dist);
+    if (!wide_temporal(c)) launch_bface32(c, c.U, c.dist);
     return step_sgs(c);
 }
 } // namespace fsl
@@ -1036,20 +1045,27 @@ int fsl_step(fsl_ctx *h, int nsteps)
     if (c.cur != 0) return fail(c, FSL_ERR_ARG, "fsl_step: the current-stage buffer is not U^n");
     if (c.p.precision == FSL_PREC_FP32) {
         if ((rc = ensure_fp32(c))) return rc;
+        const bool wt = wide_temporal(c);
         for (int n = 0; n < nsteps; n++) {
             if (c.co_valid) launch_courant_apply(c);
             else launch_courant(c);
             c.step++;
             draw(c);
-            launch_ghost(c, c.U);
-            launch_bface32(c, c.U, c.dist);
+            // U^n's ghost layer: the previous step's last stage wrote it,
+            // unless that step ran before this call
+            if (!wt || n == 0) launch_ghost(c, c.U);
+            if (!wt) launch_bface32(c, c.U, c.dist);
             if ((rc = step_sgs(c))) return rc;
             if (launch_stage32(c, 1, c.U, c.U, c.Up)) return fail(c, FSL_ERR_CUDA, "FP32 stage kernel");
-            launch_ghost(c, c.Up);
-            launch_bface32(c, c.Up, c.dist);
+            if (!wt) {
+                launch_ghost(c, c.Up);
+                launch_bface32(c, c.Up, c.dist);
+            }
             launch_stage32(c, 2, c.Up, c.U, c.Uq);
-            launch_ghost(c, c.Uq);
-            launch_bface32(c, c.Uq, c.dist);
+            if (!wt) {
+                launch_ghost(c, c.Uq);
+                launch_bface32(c, c.Uq, c.dist);
+            }
             launch_stage32(c, 3, c.Uq, c.U, c.U, true);
             c.co_valid = true;
             CKL();

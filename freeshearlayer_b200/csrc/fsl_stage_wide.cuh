@@ -177,6 +177,12 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
     const long long nxf = (long long)H * D, nyf = (long long)L * D, nzf = (long long)L * H;
     const double dtx = a.ds->dtx, dty = a.ds->dty, dtz = a.ds->dtz;
     const double one_third = 1. / 3., two_thirds = 2. / 3.;
+    // temporal setup: the boundary faces' outer states are formed here from
+    // the state itself (the periodic x and z rules and the zero-gradient y
+    // rule of the boundary pass), and every boundary cell written also fills
+    // the ghost cells that copy it, so no ghost-fill or boundary pass runs
+    // between the stages
+    const bool tpl = kc.setup == FSL_SETUP_TEMPORAL;
     // this thread's halo cell (threads 0..195)
     int hr = 0, hc = 0;
     const bool hthread = t < NHALO;
@@ -277,7 +283,9 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     cell_consts(cc);
                     recon_x(cc, Un, Um, hin, lo);
                 }
-                if (i0 == 1) {
+                if (i0 == 1 && tpl) {
+                    recon_at<T, 0>(g, cu, g.idx(L, j, k), hm, tmp); // periodic x: cell LEN's face
+                } else if (i0 == 1) {
                     const long long fo = (long long)(j - 1) * D + (k - 1);
 #pragma unroll
                     for (int q = 0; q < 5; q++) hm[q] = a.bf.x0[q * nxf + fo];
@@ -345,20 +353,25 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
 #pragma unroll
                     for (int q = 0; q < 5; q++) s.Lz0[r][q] = lz[q];
                 }
-            } else if (j == H + 1 && k <= D) {
+            } else if (j == H + 1 && k <= D && !tpl) {
                 // the face below this ghost row: the top boundary's outer state
                 const long long fo = (long long)(i - 1) * D + (k - 1);
 #pragma unroll
                 for (int q = 0; q < 5; q++) s.Lo[r][l][q] = a.bf.yH[q * nyf + fo];
             } else if (k == D + 1 && j <= H) {
                 // beyond the last column: the far z boundary's outer state (shuffled to lane l-1)
-                const long long fo = (long long)(i - 1) * H + (j - 1);
+                if (tpl) {
+                    T tz[5];
+                    recon_at<T, 2>(g, cu, g.idx(i, j, 1), tz, lz); // periodic z: cell 1's face
+                } else {
+                    const long long fo = (long long)(i - 1) * H + (j - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) lz[q] = a.bf.zD[q * nzf + fo];
+                    for (int q = 0; q < 5; q++) lz[q] = a.bf.zD[q * nzf + fo];
+                }
             }
             if (r == WJ - 3) {
                 // halo row -1: its state on the face above (the tile's bottom faces)
-                if (k <= D) {
+                if (k <= D && (ybot || !tpl)) { // temporal bottom boundary: row 0's own state, below
                     T hb[5], tmp[5];
                     if (ybot) {
                         sweep_y(s, q0, -1, l, hb, tmp);
@@ -380,7 +393,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                         sweep_y(s, q0, WJ, l, tmp, lo);
 #pragma unroll
                         for (int q = 0; q < 5; q++) s.Lo[WJ][l][q] = lo[q];
-                    } else if (j0 + WJ == H + 1) {
+                    } else if (j0 + WJ == H + 1 && !tpl) {
                         const long long fo = (long long)(i - 1) * D + (k - 1);
 #pragma unroll
                         for (int q = 0; q < 5; q++) s.Lo[WJ][l][q] = a.bf.yH[q * nyf + fo];
@@ -394,6 +407,8 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     if (l < 16) {
                         if (zlft) {
                             sweep_z(s, q0, rr, -1, hv, lv);
+                        } else if (tpl) {
+                            recon_at<T, 2>(g, cu, g.idx(i, jr, D), hv, lv); // periodic z: cell DEP's face
                         } else {
                             const long long fo = (long long)(i - 1) * H + (jr - 1);
 #pragma unroll
@@ -404,6 +419,8 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     } else if (k0 + WK - 1 <= D) {
                         if (zrgt) {
                             sweep_z(s, q0, rr, WK, hv, lv);
+                        } else if (tpl) {
+                            recon_at<T, 2>(g, cu, g.idx(i, jr, 1), hv, lv); // periodic z: cell 1's face
                         } else {
                             const long long fo = (long long)(i - 1) * H + (jr - 1);
 #pragma unroll
@@ -431,14 +448,16 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     }
                     face_z<T, SST>(s, kc, q0, q0, sm1, s0, sp1, r, l, hz, lzn, Fz);
                     T F[5];
-                    face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, r, l, hy, s.Lo[r + 1][l], F);
+                    // temporal top boundary (zero-gradient y): both sides take the cell's own state
+                    face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, r, l, hy, (tpl && j == H) ? hy : s.Lo[r + 1][l], F);
 #pragma unroll
                     for (int q = 0; q < 5; q++) s.Fy[r + 1][l][q] = F[q];
                 }
             }
             if (r == WJ - 4 && k <= D && j0 <= H) {
                 T F[5];
-                face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, -1, l, s.HyB[l], s.Lo[0][l], F);
+                face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, -1, l, (tpl && !ybot) ? s.Lo[0][l] : s.HyB[l], s.Lo[0][l],
+                               F);
 #pragma unroll
                 for (int q = 0; q < 5; q++) s.Fy[0][l][q] = F[q];
             }
@@ -460,6 +479,9 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
 #pragma unroll
                     for (int q = 0; q < 5; q++) fw2[q] = T(pown[q]);
                     recon_x(cc, fw2, s.U[q0][r + 2][l + 2], hin, lo);
+                } else if (tpl) {
+                    T tx[5];
+                    recon_at<T, 0>(g, cu, g.idx(1, j, k), tx, lo); // periodic x: cell 1's face
                 } else {
                     const long long fo = (long long)(j - 1) * D + (k - 1);
 #pragma unroll
@@ -495,6 +517,22 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     else o = one_third * unv[q] + two_thirds * (base[q] + inc);
                     a.out[q * fs + c] = o;
                     base[q] = o;
+                }
+                if (tpl && (i == 1 || i == L || j == 1 || j == H || k == 1 || k == D)) {
+                    // the ghost cells that copy this cell (the ghost pass's
+                    // periodic x and z and zero-gradient y rules, edges and
+                    // corners included)
+                    const int xi[2] = {i, i == L ? 0 : (i == 1 ? L + 1 : -1)};
+                    const int yj[2] = {j, j == 1 ? 0 : (j == H ? H + 1 : -1)};
+                    const int zk[2] = {k, k == D ? 0 : (k == 1 ? D + 1 : -1)};
+#pragma unroll
+                    for (int e = 1; e < 8; e++) {
+                        const int gi = xi[e & 1], gj = yj[(e >> 1) & 1], gk = zk[e >> 2];
+                        if (gi < 0 || gj < 0 || gk < 0) continue;
+                        const long long gc = g.idx(gi, gj, gk);
+#pragma unroll
+                        for (int q = 0; q < 5; q++) a.out[q * fs + gc] = base[q];
+                    }
                 }
                 if (a.co && i >= a.co_i0 && i <= a.co_i1) {
                     const double Co = cell_courant(kc.cfl_mode, base[0], base[1], base[2], base[3], base[4], dtx, dty, dtz);
@@ -611,58 +649,12 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier &gb, unsigned nblock
     return ok_s != 0;
 }
 
-// The ghost layer of a temporal-setup state (periodic x and z, zero-gradient
-// y; the copies of the ghost-cell pass, src/boundCondInGhostCells.c:58-94
-// with the periodic x rule): ghost cell t of the x, y and z boundary lists.
-__device__ __forceinline__ void ghost_temporal(const Grid &g, double *__restrict__ u, long long t)
-{
-    const int L = g.L, H = g.H, D = g.D;
-    const long long nx = 2LL * (H + 2) * (D + 2), ny = 2LL * L * (D + 2);
-    int i, j, k;
-    if (t < nx) {
-        const long long q = (long long)(H + 2) * (D + 2);
-        i = (t / q) ? L + 1 : 0;
-        const long long rr = t % q;
-        j = (int)(rr / (D + 2));
-        k = (int)(rr % (D + 2));
-    } else if ((t -= nx) < ny) {
-        const long long q = (long long)L * (D + 2);
-        j = (t / q) ? H + 1 : 0;
-        const long long rr = t % q;
-        i = 1 + (int)(rr / (D + 2));
-        k = (int)(rr % (D + 2));
-    } else {
-        t -= ny;
-        const long long q = (long long)L * H;
-        k = (t / q) ? D + 1 : 0;
-        const long long rr = t % q;
-        i = 1 + (int)(rr / H);
-        j = 1 + (int)(rr % H);
-    }
-    const int jj = j == 0 ? 1 : j == H + 1 ? H : j;
-    const int kk = k == 0 ? D : k == D + 1 ? 1 : k;
-    const int si = i == 0 ? L : i == L + 1 ? 1 : i;
-    const long long src = g.idx(si, jj, kk), dst = g.idx(i, j, k), fs = g.fstride;
-#pragma unroll
-    for (int q = 0; q < 5; q++) u[q * fs + dst] = u[q * fs + src];
-}
-
-__device__ __forceinline__ long long ghost_count(const Grid &g)
-{
-    return 2LL * (g.H + 2) * (g.D + 2) + 2LL * g.L * (g.D + 2) + 2LL * g.L * g.H;
-}
-
-__device__ __forceinline__ long long bface_count(const Grid &g)
-{
-    return (long long)g.H * g.D + (long long)g.L * g.D + (long long)g.L * g.H;
-}
-
 // The work of one persistent launch: stages s_begin .. s_end of nmem domains
 // (m0 alone when mem is null).  With items, block x runs the (domain, block)
 // pairs items[start[x] .. start[x+1]); without, block x is block x of the
 // single domain.  Between two stages of one launch the blocks meet at a grid
-// barrier and fill the new state's ghost layer and boundary faces (temporal
-// setup), so a whole step of many domains is one launch.
+// barrier (the temporal setup's stages write their own ghost cells and form
+// their boundary states), so a whole step of many domains is one launch.
 struct WideWork {
     WideMember m0;
     const WideMember *mem;
@@ -705,41 +697,27 @@ __global__ void __launch_bounds__(NT, 1) k_wide(WideWork w)
         wide_block<float, SST>(s, w.m0.g, w.m0.kc, member_args(w.m0, w.s_begin, w.courant != 0), blockIdx.x,
                                w.m0.nb);
     } else {
-    for (int st = w.s_begin; st <= w.s_end; st++) {
-        const int i0 = w.start[blockIdx.x], i1 = w.start[blockIdx.x + 1];
-        for (int it = i0; it < i1; it++) {
-            const int2 x = w.items[it];
-            const int mi = x.x, b = x.y;
-            // the member's descriptor and stage arguments in shared memory:
-            // the block code reads them where it needs them instead of
-            // holding them in registers
-            __shared__ WideMember sm;
-            __shared__ Args<float> sa;
-            __syncthreads(); // the previous item's readers are done
-            if (threadIdx.x == 0) {
-                sm = w.mem[mi];
-                sa = member_args(sm, st, w.courant != 0);
+        for (int st = w.s_begin; st <= w.s_end; st++) {
+            const int i0 = w.start[blockIdx.x], i1 = w.start[blockIdx.x + 1];
+            for (int it = i0; it < i1; it++) {
+                const int2 x = w.items[it];
+                const int mi = x.x, b = x.y;
+                // the member's descriptor and stage arguments in shared memory:
+                // the block code reads them where it needs them instead of
+                // holding them in registers
+                __shared__ WideMember sm;
+                __shared__ Args<float> sa;
+                __syncthreads(); // the previous item's readers are done
+                if (threadIdx.x == 0) {
+                    sm = w.mem[mi];
+                    sa = member_args(sm, st, w.courant != 0);
+                }
+                __syncthreads();
+                wide_block<float, SST>(s, sm.g, sm.kc, sa, b, sm.nb);
             }
-            __syncthreads();
-            wide_block<float, SST>(s, sm.g, sm.kc, sa, b, sm.nb);
-        }
-        if (st == w.s_end) break;
-        // the new state's ghost layer, then its boundary faces, all domains
-        const long long nthr = (long long)gridDim.x * NT, t0 = (long long)blockIdx.x * NT + threadIdx.x;
-        if (!grid_sync(w.bar, gridDim.x)) return;
-        for (int m = 0; m < w.nmem; m++) {
-            const WideMember &M = w.mem[m];
-            const long long n = ghost_count(M.g);
-            for (long long t = t0; t < n; t += nthr) ghost_temporal(M.g, M.out[st - 1], t);
-        }
-        if (!grid_sync(w.bar, gridDim.x)) return;
-        for (int m = 0; m < w.nmem; m++) {
-            const WideMember &M = w.mem[m];
-            const long long n = bface_count(M.g);
-            for (long long t = t0; t < n; t += nthr)
-                stage::bface_one<float>(M.g, M.setup, M.BL_HIG, M.dist, M.out[st - 1], M.bf, t);
-        }
-        if (!grid_sync(w.bar, gridDim.x)) return;
+            if (st == w.s_end) break;
+            // the stage's outputs (ghost cells included) complete before the next reads them
+            if (!grid_sync(w.bar, gridDim.x)) return;
     }
     }
 }
