@@ -1046,6 +1046,10 @@ int fsl_step(fsl_ctx *h, int nsteps)
     if (c.p.precision == FSL_PREC_FP32) {
         if ((rc = ensure_fp32(c))) return rc;
         const bool wt = wide_temporal(c);
+        // the learned closure's feature velocities: the last stage of a step
+        // writes those of U^{n+1}, so only the first step of a call (whose
+        // U^n the caller may have written) runs the velocity pass
+        float *vel = (wt && c.p.sgs == FSL_SGS_LEARNED && c.cl_alloc) ? c.cl_vel : nullptr;
         for (int n = 0; n < nsteps; n++) {
             if (c.co_valid) launch_courant_apply(c);
             else launch_courant(c);
@@ -1055,7 +1059,10 @@ int fsl_step(fsl_ctx *h, int nsteps)
             // unless that step ran before this call
             if (!wt || n == 0) launch_ghost(c, c.U);
             if (!wt) launch_bface32(c, c.U, c.dist);
-            if ((rc = step_sgs(c))) return rc;
+            c.vel_fresh = vel && n > 0;
+            rc = step_sgs(c);
+            c.vel_fresh = false;
+            if (rc) return rc;
             if (launch_stage32(c, 1, c.U, c.U, c.Up)) return fail(c, FSL_ERR_CUDA, "FP32 stage kernel");
             if (!wt) {
                 launch_ghost(c, c.Up);
@@ -1066,7 +1073,7 @@ int fsl_step(fsl_ctx *h, int nsteps)
                 launch_ghost(c, c.Uq);
                 launch_bface32(c, c.Uq, c.dist);
             }
-            launch_stage32(c, 3, c.Uq, c.U, c.U, true);
+            launch_stage32(c, 3, c.Uq, c.U, c.U, true, vel);
             c.co_valid = true;
             CKL();
         }

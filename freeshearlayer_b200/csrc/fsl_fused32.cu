@@ -27,7 +27,7 @@ void launch_bface32(Ctx &c, const double *cur, const Disturb &d)
 }
 
 template <bool SST>
-static int stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant)
+static int stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant, float *vel)
 {
     if (c.p.recon == FSL_RECON_PPM) {
         // PPM: halo 2, a ring of four planes; 16 rows measured fastest at
@@ -39,18 +39,18 @@ static int stage32(Ctx &c, int stage, const double *cur, const double *un, doubl
         }
     }
     switch (c.stage_tje) {
-    case 0: return wide::launch_wide<SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
+    case 0: return wide::launch_wide<SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant, vel);
     case 8: return stage::launch_stage_t<float, 8, 2, false, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
     case 12: return stage::launch_stage_t<float, 12, 1, false, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
     default: return stage::launch_stage_t<float, 16, 1, false, SST>(c, stage, cur, un, out, c.mu32, bf32(c), courant);
     }
 }
 
-int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant)
+int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant, float *vel)
 {
     // the static Smagorinsky model forms the face viscosity in the kernel
-    if (c.p.sgs == FSL_SGS_STATIC) return stage32<true>(c, stage, cur, un, out, courant);
-    return stage32<false>(c, stage, cur, un, out, courant);
+    if (c.p.sgs == FSL_SGS_STATIC) return stage32<true>(c, stage, cur, un, out, courant, vel);
+    return stage32<false>(c, stage, cur, un, out, courant, vel);
 }
 
 // ---- persistent multi-domain stages ------------------------------------------

@@ -117,6 +117,7 @@ struct Ctx {
     float *mu32_alt = nullptr;  // closure mu on judgement steps (FP32 path)
     int *cl_err = nullptr;      // device error flag of the tensor-core kernels
     float *cl_vel = nullptr;    // FP32 velocities of the padded cells (closure features), 3 fields
+    bool vel_fresh = false;     // cl_vel holds U's velocities (the last stage wrote them): no velocity pass
     double *judge_rows = nullptr; // [2][HIG][4] plane sums of the judgement (Cs^2, mu_SGS)
     bool cl_alloc = false, cl_weights = false;
     int infer_poly = 2;         // closure inference: SiLU pairs of 8 on the FMA-pipe tanh (0, 2, 3, 4)
@@ -238,7 +239,10 @@ void launch_bface(Ctx &c, const double *cur, const Disturb &d);
 int launch_stage(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant = false);
 // FP32-bulk variants (fsl_fused32.cu): boundary states in bf32, SGS viscosity in mu32.
 void launch_bface32(Ctx &c, const double *cur, const Disturb &d);
-int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant = false);
+// vel (full-lane tile, temporal setup, stage 3 only): also write the FP32
+// velocities of `out` into that field (the closure's feature velocities)
+int launch_stage32(Ctx &c, int stage, const double *cur, const double *un, double *out, bool courant = false,
+                   float *vel = nullptr);
 // The three stages of an FP32-bulk step of several domains in one persistent
 // cooperative launch (fsl_fused32.cu); opaque plan built per member set.
 struct WidePlan;

@@ -766,9 +766,11 @@ static int infer_np(Ctx &c, const double *U, double *mu64, float *mu32, float *c
 int launch_closure_infer(Ctx &c, const double *U, double *mu64, float *mu32, float *cs2_out, const float *P, int *err)
 {
     if ((long long)c.g.L * c.g.H * c.g.D >= (1LL << 31)) return -1; // feat_load's 32-bit indices
-    prof_begin(c, FSL_K_SGS);
-    mlp::k_closure_vel<<<148 * 8, 256, 0, c.stream>>>(c.g, U, c.cl_vel);
-    prof_end(c, FSL_K_SGS, 1);
+    if (!(c.vel_fresh && U == c.U)) {
+        prof_begin(c, FSL_K_SGS);
+        mlp::k_closure_vel<<<148 * 8, 256, 0, c.stream>>>(c.g, U, c.cl_vel);
+        prof_end(c, FSL_K_SGS, 1);
+    }
     switch (c.infer_poly) {
     case 0: return infer_np<0>(c, U, mu64, mu32, cs2_out, P, err);
     case 3: return infer_np<3>(c, U, mu64, mu32, cs2_out, P, err);

@@ -179,6 +179,9 @@ template <typename T> struct Args {
     unsigned int *status;   // bit 1 set on a non-positive output density (with co)
     int stage;
     int seg;
+    // non-null (full-lane tile, temporal setup): also write the FP32 velocities
+    // of `out`, ghost cells included, as the closure's velocity pass forms them
+    float *vel;
 };
 
 // Own column of plane `pl` (and, on the tile edge, the halo neighbour the y
@@ -619,6 +622,7 @@ int launch_stage_t(Ctx &c, int stage, const double *cur, const double *un, doubl
     a.co_i1 = c.co_i1;
     a.status = &c.ds->status;
     a.seg = c.stage_seg;
+    a.vel = nullptr;
     const size_t smem = sizeof(Smem<T, TJE, PPM>);
     static std::atomic<uint64_t> attr{0};
     if (!smem_limit_once((const void *)k_stage<T, TJE, MINB, PPM, SST>, smem, attr)) return -1;

@@ -214,14 +214,19 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
         pos += i1 - i0 + 1;
         const int k0 = (int)(tile % ntk) * WK + 1, j0 = (int)(tile / ntk) * WJ + 1;
         const int j = j0 + r, k = k0 + l;
+        // temporal setup (periodic z): the ring's columns beyond the ghost
+        // columns, k = -1 and k = DEP+2, hold cells DEP-1 and 2, so the z
+        // boundary faces' outer states are sweeps over the ring like any
+        // other face's
+        const int kmin = tpl ? -1 : 0, kmax = tpl ? D + 2 : D + 1;
         const bool own = j <= H && k <= D;               // interior cell of this thread
-        const bool live = j <= H + 1 && k <= D + 1;      // cell in the padded array
-        const long long cj = g.idx(0, j, k);
+        const bool live = j <= H + 1 && k <= kmax;       // cell in the padded array (or its periodic image)
+        const long long cj = g.idx(0, j, k == D + 2 ? 2 : k);
         // halo cell of this thread (padded indices)
         const int hj = j0 + hr, hk = k0 + hc;
-        const bool hlive = hthread && hj >= 0 && hj <= H + 1 && hk >= 0 && hk <= D + 1;
+        const bool hlive = hthread && hj >= 0 && hj <= H + 1 && hk >= kmin && hk <= kmax;
         const bool hvlive = hvel && hlive;
-        const long long hcj = g.idx(0, hj, hk);
+        const long long hcj = g.idx(0, hj, hk == -1 ? D - 1 : hk == D + 2 ? 2 : hk);
         const bool ybot = j0 > 1, ytop = j0 + WJ <= H, zlft = k0 > 1, zrgt = k0 + WK <= D;
 
         T hix[5], Fxp[5];
@@ -362,7 +367,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 // beyond the last column: the far z boundary's outer state (shuffled to lane l-1)
                 if (tpl) {
                     T tz[5];
-                    recon_at<T, 2>(g, cu, g.idx(i, j, 1), tz, lz); // periodic z: cell 1's face
+                    sweep_z(s, q0, r, l, tz, lz); // periodic z: this ghost column holds cell 1
                 } else {
                     const long long fo = (long long)(i - 1) * H + (j - 1);
 #pragma unroll
@@ -405,10 +410,8 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 if (jr <= H) {
                     T hv[5], lv[5];
                     if (l < 16) {
-                        if (zlft) {
+                        if (zlft || tpl) { // periodic z: ghost column -1 holds cell DEP
                             sweep_z(s, q0, rr, -1, hv, lv);
-                        } else if (tpl) {
-                            recon_at<T, 2>(g, cu, g.idx(i, jr, D), hv, lv); // periodic z: cell DEP's face
                         } else {
                             const long long fo = (long long)(i - 1) * H + (jr - 1);
 #pragma unroll
@@ -417,10 +420,8 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
 #pragma unroll
                         for (int q = 0; q < 5; q++) s.HzL[rr][q] = hv[q];
                     } else if (k0 + WK - 1 <= D) {
-                        if (zrgt) {
+                        if (zrgt || tpl) { // periodic z: ghost column 32 holds cell 1
                             sweep_z(s, q0, rr, WK, hv, lv);
-                        } else if (tpl) {
-                            recon_at<T, 2>(g, cu, g.idx(i, jr, 1), hv, lv); // periodic z: cell 1's face
                         } else {
                             const long long fo = (long long)(i - 1) * H + (jr - 1);
 #pragma unroll
@@ -518,7 +519,30 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     a.out[q * fs + c] = o;
                     base[q] = o;
                 }
-                if (tpl && (i == 1 || i == L || j == 1 || j == H || k == 1 || k == D)) {
+                // the FP32 velocities of the closure's features (rho u as
+                // float times the float of the FP64 reciprocal)
+                float vu = 0.f, vv = 0.f, vw = 0.f;
+                if (a.vel) {
+                    const float rr = (float)(1. / base[0]);
+                    vu = (float)base[1] * rr;
+                    vv = (float)base[2] * rr;
+                    vw = (float)base[3] * rr;
+                    a.vel[c] = vu;
+                    a.vel[fs + c] = vv;
+                    a.vel[2 * fs + c] = vw;
+                }
+                const bool bx = i == 1 || i == L, by = j == 1 || j == H, bz = k == 1 || k == D;
+                if (tpl && bz && !(bx || by)) {
+                    // the one ghost cell that copies a z-edge cell (periodic z)
+                    const long long gc = c + ((k == D ? 0 : D + 1) - k);
+#pragma unroll
+                    for (int q = 0; q < 5; q++) a.out[q * fs + gc] = base[q];
+                    if (a.vel) {
+                        a.vel[gc] = vu;
+                        a.vel[fs + gc] = vv;
+                        a.vel[2 * fs + gc] = vw;
+                    }
+                } else if (tpl && (bx || by || bz)) {
                     // the ghost cells that copy this cell (the ghost pass's
                     // periodic x and z and zero-gradient y rules, edges and
                     // corners included)
@@ -532,6 +556,11 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                         const long long gc = g.idx(gi, gj, gk);
 #pragma unroll
                         for (int q = 0; q < 5; q++) a.out[q * fs + gc] = base[q];
+                        if (a.vel) {
+                            a.vel[gc] = vu;
+                            a.vel[fs + gc] = vv;
+                            a.vel[2 * fs + gc] = vw;
+                        }
                     }
                 }
                 if (a.co && i >= a.co_i0 && i <= a.co_i1) {
@@ -607,6 +636,7 @@ struct WideMember {
     int nb;
     int setup, BL_HIG;
     Disturb dist;
+    float *vel; // stage 3 also writes the FP32 velocities of its output (null: no)
 };
 
 // A grid-wide barrier with a bounded wait: false (and *err set) when the
@@ -681,6 +711,7 @@ __device__ __forceinline__ Args<float> member_args(const WideMember &M, int st, 
     a.status = M.status;
     a.stage = st;
     a.seg = 0;
+    a.vel = st == 3 ? M.vel : nullptr;
     return a;
 }
 
@@ -754,6 +785,7 @@ inline WideMember wide_member(const Ctx &c, const float *mu, BF<float> bf, int s
     m.setup = c.k.setup;
     m.BL_HIG = c.k.BL_HIG;
     m.dist = c.dist;
+    m.vel = nullptr;
     return m;
 }
 
@@ -767,12 +799,13 @@ template <bool SST, bool MULTI> inline bool wide_attr()
 // reconstruction).  The buffers are the context's fixed stage sequence.
 template <bool SST>
 int launch_wide(Ctx &c, int stage, const double *cur, const double *un, double *out, const float *mu,
-                BF<float> bf, bool courant)
+                BF<float> bf, bool courant, float *vel)
 {
     (void)cur; (void)un; (void)out; // always U -> Up -> Uq -> U with U^n = U
     if (!wide_attr<SST, false>()) return -1;
     WideWork w{};
     w.m0 = wide_member(c, mu, bf, c.sms);
+    w.m0.vel = vel;
     w.mem = nullptr;
     w.nmem = 1;
     w.items = nullptr;

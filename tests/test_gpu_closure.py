@@ -246,3 +246,26 @@ def test_shipped_weights_on_an_active_state(fsl, oracle_lib):
           "cs2_profile_err %.3f" % (st.dyn_ratio, st.active_rows, st.mu_active_err, st.mu_profile_err,
                                     st.visc_err, st.profile_err))
     assert st.active_rows > 0 and np.isfinite(st.mu_active_err)
+
+
+@pytest.mark.parametrize("judge_every", [0, 3])
+def test_stage_written_feature_velocities(fsl, oracle_lib, judge_every):
+    """On the FP32 bulk's full-lane temporal path the last stage of a step
+    writes the FP32 velocities of the new state (ghost cells included) for the
+    next step's closure features, and only the first step of an fsl_step call
+    runs the velocity pass. Seven steps in one call equal seven calls of one
+    step (velocity pass before each) bit for bit, with and without
+    judgements."""
+    p, s, dU = _active_state(fsl, oracle_lib)
+    out = []
+    for calls in ((7,), (1,) * 7):
+        d = fsl.Domain(dict(p, sgs=1, precision=1))
+        d.upload_state(s)
+        d.closure_set_scales(1.0 / dU, 1.0)
+        d.closure_set_weights(fsl.closure_weights())
+        d.closure_judge(judge_every, 1e9)
+        for n in calls:
+            d.step(n)
+        out.append(d.download_state())
+        d.close()
+    assert np.array_equal(out[0], out[1])

@@ -388,3 +388,26 @@ def test_fp32_full_lane_tile_matches_ring_tile(fsl, oracle_lib, setup, grid, sgs
     mscale = max(np.linalg.norm(b[:, :, v]) for v in (1, 2, 3))
     for v in (2, 3):
         assert np.linalg.norm(a[:, :, v] - b[:, :, v]) / mscale < 1e-6, (v, diff)
+
+
+@pytest.mark.parametrize("grid", [(24, 12, 16), (33, 17, 33)])
+@pytest.mark.parametrize("sgs", [0, 2])
+def test_full_lane_ghost_images_match_ghost_pass(fsl, oracle_lib, grid, sgs):
+    """On the temporal setup the full-lane kernel writes its output's ghost
+    cells itself, and fsl_step runs the ghost pass only before the first step
+    of a call. Six steps in one call (ghost cells from the kernel) must equal
+    six calls of one step (ghost cells from the ghost pass before each) bit for
+    bit: the kernel's ghost images are exactly the ghost pass's."""
+    L, H, D = grid
+    p = temporal_params(L=L, H=H, D=D, sgs=sgs, Re=5000.0)
+    s, _ = oracle_lib.Oracle.temporal_state(p, 0.4, amp=0.02)
+    out = []
+    for calls in ((6,), (1,) * 6):
+        d = fsl.Domain(dict(p, precision=1))
+        d.tune(d.TUNE_STAGE_ROWS, 0)
+        d.upload_state(s)
+        for n in calls:
+            d.step(n)
+        out.append(d.download_state())
+        d.close()
+    _assert_same(out[0], out[1], "one call of 6 steps vs 6 calls of one step, full-lane tile")
