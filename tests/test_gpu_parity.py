@@ -411,3 +411,28 @@ def test_full_lane_ghost_images_match_ghost_pass(fsl, oracle_lib, grid, sgs):
         out.append(d.download_state())
         d.close()
     _assert_same(out[0], out[1], "one call of 6 steps vs 6 calls of one step, full-lane tile")
+
+
+@pytest.mark.parametrize("prec,rows", [(0, None), (1, 16), (1, 0)])
+@pytest.mark.parametrize("setup,cfl,Mc", [(0, 0, None), (0, 1, None), (1, 1, 0.4), (1, 1, 0.9)])
+def test_fused_courant_maximum_is_the_reduction(fsl, oracle_lib, prec, rows, setup, cfl, Mc):
+    """The last stage of a fused step accumulates the Courant maximum of the
+    state it writes: it equals the standalone reduction over the same state
+    bit for bit, in both setups, both Courant definitions, both precisions
+    and both FP32 tiles."""
+    if setup == 0:
+        p = spatial_params(L=20, H=10, D=12, cfl_mode=cfl)
+        from oracle.oracle import spatial_initial_state
+        s = spatial_initial_state(p)
+    else:
+        p = temporal_params(L=40, H=20, D=40, Mc=Mc, Re=5000.0)
+        s, _ = oracle_lib.Oracle.temporal_state(p, Mc, amp=0.02)
+    d = fsl.Domain(dict(p, precision=prec))
+    if rows is not None:
+        d.tune(d.TUNE_STAGE_ROWS, rows)
+    d.upload_state(s)
+    d.step(3)
+    fused = d.get_courant_max()
+    md, _ = d.check_courant()
+    assert fused == md, (fused, md)
+    d.close()
