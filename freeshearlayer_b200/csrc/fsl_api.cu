@@ -1171,7 +1171,7 @@ int fsl_tune(fsl_ctx *h, int key, int value)
         c.stage_seg = value;
         return FSL_OK;
     case FSL_TUNE_CLOSURE_POLY:
-        if (value != 0 && value != 2 && value != 3 && value != 4) return FSL_ERR_ARG;
+        if (value < 0 || value > 6 || value == 1) return FSL_ERR_ARG;
         c.infer_poly = value;
         return FSL_OK;
     default:

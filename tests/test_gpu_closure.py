@@ -86,7 +86,7 @@ def test_features_and_forward_match_oracle(fsl):
     d.closure_set_weights(params)
     ref = mo.cs2(params, X)
     # every split of the SiLU tanh between the MUFU and the FMA-pipe polynomial
-    for poly in (0, 2, 3, 4):
+    for poly in (0, 2, 3, 4, 5, 6):
         d.tune(d.TUNE_CLOSURE_POLY, poly)
         _, cs2_mlp, cs2_dyn = d.closure_compare(fields=True)
         got = cs2_mlp[3:-3, 3:-3, 3:-3].ravel()
