@@ -125,6 +125,9 @@ PERSISTENT = [
     dict(L=16, H=24, D=12, Mc=0.7, Re=1000.0, precision=1, sgs=1, seed=13),
     dict(L=40, H=20, D=40, Mc=0.4, Re=500.0, precision=1, sgs=0, seed=14),
     dict(L=48, H=33, D=65, Mc=0.6, Re=800.0, precision=1, sgs=1, seed=15),
+    # longer members: more blocks than tiles, heads and tails
+    dict(L=128, H=20, D=40, Mc=0.5, Re=600.0, precision=1, sgs=0, seed=16),
+    dict(L=256, H=16, D=32, Mc=0.4, Re=500.0, precision=1, sgs=1, seed=17),
 ]
 
 

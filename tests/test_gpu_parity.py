@@ -436,3 +436,31 @@ def test_fused_courant_maximum_is_the_reduction(fsl, oracle_lib, prec, rows, set
     md, _ = d.check_courant()
     assert fused == md, (fused, md)
     d.close()
+
+
+@pytest.mark.parametrize("grid", [(128, 20, 40), (256, 33, 65)])
+def test_full_lane_long_domains(fsl, oracle_lib, grid):
+    """Domains whose full-lane launch splits every tile's planes between a
+    head block and the tail blocks (more blocks than tiles), with partial
+    tiles: the steps match the ring tile to FP32 rounding and the FP64 oracle
+    within the FP32 bar, and repeat bit for bit."""
+    L, H, D = grid
+    p = temporal_params(L=L, H=H, D=D, Re=5000.0)
+    s, _ = oracle_lib.Oracle.temporal_state(p, 0.4, amp=0.02)
+    o = oracle_lib.Oracle(p)
+    o.set_state(s)
+    o.step(3)
+    ref = o.state()
+    out = []
+    for rows in (0, 0, 16):
+        d = fsl.Domain(dict(p, precision=1))
+        d.tune(d.TUNE_STAGE_ROWS, rows)
+        d.upload_state(s)
+        d.step(3)
+        out.append(d.download_state())
+        d.close()
+        errs = per_var_rel_l2(out[-1], ref, p)
+        assert errs[0] < FP32_RTOL and errs[4] < FP32_RTOL, (rows, errs)
+    assert np.array_equal(out[0], out[1])
+    diff = per_var_rel_l2(out[0], out[2], p)
+    assert max(diff[0], diff[1], diff[4]) < 1e-6, diff
