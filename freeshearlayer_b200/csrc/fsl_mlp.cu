@@ -189,18 +189,23 @@ __device__ __forceinline__ void stage_weights(SmemW &s, const float *__restrict_
 // BF16 high and low part, and weights and biases of the hidden layers are
 // pre-scaled by 1/2, so the accumulator holds h = (z + b) / 2 and
 // silu(z + b) = h + h tanh(h) needs no further FP32 work.  The output layer
-// (w4, b4) is a fourth product with N = 16 (row 0 live).
+// is a fourth product with N = 16 (row 0 live, K = 64) plus b4 in FP32.
+// The feature tile (128 x 16) occupies the first 4 KB of the activation
+// tile, which the first layer's epilogue overwrites only after the first
+// product has read it: 45 KB per block, five blocks per SM.
 constexpr int kKH = 80; // K of the hidden-layer operands
 
 struct SmemInfer {
     alignas(128) __nv_bfloat16 W1[64 * 16];
     alignas(128) __nv_bfloat16 W2[64 * kKH];
     alignas(128) __nv_bfloat16 W3[64 * kKH];
-    alignas(128) __nv_bfloat16 W4[16 * kKH];
-    alignas(128) __nv_bfloat16 A0[128 * 16];  // features (K-major tile; columns 8, 9 one, 10..15 zero)
-    alignas(128) __nv_bfloat16 A[128 * kKH];  // activations (K-major; columns 64, 65 one, 66..79 zero)
+    alignas(128) __nv_bfloat16 W4[16 * 64];
+    // activations (K-major; columns 64, 65 one, 66..79 zero); before the
+    // first product, the features (K = 16; columns 8, 9 one, 10..15 zero)
+    alignas(128) __nv_bfloat16 A[128 * kKH];
     uint64_t mbar;
     uint32_t tholder;
+    float b4;
 };
 
 __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
@@ -234,10 +239,11 @@ __device__ __forceinline__ void stage_infer_weights(SmemInfer &s, const float *_
         tile_el(s.W2, o, i, kKH) = v2;
         tile_el(s.W3, o, i, kKH) = v3;
     }
-    for (int e = t; e < 16 * kKH; e += nt) {
-        const int o = e / kKH, i = e % kKH;
-        tile_el(s.W4, o, i, kKH) = (o == 0 && i < 64) ? __float2bfloat16_rn(P[kOffW4 + i]) : z;
+    for (int e = t; e < 16 * 64; e += nt) {
+        const int o = e / 64, i = e % 64;
+        tile_el(s.W4, o, i, 64) = o == 0 ? __float2bfloat16_rn(P[kOffW4 + i]) : z;
     }
+    if (t == 0) s.b4 = P[kOffB4];
     __syncthreads(); // the bias columns below overwrite zeros written above
     if (t < 64) {
         __nv_bfloat16 hi, lo;
@@ -250,11 +256,6 @@ __device__ __forceinline__ void stage_infer_weights(SmemInfer &s, const float *_
         split_bf16(0.5f * P[kOffB3 + t], hi, lo);
         tile_el(s.W3, t, 64, kKH) = hi;
         tile_el(s.W3, t, 65, kKH) = lo;
-    } else if (t == 64) {
-        __nv_bfloat16 hi, lo;
-        split_bf16(P[kOffB4], hi, lo);
-        tile_el(s.W4, 0, 64, kKH) = hi;
-        tile_el(s.W4, 0, 65, kKH) = lo;
     }
 }
 
@@ -318,15 +319,15 @@ __device__ __forceinline__ uint32_t silu2_poly(float h0, float h1)
 }
 
 // one tensor-core layer: D = A W^T into TMEM, wait; returns false on timeout
-__device__ __forceinline__ bool layer_mma(uint32_t tmem, uint32_t a, uint32_t b, int K, int N, uint64_t *mbar,
-                                          uint32_t &phase, int t)
+__device__ __forceinline__ bool layer_mma(uint32_t tmem, uint32_t a, int Ka, uint32_t b, int Kb, int K, int N,
+                                          uint64_t *mbar, uint32_t &phase, int t)
 {
     umma::fence_async_smem();
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
     if (t == 0) {
-        umma::gemm_issue(tmem, a, b, K, N, false);
+        umma::gemm_issue2(tmem, a, Ka, b, Kb, K, N);
         umma::commit(mbar);
     }
     bool ok = umma::mbar_wait(mbar, phase, kWaitLimit);
@@ -342,10 +343,15 @@ __device__ __forceinline__ bool layer_mma(uint32_t tmem, uint32_t a, uint32_t b,
 // the rest the MUFU one: the MUFU pipe sets the kernel's pace, and a MUFU
 // tanh of a warp's 64 values leaves ~13 issue slots free on its scheduler
 // (FSL_TUNE_CLOSURE_POLY picks the split).
-template <int kPolyPairs>
+template <int kPolyPairs, bool kOnes>
 __device__ __forceinline__ void epilogue_to_tile(uint32_t taddr, unsigned char *A, int t)
 {
     const uint32_t row = (uint32_t)(t >> 3) * (uint32_t)(kKH * 16) + (uint32_t)(t & 7) * 16u;
+    if constexpr (kOnes) {
+        // columns 64..79 = (1, 1, 0, ...): the feature tile overlaid them
+        *reinterpret_cast<uint4 *>(A + row + 8u * 128u) = make_uint4(0x3F803F80u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4 *>(A + row + 9u * 128u) = make_uint4(0u, 0u, 0u, 0u);
+    }
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         float v[16];
@@ -375,7 +381,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // hidden-layer SiLU runs in packed BF16 (its results are BF16 operands of the
 // next product either way); the last layer's dot product with w4 is FP32.
 template <typename MT, int NP>
-__global__ void __launch_bounds__(128, 4) k_closure_infer(Grid g, ClosureScales sc, const double *__restrict__ U,
+__global__ void __launch_bounds__(128, NP <= 3 ? 5 : 4) k_closure_infer(Grid g, ClosureScales sc, const double *__restrict__ U,
                                                           const float *__restrict__ vel,
                                                           const float *__restrict__ P, MT *__restrict__ mu,
                                                           float *__restrict__ cs2_out, int *err)
@@ -384,16 +390,11 @@ __global__ void __launch_bounds__(128, 4) k_closure_infer(Grid g, ClosureScales 
     SmemInfer &s = *reinterpret_cast<SmemInfer *>(smraw);
     const int t = threadIdx.x, wp = t >> 5;
     stage_infer_weights(s, P, t, 128);
-    unsigned char *A0 = reinterpret_cast<unsigned char *>(s.A0);
     unsigned char *A = reinterpret_cast<unsigned char *>(s.A);
     const uint32_t one2 = 0x3F803F80u; // two BF16 ones
-    // feature row t: columns 0..7 at +0; columns 8..15 = (1, 1, 0, ...) at +128
+    // feature row t (the 128 x 16 tile at the start of A): columns 0..7 at
+    // +0, columns 8..15 = (1, 1, 0, ...) at +128
     const uint32_t frow = (uint32_t)(t >> 3) * 256u + (uint32_t)(t & 7) * 16u;
-    *reinterpret_cast<uint4 *>(A0 + frow + 128u) = make_uint4(one2, 0u, 0u, 0u);
-    // activation row t: columns 64..79 = (1, 1, 0, ...) in core-matrix groups 8, 9
-    const uint32_t arow = (uint32_t)(t >> 3) * (uint32_t)(kKH * 16) + (uint32_t)(t & 7) * 16u;
-    *reinterpret_cast<uint4 *>(A + arow + 8u * 128u) = make_uint4(one2, 0u, 0u, 0u);
-    *reinterpret_cast<uint4 *>(A + arow + 9u * 128u) = make_uint4(0u, 0u, 0u, 0u);
     if (t == 0) umma::mbar_init(&s.mbar, 1);
     if (wp == 0) umma::tmem_alloc(&s.tholder, 64);
     umma::fence_before_sync();
@@ -401,8 +402,9 @@ __global__ void __launch_bounds__(128, 4) k_closure_infer(Grid g, ClosureScales 
     umma::fence_after_sync();
     const uint32_t tmem = s.tholder;
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * wp) << 16);
-    const uint32_t aA0 = umma::smem_u32(s.A0), aA = umma::smem_u32(s.A), aW1 = umma::smem_u32(s.W1),
-                   aW2 = umma::smem_u32(s.W2), aW3 = umma::smem_u32(s.W3), aW4 = umma::smem_u32(s.W4);
+    const uint32_t aA = umma::smem_u32(s.A), aW1 = umma::smem_u32(s.W1), aW2 = umma::smem_u32(s.W2),
+                   aW3 = umma::smem_u32(s.W3), aW4 = umma::smem_u32(s.W4);
+    const float b4 = s.b4;
     uint32_t phase = 0;
     bool ok = true;
     const long long ncell = (long long)g.L * g.H * g.D;
@@ -414,25 +416,26 @@ __global__ void __launch_bounds__(128, 4) k_closure_infer(Grid g, ClosureScales 
         const long long c = in.c;
         float f[8] = {0, 0, 0, 0, 0, 0, 0, 0}, rho = 0.f, Smag = 0.f;
         if (valid) cell_features_v(in, sc, f, rho, Smag);
-        *reinterpret_cast<uint4 *>(A0 + frow) =
+        *reinterpret_cast<uint4 *>(A + frow) =
             make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
+        *reinterpret_cast<uint4 *>(A + frow + 128u) = make_uint4(one2, 0u, 0u, 0u);
         // the next tile's inputs load while this tile is on the tensor cores
         feat_load(g, U, vel, (tile + gridDim.x) * 128 + t, ncell, in);
-        ok = layer_mma(tmem, aA0, aW1, 16, 64, &s.mbar, phase, t);
+        ok = layer_mma(tmem, aA, 16, aW1, 16, 16, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile<NP>(lane_addr, A, t);
-        ok = layer_mma(tmem, aA, aW2, kKH, 64, &s.mbar, phase, t);
+        epilogue_to_tile<NP, true>(lane_addr, A, t);
+        ok = layer_mma(tmem, aA, kKH, aW2, kKH, kKH, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile<NP>(lane_addr, A, t);
-        ok = layer_mma(tmem, aA, aW3, kKH, 64, &s.mbar, phase, t);
+        epilogue_to_tile<NP, false>(lane_addr, A, t);
+        ok = layer_mma(tmem, aA, kKH, aW3, kKH, kKH, 64, &s.mbar, phase, t);
         if (!ok) break;
-        epilogue_to_tile<NP>(lane_addr, A, t);
-        ok = layer_mma(tmem, aA, aW4, kKH, 16, &s.mbar, phase, t);
+        epilogue_to_tile<NP, false>(lane_addr, A, t);
+        ok = layer_mma(tmem, aA, kKH, aW4, 64, 64, 16, &s.mbar, phase, t);
         if (!ok) break;
         float v[16];
         umma::tmem_ld16(lane_addr, v);
         umma::tmem_wait_ld();
-        const float cs2 = fminf(fmaxf(v[0], 0.f), 0.15f);
+        const float cs2 = fminf(fmaxf(v[0] + b4, 0.f), 0.15f);
         if (valid) {
             mu[c] = (MT)(rho * cs2 * sc.DD * Smag);
             if (cs2_out) cs2_out[c] = cs2;
@@ -770,7 +773,21 @@ static int infer_np(Ctx &c, const double *U, double *mu64, float *mu32, float *c
     if (!smem_limit_once((const void *)mlp::k_closure_infer<double, NP>, smem, attr64) ||
         !smem_limit_once((const void *)mlp::k_closure_infer<float, NP>, smem, attr32))
         return -1;
-    const int blocks = c.sms * 4;
+    // five blocks per SM (45 KB of shared memory and at most 96 registers a
+    // thread each, with all of the SM's unified memory as shared memory);
+    // four for the wider polynomial splits, whose registers allow four
+    static std::atomic<bool> carve{false};
+    if (!carve.load()) {
+        if (cudaFuncSetAttribute((const void *)mlp::k_closure_infer<float, NP>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute((const void *)mlp::k_closure_infer<double, NP>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared) !=
+                cudaSuccess)
+            return -1;
+        carve.store(true);
+    }
+    const int blocks = c.sms * (NP <= 3 ? 5 : 4);
     prof_begin(c, FSL_K_SGS);
     if (mu32)
         mlp::k_closure_infer<float, NP><<<blocks, 128, smem, c.stream>>>(c.g, c.cls, U, c.cl_vel, P, mu32, cs2_out,

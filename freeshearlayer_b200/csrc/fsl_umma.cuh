@@ -72,6 +72,19 @@ __device__ __forceinline__ void gemm_issue(uint32_t tmem_d, uint32_t a_addr, uin
     }
 }
 
+// The same with operands of different stored widths: A stored with width Ka,
+// B with width Kb, the product over the first K columns of both.
+__device__ __forceinline__ void gemm_issue2(uint32_t tmem_d, uint32_t a_addr, int Ka, uint32_t b_addr, int Kb, int K,
+                                            int N)
+{
+    const uint32_t id = idesc_bf16_f32(N);
+    for (int s = 0; s < K / 16; s++) {
+        const uint64_t da = smem_desc(a_addr + s * 256u, 128u, (uint32_t)Ka * 16u);
+        const uint64_t db = smem_desc(b_addr + s * 256u, 128u, (uint32_t)Kb * 16u);
+        mma_bf16(tmem_d, da, db, id, s > 0 ? 1u : 0u);
+    }
+}
+
 __device__ __forceinline__ void commit(uint64_t *mbar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
