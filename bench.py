@@ -264,17 +264,23 @@ def time_steps(torch, d, run, steps, barrier, clocks=None):
 
 
 def profiled_traffic(prec):
-    """DRAM bytes per cell of one stage-2 launch of the fused stage kernel,
-    from the committed ncu summary of the 256x128x128 capture (the line
-    'derived: ... per cell X B'), or None."""
+    """DRAM bytes per cell of one stage-2 launch of the fused stage kernel
+    (FP64: the ring tile; FP32 bulk: the full-lane tile), from the committed
+    ncu summary: the full-size 512x256x256 capture when it has one (the line
+    'full size: ... per cell X B'), else the 256x128x128 capture ('derived:
+    ... per cell X B'). Returns (bytes per cell, which capture) or (None, None)."""
     import re
-    name = "k_stage_fp64_256x128x128.txt" if prec == 0 else "k_stage_fp32_256x128x128.txt"
+    name = "k_stage_fp64_256x128x128.txt" if prec == 0 else "k_wide_fp32_256x128x128.txt"
     try:
         with open(os.path.join(ROOT, "profiles", name)) as f:
-            m = re.search(r"per cell ([0-9.]+) B", f.read())
-        return float(m.group(1)) if m else None
+            txt = f.read()
     except OSError:
-        return None
+        return None, None
+    m = re.search(r"full size: .*per cell ([0-9.]+) B", txt)
+    if m:
+        return float(m.group(1)), "512x256x256"
+    m = re.search(r"derived: .*per cell ([0-9.]+) B", txt)
+    return (float(m.group(1)), "256x128x128") if m else (None, None)
 
 
 def stage_roofline(kt, names, ncell, prec, peaks, traffic):
@@ -286,14 +292,17 @@ def stage_roofline(kt, names, ncell, prec, peaks, traffic):
     achieved = alg / (avg_ms / 1e3) / 1e9
     note = None
     if traffic is None:
-        per_cell = profiled_traffic(prec)
+        per_cell, where = profiled_traffic(prec)
         if per_cell is not None:
             traffic = per_cell * ncell
-            note = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-2 launch at 256x128x128 "
+            note = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-2 launch at %s "
                     "(%.2f B/cell; that stage's algorithmic bytes are %d B/cell), scaled by cells"
-                    % (per_cell, 128 if prec == 0 else 124))
-    return {"bound": "hbm", "kernel": "k_stage<%s> (fused reconstruction + Riemann + viscous flux + "
-                                       "divergence + RK stage)" % ("double" if prec == 0 else "float"),
+                    % (where, per_cell, 128 if prec == 0 else 124))
+    kernel = ("k_stage<double> (ring tile: fused reconstruction + Riemann + viscous flux + divergence + RK stage)"
+              if prec == 0 else
+              "k_wide (FP32 full-lane persistent tile: fused reconstruction + Riemann + viscous flux + divergence "
+              "+ RK stage)")
+    return {"bound": "hbm", "kernel": kernel,
             "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic, "traffic_note": note,
             "peak_source": peaks["source"] + " HBM copy bandwidth (burst)",

@@ -311,9 +311,9 @@ int fsl_step_stage(fsl_ctx *ctx);
                                  reference reconstruction; elsewhere 0 runs 16) */
 #define FSL_TUNE_STAGE_SEG 2  /* x planes marched per stage block (default 48 FP32 bulk, 32 FP64) */
 #define FSL_TUNE_CLOSURE_POLY 3 /* learned-closure inference: of every 8 SiLU value pairs, how many take
-                                   the FMA-pipe polynomial tanh instead of the MUFU one: 0, 2, 3 or 4
-                                   (default 2: 2.37 ms against 2.48 for 0 and 2.51 for 3 per step at
-                                   512x256x256, velocity pre-pass included) */
+                                   the FMA-pipe polynomial tanh instead of the MUFU one: 0 or 2..6
+                                   (default 2: 1.97 ms against 2.20 for 0 and 1.99 for 3 per step at
+                                   512x256x256) */
 int fsl_tune(fsl_ctx *ctx, int key, int value);
 
 /* ---- debug / parity access ----------------------------------------------- */

@@ -30,9 +30,10 @@ def test_stage_roofline_and_compute_roof(prec):
     assert roof["achieved"] == pytest.approx(want, rel=1e-4)
     assert roof["frac"] == pytest.approx(want / 6650.0, abs=1e-4)
     assert roof["bound"] == "hbm" and roof["unit"] == "GB/s" and roof["launches"] == 10
-    per_cell = bench.profiled_traffic(prec)
+    per_cell, where = bench.profiled_traffic(prec)
     if per_cell is not None:
         assert roof["traffic"] == pytest.approx(per_cell * ncell)
+        assert where in roof["traffic_note"]
         assert 100.0 < per_cell < 200.0               # near the algorithmic bytes, not re-read
     assert kl["stage"] == 10 and kms["sgs"] == 25.0
     cr = bench.compute_roof(roof, prec, {"sm_mhz": 1965.0})
