@@ -192,11 +192,24 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
 
     const int ntk = (D + WK - 1) / WK, ntj = (H + WJ - 1) / WJ;
     const long long ntiles = (long long)ntk * ntj, total = ntiles * L;
-    // heads: planes 1..Hd of every tile; tails: planes Hd+1..L of every tile
-    const long long Hd = min((long long)L, total / nb);
+    // heads: planes 1..Hd of every tile; tails: planes Hd+1..L of every tile.
+    // With more blocks than tiles, block b < ntiles takes the head of tile b
+    // and the other blocks share the tails; a tail plane counts 1.06 head
+    // planes (the tail blocks start several segments, each with a prologue
+    // and out of step with their neighbours: measured 3 to 10 % slower per
+    // plane at 512x256x256), so the heads are a little longer.
+    long long Hd, pos, end;
+    if (nb > ntiles) {
+        Hd = min((long long)L, (106LL * ntiles * L) / (100LL * (nb - ntiles) + 106LL * ntiles));
+        const long long tails = ntiles * (L - Hd), nt = nb - ntiles;
+        pos = b < ntiles ? b * Hd : ntiles * Hd + tails * (b - ntiles) / nt;
+        end = b < ntiles ? (b + 1) * Hd : ntiles * Hd + tails * (b - ntiles + 1) / nt;
+    } else {
+        Hd = min((long long)L, total / nb);
+        pos = total * b / nb;
+        end = total * (b + 1) / nb;
+    }
     const long long Lt = L - Hd, nhead = ntiles * Hd;
-    long long pos = total * b / nb;
-    const long long end = total * (b + 1) / nb;
     while (pos < end) {
         long long tile, run;
         int i0;
