@@ -418,31 +418,31 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     }
                 }
             } else if (r == WJ - 1) {
-                // halo columns -1 (lanes 0..15) and 32 (lanes 16..31)
+                // halo columns -1 (lanes 0..15) and 32 (lanes 16..31): one
+                // sweep for the whole warp, each half on its own column
                 const int rr = l & 15, jr = j0 + rr;
-                if (jr <= H) {
+                const bool left = l < 16;
+                const bool act = jr <= H && (left || k0 + WK - 1 <= D);
+                // periodic z: ghost column -1 holds cell DEP, ghost column 32 cell 1
+                const bool ring = left ? (zlft || tpl) : (zrgt || tpl);
+                // the left half keeps the state on the face beyond its column,
+                // the right half the state on the face before its column
+                T o[5];
+                if (act && ring) {
                     T hv[5], lv[5];
-                    if (l < 16) {
-                        if (zlft || tpl) { // periodic z: ghost column -1 holds cell DEP
-                            sweep_z(s, q0, rr, -1, hv, lv);
-                        } else {
-                            const long long fo = (long long)(i - 1) * H + (jr - 1);
+                    sweep_z(s, q0, rr, left ? -1 : WK, hv, lv);
 #pragma unroll
-                            for (int q = 0; q < 5; q++) hv[q] = a.bf.z0[q * nzf + fo];
-                        }
+                    for (int q = 0; q < 5; q++) o[q] = left ? hv[q] : lv[q];
+                } else if (act) {
+                    const long long fo = (long long)(i - 1) * H + (jr - 1);
+                    const T *bfz = left ? a.bf.z0 : a.bf.zD;
 #pragma unroll
-                        for (int q = 0; q < 5; q++) s.HzL[rr][q] = hv[q];
-                    } else if (k0 + WK - 1 <= D) {
-                        if (zrgt || tpl) { // periodic z: ghost column 32 holds cell 1
-                            sweep_z(s, q0, rr, WK, hv, lv);
-                        } else {
-                            const long long fo = (long long)(i - 1) * H + (jr - 1);
+                    for (int q = 0; q < 5; q++) o[q] = bfz[q * nzf + fo];
+                }
+                if (act) {
+                    T *dst = left ? s.HzL[rr] : s.LzR[rr];
 #pragma unroll
-                            for (int q = 0; q < 5; q++) lv[q] = a.bf.zD[q * nzf + fo];
-                        }
-#pragma unroll
-                        for (int q = 0; q < 5; q++) s.LzR[rr][q] = lv[q];
-                    }
+                    for (int q = 0; q < 5; q++) dst[q] = o[q];
                 }
             }
             __syncthreads();
