@@ -11,7 +11,9 @@
 //   - loads of the state halo (two rows and two columns on each side) and the
 //     velocities of the one-cell ring: threads 0..195, one cell each;
 //   - the y sweeps of the two halo rows and the z sweeps of the two halo
-//     columns (warps 13, 14, 15), before the first barrier of a plane;
+//     columns (warps 13, 14, 15; one warp-wide pass for both columns), one
+//     plane ahead, between the two barriers of the plane before, so that the
+//     sweep phase before a plane's first barrier has the own sweeps only;
 //   - the fluxes of the tile's bottom y faces and left z faces (warps 12
 //     and 11), between the two barriers.
 // The tile's own faces (the y face above each cell, the z face beyond it,
@@ -50,11 +52,13 @@ template <typename T> struct Smem {
     T U[2][WJ + 4][WK + 4][5];  // state of planes i, i+1: rows -2..17, cols -2..33
     T R[3][WJ + 2][WK + 2][3];  // velocities by reciprocal, planes i-1, i, i+1: rows -1..16, cols -1..32
     T Dv[2][WJ + 2][WK + 2][5]; // velocities by division, T, face-averaged mu: planes i, i+1
-    T Lo[WJ + 1][WK][5];        // y sweep, state on the face below: rows 0..16
+    T Lo[WJ][WK][5];            // y sweep, state on the face below: rows 0..15
     T Fy[WJ + 1][WK][5];        // y flux of the face below row r (r = 0..16: faces j0-1/2 .. j0+15+1/2)
-    T HyB[WK][5];               // y sweep of halo row -1, state on the face above it
-    T HzL[WJ][5];               // z sweep of halo column -1, state on the face beyond it
-    T LzR[WJ][5];               // z sweep of halo column 32, state on the face before it
+    // the halo sweeps, by plane parity (computed one plane ahead):
+    T HyB[2][WK][5];            // y sweep of halo row -1, state on the face above it
+    T LoH[2][WK][5];            // y sweep of halo row 16, state on the face below it
+    T HzL[2][WJ][5];            // z sweep of halo column -1, state on the face beyond it
+    T LzR[2][WJ][5];            // z sweep of halo column 32, state on the face before it
     T Lz0[WJ][5];               // z sweep of column 0, state on the face before it
     T FzL[WJ][5];               // z flux of the face before column 0
     double comax[WJ][WK];       // Courant maxima of the cells written
@@ -161,6 +165,78 @@ __device__ __forceinline__ void face_z(const Smem<T> &s, const Consts &kc, int q
     fused_face<T, 3, SST>(Lm, Rp, vm, vm[3], vp, vp[3], s.R[sp1][a][b + 1], s.R[sp1][a][b], s.R[sm1][a][b + 1],
                           s.R[sm1][a][b], s.R[s0][a + 1][b + 1], s.R[s0][a + 1][b], s.R[s0][a - 1][b + 1],
                           s.R[s0][a - 1][b], m_f, kc, F);
+}
+
+// The halo sweeps of plane p (warps 13, 14, 15; ring slot p & 1) into the
+// buffers of p's parity: run for a segment's first plane in its prologue and
+// for plane i+1 while plane i's faces are formed, so the sweep phase before a
+// plane's first barrier has the own sweeps only.  nyf, nzf: the y and z
+// boundary-face array strides of the non-temporal setups.
+template <typename T>
+__device__ __forceinline__ void halo_sweeps(Smem<T> &s, const Args<T> &a, int p, int r, int l, int j0, int k0, int H,
+                                            int D, long long nyf, long long nzf, bool tpl, bool ybot, bool ytop,
+                                            bool zlft, bool zrgt)
+{
+    const int k = k0 + l;
+    const int qp = p & 1;
+    if (r == WJ - 3) {
+        // halo row -1: its state on the face above (the tile's bottom faces)
+        if (k <= D && (ybot || !tpl)) { // temporal bottom boundary: row 0's own state, below
+            T hb[5], tmp[5];
+            if (ybot) {
+                sweep_y(s, qp, -1, l, hb, tmp);
+            } else {
+                const long long fo = (long long)(p - 1) * D + (k - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) hb[q] = a.bf.y0[q * nyf + fo];
+            }
+#pragma unroll
+            for (int q = 0; q < 5; q++) s.HyB[qp][l][q] = hb[q];
+        }
+    } else if (r == WJ - 2) {
+        // halo row 16: its state on the face below (the tile's top
+        // faces), or the top boundary's outer state when row 16 is
+        // the ghost row
+        if (k <= D) {
+            if (ytop) {
+                T lo[5], tmp[5];
+                sweep_y(s, qp, WJ, l, tmp, lo);
+#pragma unroll
+                for (int q = 0; q < 5; q++) s.LoH[qp][l][q] = lo[q];
+            } else if (j0 + WJ == H + 1 && !tpl) {
+                const long long fo = (long long)(p - 1) * D + (k - 1);
+#pragma unroll
+                for (int q = 0; q < 5; q++) s.LoH[qp][l][q] = a.bf.yH[q * nyf + fo];
+            }
+        }
+    } else if (r == WJ - 1) {
+        // halo columns -1 (lanes 0..15) and 32 (lanes 16..31): one
+        // sweep for the whole warp, each half on its own column
+        const int rr = l & 15, jr = j0 + rr;
+        const bool left = l < 16;
+        const bool act = jr <= H && (left || k0 + WK - 1 <= D);
+        // periodic z: ghost column -1 holds cell DEP, ghost column 32 cell 1
+        const bool ring = left ? (zlft || tpl) : (zrgt || tpl);
+        // the left half keeps the state on the face beyond its column,
+        // the right half the state on the face before its column
+        T o[5];
+        if (act && ring) {
+            T hv[5], lv[5];
+            sweep_z(s, qp, rr, left ? -1 : WK, hv, lv);
+#pragma unroll
+            for (int q = 0; q < 5; q++) o[q] = left ? hv[q] : lv[q];
+        } else if (act) {
+            const long long fo = (long long)(p - 1) * H + (jr - 1);
+            const T *bfz = left ? a.bf.z0 : a.bf.zD;
+#pragma unroll
+            for (int q = 0; q < 5; q++) o[q] = bfz[q * nzf + fo];
+        }
+        if (act) {
+            T *dst = left ? s.HzL[qp][rr] : s.LzR[qp][rr];
+#pragma unroll
+            for (int q = 0; q < 5; q++) dst[q] = o[q];
+        }
+    }
 }
 
 // Block b of a domain's stage launch of nb blocks: its share of the
@@ -291,6 +367,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 cell_prims<T, SST>(s, i0 + 1, hr, hc, hmu1, hmu0);
             }
             __syncthreads();
+            if (r >= WJ - 3) halo_sweeps(s, a, i0, r, l, j0, k0, H, D, nyf, nzf, tpl, ybot, ytop, zlft, zrgt);
             if (own) {
                 T hm[5], lo[5], hin[5], dm[4], tmp[5];
                 const T *Uc = s.U[i0 & 1][r + 2][l + 2], *Un = s.U[(i0 + 1) & 1][r + 2][l + 2];
@@ -387,67 +464,10 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     for (int q = 0; q < 5; q++) lz[q] = a.bf.zD[q * nzf + fo];
                 }
             }
-            if (r == WJ - 3) {
-                // halo row -1: its state on the face above (the tile's bottom faces)
-                if (k <= D && (ybot || !tpl)) { // temporal bottom boundary: row 0's own state, below
-                    T hb[5], tmp[5];
-                    if (ybot) {
-                        sweep_y(s, q0, -1, l, hb, tmp);
-                    } else {
-                        const long long fo = (long long)(i - 1) * D + (k - 1);
-#pragma unroll
-                        for (int q = 0; q < 5; q++) hb[q] = a.bf.y0[q * nyf + fo];
-                    }
-#pragma unroll
-                    for (int q = 0; q < 5; q++) s.HyB[l][q] = hb[q];
-                }
-            } else if (r == WJ - 2) {
-                // halo row 16: its state on the face below (the tile's top
-                // faces), or the top boundary's outer state when row 16 is
-                // the ghost row
-                if (k <= D) {
-                    if (ytop) {
-                        T lo[5], tmp[5];
-                        sweep_y(s, q0, WJ, l, tmp, lo);
-#pragma unroll
-                        for (int q = 0; q < 5; q++) s.Lo[WJ][l][q] = lo[q];
-                    } else if (j0 + WJ == H + 1 && !tpl) {
-                        const long long fo = (long long)(i - 1) * D + (k - 1);
-#pragma unroll
-                        for (int q = 0; q < 5; q++) s.Lo[WJ][l][q] = a.bf.yH[q * nyf + fo];
-                    }
-                }
-            } else if (r == WJ - 1) {
-                // halo columns -1 (lanes 0..15) and 32 (lanes 16..31): one
-                // sweep for the whole warp, each half on its own column
-                const int rr = l & 15, jr = j0 + rr;
-                const bool left = l < 16;
-                const bool act = jr <= H && (left || k0 + WK - 1 <= D);
-                // periodic z: ghost column -1 holds cell DEP, ghost column 32 cell 1
-                const bool ring = left ? (zlft || tpl) : (zrgt || tpl);
-                // the left half keeps the state on the face beyond its column,
-                // the right half the state on the face before its column
-                T o[5];
-                if (act && ring) {
-                    T hv[5], lv[5];
-                    sweep_z(s, q0, rr, left ? -1 : WK, hv, lv);
-#pragma unroll
-                    for (int q = 0; q < 5; q++) o[q] = left ? hv[q] : lv[q];
-                } else if (act) {
-                    const long long fo = (long long)(i - 1) * H + (jr - 1);
-                    const T *bfz = left ? a.bf.z0 : a.bf.zD;
-#pragma unroll
-                    for (int q = 0; q < 5; q++) o[q] = bfz[q * nzf + fo];
-                }
-                if (act) {
-                    T *dst = left ? s.HzL[rr] : s.LzR[rr];
-#pragma unroll
-                    for (int q = 0; q < 5; q++) dst[q] = o[q];
-                }
-            }
             __syncthreads();
             // (c) the own faces: y above, z beyond, x ahead; the tile's bottom
-            // y faces (warp 12) and left z faces (warp 11)
+            // y faces (warp 12), left z faces (warp 11), and the next plane's
+            // halo sweeps (warps 13, 14, 15)
             T Fz[5], Fx[5], hin[5];
 #pragma unroll
             for (int q = 0; q < 5; q++) Fz[q] = Fx[q] = hin[q] = T(0.);
@@ -458,26 +478,33 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 if (own) {
                     if (l == WK - 1) {
 #pragma unroll
-                        for (int q = 0; q < 5; q++) lzn[q] = s.LzR[r][q];
+                        for (int q = 0; q < 5; q++) lzn[q] = s.LzR[q0][r][q];
                     }
                     face_z<T, SST>(s, kc, q0, q0, sm1, s0, sp1, r, l, hz, lzn, Fz);
                     T F[5];
-                    // temporal top boundary (zero-gradient y): both sides take the cell's own state
-                    face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, r, l, hy, (tpl && j == H) ? hy : s.Lo[r + 1][l], F);
+                    // the state above the face: row r+1's (the halo row's for
+                    // row 15); at the temporal top boundary the cell's own
+                    T up[5];
+                    {
+                        const T *src = r + 1 < WJ ? s.Lo[r + 1][l] : s.LoH[q0][l];
+#pragma unroll
+                        for (int q = 0; q < 5; q++) up[q] = (tpl && j == H) ? hy[q] : src[q];
+                    }
+                    face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, r, l, hy, up, F);
 #pragma unroll
                     for (int q = 0; q < 5; q++) s.Fy[r + 1][l][q] = F[q];
                 }
             }
             if (r == WJ - 4 && k <= D && j0 <= H) {
                 T F[5];
-                face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, -1, l, (tpl && !ybot) ? s.Lo[0][l] : s.HyB[l], s.Lo[0][l],
+                face_y<T, SST>(s, kc, q0, q0, sm1, s0, sp1, -1, l, (tpl && !ybot) ? s.Lo[0][l] : s.HyB[q0][l], s.Lo[0][l],
                                F);
 #pragma unroll
                 for (int q = 0; q < 5; q++) s.Fy[0][l][q] = F[q];
             }
             if (r == WJ - 5 && l < WJ && j0 + l <= H && k0 <= D) {
                 T F[5];
-                face_z<T, SST>(s, kc, q0, q0, sm1, s0, sp1, l, -1, s.HzL[l], s.Lz0[l], F);
+                face_z<T, SST>(s, kc, q0, q0, sm1, s0, sp1, l, -1, s.HzL[q0][l], s.Lz0[l], F);
 #pragma unroll
                 for (int q = 0; q < 5; q++) s.FzL[l][q] = F[q];
             }
@@ -507,6 +534,9 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                                       s.R[sp1][r][l + 1], s.R[s0][r][l + 1], s.R[sp1][r + 1][l + 2],
                                       s.R[s0][r + 1][l + 2], s.R[sp1][r + 1][l], s.R[s0][r + 1][l], m_f, kc, Fx);
             }
+            // the next plane's halo sweeps (its state is in the ring)
+            if (r >= WJ - 3 && i < i1)
+                halo_sweeps(s, a, i + 1, r, l, j0, k0, H, D, nyf, nzf, tpl, ybot, ytop, zlft, zrgt);
             T Fzm[5];
 #pragma unroll
             for (int q = 0; q < 5; q++) Fzm[q] = __shfl_up_sync(0xffffffffu, Fz[q], 1);
