@@ -12,8 +12,8 @@
 //     velocities of the one-cell ring: threads 0..195, one cell each;
 //   - the y sweeps of the two halo rows and the z sweeps of the two halo
 //     columns (warps 13, 14, 15; one warp-wide pass for both columns), one
-//     plane ahead, between the two barriers of the plane before, so that the
-//     sweep phase before a plane's first barrier has the own sweeps only;
+//     plane ahead, after the stage combination of the plane before, so that
+//     the sweep phase before a plane's first barrier has the own sweeps only;
 //   - the fluxes of the tile's bottom y faces and left z faces (warps 12
 //     and 11), between the two barriers.
 // The tile's own faces (the y face above each cell, the z face beyond it,
@@ -169,7 +169,7 @@ __device__ __forceinline__ void face_z(const Smem<T> &s, const Consts &kc, int q
 
 // The halo sweeps of plane p (warps 13, 14, 15; ring slot p & 1) into the
 // buffers of p's parity: run for a segment's first plane in its prologue and
-// for plane i+1 while plane i's faces are formed, so the sweep phase before a
+// for plane i+1 after plane i's stage combination, so the sweep phase before a
 // plane's first barrier has the own sweeps only.  nyf, nzf: the y and z
 // boundary-face array strides of the non-temporal setups.
 template <typename T>
@@ -466,8 +466,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
             }
             __syncthreads();
             // (c) the own faces: y above, z beyond, x ahead; the tile's bottom
-            // y faces (warp 12), left z faces (warp 11), and the next plane's
-            // halo sweeps (warps 13, 14, 15)
+            // y faces (warp 12) and left z faces (warp 11)
             T Fz[5], Fx[5], hin[5];
 #pragma unroll
             for (int q = 0; q < 5; q++) Fz[q] = Fx[q] = hin[q] = T(0.);
@@ -534,9 +533,6 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                                       s.R[sp1][r][l + 1], s.R[s0][r][l + 1], s.R[sp1][r + 1][l + 2],
                                       s.R[s0][r + 1][l + 2], s.R[sp1][r + 1][l], s.R[s0][r + 1][l], m_f, kc, Fx);
             }
-            // the next plane's halo sweeps (its state is in the ring)
-            if (r >= WJ - 3 && i < i1)
-                halo_sweeps(s, a, i + 1, r, l, j0, k0, H, D, nyf, nzf, tpl, ybot, ytop, zlft, zrgt);
             T Fzm[5];
 #pragma unroll
             for (int q = 0; q < 5; q++) Fzm[q] = __shfl_up_sync(0xffffffffu, Fz[q], 1);
@@ -613,6 +609,9 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     if (!(base[0] > 0.0)) atomicOr(a.status, 2u);
                 }
             }
+            // the next plane's halo sweeps (its state is in the ring)
+            if (r >= WJ - 3 && i < i1)
+                halo_sweeps(s, a, i + 1, r, l, j0, k0, H, D, nyf, nzf, tpl, ybot, ytop, zlft, zrgt);
             // (e) plane i+2 into the state ring slot of plane i and its
             // velocities into the slots of planes i-1 (reciprocal) and i
             // (division); advance the march
