@@ -349,8 +349,11 @@ def test_static_smagorinsky_ppm_and_fp32(fsl, oracle_lib):
     assert errs[0] < FP32_RTOL and errs[4] < FP32_RTOL, errs
 
 
+# (24, 33, 65) and (28, 20, 65): blocks whose segments are 1 to 3 planes long
+# (the halo sweeps run one plane ahead, so the shortest segments matter)
 @pytest.mark.parametrize("setup,grid", [(1, (24, 12, 16)), (1, (40, 20, 40)), (1, (33, 17, 33)),
-                                        (1, (20, 16, 32)), (0, (20, 10, 12)), (0, (18, 33, 35))])
+                                        (1, (20, 16, 32)), (0, (20, 10, 12)), (0, (18, 33, 35)),
+                                        (1, (24, 33, 65)), (0, (28, 20, 65))])
 @pytest.mark.parametrize("sgs", [0, 2])
 def test_fp32_full_lane_tile_matches_ring_tile(fsl, oracle_lib, setup, grid, sgs):
     """The FP32 bulk's full-lane persistent stage kernel (rows 0, the default)
@@ -390,7 +393,7 @@ def test_fp32_full_lane_tile_matches_ring_tile(fsl, oracle_lib, setup, grid, sgs
         assert np.linalg.norm(a[:, :, v] - b[:, :, v]) / mscale < 1e-6, (v, diff)
 
 
-@pytest.mark.parametrize("grid", [(24, 12, 16), (33, 17, 33)])
+@pytest.mark.parametrize("grid", [(24, 12, 16), (33, 17, 33), (24, 33, 65)])
 @pytest.mark.parametrize("sgs", [0, 2])
 def test_full_lane_ghost_images_match_ghost_pass(fsl, oracle_lib, grid, sgs):
     """On the temporal setup the full-lane kernel writes its output's ghost
