@@ -549,21 +549,26 @@ template <typename T> FSL_HD void vdiv(const T *U, T *o)
 
 // Courant number of one cell from its conserved variables: the reference's
 // streamwise u dt/dx (src/helpers.c:31-43) or the acoustic sum
-// dt((|u|+c)/dx + (|v|+c)/dy + (|w|+c)/dz).  Every operation is an explicitly
-// rounded FP64 intrinsic, so the value does not depend on the contraction
-// flags of the translation unit: the standalone reduction and the fused
-// stage kernels (FP64 and FP32 bulk) produce the same bits.
+// dt((|u|+c)/dx + (|v|+c)/dy + (|w|+c)/dz) (a project extension, formed with
+// the reciprocal ir = 1/rho: one division instead of four).  Every operation
+// is an explicitly rounded FP64 intrinsic, so the value does not depend on
+// the contraction flags of the translation unit: the standalone reduction and
+// the fused stage kernels (FP64 and FP32 bulk) produce the same bits.
+__device__ __forceinline__ double cell_courant_ir(int mode, double R, double ir, double mu, double mv, double mw,
+                                                  double E, double dtx, double dty, double dtz)
+{
+    if (mode != 1) return __dmul_rn(__ddiv_rn(mu, R), dtx);
+    const double Uv = __dmul_rn(mu, ir), V = __dmul_rn(mv, ir), W = __dmul_rn(mw, ir);
+    const double q = __dadd_rn(__dadd_rn(__dmul_rn(Uv, Uv), __dmul_rn(V, V)), __dmul_rn(W, W));
+    const double P = __dmul_rn(__dsub_rn(E, __dmul_rn(__dmul_rn(0.5, R), q)), 0.4);
+    const double Cs = __dsqrt_rn(__dmul_rn(__dmul_rn(1.4, P), ir));
+    return __dadd_rn(__dadd_rn(__dmul_rn(__dadd_rn(fabs(Uv), Cs), dtx), __dmul_rn(__dadd_rn(fabs(V), Cs), dty)),
+                     __dmul_rn(__dadd_rn(fabs(W), Cs), dtz));
+}
 __device__ __forceinline__ double cell_courant(int mode, double R, double mu, double mv, double mw, double E,
                                                double dtx, double dty, double dtz)
 {
-    const double Uv = __ddiv_rn(mu, R);
-    if (mode != 1) return __dmul_rn(Uv, dtx);
-    const double V = __ddiv_rn(mv, R), W = __ddiv_rn(mw, R);
-    const double q = __dadd_rn(__dadd_rn(__dmul_rn(Uv, Uv), __dmul_rn(V, V)), __dmul_rn(W, W));
-    const double P = __dmul_rn(__dsub_rn(E, __dmul_rn(__dmul_rn(0.5, R), q)), 0.4);
-    const double Cs = __dsqrt_rn(__ddiv_rn(__dmul_rn(1.4, P), R));
-    return __dadd_rn(__dadd_rn(__dmul_rn(__dadd_rn(fabs(Uv), Cs), dtx), __dmul_rn(__dadd_rn(fabs(V), Cs), dty)),
-                     __dmul_rn(__dadd_rn(fabs(W), Cs), dtz));
+    return cell_courant_ir(mode, R, mode == 1 ? __ddiv_rn(1.0, R) : 0.0, mu, mv, mw, E, dtx, dty, dtz);
 }
 
 } // namespace fsl

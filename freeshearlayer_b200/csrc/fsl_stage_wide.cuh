@@ -562,8 +562,11 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 // the FP32 velocities of the closure's features (rho u as
                 // float times the float of the FP64 reciprocal)
                 float vu = 0.f, vv = 0.f, vw = 0.f;
+                // 1/rho of the written cell, shared by the velocities and the
+                // acoustic Courant number (the last stage only)
+                const double ir = (a.vel || a.co) ? 1. / base[0] : 0.;
                 if (a.vel) {
-                    const float rr = (float)(1. / base[0]);
+                    const float rr = (float)ir;
                     vu = (float)base[1] * rr;
                     vv = (float)base[2] * rr;
                     vw = (float)base[3] * rr;
@@ -604,7 +607,8 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     }
                 }
                 if (a.co && i >= a.co_i0 && i <= a.co_i1) {
-                    const double Co = cell_courant(kc.cfl_mode, base[0], base[1], base[2], base[3], base[4], dtx, dty, dtz);
+                    const double Co =
+                        cell_courant_ir(kc.cfl_mode, base[0], ir, base[1], base[2], base[3], base[4], dtx, dty, dtz);
                     const double m = s.comax[r][l];
                     s.comax[r][l] = (Co > m) ? Co : m;
                     if (!(base[0] > 0.0)) atomicOr(a.status, 2u);

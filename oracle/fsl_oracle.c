@@ -1091,14 +1091,16 @@ double orc_check_courant(orc_ctx *o)
         for (j = 1; j < o->H + 1; j++)
             for (i = 1; i < o->L + 1; i++) {
                 size_t c = IC(o, i, j, k);
-                double R = o->U[0][c], U = o->U[1][c] / R;
+                double R = o->U[0][c];
                 if (o->p.cfl_mode == ORC_CFL_ACOUSTIC) {
-                    double V = o->U[2][c] / R, W = o->U[3][c] / R;
+                    /* the extension's own form: the reciprocal of rho once */
+                    double ir = 1.0 / R;
+                    double U = o->U[1][c] * ir, V = o->U[2][c] * ir, W = o->U[3][c] * ir;
                     double P = (o->U[4][c] - 0.5 * R * (U * U + V * V + W * W)) * K_1;
-                    double Cs = sqrt(K * P / R);
+                    double Cs = sqrt(K * P * ir);
                     CoNum = (fabs(U) + Cs) * o->dtx + (fabs(V) + Cs) * o->dty + (fabs(W) + Cs) * o->dtz;
                 } else {
-                    CoNum = U * o->dtx;
+                    CoNum = o->U[1][c] / R * o->dtx;
                 }
                 maxCo = (CoNum > maxCo) ? CoNum : maxCo;
             }

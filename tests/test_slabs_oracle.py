@@ -61,14 +61,14 @@ class OracleDomain:
         U = [self.o.cells(0, q)[self.co0:self.co1 + 1, 1:-1, 1:-1] for q in range(5)]
         dtx, dty, dtz = self.dt / self.p["deltaX"], self.dt / self.p["deltaY"], self.dt / self.p["deltaZ"]
         R = U[0]
-        u = U[1] / R
         if self.p["cfl_mode"] == 1:
-            v, w = U[2] / R, U[3] / R
+            ir = 1.0 / R
+            u, v, w = U[1] * ir, U[2] * ir, U[3] * ir
             P = (U[4] - 0.5 * R * (u * u + v * v + w * w)) * 0.4
-            Cs = np.sqrt(1.4 * P / R)
+            Cs = np.sqrt(1.4 * P * ir)
             co = (np.abs(u) + Cs) * dtx + (np.abs(v) + Cs) * dty + (np.abs(w) + Cs) * dtz
         else:
-            co = u * dtx
+            co = U[1] / R * dtx
         return max(0.0, float(np.max(co)))
 
     def courant_prepare(self):
