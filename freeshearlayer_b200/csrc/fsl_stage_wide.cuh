@@ -271,13 +271,14 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
     const long long ntiles = (long long)ntk * ntj, total = ntiles * L;
     // heads: planes 1..Hd of every tile; tails: planes Hd+1..L of every tile.
     // With more blocks than tiles, block b < ntiles takes the head of tile b
-    // and the other blocks share the tails; a tail plane counts 1.06 head
-    // planes (the tail blocks start several segments, each with a prologue
-    // and out of step with their neighbours: measured 3 to 10 % slower per
-    // plane at 512x256x256), so the heads are a little longer.
+    // and the other blocks share the tails; a tail plane counts 1.03 head
+    // planes (the tail blocks start several segments, each with a prologue,
+    // and run out of step with their neighbours), so the heads are a little
+    // longer.  Measured at 512x256x256 per stage launch: 2.404, 2.373, 2.349,
+    // 2.357, 2.362 ms for weights 1.00, 1.01, 1.03, 1.06, 1.09.
     long long Hd, pos, end;
     if (nb > ntiles) {
-        Hd = min((long long)L, (106LL * ntiles * L) / (100LL * (nb - ntiles) + 106LL * ntiles));
+        Hd = min((long long)L, (103LL * ntiles * L) / (100LL * (nb - ntiles) + 103LL * ntiles));
         const long long tails = ntiles * (L - Hd), nt = nb - ntiles;
         pos = b < ntiles ? b * Hd : ntiles * Hd + tails * (b - ntiles) / nt;
         end = b < ntiles ? (b + 1) * Hd : ntiles * Hd + tails * (b - ntiles + 1) / nt;
