@@ -309,7 +309,8 @@ int fsl_step_stage(fsl_ctx *ctx);
 #define FSL_TUNE_STAGE_ROWS 1 /* rows per ring stage tile incl. 2 halo rows: 8, 12 or 16; or 0, the
                                  full-lane persistent 16 x 32 tile (the FP32 bulk's default with the
                                  reference reconstruction; elsewhere 0 runs 16) */
-#define FSL_TUNE_STAGE_SEG 2  /* x planes marched per stage block (default 48 FP32 bulk, 32 FP64) */
+#define FSL_TUNE_STAGE_SEG 2  /* x planes marched per ring-tile stage block (default 48 FP32 bulk, 32 FP64;
+                                 the full-lane tile splits the planes among its blocks itself) */
 #define FSL_TUNE_CLOSURE_POLY 3 /* learned-closure inference: of every 8 SiLU value pairs, how many take
                                    the FMA-pipe polynomial tanh instead of the MUFU one: 0 or 2..6
                                    (default 2: 1.97 ms against 2.20 for 0 and 1.99 for 3 per step at
