@@ -224,13 +224,15 @@ STAGE_FLOPS = {p: o["add"] + o["mul"] + o["div"] + o["sqrt"] for p, o in STAGE_O
 SMS = 148
 
 
-def make_domain(fsl, grid, arm, state, dU, rows=0, seg=0, recon=0):
+def make_domain(fsl, grid, arm, state, dU, rows=0, seg=0, recon=0, poly=-1):
     prec, sgs = ARMS[arm]
     d = fsl.Domain(workload_params(grid, precision=prec, sgs=sgs, recon=recon))
     if rows:
         d.tune(d.TUNE_STAGE_ROWS, rows)
     if seg:
         d.tune(d.TUNE_STAGE_SEG, seg)
+    if poly >= 0:
+        d.tune(d.TUNE_CLOSURE_POLY, poly)
     d.upload_state(state)
     if sgs == 1:
         d.closure_set_scales(DW0 / dU, DW0)
@@ -610,7 +612,7 @@ def main_gpu(args):
         dev_uuid = str(local)
 
     # ---- the headline arm: K steps, state resident in HBM ----
-    d = make_domain(fsl, grid, arm, state, dU, args.rows, args.seg)
+    d = make_domain(fsl, grid, arm, state, dU, args.rows, args.seg, poly=args.closure_poly)
     run = d.step_phased if args.phased else d.step
     for _ in range(args.warmup):
         run(1)
@@ -850,6 +852,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--rows", type=int, default=0, help="fused stage tile rows (8, 12, 16)")
     ap.add_argument("--seg", type=int, default=0, help="x planes per fused stage block")
+    ap.add_argument("--closure-poly", type=int, default=-1,
+                    help="closure SiLU pairs of 8 on the FMA-pipe tanh (0, 2..6; -1: the library default)")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 path beside the arm")

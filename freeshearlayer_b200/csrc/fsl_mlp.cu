@@ -272,49 +272,30 @@ __device__ __forceinline__ uint32_t silu2_bf16(float h0, float h1)
     return y;
 }
 
-// packed FP32 pairs (sm_100: one instruction issues two FP32 FMAs)
-__device__ __forceinline__ uint64_t f2_pack(float a, float b)
-{
-    uint64_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c)
-{
-    uint64_t d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b)
-{
-    uint64_t d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-
 // silu of two values on the FMA pipe (the MUFU pipe runs the others): tanh
 // from an odd polynomial of degree 13 on [-3.3, 3.3], h clamped there,
 // coefficients this project fitted near-minimax on Chebyshev nodes with
 // Lawson's iteratively reweighted least squares (max |error| 1.4e-3,
 // including the clamp; the BF16 result rounds at 2^-9 relative), then
 // silu = h + h tanh(h) and one rounding to BF16.  The pair is evaluated in
-// packed FP32 arithmetic (fma.rn.f32x2: two FMAs per issue slot).
+// packed FP32 arithmetic (sm_100 issues two FP32 FMAs per instruction),
+// written with the compiler's packed builtins rather than inline PTX so the
+// compiler sees the coefficient pairs as constants (the same roundings; the
+// step 0.7 % faster than the inline-PTX form).
 __device__ __forceinline__ uint32_t silu2_poly(float h0, float h1)
 {
-    const float x0 = fminf(fmaxf(h0, -3.3f), 3.3f), x1 = fminf(fmaxf(h1, -3.3f), 3.3f);
-    const uint64_t x = f2_pack(x0, x1), h = f2_pack(h0, h1), x2 = f2_mul(x, x);
-    uint64_t p = f2_fma(f2_pack(2.460764335e-06f, 2.460764335e-06f), x2,
-                        f2_pack(-1.012231442e-04f, -1.012231442e-04f));
-    p = f2_fma(p, x2, f2_pack(1.705276780e-03f, 1.705276780e-03f));
-    p = f2_fma(p, x2, f2_pack(-1.538222842e-02f, -1.538222842e-02f));
-    p = f2_fma(p, x2, f2_pack(8.308345824e-02f, 8.308345824e-02f));
-    p = f2_fma(p, x2, f2_pack(-2.995448709e-01f, -2.995448709e-01f));
-    p = f2_fma(p, x2, f2_pack(9.929457903e-01f, 9.929457903e-01f));
-    const uint64_t y = f2_fma(h, f2_mul(p, x), h);
-    float y0, y1;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(y0), "=f"(y1) : "l"(y));
+    const float2 x = make_float2(fminf(fmaxf(h0, -3.3f), 3.3f), fminf(fmaxf(h1, -3.3f), 3.3f));
+    const float2 h = make_float2(h0, h1), x2 = __fmul2_rn(x, x);
+    float2 p = __ffma2_rn(make_float2(2.460764335e-06f, 2.460764335e-06f), x2,
+                          make_float2(-1.012231442e-04f, -1.012231442e-04f));
+    p = __ffma2_rn(p, x2, make_float2(1.705276780e-03f, 1.705276780e-03f));
+    p = __ffma2_rn(p, x2, make_float2(-1.538222842e-02f, -1.538222842e-02f));
+    p = __ffma2_rn(p, x2, make_float2(8.308345824e-02f, 8.308345824e-02f));
+    p = __ffma2_rn(p, x2, make_float2(-2.995448709e-01f, -2.995448709e-01f));
+    p = __ffma2_rn(p, x2, make_float2(9.929457903e-01f, 9.929457903e-01f));
+    const float2 y = __ffma2_rn(h, __fmul2_rn(p, x), h);
     uint32_t r;
-    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(y1), "f"(y0));
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(y.y), "f"(y.x));
     return r;
 }
 

@@ -313,8 +313,8 @@ int fsl_step_stage(fsl_ctx *ctx);
                                  the full-lane tile splits the planes among its blocks itself) */
 #define FSL_TUNE_CLOSURE_POLY 3 /* learned-closure inference: of every 8 SiLU value pairs, how many take
                                    the FMA-pipe polynomial tanh instead of the MUFU one: 0 or 2..6
-                                   (default 2: 1.97 ms against 2.20 for 0 and 1.99 for 3 per step at
-                                   512x256x256) */
+                                   (default 2: 1.94 ms per step at 512x256x256 against 1.97 for 3;
+                                   0, every pair on the MUFU pipe, runs about 10 % slower) */
 int fsl_tune(fsl_ctx *ctx, int key, int value);
 
 /* ---- debug / parity access ----------------------------------------------- */
