@@ -187,6 +187,56 @@ class Clocks:
                 "power_w_max": max(power) if power else None}
 
 
+def cpu_ranges(cpus) -> str:
+    """'0-55,112-167' for a sorted CPU list."""
+    out, start, prev = [], None, None
+    for c in cpus:
+        if start is None:
+            start = prev = c
+        elif c == prev + 1:
+            prev = c
+        else:
+            out.append("%d-%d" % (start, prev) if prev > start else str(start))
+            start = prev = c
+    if start is not None:
+        out.append("%d-%d" % (start, prev) if prev > start else str(start))
+    return ",".join(out)
+
+
+def gpu_local_cpus(dev_uuid: str):
+    """The host CPUs on the NUMA node of the GPU's PCIe root (NVML's CPU
+    affinity of the device), restricted to the CPUs this process may use;
+    None when NVML cannot say."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByUUID(dev_uuid)
+            ncpu = os.cpu_count() or 1
+            words = pynvml.nvmlDeviceGetCpuAffinity(h, (ncpu + 63) // 64)
+        finally:
+            pynvml.nvmlShutdown()
+        cpus = {64 * w + b for w, m in enumerate(words) for b in range(64) if (int(m) >> b) & 1}
+        cpus &= os.sched_getaffinity(0)
+        return sorted(cpus) or None
+    except Exception:
+        return None
+
+
+def bind_near_gpu(dev_uuid: str):
+    """Run this process on the GPU's local CPUs, so that the pinned host
+    buffers of the end-to-end leg are allocated on the NUMA node whose PCIe
+    root the GPU sits under (host<->device copies from the other socket's
+    memory cross the inter-socket link).  Returns the CPU list, or None."""
+    cpus = gpu_local_cpus(dev_uuid)
+    if cpus:
+        try:
+            os.sched_setaffinity(0, cpus)
+        except OSError:
+            return None
+    return cpus
+
+
 def measured_peaks() -> dict:
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -610,6 +660,7 @@ def main_gpu(args):
             dev_uuid = "GPU-" + dev_uuid
     except Exception:
         dev_uuid = str(local)
+    near = None if args.no_numa_bind else bind_near_gpu(dev_uuid)
 
     # ---- the headline arm: K steps, state resident in HBM ----
     d = make_domain(fsl, grid, arm, state, dU, args.rows, args.seg, poly=args.closure_poly)
@@ -650,7 +701,9 @@ def main_gpu(args):
            "steps": ne, "note": "per step: fsl_upload_state_async (pinned host -> HBM), fsl_step(1), "
                                 "fsl_download_state_async (HBM -> pinned host); the copies run on copy "
                                 "streams of their own, overlapping the neighbouring steps; timed to "
-                                "fsl_transfer_wait after the last"}
+                                "fsl_transfer_wait after the last",
+           "host_cpus": ("process bound to the GPU's local CPUs %s (pinned buffers on that NUMA node)"
+                         % cpu_ranges(near)) if near else "not bound"}
     d.close()
 
     # ---- the plain FP64 dynamic-Smagorinsky GPU path on the same box ----
@@ -850,6 +903,8 @@ def main():
     ap.add_argument("--arm", default="fp32-learned", choices=sorted(ARMS))
     ap.add_argument("--phased", action="store_true", help="per-phase kernels instead of the fused step")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-numa-bind", action="store_true",
+                    help="leave the process on all CPUs (default: the GPU's local CPUs)")
     ap.add_argument("--rows", type=int, default=0, help="fused stage tile rows (8, 12, 16)")
     ap.add_argument("--seg", type=int, default=0, help="x planes per fused stage block")
     ap.add_argument("--closure-poly", type=int, default=-1,

@@ -80,3 +80,14 @@ def test_gpus_flag_must_match_the_launcher():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "4", "--launcher-check"],
                        capture_output=True, text=True, timeout=60, env=env, cwd=ROOT)
     assert r.returncode != 0 and "WORLD_SIZE" in r.stderr
+
+
+def test_cpu_ranges_and_binding_without_nvml_device():
+    """The end-to-end leg's CPU binding: the range string it reports, and no
+    binding (None) when NVML knows no such device (as on a host without a GPU)."""
+    assert bench.cpu_ranges([0, 1, 2, 3, 8, 10, 11]) == "0-3,8,10-11"
+    assert bench.cpu_ranges([5]) == "5"
+    assert bench.cpu_ranges([]) == ""
+    before = os.sched_getaffinity(0)
+    assert bench.bind_near_gpu("GPU-00000000-0000-0000-0000-000000000000") is None
+    assert os.sched_getaffinity(0) == before
