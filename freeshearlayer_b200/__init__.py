@@ -32,11 +32,13 @@ __all__ = ["Params", "Domain", "FslError", "lib", "LIB_PATH", "default_params",
            "SETUP_SPATIAL", "SETUP_TEMPORAL", "CFL_STREAMWISE", "CFL_ACOUSTIC",
            "PREC_FP64", "PREC_FP32", "SGS_DYNAMIC", "SGS_LEARNED", "SGS_STATIC", "SGS_NONE", "RECON_CHARMINMOD",
            "RECON_PPM", "Trainer", "Ensemble", "closure_weights", "shear_statistics", "favre_from_probes",
-           "favre_profiles",
+           "favre_profiles", "debug_bounds",
            "tecplot_write"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfsl_gpu.so")
+# FSL_GPU_LIB=checked loads the bounds-checked debug build (libfsl_gpu_checked.so)
+LIB_PATH = os.path.join(HERE, "libfsl_gpu_checked.so" if os.environ.get("FSL_GPU_LIB") == "checked"
+                        else "libfsl_gpu.so")
 
 FSL_OK = 0
 ERRORS = {-1: "FSL_ERR_ARG", -2: "FSL_ERR_NOMEM", -3: "FSL_ERR_CUDA", -4: "FSL_ERR_NONFINITE",
@@ -95,6 +97,11 @@ class ClosureStats(C.Structure):
                 ("dynamic_steps", C.c_int)]
 
 
+class BoundsReport(C.Structure):
+    _fields_ = [("hits", C.c_ulonglong), ("unit", C.c_int), ("line", C.c_int), ("index", C.c_longlong),
+                ("extent", C.c_longlong)]
+
+
 class KTimes(C.Structure):
     _fields_ = [("ms", C.c_double * 8), ("launches", C.c_ulonglong * 8)]
 
@@ -111,7 +118,8 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise FslError(-8, "libfsl_gpu.so not built: run `make -C %s`" % HERE)
+            raise FslError(-8, "%s not built: run `make -C %s%s`"
+                           % (os.path.basename(LIB_PATH), HERE, " checked" if "checked" in LIB_PATH else ""))
         L = C.CDLL(LIB_PATH)
         vp, i, d, u = C.c_void_p, C.c_int, C.c_double, C.c_uint
         P = C.POINTER(Params)
@@ -173,6 +181,7 @@ def lib():
             "fsl_get_courant_max": [vp, C.POINTER(C.c_double)], "fsl_set_courant_max": [vp, d],
         })
         sig["fsl_tune"] = [vp, i, i]
+        sig["fsl_debug_bounds"] = [C.POINTER(BoundsReport), i]
         sig["fsl_profile"] = [vp, i]
         sig["fsl_profile_read"] = [vp, C.POINTER(KTimes)]
         for name, args in sig.items():
@@ -199,6 +208,17 @@ def _check(rc: int, h=None):
     if rc != FSL_OK:
         what = lib().fsl_last_error(h).decode() if h else ""
         raise FslError(rc, what)
+
+
+def debug_bounds(clear: bool = False) -> dict:
+    """The bounds-checked build's report (FSL_GPU_LIB=checked): offending
+    global-memory accesses since the last clear and the first one's file
+    (1 fsl_fused.cu, 2 fsl_fused32.cu, 3 fsl_mlp.cu, 4 fsl_phase.cu), line,
+    index and extent.  Raises FslError (FSL_ERR_UNSUPPORTED) in the product
+    build."""
+    r = BoundsReport()
+    _check(lib().fsl_debug_bounds(C.byref(r), 1 if clear else 0))
+    return {"hits": int(r.hits), "unit": r.unit, "line": r.line, "index": r.index, "extent": r.extent}
 
 
 def default_params(**kw) -> Params:

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <new>
 
+#include "fsl_check.cuh"
 #include "fsl_internal.h"
 
 using namespace fsl;
@@ -1155,6 +1156,31 @@ int fsl_step_stage(fsl_ctx *h)
     }
     CKL();
     return FSL_OK;
+}
+
+int fsl_debug_bounds(fsl_bounds_report *out, int clear)
+{
+    if (!out) return FSL_ERR_ARG;
+    *out = fsl_bounds_report{};
+#if FSL_BOUNDS_CHECK
+    if (cudaDeviceSynchronize() != cudaSuccess) return FSL_ERR_CUDA;
+    int (*const readers[4])(chk::Record *, bool) = {chk_read_fused, chk_read_fused32, chk_read_mlp, chk_read_phase};
+    for (int u = 0; u < 4; u++) {
+        chk::Record r{};
+        if (readers[u](&r, clear != 0) != 0) return FSL_ERR_CUDA;
+        if (r.hits && !out->hits) {
+            out->unit = u + 1;
+            out->line = r.line;
+            out->index = r.index;
+            out->extent = r.extent;
+        }
+        out->hits += r.hits;
+    }
+    return FSL_OK;
+#else
+    (void)clear;
+    return FSL_ERR_UNSUPPORTED;
+#endif
 }
 
 int fsl_tune(fsl_ctx *h, int key, int value)

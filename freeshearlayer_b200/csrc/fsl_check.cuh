@@ -1,0 +1,87 @@
+// fsl_check.cuh -- debug bounds checks of global-memory indices.
+//
+// Built with -DFSL_BOUNDS_CHECK=1 (`make -C freeshearlayer_b200 checked`,
+// libfsl_gpu_checked.so), every index wrapped in FSL_CELL or FSL_FACE is
+// tested against the extent of the array it indexes before the access: a
+// cell index against one field of the padded box ([0, fstride); the field
+// offset q * fstride is added outside the check), a face index against one
+// field of a boundary-face array.  The first offending access records its
+// translation unit, source line, index and extent in a device word of that
+// unit, every offending access counts, and the access is redirected to
+// element 0 so it cannot leave the allocation.  fsl_debug_bounds reads the
+// records.  In the product build the macros are the bare index.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace fsl {
+namespace chk {
+
+struct Record {
+    unsigned long long hits; // offending accesses since the last clear
+    int unit, line;          // of the first one
+    long long index, extent;
+};
+
+#if FSL_BOUNDS_CHECK
+// one record per translation unit (no relocatable device code needed)
+static __device__ Record g_rec;
+
+__device__ __forceinline__ long long at(long long i, long long n, int unit, int line)
+{
+    if ((unsigned long long)i < (unsigned long long)n) return i;
+    if (atomicAdd(&g_rec.hits, 1ull) == 0ull) {
+        g_rec.unit = unit;
+        g_rec.line = line;
+        g_rec.index = i;
+        g_rec.extent = n;
+    }
+    return 0;
+}
+
+// this unit's record, read (and with clear, reset) from the host
+static inline int read_unit(Record *out, bool clear)
+{
+    if (cudaMemcpyFromSymbol(out, g_rec, sizeof(Record)) != cudaSuccess) return -1;
+    if (clear) {
+        const Record z{};
+        if (cudaMemcpyToSymbol(g_rec, &z, sizeof(Record)) != cudaSuccess) return -1;
+    }
+    return 0;
+}
+#endif
+
+} // namespace chk
+} // namespace fsl
+
+namespace fsl {
+// the units' record readers (-1 when built without checks)
+int chk_read_fused(chk::Record *out, bool clear);
+int chk_read_fused32(chk::Record *out, bool clear);
+int chk_read_mlp(chk::Record *out, bool clear);
+int chk_read_phase(chk::Record *out, bool clear);
+} // namespace fsl
+
+// Translation-unit ids of the records (FSL_CHK_UNIT must be defined before
+// this header in every unit that checks).
+#define FSL_CHK_FUSED 1   // fsl_fused.cu: FP64 ring-tile stage kernels
+#define FSL_CHK_FUSED32 2 // fsl_fused32.cu: FP32 ring-tile and full-lane stage kernels, ensembles
+#define FSL_CHK_MLP 3     // fsl_mlp.cu: closure features and inference
+#define FSL_CHK_PHASE 4   // fsl_phase.cu: state scatter/gather
+
+#if FSL_BOUNDS_CHECK
+#define FSL_CELL(c, fs) (::fsl::chk::at((c), (fs), FSL_CHK_UNIT, __LINE__))
+#define FSL_FACE(f, n) (::fsl::chk::at((f), (n), FSL_CHK_UNIT, __LINE__))
+// the host reader of this unit's record: int fsl_chk_read_<name>(Record*, bool)
+#define FSL_CHK_EXPORT(name)                                                                                          \
+    namespace fsl {                                                                                                   \
+    int chk_read_##name(chk::Record *out, bool clear) { return chk::read_unit(out, clear); }                         \
+    }
+#else
+#define FSL_CELL(c, fs) (c)
+#define FSL_FACE(f, n) (f)
+#define FSL_CHK_EXPORT(name)                                                                                          \
+    namespace fsl {                                                                                                   \
+    int chk_read_##name(chk::Record *, bool) { return -1; }                                                           \
+    }
+#endif

@@ -1,7 +1,10 @@
 // fsl_fused.cu -- FP64 instantiation of the fused stage kernel (the plain
 // method).  Compiled with --fmad=false: every value is formed with the
 // reference's expressions and rounds exactly like the reference's serial code.
+#define FSL_CHK_UNIT FSL_CHK_FUSED
 #include "fsl_stage.cuh"
+
+FSL_CHK_EXPORT(fused)
 
 namespace fsl {
 

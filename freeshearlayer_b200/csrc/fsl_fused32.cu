@@ -9,8 +9,11 @@
 #include <algorithm>
 #include <new>
 
+#define FSL_CHK_UNIT FSL_CHK_FUSED32
 #include "fsl_stage.cuh"
 #include "fsl_stage_wide.cuh"
+
+FSL_CHK_EXPORT(fused32)
 
 namespace fsl {
 

@@ -13,9 +13,13 @@
 // M = 128 with K-major operands.
 #include <cuda_bf16.h>
 
+#define FSL_CHK_UNIT FSL_CHK_MLP
+#include "fsl_check.cuh"
 #include "fsl_internal.h"
 #include "fsl_mlp.h"
 #include "fsl_umma.cuh"
+
+FSL_CHK_EXPORT(mlp)
 
 namespace fsl {
 namespace mlp {
@@ -70,7 +74,7 @@ __global__ void k_closure_vel(Grid g, const double *__restrict__ U, float *__res
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         if ((int)(t % g.pk) >= g.D + 2) continue; // row padding
-        const long long a = g.off + t;
+        const long long a = FSL_CELL(g.off + t, fs);
         const double r = U[a];
         const float rr = (float)(1. / r);
         vel[a] = (float)U[fs + a] * rr;
@@ -105,12 +109,12 @@ __device__ __forceinline__ void feat_load(const Grid &g, const double *__restric
     const long long off[7] = {0, g.pi, -g.pi, (long long)g.pk, -(long long)g.pk, 1, -1};
 #pragma unroll
     for (int n = 1; n < 7; n++) {
-        const long long a = c + off[n];
+        const long long a = FSL_CELL(c + off[n], fs);
         p.u[n] = vel[a];
         p.v[n] = vel[fs + a];
         p.w[n] = vel[2 * fs + a];
     }
-    p.r = U[c];
+    p.r = U[FSL_CELL(c, fs)];
     p.c = c;
 }
 
@@ -418,8 +422,9 @@ __global__ void __launch_bounds__(128, NP <= 3 ? 5 : 4) k_closure_infer(Grid g, 
         umma::tmem_wait_ld();
         const float cs2 = fminf(fmaxf(v[0] + b4, 0.f), 0.15f);
         if (valid) {
-            mu[c] = (MT)(rho * cs2 * sc.DD * Smag);
-            if (cs2_out) cs2_out[c] = cs2;
+            const long long cc = FSL_CELL(c, g.fstride);
+            mu[cc] = (MT)(rho * cs2 * sc.DD * Smag);
+            if (cs2_out) cs2_out[cc] = cs2;
         }
     }
     if (!ok) {

@@ -7,9 +7,13 @@
 // results equal the reference's serial FP64 code bit for bit.
 #include <algorithm>
 
+#define FSL_CHK_UNIT FSL_CHK_PHASE
+#include "fsl_check.cuh"
 #include "fsl_dyn.cuh"
 #include "fsl_internal.h"
 #include "fsl_phys.cuh"
+
+FSL_CHK_EXPORT(phase)
 
 namespace fsl {
 
@@ -514,7 +518,7 @@ __global__ void k_state_scatter(Grid g, double *__restrict__ dst, const double *
         const int v = (int)(r % 5); r /= 5;
         const int j = (int)(r % g.H);
         const int i = (int)(r / g.H);
-        dst[v * g.fstride + g.idx(i + i0, j + 1, k + 1)] = packed[t];
+        dst[v * g.fstride + FSL_CELL(g.idx(i + i0, j + 1, k + 1), g.fstride)] = packed[t];
     }
 }
 
@@ -529,7 +533,7 @@ __global__ void k_state_gather(Grid g, const double *__restrict__ src, double *_
         const int v = (int)(r % 5); r /= 5;
         const int j = (int)(r % g.H);
         const int i = (int)(r / g.H);
-        packed[t] = src[v * g.fstride + g.idx(i + i0, j + 1, k + 1)];
+        packed[t] = src[v * g.fstride + FSL_CELL(g.idx(i + i0, j + 1, k + 1), g.fstride)];
     }
 }
 

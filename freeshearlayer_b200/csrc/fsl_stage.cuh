@@ -20,6 +20,7 @@
 // rules (src/bounCondOnInterfaces.c:11-110) to the reconstructed boundary cells.
 #pragma once
 
+#include "fsl_check.cuh"
 #include "fsl_internal.h"
 #include "fsl_phys.cuh"
 
@@ -34,7 +35,7 @@ template <typename T>
 __device__ __forceinline__ void load5(const double *__restrict__ u, long long fs, long long c, T *v)
 {
 #pragma unroll
-    for (int q = 0; q < 5; q++) v[q] = T(u[q * fs + c]);
+    for (int q = 0; q < 5; q++) v[q] = T(u[q * fs + FSL_CELL(c, fs)]);
 }
 
 // reconstruction sweep DIR (0 x, 1 y, 2 z) of the padded cell c
@@ -50,10 +51,11 @@ __device__ __forceinline__ void recon_at(const Grid &g, const double *__restrict
     const int p2 = DIR == 0 ? 2 : DIR == 1 ? 3 : 1;
     const int p3 = DIR == 0 ? 3 : DIR == 1 ? 1 : 2;
     T fw[5], bw[5];
-    fw[0] = T(u[c + d]); fw[1] = T(u[p1 * fs + c + d]); fw[2] = T(u[p2 * fs + c + d]);
-    fw[3] = T(u[p3 * fs + c + d]); fw[4] = T(u[4 * fs + c + d]);
-    bw[0] = T(u[c - d]); bw[1] = T(u[p1 * fs + c - d]); bw[2] = T(u[p2 * fs + c - d]);
-    bw[3] = T(u[p3 * fs + c - d]); bw[4] = T(u[4 * fs + c - d]);
+    const long long cf = FSL_CELL(c + d, fs), cb = FSL_CELL(c - d, fs);
+    fw[0] = T(u[cf]); fw[1] = T(u[p1 * fs + cf]); fw[2] = T(u[p2 * fs + cf]);
+    fw[3] = T(u[p3 * fs + cf]); fw[4] = T(u[4 * fs + cf]);
+    bw[0] = T(u[cb]); bw[1] = T(u[p1 * fs + cb]); bw[2] = T(u[p2 * fs + cb]);
+    bw[3] = T(u[p3 * fs + cb]); bw[4] = T(u[4 * fs + cb]);
     if (DIR == 0) recon_x(cc, fw, bw, hi, lo);
     else if (DIR == 1) recon_y(cc, fw, bw, hi, lo);
     else recon_z(cc, fw, bw, hi, lo);
@@ -113,37 +115,38 @@ __device__ __noinline__ void bface_one(Grid g, int setup, int BL_HIG, Disturb d,
                 v[0] = R; v[1] = R * U; v[2] = 0.; v[3] = 0.; v[4] = P / 0.4 + 0.5 * R * (U * U);
             }
 #pragma unroll
-            for (int q = 0; q < 5; q++) bf.x0[q * nx + fo] = T(v[q]);
+            for (int q = 0; q < 5; q++) bf.x0[q * nx + FSL_FACE(fo, nx)] = T(v[q]);
             // :62-71 outflow from the minus state of face LEN
             recon_at<T, 0>(g, u, g.idx(L, j, k), hi, lo);
             const T r = hi[0], mu_ = hi[1], mv = hi[2], mw = hi[3];
             const T P_ = T(100000.);
-            bf.xL[fo] = r; bf.xL[nx + fo] = mu_; bf.xL[2 * nx + fo] = mv; bf.xL[3 * nx + fo] = mw;
-            bf.xL[4 * nx + fo] = P_ / kc::K_1 + T(0.5) * (mu_ * mu_ + mv * mv + mw * mw) / r;
+            const long long fc = FSL_FACE(fo, nx);
+            bf.xL[fc] = r; bf.xL[nx + fc] = mu_; bf.xL[2 * nx + fc] = mv; bf.xL[3 * nx + fc] = mw;
+            bf.xL[4 * nx + fc] = P_ / kc::K_1 + T(0.5) * (mu_ * mu_ + mv * mv + mw * mw) / r;
         } else { // periodic x, the reference's z rule (:94-109)
             recon_at<T, 0>(g, u, g.idx(L, j, k), hi, lo);
 #pragma unroll
-            for (int q = 0; q < 5; q++) bf.x0[q * nx + fo] = hi[q];
+            for (int q = 0; q < 5; q++) bf.x0[q * nx + FSL_FACE(fo, nx)] = hi[q];
             recon_at<T, 0>(g, u, g.idx(1, j, k), hi, lo);
 #pragma unroll
-            for (int q = 0; q < 5; q++) bf.xL[q * nx + fo] = lo[q];
+            for (int q = 0; q < 5; q++) bf.xL[q * nx + FSL_FACE(fo, nx)] = lo[q];
         }
     } else if ((t -= nx) < ny) { // :75-90
         const int i = (int)(t / D) + 1, k = (int)(t % D) + 1;
         recon_at<T, 1>(g, u, g.idx(i, 1, k), hi, lo);
 #pragma unroll
-        for (int q = 0; q < 5; q++) bf.y0[q * ny + t] = (q == 2 && spatial) ? -lo[q] : lo[q];
+        for (int q = 0; q < 5; q++) bf.y0[q * ny + FSL_FACE(t, ny)] = (q == 2 && spatial) ? -lo[q] : lo[q];
         recon_at<T, 1>(g, u, g.idx(i, H, k), hi, lo);
 #pragma unroll
-        for (int q = 0; q < 5; q++) bf.yH[q * ny + t] = (q == 2 && spatial) ? -hi[q] : hi[q];
+        for (int q = 0; q < 5; q++) bf.yH[q * ny + FSL_FACE(t, ny)] = (q == 2 && spatial) ? -hi[q] : hi[q];
     } else if ((t -= ny) < nz) { // :94-109
         const int i = (int)(t / H) + 1, j = (int)(t % H) + 1;
         recon_at<T, 2>(g, u, g.idx(i, j, D), hi, lo);
 #pragma unroll
-        for (int q = 0; q < 5; q++) bf.z0[q * nz + t] = hi[q];
+        for (int q = 0; q < 5; q++) bf.z0[q * nz + FSL_FACE(t, nz)] = hi[q];
         recon_at<T, 2>(g, u, g.idx(i, j, 1), hi, lo);
 #pragma unroll
-        for (int q = 0; q < 5; q++) bf.zD[q * nz + t] = lo[q];
+        for (int q = 0; q < 5; q++) bf.zD[q * nz + FSL_FACE(t, nz)] = lo[q];
     }
 }
 
@@ -319,9 +322,9 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             }
             vel_rcp(Um[0], Um[1], Um[2], Um[3], s.R[(i0 - 1) % 3][r][l]);
             if constexpr (!SST) {
-                mum = mu[cj + (long long)(i0 - 1) * g.pi];
-                mu0 = mu[cj + (long long)i0 * g.pi];
-                mu1 = mu[cj + (long long)(i0 + 1) * g.pi];
+                mum = mu[FSL_CELL(cj + (long long)(i0 - 1) * g.pi, fs)];
+                mu0 = mu[FSL_CELL(cj + (long long)i0 * g.pi, fs)];
+                mu1 = mu[FSL_CELL(cj + (long long)(i0 + 1) * g.pi, fs)];
             }
             plane_prims<T, TJE, PPM, SST>(s, i0, r, l, mu0, mum);
             plane_prims<T, TJE, PPM, SST>(s, i0 + 1, r, l, mu1, mu0);
@@ -346,7 +349,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             if (i0 == 1) {
                 const long long fo = (long long)(j - 1) * D + (k - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) hm[q] = a.bf.x0[q * nxf + fo];
+                for (int q = 0; q < 5; q++) hm[q] = a.bf.x0[q * nxf + FSL_FACE(fo, nxf)];
             } else if (PPM && i0 - 1 >= 2 && i0 - 1 <= L - 1) {
                 ppm_at_x<T>(g, cu, cj + (long long)(i0 - 1) * g.pi, hm, tmp);
             } else {
@@ -379,7 +382,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
         // were formed at the end of the previous iteration, or in the prologue)
         plane_issue<T, TJE, PPM>(g, cu, i + (PPM ? 3 : 2), r, l, j, k, live, pl);
         if (inter) {
-            const long long c = cj + (long long)i * g.pi;
+            const long long c = FSL_CELL(cj + (long long)i * g.pi, fs);
             // FP32 bulk keeps only a converted copy of the state in shared
             // memory; the FP64 operands of the combination are fetched here
             if (sizeof(T) != 8) {
@@ -391,7 +394,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
                 }
             }
         }
-        if (!SST && live && i + 2 <= L + 1) mu2 = mu[cj + (long long)(i + 2) * g.pi];
+        if (!SST && live && i + 2 <= L + 1) mu2 = mu[FSL_CELL(cj + (long long)(i + 2) * g.pi, fs)];
         // (b) y and z reconstruction of cell (i, j, k): reads the state ring
         // only (plane i, stored two iterations ago)
         T hy[5], hz[5], lz[5];
@@ -441,22 +444,22 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             if (ycol && j == 0) {
                 const long long fo = (long long)(i - 1) * D + (k - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) hy[q] = a.bf.y0[q * nyf + fo];
+                for (int q = 0; q < 5; q++) hy[q] = a.bf.y0[q * nyf + FSL_FACE(fo, nyf)];
             }
             if (ycol && j == H + 1) {
                 const long long fo = (long long)(i - 1) * D + (k - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) s.Lo[r][l][q] = a.bf.yH[q * nyf + fo];
+                for (int q = 0; q < 5; q++) s.Lo[r][l][q] = a.bf.yH[q * nyf + FSL_FACE(fo, nyf)];
             }
             if (zrow && k == 0) {
                 const long long fo = (long long)(i - 1) * H + (j - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) hz[q] = a.bf.z0[q * nzf + fo];
+                for (int q = 0; q < 5; q++) hz[q] = a.bf.z0[q * nzf + FSL_FACE(fo, nzf)];
             }
             if (zrow && k == D + 1) {
                 const long long fo = (long long)(i - 1) * H + (j - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) lz[q] = a.bf.zD[q * nzf + fo];
+                for (int q = 0; q < 5; q++) lz[q] = a.bf.zD[q * nzf + FSL_FACE(fo, nzf)];
             }
         }
         __syncthreads();
@@ -522,7 +525,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
             } else {
                 const long long fo = (long long)(j - 1) * D + (k - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) lo[q] = a.bf.xL[q * nxf + fo];
+                for (int q = 0; q < 5; q++) lo[q] = a.bf.xL[q * nxf + FSL_FACE(fo, nxf)];
             }
             const T *dc = s.Dv[u0][r][l], *dn = s.Dv[u1][r][l];
             const T m_f = SST ? T(0.5) * (s.U[q1][r + HW][l + HW][0] + s.U[q0][r + HW][l + HW][0]) : dn[4];
@@ -533,7 +536,7 @@ __global__ void __launch_bounds__(TJE * 32, MINB) k_stage(Grid g, Consts kc, Arg
         __syncthreads();
         // (f) divergence and stage combination (src/evolution.c:29-161), FP64
         if (inter) {
-            const long long c = cj + (long long)i * g.pi;
+            const long long c = FSL_CELL(cj + (long long)i * g.pi, fs);
             const T *Uc = s.U[q0][r + HW][l + HW];
             (void)Uc;
 #pragma unroll

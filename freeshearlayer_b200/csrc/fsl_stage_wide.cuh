@@ -189,7 +189,7 @@ __device__ __forceinline__ void halo_sweeps(Smem<T> &s, const Args<T> &a, int p,
             } else {
                 const long long fo = (long long)(p - 1) * D + (k - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) hb[q] = a.bf.y0[q * nyf + fo];
+                for (int q = 0; q < 5; q++) hb[q] = a.bf.y0[q * nyf + FSL_FACE(fo, nyf)];
             }
 #pragma unroll
             for (int q = 0; q < 5; q++) s.HyB[qp][l][q] = hb[q];
@@ -207,7 +207,7 @@ __device__ __forceinline__ void halo_sweeps(Smem<T> &s, const Args<T> &a, int p,
             } else if (j0 + WJ == H + 1 && !tpl) {
                 const long long fo = (long long)(p - 1) * D + (k - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) s.LoH[qp][l][q] = a.bf.yH[q * nyf + fo];
+                for (int q = 0; q < 5; q++) s.LoH[qp][l][q] = a.bf.yH[q * nyf + FSL_FACE(fo, nyf)];
             }
         }
     } else if (r == WJ - 1) {
@@ -230,7 +230,7 @@ __device__ __forceinline__ void halo_sweeps(Smem<T> &s, const Args<T> &a, int p,
             const long long fo = (long long)(p - 1) * H + (jr - 1);
             const T *bfz = left ? a.bf.z0 : a.bf.zD;
 #pragma unroll
-            for (int q = 0; q < 5; q++) o[q] = bfz[q * nzf + fo];
+            for (int q = 0; q < 5; q++) o[q] = bfz[q * nzf + FSL_FACE(fo, nzf)];
         }
         if (act) {
             T *dst = left ? s.HzL[qp][rr] : s.LzR[qp][rr];
@@ -349,9 +349,9 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 load5(cu, fs, cj + (long long)(i0 - 1) * g.pi, Um);
                 vel_rcp(Um[0], Um[1], Um[2], Um[3], s.R[(i0 - 1) % 3][r + 1][l + 1]);
                 if constexpr (!SST) {
-                    mum = mu[cj + (long long)(i0 - 1) * g.pi];
-                    mu0 = mu[cj + (long long)i0 * g.pi];
-                    mu1 = mu[cj + (long long)(i0 + 1) * g.pi];
+                    mum = mu[FSL_CELL(cj + (long long)(i0 - 1) * g.pi, fs)];
+                    mu0 = mu[FSL_CELL(cj + (long long)i0 * g.pi, fs)];
+                    mu1 = mu[FSL_CELL(cj + (long long)(i0 + 1) * g.pi, fs)];
                 }
                 cell_prims<T, SST>(s, i0, r, l, mu0, mum);
                 cell_prims<T, SST>(s, i0 + 1, r, l, mu1, mu0);
@@ -361,9 +361,9 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 load5(cu, fs, hcj + (long long)(i0 - 1) * g.pi, Hm);
                 vel_rcp(Hm[0], Hm[1], Hm[2], Hm[3], s.R[(i0 - 1) % 3][hr + 1][hc + 1]);
                 if constexpr (!SST) {
-                    hmum = mu[hcj + (long long)(i0 - 1) * g.pi];
-                    hmu0 = mu[hcj + (long long)i0 * g.pi];
-                    hmu1 = mu[hcj + (long long)(i0 + 1) * g.pi];
+                    hmum = mu[FSL_CELL(hcj + (long long)(i0 - 1) * g.pi, fs)];
+                    hmu0 = mu[FSL_CELL(hcj + (long long)i0 * g.pi, fs)];
+                    hmu1 = mu[FSL_CELL(hcj + (long long)(i0 + 1) * g.pi, fs)];
                 }
                 cell_prims<T, SST>(s, i0, hr, hc, hmu0, hmum);
                 cell_prims<T, SST>(s, i0 + 1, hr, hc, hmu1, hmu0);
@@ -385,7 +385,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 } else if (i0 == 1) {
                     const long long fo = (long long)(j - 1) * D + (k - 1);
 #pragma unroll
-                    for (int q = 0; q < 5; q++) hm[q] = a.bf.x0[q * nxf + fo];
+                    for (int q = 0; q < 5; q++) hm[q] = a.bf.x0[q * nxf + FSL_FACE(fo, nxf)];
                 } else {
                     recon_at<T, 0>(g, cu, cj + (long long)(i0 - 1) * g.pi, hm, tmp);
                 }
@@ -408,7 +408,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
             if (live && i + 2 <= L + 1) load5(cu, fs, cj + (long long)(i + 2) * g.pi, pown);
             if (hlive && i + 2 <= L + 1) load5(cu, fs, hcj + (long long)(i + 2) * g.pi, phal);
             if (own) {
-                const long long c = cj + (long long)i * g.pi;
+                const long long c = FSL_CELL(cj + (long long)i * g.pi, fs);
 #pragma unroll
                 for (int q = 0; q < 5; q++) base[q] = cu[q * fs + c];
                 if (a.stage != 1) {
@@ -417,8 +417,8 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 }
             }
             if constexpr (!SST) {
-                if (live && i + 2 <= L + 1) mu2 = mu[cj + (long long)(i + 2) * g.pi];
-                if (hvlive && i + 2 <= L + 1) hmu2 = mu[hcj + (long long)(i + 2) * g.pi];
+                if (live && i + 2 <= L + 1) mu2 = mu[FSL_CELL(cj + (long long)(i + 2) * g.pi, fs)];
+                if (hvlive && i + 2 <= L + 1) hmu2 = mu[FSL_CELL(hcj + (long long)(i + 2) * g.pi, fs)];
             }
             // (b) y and z sweeps of the own cell, the boundary outer states,
             // and the halo sweeps (warps 13..15)
@@ -454,7 +454,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 // the face below this ghost row: the top boundary's outer state
                 const long long fo = (long long)(i - 1) * D + (k - 1);
 #pragma unroll
-                for (int q = 0; q < 5; q++) s.Lo[r][l][q] = a.bf.yH[q * nyf + fo];
+                for (int q = 0; q < 5; q++) s.Lo[r][l][q] = a.bf.yH[q * nyf + FSL_FACE(fo, nyf)];
             } else if (k == D + 1 && j <= H) {
                 // beyond the last column: the far z boundary's outer state (shuffled to lane l-1)
                 if (tpl) {
@@ -463,7 +463,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 } else {
                     const long long fo = (long long)(i - 1) * H + (j - 1);
 #pragma unroll
-                    for (int q = 0; q < 5; q++) lz[q] = a.bf.zD[q * nzf + fo];
+                    for (int q = 0; q < 5; q++) lz[q] = a.bf.zD[q * nzf + FSL_FACE(fo, nzf)];
                 }
             }
             __syncthreads();
@@ -527,7 +527,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 } else {
                     const long long fo = (long long)(j - 1) * D + (k - 1);
 #pragma unroll
-                    for (int q = 0; q < 5; q++) lo[q] = a.bf.xL[q * nxf + fo];
+                    for (int q = 0; q < 5; q++) lo[q] = a.bf.xL[q * nxf + FSL_FACE(fo, nxf)];
                 }
                 const T *dc = s.Dv[q0][r + 1][l + 1], *dn = s.Dv[q1][r + 1][l + 1];
                 const T m_f = SST ? T(0.5) * (s.U[q1][r + 2][l + 2][0] + s.U[q0][r + 2][l + 2][0]) : dn[4];
@@ -546,7 +546,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
 #pragma unroll
                     for (int q = 0; q < 5; q++) Fzm[q] = s.FzL[r][q];
                 }
-                const long long c = cj + (long long)i * g.pi;
+                const long long c = FSL_CELL(cj + (long long)i * g.pi, fs);
 #pragma unroll
                 for (int q = 0; q < 5; q++) {
                     const T X = T(dtx) * (Fxp[q] - Fx[q]);
@@ -578,7 +578,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                 const bool bx = i == 1 || i == L, by = j == 1 || j == H, bz = k == 1 || k == D;
                 if (tpl && bz && !(bx || by)) {
                     // the one ghost cell that copies a z-edge cell (periodic z)
-                    const long long gc = c + ((k == D ? 0 : D + 1) - k);
+                    const long long gc = FSL_CELL(c + ((k == D ? 0 : D + 1) - k), fs);
 #pragma unroll
                     for (int q = 0; q < 5; q++) a.out[q * fs + gc] = base[q];
                     if (a.vel) {
@@ -597,7 +597,7 @@ __device__ __forceinline__ void wide_block(Smem<T> &s, const Grid &g, const Cons
                     for (int e = 1; e < 8; e++) {
                         const int gi = xi[e & 1], gj = yj[(e >> 1) & 1], gk = zk[e >> 2];
                         if (gi < 0 || gj < 0 || gk < 0) continue;
-                        const long long gc = g.idx(gi, gj, gk);
+                        const long long gc = FSL_CELL(g.idx(gi, gj, gk), fs);
 #pragma unroll
                         for (int q = 0; q < 5; q++) a.out[q * fs + gc] = base[q];
                         if (a.vel) {

@@ -317,6 +317,28 @@ int fsl_step_stage(fsl_ctx *ctx);
                                    0, every pair on the MUFU pipe, runs about 10 % slower) */
 int fsl_tune(fsl_ctx *ctx, int key, int value);
 
+/* ---- debug bounds checks ---------------------------------------------------
+ * libfsl_gpu_checked.so (`make -C freeshearlayer_b200 checked`) is this
+ * library built with every global-memory index of the fused stage kernels
+ * (ring tile and full lane, both precisions, ensembles), the closure features
+ * and inference, and the state scatter/gather tested against the extent of
+ * the array it indexes.  An offending access is counted, the first one of
+ * each source file recorded, and the access redirected to element 0 of that
+ * array, so it never leaves the allocation.  No counterpart in the reference
+ * (its arrays are unchecked C). */
+typedef struct fsl_bounds_report {
+    unsigned long long hits; /* offending accesses since the last clear, all files */
+    int unit;                /* file of the first one reported: 1 fsl_fused.cu, 2 fsl_fused32.cu,
+                                3 fsl_mlp.cu, 4 fsl_phase.cu; 0 when hits is 0 */
+    int line;                /* its source line (in the file or a header it includes) */
+    long long index, extent; /* the index and the extent it was checked against */
+} fsl_bounds_report;
+/* Synchronise the current device, then report (and with clear != 0 reset)
+ * the records of every checked file; the first offending access reported is
+ * that of the lowest-numbered file with one.  FSL_ERR_UNSUPPORTED in the
+ * product build, which has no checks. */
+int fsl_debug_bounds(fsl_bounds_report *out, int clear);
+
 /* ---- debug / parity access ----------------------------------------------- */
 
 /* which: 0 = U^n, 1 = stage buffer, 2 = current-stage buffer, 3 = mu_SGS. */
