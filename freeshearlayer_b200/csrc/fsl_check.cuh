@@ -27,16 +27,29 @@ struct Record {
 // one record per translation unit (no relocatable device code needed)
 static __device__ Record g_rec;
 
-__device__ __forceinline__ long long at(long long i, long long n, int unit, int line)
+__device__ __forceinline__ void record(long long i, long long n, int unit, int line)
 {
-    if ((unsigned long long)i < (unsigned long long)n) return i;
     if (atomicAdd(&g_rec.hits, 1ull) == 0ull) {
         g_rec.unit = unit;
         g_rec.line = line;
         g_rec.index = i;
         g_rec.extent = n;
     }
+}
+
+__device__ __forceinline__ long long at(long long i, long long n, int unit, int line)
+{
+    if ((unsigned long long)i < (unsigned long long)n) return i;
+    record(i, n, unit, line);
     return 0;
+}
+
+// the stencil c + lo .. c + hi (lo <= 0 <= hi) inside [0, n)
+__device__ __forceinline__ bool span(long long c, long long lo, long long hi, long long n, int unit, int line)
+{
+    if (c + lo >= 0 && c + hi < n) return true;
+    record(c + lo < 0 ? c + lo : c + hi, n, unit, line);
+    return false;
 }
 
 // this unit's record, read (and with clear, reset) from the host
@@ -60,6 +73,7 @@ int chk_read_fused(chk::Record *out, bool clear);
 int chk_read_fused32(chk::Record *out, bool clear);
 int chk_read_mlp(chk::Record *out, bool clear);
 int chk_read_phase(chk::Record *out, bool clear);
+int chk_read_dyn32(chk::Record *out, bool clear);
 } // namespace fsl
 
 // Translation-unit ids of the records (FSL_CHK_UNIT must be defined before
@@ -67,11 +81,15 @@ int chk_read_phase(chk::Record *out, bool clear);
 #define FSL_CHK_FUSED 1   // fsl_fused.cu: FP64 ring-tile stage kernels
 #define FSL_CHK_FUSED32 2 // fsl_fused32.cu: FP32 ring-tile and full-lane stage kernels, ensembles
 #define FSL_CHK_MLP 3     // fsl_mlp.cu: closure features and inference
-#define FSL_CHK_PHASE 4   // fsl_phase.cu: state scatter/gather
+#define FSL_CHK_PHASE 4   // fsl_phase.cu: state scatter/gather, FP64 dynamic procedure
+#define FSL_CHK_DYN32 5   // fsl_dyn32.cu: FP32 dynamic procedure
 
 #if FSL_BOUNDS_CHECK
 #define FSL_CELL(c, fs) (::fsl::chk::at((c), (fs), FSL_CHK_UNIT, __LINE__))
 #define FSL_FACE(f, n) (::fsl::chk::at((f), (n), FSL_CHK_UNIT, __LINE__))
+// a stencil's extremes: true when inside (a kernel without block barriers
+// skips the cell otherwise); always true in the product build
+#define FSL_SPAN(c, lo, hi, n) (::fsl::chk::span((c), (lo), (hi), (n), FSL_CHK_UNIT, __LINE__))
 // the host reader of this unit's record: int fsl_chk_read_<name>(Record*, bool)
 #define FSL_CHK_EXPORT(name)                                                                                          \
     namespace fsl {                                                                                                   \
@@ -80,6 +98,7 @@ int chk_read_phase(chk::Record *out, bool clear);
 #else
 #define FSL_CELL(c, fs) (c)
 #define FSL_FACE(f, n) (f)
+#define FSL_SPAN(c, lo, hi, n) true
 #define FSL_CHK_EXPORT(name)                                                                                          \
     namespace fsl {                                                                                                   \
     int chk_read_##name(chk::Record *, bool) { return -1; }                                                           \

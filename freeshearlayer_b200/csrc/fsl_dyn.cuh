@@ -5,6 +5,7 @@
 // filtering and coefficient).  The conserved state U stays FP64 in both.
 #pragma once
 
+#include "fsl_check.cuh"
 #include "fsl_internal.h"
 
 namespace fsl {
@@ -24,7 +25,7 @@ template <typename T> __global__ void k_dyn_vel(Grid g, const double *__restrict
     const long long fs = g.fstride;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
-        const long long c = g.off + t;
+        const long long c = FSL_CELL(g.off + t, fs);
         const T rr = T(1.) / T(U[c]); // :201-205
         vel[c] = T(U[fs + c]) * rr;
         vel[fs + c] = T(U[2 * fs + c]) * rr;
@@ -41,6 +42,7 @@ template <typename T> __global__ void k_filt_y_vel(Grid g, const T *__restrict__
     const int i = blockIdx.z;
     if (k > g.D || j > g.H) return;
     const long long fs = g.fstride, c = g.idx(i, j, k);
+    if (!FSL_SPAN(c, -(long long)g.pk, (long long)g.pk, fs)) return;
     T a[3][3];
 #pragma unroll
     for (int r = 0; r < 3; r++) {
@@ -71,6 +73,7 @@ template <typename T> __global__ void k_filt_y(Grid g, int nf, const T *__restri
     const int i = blockIdx.z;
     if (k > g.D || j > g.H) return;
     const long long fs = g.fstride, c = g.idx(i, j, k);
+    if (!FSL_SPAN(c, -(long long)g.pk, (long long)g.pk, fs)) return;
     for (int m = 0; m < nf; m++) {
         const T *s = src + m * fs;
         T t = 0.;
@@ -87,6 +90,7 @@ template <typename T> __global__ void k_filt_z(Grid g, int nf, const T *__restri
     const int i = blockIdx.z;
     if (k > g.D || j > g.H) return;
     const long long fs = g.fstride, c = g.idx(i, j, k);
+    if (!FSL_SPAN(c, -1LL, 1LL, fs)) return;
     for (int m = 0; m < nf; m++) {
         const T *s = t1 + m * fs;
         T t = 0.;
@@ -104,6 +108,7 @@ template <typename T> __global__ void k_filt_x(Grid g, int nf, const T *__restri
     const int i = blockIdx.z + 1;
     if (k > g.D || j > g.H) return;
     const long long fs = g.fstride, c = g.idx(i, j, k);
+    if (!FSL_SPAN(c, -g.pi, g.pi, fs)) return;
     for (int m = 0; m < nf; m++) {
         const T *s = t2 + m * fs;
         T t = 0.;
@@ -123,6 +128,7 @@ __global__ void k_dyn_mid(Grid g, Consts kc, const T *__restrict__ vel, const T 
     const int i = blockIdx.z + 1;
     if (k > g.D || j > g.H) return;
     const long long fs = g.fstride, c = g.idx(i, j, k);
+    if (!FSL_SPAN(c, -g.pi, g.pi, fs)) return;
     const T f0 = F[c], f1 = F[fs + c], f2 = F[2 * fs + c];
     Lst[c] = F[3 * fs + c] - f0 * f0;
     Lst[fs + c] = F[4 * fs + c] - f0 * f1;
@@ -168,6 +174,7 @@ __global__ void k_dyn_final(Grid g, Consts kc, const double *__restrict__ rho, c
     const int i = blockIdx.z + 1;
     if (k > g.D || j > g.H) return;
     const long long fs = g.fstride, c = g.idx(i, j, k);
+    if (!FSL_SPAN(c, 0LL, 0LL, fs)) return;
     const T DD = T(kc.DD);
     const T M11 = DD * (4 * B[c] - Ahat[c]);
     const T M12 = DD * (4 * B[fs + c] - Ahat[fs + c]);
@@ -244,7 +251,7 @@ __global__ void __launch_bounds__(32 * TJ) k_dyn_filter9(Grid g, int seg, const 
             const int rr = e / 34, cc = e % 34, jj = j0 - 1 + rr, kk = k0 - 1 + cc;
             pre[s][0] = pre[s][1] = pre[s][2] = T(0.);
             if (e < (TJ + 2) * 34 && ip <= L && jj <= H + 1 && kk >= 0 && kk <= D + 1) {
-                const long long q = g.idx(ip, jj, kk);
+                const long long q = FSL_CELL(g.idx(ip, jj, kk), fs);
                 pre[s][0] = vel[q]; pre[s][1] = vel[fs + q]; pre[s][2] = vel[2 * fs + q];
             }
         }
@@ -303,7 +310,7 @@ __global__ void __launch_bounds__(32 * TJ) k_dyn_filter9(Grid g, int seg, const 
             }
             // plane 0 keeps its pass-1 value
             if (ip == 0 && own) {
-                const long long c = g.idx(0, j, k);
+                const long long c = FSL_CELL(g.idx(0, j, k), fs);
 #pragma unroll
                 for (int m = 0; m < 9; m++) F[m * fs + c] = t1[r][l + 1][m];
             }
@@ -315,7 +322,7 @@ __global__ void __launch_bounds__(32 * TJ) k_dyn_filter9(Grid g, int seg, const 
         // pass 3 (x) of plane ip-1
         const int io = ip - 1;
         if (io >= max(i0, 1) && io <= i1 && own && k >= 1) {
-            const long long c = g.idx(io, j, k);
+            const long long c = FSL_CELL(g.idx(io, j, k), fs);
 #pragma unroll
             for (int m = 0; m < 9; m++) {
                 T t = 0.;
@@ -341,6 +348,7 @@ __global__ void k_dyn_strain(Grid g, Consts kc, const T *__restrict__ vel, T *__
     const int i = blockIdx.z + 1;
     if (k > g.D || j > g.H) return;
     const long long fs = g.fstride, c = g.idx(i, j, k);
+    if (!FSL_SPAN(c, -g.pi, g.pi, fs)) return;
     const long long dI = g.pi, dJ = g.pk;
     const T *uu = vel, *vv = vel + fs, *ww = vel + 2 * fs;
     const T du_dx = (uu[c + dI] - uu[c - dI]) * T(kc.r2dx);
@@ -390,7 +398,7 @@ __global__ void __launch_bounds__(32 * TJ)
 #pragma unroll
             for (int m = 0; m < 6; m++) pre[s][m] = T(0.);
             if (e < (TJ + 2) * 34 && ip >= 1 && ip <= L && jj <= H + 1 && kk <= D + 1) {
-                const long long q = g.idx(ip, jj, kk);
+                const long long q = FSL_CELL(g.idx(ip, jj, kk), fs);
 #pragma unroll
                 for (int m = 0; m < 6; m++) pre[s][m] = A[m * fs + q];
             }
@@ -446,7 +454,8 @@ __global__ void __launch_bounds__(32 * TJ)
                 t += p2[m] * T(H3); t += p1[m] * T(H3); t += cur[m] * T(H3);
                 Ah[m] = t;
             }
-            const long long c = g.idx(io, j, k);
+            const long long c = FSL_CELL(g.idx(io, j, k), fs);
+            (void)FSL_SPAN(c, -g.pi, g.pi, fs); // its strain stencil (the block barriers forbid a skip)
             // Leonard stress (src/turbulence.c:250-270)
             const T f0 = F[c], f1 = F[fs + c], f2 = F[2 * fs + c];
             T L11 = F[3 * fs + c] - f0 * f0, L12 = F[4 * fs + c] - f0 * f1, L13 = F[5 * fs + c] - f0 * f2;

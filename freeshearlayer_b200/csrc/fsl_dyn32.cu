@@ -4,7 +4,10 @@
 // Its scratch fields are FP32 buffers of its own (DynScratch32).
 #include <algorithm>
 
+#define FSL_CHK_UNIT FSL_CHK_DYN32
 #include "fsl_dyn.cuh"
+
+FSL_CHK_EXPORT(dyn32)
 
 namespace fsl {
 

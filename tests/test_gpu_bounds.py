@@ -1,8 +1,9 @@
 """The bounds-checked debug build (libfsl_gpu_checked.so): every step path
 whose kernels carry the checks (FP64 and FP32 ring tiles, the FP32 full-lane
-tile, PPM, the static and learned closures, the persistent ensemble, the
-state scatter/gather of the asynchronous transfers), on grids with partial
-tiles in every direction and on both setups, makes no out-of-range
+tile, PPM, the dynamic procedure in both precisions, the static and learned
+closures, the persistent ensemble, the state scatter/gather of the
+asynchronous transfers, the allocation-free SGS entry point), on grids with
+partial tiles in every direction and on both setups, makes no out-of-range
 global-memory access.  The workload runs in a child process that loads the
 checked library (FSL_GPU_LIB=checked); this file is also that child."""
 import json
@@ -78,6 +79,28 @@ def _workload():
     e.sync()
     e.close()
     runs += 1
+    # the allocation-free SGS entry point (the unfused dynamic procedure on
+    # its static scratch array), on a padded state with its ghost layer
+    import ctypes as C
+
+    import torch
+    p = temporal_params(L=19, H=13, D=17, Mc=0.5)
+    s, _ = fsl.temporal_state(p, 0.5, 1.0, 2e-2, 11)
+    d = fsl.Domain(p)
+    d.upload_state(s)
+    d.ghost_bc()
+    U = torch.from_numpy(np.ascontiguousarray(np.stack([d.cells(0, v) for v in range(4)]))).cuda()
+    mu = torch.zeros(d.cells(3).shape, dtype=torch.float64, device="cuda")
+    fn = fsl.lib().fsl_dynamic_smagorinsky_noalloc
+    fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                   C.c_void_p]
+    fn.restype = C.c_int
+    torch.cuda.synchronize()
+    rc = fn(U.data_ptr(), mu.data_ptr(), p["LEN"], p["HIG"], p["DEP"], p["deltaX"], p["deltaY"], p["deltaZ"],
+            C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0, rc
+    torch.cuda.synchronize()
+    runs += 1
     rep = fsl.debug_bounds()
     rep["runs"] = runs
     print(json.dumps(rep))
@@ -92,7 +115,7 @@ def test_checked_build_finds_no_out_of_range_access():
                        text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
     rep = json.loads(r.stdout.strip().splitlines()[-1])
-    assert rep["runs"] >= 20
+    assert rep["runs"] >= 26
     assert rep["hits"] == 0, rep
 
 
