@@ -213,8 +213,8 @@ def _check(rc: int, h=None):
 def debug_bounds(clear: bool = False) -> dict:
     """The bounds-checked build's report (FSL_GPU_LIB=checked): offending
     global-memory accesses since the last clear and the first one's file
-    (1 fsl_fused.cu, 2 fsl_fused32.cu, 3 fsl_mlp.cu, 4 fsl_phase.cu), line,
-    index and extent.  Raises FslError (FSL_ERR_UNSUPPORTED) in the product
+    (1 fsl_fused.cu, 2 fsl_fused32.cu, 3 fsl_mlp.cu, 4 fsl_phase.cu,
+    5 fsl_dyn32.cu, 6 fsl_io.cu), line, index and extent.  Raises FslError (FSL_ERR_UNSUPPORTED) in the product
     build."""
     r = BoundsReport()
     _check(lib().fsl_debug_bounds(C.byref(r), 1 if clear else 0))

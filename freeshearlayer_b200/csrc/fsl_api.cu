@@ -1164,9 +1164,9 @@ int fsl_debug_bounds(fsl_bounds_report *out, int clear)
     *out = fsl_bounds_report{};
 #if FSL_BOUNDS_CHECK
     if (cudaDeviceSynchronize() != cudaSuccess) return FSL_ERR_CUDA;
-    int (*const readers[5])(chk::Record *, bool) = {chk_read_fused, chk_read_fused32, chk_read_mlp, chk_read_phase,
-                                                    chk_read_dyn32};
-    for (int u = 0; u < 5; u++) {
+    int (*const readers[6])(chk::Record *, bool) = {chk_read_fused, chk_read_fused32, chk_read_mlp, chk_read_phase,
+                                                    chk_read_dyn32, chk_read_io};
+    for (int u = 0; u < 6; u++) {
         chk::Record r{};
         if (readers[u](&r, clear != 0) != 0) return FSL_ERR_CUDA;
         if (r.hits && !out->hits) {

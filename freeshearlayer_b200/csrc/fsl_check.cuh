@@ -74,6 +74,7 @@ int chk_read_fused32(chk::Record *out, bool clear);
 int chk_read_mlp(chk::Record *out, bool clear);
 int chk_read_phase(chk::Record *out, bool clear);
 int chk_read_dyn32(chk::Record *out, bool clear);
+int chk_read_io(chk::Record *out, bool clear);
 } // namespace fsl
 
 // Translation-unit ids of the records (FSL_CHK_UNIT must be defined before
@@ -81,8 +82,9 @@ int chk_read_dyn32(chk::Record *out, bool clear);
 #define FSL_CHK_FUSED 1   // fsl_fused.cu: FP64 ring-tile stage kernels
 #define FSL_CHK_FUSED32 2 // fsl_fused32.cu: FP32 ring-tile and full-lane stage kernels, ensembles
 #define FSL_CHK_MLP 3     // fsl_mlp.cu: closure features and inference
-#define FSL_CHK_PHASE 4   // fsl_phase.cu: state scatter/gather, FP64 dynamic procedure
+#define FSL_CHK_PHASE 4   // fsl_phase.cu: per-phase kernels, state transfers, reductions, FP64 dynamic procedure
 #define FSL_CHK_DYN32 5   // fsl_dyn32.cu: FP32 dynamic procedure
+#define FSL_CHK_IO 6      // fsl_io.cu: probes and Tecplot fields
 
 #if FSL_BOUNDS_CHECK
 #define FSL_CELL(c, fs) (::fsl::chk::at((c), (fs), FSL_CHK_UNIT, __LINE__))

@@ -7,7 +7,11 @@
 #include <string>
 #include <vector>
 
+#define FSL_CHK_UNIT FSL_CHK_IO
+#include "fsl_check.cuh"
 #include "fsl_internal.h"
+
+FSL_CHK_EXPORT(io)
 
 using namespace fsl;
 
@@ -23,7 +27,7 @@ __global__ void k_probe_rows(Grid g, const double *__restrict__ U, double *__res
     const int st[3] = {g.L / 2, 3 * g.L / 4, g.L};
 #pragma unroll
     for (int s = 0; s < 3; s++) {
-        const long long c = g.idx(st[s], j + 1, k);
+        const long long c = FSL_CELL(g.idx(st[s], j + 1, k), g.fstride);
         rows[(s * 2 + 0) * g.H + j] = U[c];
         rows[(s * 2 + 1) * g.H + j] = U[g.fstride + c];
     }
@@ -37,7 +41,7 @@ __global__ void k_probe_accumulate(Grid g, const double *__restrict__ U, double 
     const int st[3] = {g.L / 2, 3 * g.L / 4, g.L};
 #pragma unroll
     for (int s = 0; s < 3; s++) {
-        const long long c = g.idx(st[s], j + 1, k);
+        const long long c = FSL_CELL(g.idx(st[s], j + 1, k), g.fstride);
         acc[(s * 2 + 0) * g.H + j] += U[c];
         acc[(s * 2 + 1) * g.H + j] += U[g.fstride + c];
     }
@@ -310,6 +314,7 @@ __global__ void k_output_fields(Grid g, Consts kc, double Cs, const double *__re
         const long long r = t / g.L;
         const int j = (int)(r % g.H) + 1, k = (int)(r / g.H) + 1;
         const long long c = g.idx(i, j, k), xi = g.pi, yj = g.pk;
+        if (!FSL_SPAN(c, -xi, xi, fs)) continue; // the strain stencil's extremes
         double *q = out + 12 * t;
         q[0] = (i - 1) * kc.deltaX + 0.5 * kc.deltaX;
         q[1] = (j - 1) * kc.deltaY + 0.5 * kc.deltaY;

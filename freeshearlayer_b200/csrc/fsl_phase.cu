@@ -21,15 +21,15 @@ namespace {
 
 __device__ __forceinline__ long long ixf(int L, int H, int D, int i, int j, int k)
 {
-    return ((long long)i * H + j) * D + k;
+    return FSL_FACE(((long long)i * H + j) * D + k, (long long)(L + 1) * H * D);
 }
 __device__ __forceinline__ long long iyf(int L, int H, int D, int i, int j, int k)
 {
-    return ((long long)i * (H + 1) + j) * D + k;
+    return FSL_FACE(((long long)i * (H + 1) + j) * D + k, (long long)L * (H + 1) * D);
 }
 __device__ __forceinline__ long long izf(int L, int H, int D, int i, int j, int k)
 {
-    return ((long long)i * H + j) * (D + 1) + k;
+    return FSL_FACE(((long long)i * H + j) * (D + 1) + k, (long long)L * H * (D + 1));
 }
 
 // ---------------------------------------------------------------------------
@@ -86,7 +86,7 @@ __global__ void k_ghost(Grid g, int setup, double *__restrict__ u)
         int si = i;
         if (i == 0) si = L;               // temporal: periodic x
         else if (i == L + 1) si = spatial ? L : 1;
-        long long s = g.idx(si, jj, kk);
+        long long s = FSL_CELL(g.idx(si, jj, kk), fs);
 #pragma unroll
         for (int q = 0; q < 5; q++) v[q] = u[q * fs + s];
         if (i == L + 1 && spatial) {
@@ -96,7 +96,7 @@ __global__ void k_ghost(Grid g, int setup, double *__restrict__ u)
         }
     }
     if (flip) v[2] = -v[2];
-    long long d = g.idx(i, j, k);
+    long long d = FSL_CELL(g.idx(i, j, k), fs);
 #pragma unroll
     for (int q = 0; q < 5; q++) u[q * fs + d] = v[q];
 }
@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(128) k_recon(Grid g, const double *__restrict_
     if (k > D || j > H) return;
     const long long fs = g.fstride;
     const long long c0 = g.idx(i, j, k);
+    if (!FSL_SPAN(c0, -g.pi, g.pi, fs)) return; // the one-neighbour stencil in x, the widest
     CellC<double> c;
 #pragma unroll
     for (int q = 0; q < 5; q++) c.u[q] = u[q * fs + c0];
@@ -287,6 +288,9 @@ __global__ void __launch_bounds__(128) k_flux(Grid g, Consts kc, const double *_
         rdn = kc.rdz; rt1 = kc.r4dx; rt2 = kc.r4dy;
     }
     const long long minus = plus - dn;
+    // the neighbours read: plus and minus, each with both tangential offsets
+    if (!FSL_SPAN(plus, -dn - (dt1 > dt2 ? dt1 : dt2), dt1 > dt2 ? dt1 : dt2, fs)) return;
+    fi = FSL_FACE(fi, (long long)na * nb * nc);
     double Lm[5], Rp[5];
 #pragma unroll
     for (int q = 0; q < 5; q++) { Lm[q] = mS[q][fi]; Rp[q] = pS[q][fi]; }
@@ -339,7 +343,7 @@ __global__ void k_evolution(Grid g, int mode, const DevScalars *__restrict__ ds,
     if (k > D || j > H) return;
     const double dtx = ds->dtx, dty = ds->dty, dtz = ds->dtz;
     const double one_third = 1. / 3., two_thirds = 2. / 3.;
-    const long long c = g.idx(i, j, k), fs = g.fstride;
+    const long long fs = g.fstride, c = FSL_CELL(g.idx(i, j, k), fs);
     const long long xm = ixf(L, H, D, i - 1, j - 1, k - 1), xp = ixf(L, H, D, i, j - 1, k - 1);
     const long long ym = iyf(L, H, D, i - 1, j - 1, k - 1), yp = iyf(L, H, D, i - 1, j, k - 1);
     const long long zm = izf(L, H, D, i - 1, j - 1, k - 1), zp = izf(L, H, D, i - 1, j - 1, k);
@@ -384,7 +388,7 @@ __global__ void k_courant_partial(Grid g, Consts kc, const double *__restrict__ 
         const long long r = t / D;
         const int j = (int)(r % H) + 1;
         const int i = (int)(r / H) + i0;
-        const long long c = g.idx(i, j, k);
+        const long long c = FSL_CELL(g.idx(i, j, k), g.fstride);
         const double R = U[c];
         const double Co = cell_courant(kc.cfl_mode, R, U[fs + c], kc.cfl_mode == FSL_CFL_ACOUSTIC ? U[2 * fs + c] : 0.,
                                        kc.cfl_mode == FSL_CFL_ACOUSTIC ? U[3 * fs + c] : 0.,
@@ -484,7 +488,7 @@ __global__ void k_judge_rows(Grid g, const TA *__restrict__ a, const TB *__restr
     for (long long t = threadIdx.x; t < n; t += blockDim.x) {
         const int k = (int)(t % bD) + 3;
         const int i = (int)(t / bD) + 3;
-        const long long c = g.idx(i, j, k);
+        const long long c = FSL_CELL(g.idx(i, j, k), g.fstride);
         const double x = a[c], y = b[c];
         s[0] += x; s[1] += y; s[2] += (x - y) * (x - y); s[3] += y * y;
     }
@@ -549,7 +553,7 @@ __global__ void k_sums_partial(Grid g, int i0, int ni, const double *__restrict_
         const long long r = t / g.D;
         const int j = (int)(r % g.H) + 1;
         const int i = (int)(r / g.H) + i0;
-        const long long c = g.idx(i, j, k);
+        const long long c = FSL_CELL(g.idx(i, j, k), g.fstride);
 #pragma unroll
         for (int q = 0; q < 5; q++) s[q] += U[q * g.fstride + c];
     }
@@ -589,7 +593,7 @@ __global__ void k_plane_sums(Grid g, int i0, int ni, const double *__restrict__ 
     for (long long t = threadIdx.x; t < n; t += blockDim.x) {
         const int k = (int)(t % g.D) + 1;
         const int i = (int)(t / g.D) + i0;
-        const long long c = g.idx(i, j, k);
+        const long long c = FSL_CELL(g.idx(i, j, k), g.fstride);
         const double r = U[c], u = U[g.fstride + c] / r, v = U[2 * g.fstride + c] / r,
                      w = U[3 * g.fstride + c] / r;
         s[0] += r; s[1] += r * u; s[2] += r * v; s[3] += r * w;

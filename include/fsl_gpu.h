@@ -319,17 +319,20 @@ int fsl_tune(fsl_ctx *ctx, int key, int value);
 
 /* ---- debug bounds checks ---------------------------------------------------
  * libfsl_gpu_checked.so (`make -C freeshearlayer_b200 checked`) is this
- * library built with every global-memory index of the fused stage kernels
- * (ring tile and full lane, both precisions, ensembles), the closure features
- * and inference, the dynamic procedure (both precisions) and the state
- * scatter/gather tested against the extent of the array it indexes.  An offending access is counted, the first one of
+ * library built with the global-memory indices of the step's kernels tested
+ * against the extent of the array they index: the fused stage kernels (ring
+ * tile and full lane, both precisions, ensembles), the per-phase kernels, the
+ * dynamic procedure (both precisions), the closure's features and inference,
+ * the Courant and conservation reductions, the state scatter/gather and the
+ * probe and Tecplot kernels.  An offending access is counted, the first one of
  * each source file recorded, and the access redirected to element 0 of that
  * array, so it never leaves the allocation.  No counterpart in the reference
  * (its arrays are unchecked C). */
 typedef struct fsl_bounds_report {
     unsigned long long hits; /* offending accesses since the last clear, all files */
     int unit;                /* file of the first one reported: 1 fsl_fused.cu, 2 fsl_fused32.cu,
-                                3 fsl_mlp.cu, 4 fsl_phase.cu, 5 fsl_dyn32.cu; 0 when hits is 0 */
+                                3 fsl_mlp.cu, 4 fsl_phase.cu, 5 fsl_dyn32.cu, 6 fsl_io.cu;
+                                0 when hits is 0 */
     int line;                /* its source line (in the file or a header it includes) */
     long long index, extent; /* the index and the extent it was checked against */
 } fsl_bounds_report;

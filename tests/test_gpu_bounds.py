@@ -1,11 +1,13 @@
 """The bounds-checked debug build (libfsl_gpu_checked.so): every step path
 whose kernels carry the checks (FP64 and FP32 ring tiles, the FP32 full-lane
-tile, PPM, the dynamic procedure in both precisions, the static and learned
-closures, the persistent ensemble, the state scatter/gather of the
-asynchronous transfers, the allocation-free SGS entry point), on grids with
-partial tiles in every direction and on both setups, makes no out-of-range
-global-memory access.  The workload runs in a child process that loads the
-checked library (FSL_GPU_LIB=checked); this file is also that child."""
+tile, the per-phase kernels, PPM, the dynamic procedure in both precisions,
+the static and learned closures, the persistent ensemble, the Courant and
+conservation reductions, probes and Tecplot fields, the state scatter/gather
+of the asynchronous transfers, the allocation-free SGS entry point), on grids
+with partial tiles in every direction and on both setups, makes no
+out-of-range global-memory access.  The workload runs in a child process
+that loads the checked library (FSL_GPU_LIB=checked); this file is also that
+child."""
 import json
 import os
 import subprocess
@@ -46,6 +48,20 @@ def _workload():
         if prec == 0:
             d.step_phased(1)
         assert np.all(np.isfinite(d.download_state()))
+        runs += 1
+    # per-phase kernels (PPM too), the Courant and conservation reductions,
+    # probes, Favre sums and Tecplot fields, on both setups
+    for p in (spatial_params(L=13, H=10, D=7), temporal_params(L=15, H=11, D=9, recon=1)):
+        d = fsl.Domain(p)
+        d.upload_state(fsl.initial_state(p) if p["setup"] == 0 else fsl.temporal_state(p, 0.4, 1.0, 2e-2, 3)[0])
+        d.step_phased(2)
+        d.check_courant()
+        d.sums()
+        d.plane_sums()
+        d.probe_rows()
+        d.favre_reset()
+        d.favre_accumulate()
+        assert np.all(np.isfinite(d.output_fields()))
         runs += 1
     # temporal setup: partial tiles in y and z (full lane 16 x 32, ring
     # tiles of 8, 12, 16 rows), odd extents; static and no SGS; PPM
@@ -115,7 +131,7 @@ def test_checked_build_finds_no_out_of_range_access():
                        text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
     rep = json.loads(r.stdout.strip().splitlines()[-1])
-    assert rep["runs"] >= 26
+    assert rep["runs"] >= 28
     assert rep["hits"] == 0, rep
 
 
