@@ -63,6 +63,20 @@ def test_header_declarations_exported(fsl):
     assert not missing, missing
 
 
+def test_checked_build_exports_the_same_abi(fsl):
+    """libfsl_gpu_checked.so (the bounds-checked debug build) is a drop-in
+    for libfsl_gpu.so: every declared entry point, the bounds report among
+    them.  Loaded on the CPU only; no entry point is called."""
+    path = os.path.join(os.path.dirname(fsl.LIB_PATH), "libfsl_gpu_checked.so")
+    if not os.path.exists(path):
+        pytest.skip("libfsl_gpu_checked.so not built (make -C freeshearlayer_b200 checked)")
+    lib = C.CDLL(path)
+    names = declared_functions()
+    assert "fsl_debug_bounds" in names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
 def test_params_from_ini_matches_reference_parser(fsl, tmp_path):
     path = tmp_path / "layer2.ini"
     path.write_text(SHIPPED_INI)
