@@ -23,33 +23,54 @@ struct Record {
     long long index, extent;
 };
 
+// The checks on an explicit record, compiled for host and device: the device
+// counts with an atomic, the host (single-threaded: the CPU test of this
+// logic) with a plain increment.
+__host__ __device__ inline void record_into(Record *r, long long i, long long n, int unit, int line)
+{
+#ifdef __CUDA_ARCH__
+    const unsigned long long before = atomicAdd(&r->hits, 1ull);
+#else
+    const unsigned long long before = r->hits++;
+#endif
+    if (before == 0ull) {
+        r->unit = unit;
+        r->line = line;
+        r->index = i;
+        r->extent = n;
+    }
+}
+
+// i itself when 0 <= i < n; otherwise recorded, and 0
+__host__ __device__ inline long long at_into(Record *r, long long i, long long n, int unit, int line)
+{
+    if ((unsigned long long)i < (unsigned long long)n) return i;
+    record_into(r, i, n, unit, line);
+    return 0;
+}
+
+// the stencil c + lo .. c + hi (lo <= 0 <= hi) inside [0, n); otherwise the
+// offending extreme is recorded
+__host__ __device__ inline bool span_into(Record *r, long long c, long long lo, long long hi, long long n, int unit,
+                                          int line)
+{
+    if (c + lo >= 0 && c + hi < n) return true;
+    record_into(r, c + lo < 0 ? c + lo : c + hi, n, unit, line);
+    return false;
+}
+
 #if FSL_BOUNDS_CHECK
 // one record per translation unit (no relocatable device code needed)
 static __device__ Record g_rec;
 
-__device__ __forceinline__ void record(long long i, long long n, int unit, int line)
-{
-    if (atomicAdd(&g_rec.hits, 1ull) == 0ull) {
-        g_rec.unit = unit;
-        g_rec.line = line;
-        g_rec.index = i;
-        g_rec.extent = n;
-    }
-}
-
 __device__ __forceinline__ long long at(long long i, long long n, int unit, int line)
 {
-    if ((unsigned long long)i < (unsigned long long)n) return i;
-    record(i, n, unit, line);
-    return 0;
+    return at_into(&g_rec, i, n, unit, line);
 }
 
-// the stencil c + lo .. c + hi (lo <= 0 <= hi) inside [0, n)
 __device__ __forceinline__ bool span(long long c, long long lo, long long hi, long long n, int unit, int line)
 {
-    if (c + lo >= 0 && c + hi < n) return true;
-    record(c + lo < 0 ? c + lo : c + hi, n, unit, line);
-    return false;
+    return span_into(&g_rec, c, lo, hi, n, unit, line);
 }
 
 // this unit's record, read (and with clear, reset) from the host
