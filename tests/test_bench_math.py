@@ -91,3 +91,23 @@ def test_cpu_ranges_and_binding_without_nvml_device():
     before = os.sched_getaffinity(0)
     assert bench.bind_near_gpu("GPU-00000000-0000-0000-0000-000000000000") is None
     assert os.sched_getaffinity(0) == before
+
+
+def test_bind_near_gpu_uses_the_nvml_affinity(monkeypatch):
+    """The end-to-end leg's binding takes the CPUs of NVML's affinity mask of
+    the device (64 CPUs per word), restricted to those this process may use,
+    and binds the process to them (NVML and the binding faked)."""
+    import types
+    calls = {}
+    fake = types.SimpleNamespace(
+        nvmlInit=lambda: None, nvmlShutdown=lambda: None,
+        nvmlDeviceGetHandleByUUID=lambda u: calls.setdefault("uuid", u),
+        # CPUs 0-3 and 66 of a 128-CPU host
+        nvmlDeviceGetCpuAffinity=lambda h, n: [0b1111, 1 << 2][:n])
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    monkeypatch.setattr(os, "cpu_count", lambda: 128)
+    monkeypatch.setattr(os, "sched_getaffinity", lambda pid: {1, 2, 3, 66, 70})
+    monkeypatch.setattr(os, "sched_setaffinity", lambda pid, cpus: calls.setdefault("bound", sorted(cpus)))
+    assert bench.bind_near_gpu("GPU-abc") == [1, 2, 3, 66]
+    assert calls == {"uuid": "GPU-abc", "bound": [1, 2, 3, 66]}
+    assert bench.cpu_ranges([1, 2, 3, 66]) == "1-3,66"
