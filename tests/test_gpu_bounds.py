@@ -143,6 +143,7 @@ def test_product_build_has_no_checks():
     with pytest.raises(fsl.FslError) as ex:
         fsl.debug_bounds()
     assert ex.value.code == -7
+    assert fsl.lib().fsl_debug_bounds(None, 0) == -1  # no report to fill: FSL_ERR_ARG
 
 
 if __name__ == "__main__":
